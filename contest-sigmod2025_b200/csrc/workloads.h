@@ -1,0 +1,65 @@
+/*
+ * Seeded synthetic workloads and page encoding (libb200join_workloads.so).
+ *
+ * The reference measures on JOB/IMDB, which is not available here; these
+ * generators build tables of the benchmark shapes instead (seeded, so every
+ * process that asks for the same name/seed/scale gets identical pages):
+ *
+ *   "join2"     two-table equi-join. R: 1M rows, INT32 key = permutation of
+ *               0..1M-1, INT64 payload uniform in [0, 2^40). S: 8M rows, INT32
+ *               fk uniform over R's keys with 10% NULL, INT32 payload uniform in
+ *               [0, 1e6). Output R.payload, S.payload, S.fk.
+ *   "snowflake" fact table of 50M rows with four INT32 foreign keys, each
+ *               Zipf(s=1.1) over its dimension's keys (rank->key by a seeded
+ *               permutation); dimensions of 5M / 1M / 200K / 20K rows with a
+ *               unique INT32 key, an INT32 attribute uniform in [0,1000) and a
+ *               VARCHAR of uniform length 1..64 (printable ASCII). The
+ *               dimensions are pre-filtered on attr < 10 / 50 / 300 / 600
+ *               (1% / 5% / 30% / 60%) before they reach the plan, as the
+ *               contest applies SQL filters at load time. Output: two
+ *               dimension strings and two fact keys.
+ *
+ * `scale` multiplies every row count (1.0 = the sizes above).
+ */
+#ifndef B200JOIN_WORKLOADS_H
+#define B200JOIN_WORKLOADS_H
+
+#include "../../include/b200join.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bjw_workload bjw_workload;
+typedef struct bjw_pages bjw_pages;
+
+/* Builds a named workload; returns 0 on success. */
+BJ_API int bjw_workload_create(const char* name, uint64_t seed, double scale, bjw_workload** out);
+/* Loads a plan written by bjw_save_plan. */
+BJ_API int bjw_workload_load(const char* path, bjw_workload** out);
+/* The plan view (valid until bjw_workload_free). */
+BJ_API const bj_plan* bjw_workload_plan(bjw_workload* w);
+/* Total bytes of input pages the plan's scans read. */
+BJ_API uint64_t bjw_workload_scan_bytes(bjw_workload* w);
+BJ_API void bjw_workload_free(bjw_workload* w);
+
+/* Writes a plan (with its pages) to a file; returns 0 on success. */
+BJ_API int bjw_save_plan(const char* path, const bj_plan* plan);
+/* Writes a table to a file; returns 0 on success. */
+BJ_API int bjw_save_table(const char* path, const bj_table* table);
+
+/* Encodes one column from flat arrays with the contest's packing rules.
+ * INT32: values is int32_t[n]; INT64: int64_t[n]; FP64: double[n];
+ * VARCHAR: values is ignored, str_offsets[n+1] index str_bytes.
+ * valid may be NULL (no NULLs); else valid[i] != 0 marks a non-null row. */
+BJ_API int bjw_encode_column(int32_t type, uint64_t n, const void* values, const uint8_t* valid,
+                      const uint64_t* str_offsets, const char* str_bytes, bjw_pages** out);
+BJ_API uint64_t bjw_pages_count(const bjw_pages* p);
+BJ_API const void* const* bjw_pages_ptrs(const bjw_pages* p);
+BJ_API void bjw_pages_free(bjw_pages* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

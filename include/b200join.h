@@ -1,0 +1,178 @@
+/*
+ * b200join: C ABI of the B200 execution core for the contest's join pipelines.
+ *
+ * The reference engine's public surface is the C++ contest API
+ * (include/plan.h:337-344 of the contest repository, implemented in
+ * engine/Execute.cpp:28-48). This header is the plain-C boundary under that
+ * API: plain structs, pointers and sizes, an int status on every call. The
+ * C++ drop-in (libcontest_b200.so, contest-sigmod2025_b200/csrc/contest_api.cpp)
+ * flattens a `Plan` into `bj_plan` and turns a `bj_result` back into a
+ * `ColumnarTable`; other hosts (ctypes, cgo, JNI) bind these symbols directly.
+ *
+ * Pages are the contest's 8 KiB column pages (format described in
+ * include/contest/plan.h). Input pages are borrowed for the duration of one call;
+ * result pages belong to the bj_result until bj_result_free.
+ *
+ * Threading: one context serves one caller thread at a time, like the
+ * reference (its scheduler rejects calls from other threads,
+ * engine/infra/Scheduler.cpp:170-172). Use one context per host thread.
+ */
+#ifndef B200JOIN_H
+#define B200JOIN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define BJ_API __attribute__((visibility("default")))
+#else
+#define BJ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BJ_PAGE_SIZE 8192
+
+/* Column types, in the order of the contest's DataType (attribute.h:8-13). */
+enum bj_type { BJ_INT32 = 0, BJ_INT64 = 1, BJ_FP64 = 2, BJ_VARCHAR = 3 };
+
+/* Plan node kinds, in the order of the contest's NodeType (plan.h:27-30). */
+enum bj_node_kind { BJ_NODE_JOIN = 0, BJ_NODE_SCAN = 1 };
+
+/* Status codes. The reference throws std::runtime_error where these return
+ * non-zero (engine/pipeline/PipelineFunction.cpp:13, op/CollectorTarget.cpp:36);
+ * the C++ drop-in turns a non-zero status back into std::runtime_error. */
+enum bj_status {
+    BJ_OK = 0,
+    BJ_ERR_INVALID = 1,     /* malformed plan, pages or arguments */
+    BJ_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    BJ_ERR_OOM = 3,         /* device or pinned memory exhausted */
+    BJ_ERR_UNSUPPORTED = 4, /* e.g. a non-INT32 join key */
+    BJ_ERR_INTERNAL = 5,    /* a device-side check tripped (see bj_last_error) */
+    BJ_ERR_NO_DEVICE = 6    /* no CUDA device, or the kernels are missing */
+};
+
+/* One input column: `num_pages` host (or, for bj_resident_upload only, any
+ * host-readable) page pointers. Mirrors `Column` (plan.h:56-104). */
+typedef struct bj_column {
+    int32_t type;
+    uint32_t reserved;
+    uint64_t num_pages;
+    const void* const* pages;
+} bj_column;
+
+/* One input table. Mirrors `ColumnarTable` (plan.h:101-104). A table with no
+ * rows may have no columns (engine/query/PlanImport.cpp:43-49). */
+typedef struct bj_table {
+    uint64_t num_rows;
+    uint64_t num_columns;
+    const bj_column* columns;
+} bj_table;
+
+/* One output attribute of a plan node: (column index, type), plan.h:44-46. */
+typedef struct bj_attr {
+    uint64_t index;
+    int32_t type;
+    uint32_t reserved;
+} bj_attr;
+
+/* One plan node. Mirrors `PlanNode` / `ScanNode` / `JoinNode` (plan.h:32-52).
+ * For a scan, output attribute indices name columns of the base table; for a
+ * join they index the concatenation of the left then the right child's
+ * output attributes. */
+typedef struct bj_node {
+    int32_t kind;
+    int32_t build_left; /* accepted and ignored: the engine picks its own build sides */
+    uint64_t base_table_id;
+    uint64_t left;
+    uint64_t right;
+    uint64_t left_attr;
+    uint64_t right_attr;
+    uint64_t num_output_attrs;
+    const bj_attr* output_attrs;
+} bj_node;
+
+/* A whole plan. Mirrors `Plan` (plan.h:112-149). */
+typedef struct bj_plan {
+    uint64_t num_nodes;
+    const bj_node* nodes;
+    uint64_t num_inputs;
+    const bj_table* inputs;
+    uint64_t root;
+} bj_plan;
+
+typedef struct bj_context bj_context;
+typedef struct bj_result bj_result;
+typedef struct bj_resident bj_resident;
+
+/* Per-call counters, filled by bj_result_stats. */
+typedef struct bj_stats {
+    uint64_t kernel_launches;   /* kernels this call launched */
+    uint64_t pipelines;         /* scan->probe->build/output pipelines run */
+    uint64_t h2d_bytes;         /* host->device bytes copied */
+    uint64_t d2h_bytes;         /* device->host bytes copied */
+    uint64_t input_pages;       /* pages of the scanned input columns */
+    uint64_t output_pages;      /* pages written to the result */
+    double device_ms;           /* device time of the call, CUDA events */
+    double total_ms;            /* host wall time of the call */
+} bj_stats;
+
+/* Replaces Contest::build_context (engine/Execute.cpp:42-46). Creates the CUDA
+ * state for `device`: stream, events, device arena, pinned staging, worker
+ * threads for page staging. */
+BJ_API int bj_context_create(int device, bj_context** out);
+
+/* Replaces Contest::destroy_context (engine/Execute.cpp:48). */
+BJ_API void bj_context_destroy(bj_context* ctx);
+
+/* Message of the last failed call on this context ("" if none). */
+BJ_API const char* bj_last_error(const bj_context* ctx);
+
+/* Replaces Contest::execute (engine/Execute.cpp:28-40): runs `plan` on its host
+ * input pages and returns the joined rows as host pages. The result's row
+ * multiset equals the reference engine's; row order and page packing are free
+ * (the contest harnesses sort rows before comparing, tests/read_sql.cpp:1208-1213). */
+BJ_API int bj_execute(bj_context* ctx, const bj_plan* plan, bj_result** out);
+
+/* Resident tables (no reference counterpart: the reference re-reads host pages
+ * on every call). Uploads a table's pages to HBM once; later calls name it by
+ * handle instead of re-copying the pages. */
+BJ_API int bj_resident_upload(bj_context* ctx, const bj_table* table, bj_resident** out);
+BJ_API void bj_resident_free(bj_context* ctx, bj_resident* table);
+
+/* Flags of bj_execute_resident. */
+#define BJ_RESULT_HOST 0   /* copy result pages to host memory */
+#define BJ_RESULT_DEVICE 1 /* leave result pages in device memory */
+
+/* Like bj_execute, but input i of the plan is the resident table tables[i]
+ * (plan->inputs is ignored and may be NULL). */
+BJ_API int bj_execute_resident(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables,
+                        int flags, bj_result** out);
+
+/* Result accessors. */
+BJ_API uint64_t bj_result_num_rows(const bj_result* r);
+BJ_API uint64_t bj_result_num_columns(const bj_result* r);
+BJ_API int32_t bj_result_column_type(const bj_result* r, uint64_t column);
+BJ_API uint64_t bj_result_column_num_pages(const bj_result* r, uint64_t column);
+/* Host address of a result page (NULL for a BJ_RESULT_DEVICE result). */
+BJ_API const void* bj_result_page(const bj_result* r, uint64_t column, uint64_t page);
+/* Device address of a result page (valid until bj_result_free). */
+BJ_API const void* bj_result_device_page(const bj_result* r, uint64_t column, uint64_t page);
+/* Copies all pages of `column` into caller-owned 8 KiB pages dst[0..n). */
+BJ_API int bj_result_copy_pages(const bj_result* r, uint64_t column, void* const* dst);
+BJ_API int bj_result_stats(const bj_result* r, bj_stats* out);
+BJ_API void bj_result_free(bj_result* r);
+
+/* The context's CUDA stream (a cudaStream_t), for callers timing with events. */
+BJ_API void* bj_context_stream(bj_context* ctx);
+
+/* Library version string. */
+BJ_API const char* bj_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200JOIN_H */
