@@ -1,0 +1,540 @@
+"""Python host-side mirror of the contest API over the B200 join engine.
+
+The engine itself is C++/CUDA (libb200join.so, C ABI in include/b200join.h).
+This module mirrors the contest's plan-building interface (include/plan.h of
+the contest repository: ``Plan.new_scan_node / new_join_node / new_input``,
+``ColumnarTable``, ``Contest::build_context / execute / destroy_context``) so
+tests and tools read like the reference's own tests
+(tests/unit_tests.cpp:19-663), and binds the C ABI with ctypes.
+
+The package directory name contains a hyphen; import it with
+``importlib.import_module("contest-sigmod2025_b200")``.
+
+There is no CPU fallback: if the CUDA library is missing or no GPU is
+visible, ``build_context`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import struct
+from dataclasses import dataclass, field
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PAGE_SIZE = 8192
+
+INT32, INT64, FP64, VARCHAR = 0, 1, 2, 3
+TYPE_NAMES = {INT32: "INT32", INT64: "INT64", FP64: "FP64", VARCHAR: "VARCHAR"}
+NODE_JOIN, NODE_SCAN = 0, 1
+RESULT_HOST, RESULT_DEVICE = 0, 1
+
+STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "OOM", 4: "UNSUPPORTED", 5: "INTERNAL", 6: "NO_DEVICE"}
+
+
+class EngineError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"b200join {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+# ---------------------------------------------------------------------------
+# C structures (include/b200join.h)
+
+class BjColumn(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("reserved", ctypes.c_uint32), ("num_pages", ctypes.c_uint64),
+                ("pages", ctypes.POINTER(ctypes.c_void_p))]
+
+
+class BjTable(ctypes.Structure):
+    _fields_ = [("num_rows", ctypes.c_uint64), ("num_columns", ctypes.c_uint64), ("columns", ctypes.POINTER(BjColumn))]
+
+
+class BjAttr(ctypes.Structure):
+    _fields_ = [("index", ctypes.c_uint64), ("type", ctypes.c_int32), ("reserved", ctypes.c_uint32)]
+
+
+class BjNode(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("build_left", ctypes.c_int32), ("base_table_id", ctypes.c_uint64),
+                ("left", ctypes.c_uint64), ("right", ctypes.c_uint64), ("left_attr", ctypes.c_uint64),
+                ("right_attr", ctypes.c_uint64), ("num_output_attrs", ctypes.c_uint64),
+                ("output_attrs", ctypes.POINTER(BjAttr))]
+
+
+class BjPlan(ctypes.Structure):
+    _fields_ = [("num_nodes", ctypes.c_uint64), ("nodes", ctypes.POINTER(BjNode)), ("num_inputs", ctypes.c_uint64),
+                ("inputs", ctypes.POINTER(BjTable)), ("root", ctypes.c_uint64)]
+
+
+class BjStats(ctypes.Structure):
+    _fields_ = [("kernel_launches", ctypes.c_uint64), ("pipelines", ctypes.c_uint64), ("h2d_bytes", ctypes.c_uint64),
+                ("d2h_bytes", ctypes.c_uint64), ("input_pages", ctypes.c_uint64), ("output_pages", ctypes.c_uint64),
+                ("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+
+
+# Every symbol include/b200join.h declares, with its ctypes signature.
+_VP, _U64, _I32, _INT = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int
+ABI = {
+    "bj_version": (ctypes.c_char_p, []),
+    "bj_context_create": (_INT, [_INT, ctypes.POINTER(_VP)]),
+    "bj_context_destroy": (None, [_VP]),
+    "bj_last_error": (ctypes.c_char_p, [_VP]),
+    "bj_execute": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP)]),
+    "bj_resident_upload": (_INT, [_VP, ctypes.POINTER(BjTable), ctypes.POINTER(_VP)]),
+    "bj_resident_free": (None, [_VP, _VP]),
+    "bj_execute_resident": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), _INT, ctypes.POINTER(_VP)]),
+    "bj_result_num_rows": (_U64, [_VP]),
+    "bj_result_num_columns": (_U64, [_VP]),
+    "bj_result_column_type": (_I32, [_VP, _U64]),
+    "bj_result_column_num_pages": (_U64, [_VP, _U64]),
+    "bj_result_page": (_VP, [_VP, _U64, _U64]),
+    "bj_result_device_page": (_VP, [_VP, _U64, _U64]),
+    "bj_result_copy_pages": (_INT, [_VP, _U64, ctypes.POINTER(_VP)]),
+    "bj_result_stats": (_INT, [_VP, ctypes.POINTER(BjStats)]),
+    "bj_result_free": (None, [_VP]),
+    "bj_context_stream": (_VP, [_VP]),
+}
+
+WORKLOAD_ABI = {
+    "bjw_workload_create": (_INT, [ctypes.c_char_p, _U64, ctypes.c_double, ctypes.POINTER(_VP)]),
+    "bjw_workload_load": (_INT, [ctypes.c_char_p, ctypes.POINTER(_VP)]),
+    "bjw_workload_plan": (ctypes.POINTER(BjPlan), [_VP]),
+    "bjw_workload_scan_bytes": (_U64, [_VP]),
+    "bjw_workload_free": (None, [_VP]),
+    "bjw_save_plan": (_INT, [ctypes.c_char_p, ctypes.POINTER(BjPlan)]),
+    "bjw_save_table": (_INT, [ctypes.c_char_p, ctypes.POINTER(BjTable)]),
+    "bjw_encode_column": (_INT, [_I32, _U64, _VP, _VP, _VP, _VP, ctypes.POINTER(_VP)]),
+    "bjw_pages_count": (_U64, [_VP]),
+    "bjw_pages_ptrs": (ctypes.POINTER(_VP), [_VP]),
+    "bjw_pages_free": (None, [_VP]),
+}
+
+_lib = None
+_wlib = None
+
+
+def _bind(lib, table):
+    for name, (res, args) in table.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def library_path() -> str:
+    return os.path.join(_HERE, "libb200join.so")
+
+
+def lib():
+    """The engine library (libb200join.so); raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        path = library_path()
+        if not os.path.exists(path):
+            raise EngineError(6, f"{path} is missing: run `make -C {_HERE}` (or __graft_entry__.build())")
+        _lib = _bind(ctypes.CDLL(path), ABI)
+    return _lib
+
+
+def wlib():
+    """The workload/encoder library (libb200join_workloads.so)."""
+    global _wlib
+    if _wlib is None:
+        path = os.path.join(_HERE, "libb200join_workloads.so")
+        if not os.path.exists(path):
+            raise EngineError(6, f"{path} is missing: run `make -C {_HERE}`")
+        _wlib = _bind(ctypes.CDLL(path), WORKLOAD_ABI)
+    return _wlib
+
+
+# ---------------------------------------------------------------------------
+# Tables and pages
+
+@dataclass
+class Column:
+    """A column of 8 KiB pages (mirrors the contest's Column)."""
+    type: int
+    data: bytes = b""  # num_pages * PAGE_SIZE bytes
+
+    @property
+    def num_pages(self) -> int:
+        return len(self.data) // PAGE_SIZE
+
+    def page(self, i: int) -> bytes:
+        return self.data[i * PAGE_SIZE:(i + 1) * PAGE_SIZE]
+
+
+@dataclass
+class ColumnarTable:
+    num_rows: int = 0
+    columns: List[Column] = field(default_factory=list)
+
+
+def encode_column(dtype: int, values: Sequence) -> Column:
+    """Encodes Python values (None = NULL) into pages with the contest's
+    packing rules (C++ encoder in libb200join_workloads.so)."""
+    n = len(values)
+    valid = (ctypes.c_uint8 * max(n, 1))(*[0 if v is None else 1 for v in values]) if n else None
+    out = ctypes.c_void_p()
+    if dtype == VARCHAR:
+        blobs = [b"" if v is None else (v.encode() if isinstance(v, str) else bytes(v)) for v in values]
+        offs = [0]
+        for b in blobs:
+            offs.append(offs[-1] + len(b))
+        joined = b"".join(blobs)
+        off_arr = (ctypes.c_uint64 * (n + 1))(*offs)
+        byte_buf = ctypes.create_string_buffer(joined, max(len(joined), 1))
+        st = wlib().bjw_encode_column(dtype, n, None, valid, off_arr, byte_buf, ctypes.byref(out))
+    else:
+        ctype = {INT32: ctypes.c_int32, INT64: ctypes.c_int64, FP64: ctypes.c_double}[dtype]
+        arr = (ctype * max(n, 1))(*[0 if v is None else v for v in values])
+        st = wlib().bjw_encode_column(dtype, n, arr, valid, None, None, ctypes.byref(out))
+    if st != 0:
+        raise EngineError(st, "encode_column failed")
+    try:
+        cnt = wlib().bjw_pages_count(out)
+        ptrs = wlib().bjw_pages_ptrs(out)
+        data = b"".join(ctypes.string_at(ptrs[i], PAGE_SIZE) for i in range(cnt))
+    finally:
+        wlib().bjw_pages_free(out)
+    return Column(dtype, data)
+
+
+def table_from_rows(rows: Sequence[Sequence], types: Sequence[int]) -> ColumnarTable:
+    """Row table -> ColumnarTable (the contest's Table::to_columnar)."""
+    t = ColumnarTable(num_rows=len(rows))
+    for c, ty in enumerate(types):
+        t.columns.append(encode_column(ty, [r[c] for r in rows]))
+    return t
+
+
+def decode_column(col: Column) -> List:
+    """Pages -> Python values (None = NULL); the contest's from_columnar."""
+    out: List = []
+    i = 0
+    n = col.num_pages
+    while i < n:
+        pg = col.page(i)
+        nrows, nv = struct.unpack_from("<HH", pg, 0)
+        if col.type == VARCHAR and nrows == 0xFFFF:
+            s = pg[4:4 + nv]
+            while i + 1 < n and struct.unpack_from("<H", col.page(i + 1), 0)[0] == 0xFFFE:
+                i += 1
+                q = col.page(i)
+                s += q[4:4 + struct.unpack_from("<H", q, 2)[0]]
+            out.append(s.decode("latin-1"))
+            i += 1
+            continue
+        bm = pg[PAGE_SIZE - (nrows + 7) // 8:]
+        dense = 0
+        if col.type == VARCHAR:
+            offs = struct.unpack_from(f"<{nv}H", pg, 4) if nv else ()
+            base = 4 + 2 * nv
+        for r in range(nrows):
+            if not (bm[r >> 3] >> (r & 7)) & 1:
+                out.append(None)
+                continue
+            if col.type == INT32:
+                out.append(struct.unpack_from("<i", pg, 4 + 4 * dense)[0])
+            elif col.type == INT64:
+                out.append(struct.unpack_from("<q", pg, 8 + 8 * dense)[0])
+            elif col.type == FP64:
+                out.append(struct.unpack_from("<d", pg, 8 + 8 * dense)[0])
+            else:
+                b = offs[dense - 1] if dense else 0
+                out.append(pg[base + b:base + offs[dense]].decode("latin-1"))
+            dense += 1
+        i += 1
+    return out
+
+
+def rows_of(table: ColumnarTable) -> List[Tuple]:
+    """ColumnarTable -> list of row tuples (the contest's Table::from_columnar)."""
+    cols = [decode_column(c) for c in table.columns]
+    for c in cols:
+        if len(c) != table.num_rows:
+            raise ValueError(f"column holds {len(c)} rows, table says {table.num_rows}")
+    return list(zip(*cols)) if cols else [()] * table.num_rows
+
+
+# ---------------------------------------------------------------------------
+# Plans
+
+@dataclass
+class PlanNode:
+    kind: int
+    output_attrs: List[Tuple[int, int]]
+    base_table_id: int = 0
+    build_left: bool = True
+    left: int = 0
+    right: int = 0
+    left_attr: int = 0
+    right_attr: int = 0
+
+
+class Plan:
+    """Mirrors the contest's Plan (plan.h:112-149)."""
+
+    def __init__(self):
+        self.nodes: List[PlanNode] = []
+        self.inputs: List[ColumnarTable] = []
+        self.root = 0
+
+    def new_scan_node(self, base_table_id: int, output_attrs: Iterable[Tuple[int, int]]) -> int:
+        self.nodes.append(PlanNode(NODE_SCAN, list(output_attrs), base_table_id=base_table_id))
+        return len(self.nodes) - 1
+
+    def new_join_node(self, build_left: bool, left: int, right: int, left_attr: int, right_attr: int,
+                      output_attrs: Iterable[Tuple[int, int]]) -> int:
+        self.nodes.append(PlanNode(NODE_JOIN, list(output_attrs), build_left=build_left, left=left, right=right,
+                                   left_attr=left_attr, right_attr=right_attr))
+        return len(self.nodes) - 1
+
+    def new_input(self, table: ColumnarTable) -> int:
+        self.inputs.append(table)
+        return len(self.inputs) - 1
+
+
+class CPlan:
+    """A bj_plan built from a Python Plan; keeps every buffer alive."""
+
+    def __init__(self, plan: Plan):
+        self._keep = []
+        tables = (BjTable * max(len(plan.inputs), 1))()
+        for i, t in enumerate(plan.inputs):
+            cols = (BjColumn * max(len(t.columns), 1))()
+            for c, col in enumerate(t.columns):
+                buf = ctypes.create_string_buffer(col.data, max(len(col.data), 1))
+                ptrs = (ctypes.c_void_p * max(col.num_pages, 1))(
+                    *[ctypes.addressof(buf) + k * PAGE_SIZE for k in range(col.num_pages)])
+                self._keep += [buf, ptrs]
+                cols[c].type = col.type
+                cols[c].num_pages = col.num_pages
+                cols[c].pages = ctypes.cast(ptrs, ctypes.POINTER(ctypes.c_void_p))
+            self._keep.append(cols)
+            tables[i].num_rows = t.num_rows
+            tables[i].num_columns = len(t.columns)
+            tables[i].columns = ctypes.cast(cols, ctypes.POINTER(BjColumn))
+        nodes = (BjNode * max(len(plan.nodes), 1))()
+        for n, pn in enumerate(plan.nodes):
+            attrs = (BjAttr * max(len(pn.output_attrs), 1))()
+            for a, (idx, ty) in enumerate(pn.output_attrs):
+                attrs[a].index = idx
+                attrs[a].type = ty
+            self._keep.append(attrs)
+            nodes[n].kind = pn.kind
+            nodes[n].build_left = int(pn.build_left)
+            nodes[n].base_table_id = pn.base_table_id
+            nodes[n].left, nodes[n].right = pn.left, pn.right
+            nodes[n].left_attr, nodes[n].right_attr = pn.left_attr, pn.right_attr
+            nodes[n].num_output_attrs = len(pn.output_attrs)
+            nodes[n].output_attrs = ctypes.cast(attrs, ctypes.POINTER(BjAttr))
+        self._keep += [tables, nodes]
+        self.struct = BjPlan(len(plan.nodes), ctypes.cast(nodes, ctypes.POINTER(BjNode)), len(plan.inputs),
+                             ctypes.cast(tables, ctypes.POINTER(BjTable)), plan.root)
+
+    def ref(self):
+        return ctypes.byref(self.struct)
+
+
+def save_plan(path: str, plan) -> None:
+    """Writes a plan (Plan, CPlan or POINTER(BjPlan)) in the engine's plan file format."""
+    if isinstance(plan, Plan):
+        plan = CPlan(plan)
+    p = plan.ref() if isinstance(plan, CPlan) else plan
+    st = wlib().bjw_save_plan(path.encode(), p)
+    if st != 0:
+        raise EngineError(st, f"cannot write {path}")
+
+
+def read_table_file(path: str) -> ColumnarTable:
+    """Reads a result table file ("BJTABL01", include/contest/plan_io.h)."""
+    with open(path, "rb") as f:
+        data = f.read()
+    if data[:8] != b"BJTABL01":
+        raise ValueError(f"{path}: not a table file")
+    nrows, ncols = struct.unpack_from("<QQ", data, 8)
+    off = 24
+    t = ColumnarTable(num_rows=nrows)
+    for _ in range(ncols):
+        ty, _pad, npg = struct.unpack_from("<iIQ", data, off)
+        off += 16
+        t.columns.append(Column(ty, data[off:off + npg * PAGE_SIZE]))
+        off += npg * PAGE_SIZE
+    return t
+
+
+class Workload:
+    """A seeded synthetic workload built by libb200join_workloads.so."""
+
+    def __init__(self, name: str, seed: int, scale: float = 1.0, path: Optional[str] = None):
+        h = ctypes.c_void_p()
+        if path:
+            st = wlib().bjw_workload_load(path.encode(), ctypes.byref(h))
+        else:
+            st = wlib().bjw_workload_create(name.encode(), seed, scale, ctypes.byref(h))
+        if st != 0:
+            raise EngineError(st, f"cannot build workload {name}")
+        self.handle = h
+        self.name, self.seed, self.scale = name, seed, scale
+
+    def plan_ptr(self):
+        return wlib().bjw_workload_plan(self.handle)
+
+    def scan_bytes(self) -> int:
+        return wlib().bjw_workload_scan_bytes(self.handle)
+
+    def close(self):
+        if self.handle:
+            wlib().bjw_workload_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Engine
+
+
+class Result:
+    """A bj_result: rows, per-column pages (host or device), stats."""
+
+    def __init__(self, ctx: "Context", handle):
+        self._ctx = ctx
+        self.handle = handle
+
+    @property
+    def num_rows(self) -> int:
+        return lib().bj_result_num_rows(self.handle)
+
+    @property
+    def num_columns(self) -> int:
+        return lib().bj_result_num_columns(self.handle)
+
+    def column_type(self, c: int) -> int:
+        return lib().bj_result_column_type(self.handle, c)
+
+    def column_pages(self, c: int) -> int:
+        return lib().bj_result_column_num_pages(self.handle, c)
+
+    def stats(self) -> BjStats:
+        s = BjStats()
+        lib().bj_result_stats(self.handle, ctypes.byref(s))
+        return s
+
+    def to_table(self) -> ColumnarTable:
+        t = ColumnarTable(num_rows=self.num_rows)
+        for c in range(self.num_columns):
+            n = self.column_pages(c)
+            bufs = (ctypes.c_char * (max(n, 1) * PAGE_SIZE))()
+            ptrs = (ctypes.c_void_p * max(n, 1))(*[ctypes.addressof(bufs) + k * PAGE_SIZE for k in range(n)])
+            st = lib().bj_result_copy_pages(self.handle, c, ptrs)
+            if st != 0:
+                raise EngineError(st, "bj_result_copy_pages failed")
+            t.columns.append(Column(self.column_type(c), bytes(bufs)[:n * PAGE_SIZE]))
+        return t
+
+    def table_struct(self):
+        """A BjTable view of the host pages (valid while this result lives)."""
+        cols = (BjColumn * max(self.num_columns, 1))()
+        keep = [cols]
+        for c in range(self.num_columns):
+            n = self.column_pages(c)
+            ptrs = (ctypes.c_void_p * max(n, 1))(*[lib().bj_result_page(self.handle, c, k) for k in range(n)])
+            keep.append(ptrs)
+            cols[c].type = self.column_type(c)
+            cols[c].num_pages = n
+            cols[c].pages = ctypes.cast(ptrs, ctypes.POINTER(ctypes.c_void_p))
+        t = BjTable(self.num_rows, self.num_columns, ctypes.cast(cols, ctypes.POINTER(BjColumn)))
+        return t, keep
+
+    def free(self):
+        if self.handle:
+            lib().bj_result_free(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+
+class Resident:
+    def __init__(self, ctx: "Context", handle):
+        self._ctx, self.handle = ctx, handle
+
+    def free(self):
+        if self.handle:
+            lib().bj_resident_free(self._ctx.handle, self.handle)
+            self.handle = None
+
+
+class Context:
+    """Contest::build_context / execute / destroy_context over the C ABI."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        st = lib().bj_context_create(device, ctypes.byref(h))
+        if st != 0:
+            raise EngineError(st, "bj_context_create failed (is a CUDA device visible?)")
+        self.handle = h
+
+    def _check(self, st: int, what: str):
+        if st != 0:
+            raise EngineError(st, f"{what}: {lib().bj_last_error(self.handle).decode()}")
+
+    def execute_raw(self, plan) -> Result:
+        """Runs a CPlan / POINTER(BjPlan); returns the Result handle."""
+        p = plan.ref() if isinstance(plan, CPlan) else plan
+        r = ctypes.c_void_p()
+        self._check(lib().bj_execute(self.handle, p, ctypes.byref(r)), "bj_execute")
+        return Result(self, r)
+
+    def execute(self, plan: Plan) -> ColumnarTable:
+        """Contest::execute: returns the result as a ColumnarTable."""
+        with self.execute_raw(CPlan(plan)) as r:
+            return r.to_table()
+
+    def upload(self, table_struct) -> Resident:
+        r = ctypes.c_void_p()
+        self._check(lib().bj_resident_upload(self.handle, ctypes.byref(table_struct), ctypes.byref(r)),
+                    "bj_resident_upload")
+        return Resident(self, r)
+
+    def execute_resident(self, plan, residents: Sequence[Resident], flags: int = RESULT_HOST) -> Result:
+        p = plan.ref() if isinstance(plan, CPlan) else plan
+        arr = (ctypes.c_void_p * max(len(residents), 1))(*[x.handle for x in residents])
+        r = ctypes.c_void_p()
+        self._check(lib().bj_execute_resident(self.handle, p, arr, flags, ctypes.byref(r)), "bj_execute_resident")
+        return Result(self, r)
+
+    def stream(self) -> int:
+        return lib().bj_context_stream(self.handle) or 0
+
+    def close(self):
+        if self.handle:
+            lib().bj_context_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def build_context(device: int = 0) -> Context:
+    return Context(device)
+
+
+def destroy_context(ctx: Context) -> None:
+    ctx.close()
+
+
+def execute(plan: Plan, ctx: Context) -> ColumnarTable:
+    return ctx.execute(plan)

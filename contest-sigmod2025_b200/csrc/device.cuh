@@ -1,0 +1,176 @@
+// Device-side views shared by the join engine's kernels.
+//
+// A column lives in HBM as its 8 KiB contest pages, copied verbatim and back
+// to back (page p at pages + p * 8192). Nothing is decoded ahead of time: the
+// kernels read values straight out of the pages, helped by three small index
+// arrays built once per column (k_pages.cu):
+//   row_start[p]     first row of page p (exclusive prefix of contained rows)
+//   page_of_blk[b]   page holding row b * 1024 (shortcut for the page search)
+//   dense_base[c]    non-null values before 64-row chunk c of a page, with
+//                    chunk_base[p] the first chunk of page p
+// This replaces the reference's per-thread readers (TableScan.cpp:82-239:
+// exponential page search, popcount to the non-null index, pdep/pext).
+#pragma once
+
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define BJ_HD __host__ __device__ __forceinline__
+#else
+#define BJ_HD inline
+#endif
+
+namespace bj {
+
+constexpr uint32_t kPageSize = 8192;
+constexpr uint32_t kBlkShift = 10;  // rows per page_of_blk entry = 1024
+constexpr int kMaxProbes = 16;      // children probed by one pipeline
+constexpr int kMaxSlots = 32;       // payload slots carried by one hash table
+constexpr uint64_t kNullBits = ~0ull;
+
+enum ColType : int32_t { kInt32 = 0, kInt64 = 1, kFp64 = 2, kVarchar = 3 };
+
+// Device error codes, written (first one wins) to the context's error word.
+enum DevError : uint32_t {
+    kErrNone = 0,
+    kErrPageHeader = 1,   // a page header contradicts the page format
+    kErrRowRange = 2,     // a row id beyond the column
+    kErrCapacity = 3,     // an output buffer would overflow
+    kErrLongString = 4,   // a long-string page run is malformed
+};
+
+struct DevColumn {
+    const uint8_t* pages;
+    const uint32_t* row_start;    // npages + 1
+    const uint32_t* page_of_blk;  // (nrows >> kBlkShift) + 1
+    const uint32_t* dense_base;   // per 64-row chunk
+    const uint32_t* chunk_base;   // npages + 1
+    uint32_t npages;
+    uint32_t nrows;
+    int32_t type;
+    uint32_t flags;  // bit 0: some page has NULLs; bit 1: long strings present
+};
+
+// String handle carried in a value slot: page index << 16 | value index in the
+// page; a long string (its own page run) uses value index 0xffff.
+BJ_HD uint64_t make_str_handle(uint32_t page, uint32_t dense) {
+    return (uint64_t(page) << 16) | dense;
+}
+BJ_HD uint32_t str_handle_page(uint64_t h) { return uint32_t(h >> 16); }
+BJ_HD uint32_t str_handle_dense(uint64_t h) { return uint32_t(h & 0xffff); }
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ uint16_t ld16(const uint8_t* p) { return *reinterpret_cast<const uint16_t*>(p); }
+
+// Page holding `row` (row < nrows).
+__device__ __forceinline__ uint32_t locate_page(const DevColumn& c, uint32_t row) {
+    uint32_t lo = c.page_of_blk[row >> kBlkShift];
+    uint32_t hi = c.page_of_blk[(row >> kBlkShift) + 1];  // page of the next block start (or npages - 1)
+    // Binary search for the last page p in [lo, hi] with row_start[p] <= row.
+    while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (c.row_start[mid] <= row)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Loads the bitmap bits [64k, 64k+64) of a page whose bitmap starts at `bm`
+// (bytes may be unaligned; bits beyond the page's rows are garbage).
+__device__ __forceinline__ uint64_t load_bits64(const uint8_t* bm, uint32_t k, uint32_t nbytes) {
+    uint64_t w = 0;
+    uint32_t b0 = k * 8;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        if (b0 + i < nbytes) w |= uint64_t(bm[b0 + i]) << (8 * i);
+    return w;
+}
+
+// Reads the value of `row` as a 64-bit slot. Returns false for NULL.
+// INT32 is zero-extended, INT64/FP64 are raw bits, VARCHAR yields a handle.
+__device__ __forceinline__ bool col_get(const DevColumn& c, uint32_t row, uint64_t& v) {
+    uint32_t p = locate_page(c, row);
+    uint32_t i = row - c.row_start[p];
+    const uint8_t* pg = c.pages + size_t(p) * kPageSize;
+    uint32_t nrows = ld16(pg);
+    if (c.type == kVarchar && nrows >= 0xfffe) {
+        v = make_str_handle(p, 0xffff);
+        return true;
+    }
+    uint32_t nn = ld16(pg + 2);
+    uint32_t dense = i;
+    if (nn != nrows) {
+        uint32_t nbytes = (nrows + 7) >> 3;
+        const uint8_t* bm = pg + kPageSize - nbytes;
+        if (!((bm[i >> 3] >> (i & 7)) & 1)) return false;
+        uint64_t w = load_bits64(bm, i >> 6, nbytes);
+        dense = c.dense_base[c.chunk_base[p] + (i >> 6)] + __popcll(w & ((1ull << (i & 63)) - 1));
+    }
+    switch (c.type) {
+    case kInt32: v = *reinterpret_cast<const uint32_t*>(pg + 4 + 4 * dense); break;
+    case kInt64:
+    case kFp64: v = *reinterpret_cast<const uint64_t*>(pg + 8 + 8 * size_t(dense)); break;
+    default: v = make_str_handle(p, dense); break;
+    }
+    return true;
+}
+
+#endif  // __CUDACC__
+
+// The reference's key hash (engine/op/Hashtable.hpp:35-39): the 32-bit key
+// times the 64-bit Fibonacci constant; buckets take the high bits.
+BJ_HD uint64_t key_hash(uint32_t key) {
+    return uint64_t(key) * 0x9E3779B97F4A7C15ull;
+}
+
+// Independent mix for the bloom filter (murmur3 fmix64 finaliser).
+BJ_HD uint64_t mix64(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+// Blocked bloom filter: one 32-bit word per key, four bits set in it.
+BJ_HD uint32_t bloom_bits(uint64_t g) {
+    return (1u << (g & 31)) | (1u << ((g >> 5) & 31)) | (1u << ((g >> 10) & 31)) | (1u << ((g >> 15) & 31));
+}
+BJ_HD uint32_t bloom_word(uint64_t g, uint32_t log2_words) {
+    return log2_words ? uint32_t(g >> (64 - log2_words)) : 0u;
+}
+
+// A built hash table: entries grouped by bucket (CSR), keys 32-bit, a
+// multiplicity per entry (eager aggregation folds identical tuples into one
+// entry, engine/op/Hashtable.cpp:236-248), `width` 64-bit payload slots per
+// entry with a NULL mask.
+struct HTView {
+    const uint32_t* bucket_off;  // nbuckets + 1
+    const uint32_t* keys;        // nentries
+    const uint64_t* mult;        // nentries
+    const uint64_t* pay;         // nentries * width
+    const uint32_t* pnull;       // nentries (bit j: slot j is NULL)
+    const uint32_t* bloom;       // 1 << bloom_log2 words, or null
+    uint32_t shift;              // bucket = key_hash >> shift
+    uint32_t bloom_log2;
+    uint32_t nentries;
+    uint32_t width;
+};
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ bool bloom_may_contain(const uint32_t* bloom, uint32_t log2w, uint32_t key) {
+    uint64_t g = mix64(key);
+    uint32_t bits = bloom_bits(g);
+    return (bloom[bloom_word(g, log2w)] & bits) == bits;
+}
+
+__device__ __forceinline__ void record_error(uint32_t* err, uint32_t code) {
+    if (err) atomicCAS(err, 0u, code);
+}
+
+#endif  // __CUDACC__
+
+} // namespace bj

@@ -1,0 +1,1000 @@
+// Host side of the B200 join engine: context, memory, page upload, pipeline
+// driver and the C ABI of include/b200join.h.
+//
+// Replaces, for the join path:
+//  * Contest::build_context / execute / destroy_context (engine/Execute.cpp:
+//    11-48): a context owns a CUDA stream, a device arena, pinned staging and
+//    a host thread pool for page staging (the reference's scheduler threads,
+//    engine/infra/Scheduler.cpp, are replaced by CTAs on the device);
+//  * the per-query bump allocator (engine/infra/QueryMemory.cpp:86-139): the
+//    device arena is reset after every call;
+//  * QueryPlan::runPipeline (engine/query/QueryPlan.cpp:414-678): each
+//    pipeline of the ExecPlan (planner.h) runs as probe stages, then either a
+//    hash build or the result materialisation.
+#include "../../include/b200join.h"
+#include "launch.h"
+#include "planner.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace bj {
+namespace {
+
+struct Fail {
+    int status;
+    std::string msg;
+};
+
+#define BJ_CK(call)                                                                                      \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            throw Fail{e_ == cudaErrorMemoryAllocation ? BJ_ERR_OOM : BJ_ERR_CUDA,                       \
+                       std::string(#call) + ": " + cudaGetErrorString(e_)};                              \
+    } while (0)
+
+uint32_t bit_width(uint64_t x) { return x ? 64 - __builtin_clzll(x) : 0; }
+
+size_t full_page_rows(size_t width) {
+    size_t begin = width == 8 ? 8 : 4, n = 0;
+    while (begin + (n + 1) * width + (n / 8 + 1) <= kPageSize) n++;
+    return n;
+}
+
+// ---------------------------------------------------------------------------
+// Host thread pool (page staging).
+class ThreadPool {
+    public:
+    explicit ThreadPool(unsigned n) {
+        for (unsigned i = 0; i < n; i++) workers_.emplace_back([this] { loop(); });
+    }
+    ~ThreadPool() {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+    size_t size() const { return workers_.size() + 1; }
+    // Runs fn(i) for i in [0, n) on the pool and the calling thread.
+    void parallel_for(size_t n, const std::function<void(size_t)>& fn) {
+        if (n == 0) return;
+        if (workers_.empty() || n == 1) {
+            for (size_t i = 0; i < n; i++) fn(i);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> g(m_);
+            job_ = &fn;
+            n_ = n;
+            next_ = 0;
+            active_ = workers_.size();
+            gen_++;
+        }
+        cv_.notify_all();
+        run_items();
+        std::unique_lock<std::mutex> g(m_);
+        done_cv_.wait(g, [this] { return active_ == 0; });
+        job_ = nullptr;
+    }
+
+    private:
+    void run_items() {
+        for (;;) {
+            size_t i = next_.fetch_add(1);
+            if (i >= n_) break;
+            (*job_)(i);
+        }
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> g(m_);
+                cv_.wait(g, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            run_items();
+            {
+                std::lock_guard<std::mutex> g(m_);
+                if (--active_ == 0) done_cv_.notify_all();
+            }
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(size_t)>* job_ = nullptr;
+    std::atomic<size_t> next_{0};
+    size_t n_ = 0, active_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+
+// ---------------------------------------------------------------------------
+// Device arena: bump allocation over large chunks, reset after each call.
+class Arena : public Scratch {
+    public:
+    ~Arena() override {
+        for (auto& c : chunks_) cudaFree(c.p);
+    }
+    void* alloc(size_t bytes) override {
+        bytes = (bytes + 255) & ~size_t(255);
+        if (bytes == 0) bytes = 256;
+        for (; cur_ < chunks_.size(); cur_++) {
+            Chunk& c = chunks_[cur_];
+            if (c.used + bytes <= c.size) {
+                void* p = c.p + c.used;
+                c.used += bytes;
+                high_ = std::max(high_, used_total() );
+                return p;
+            }
+        }
+        size_t sz = std::max<size_t>(bytes, size_t(1) << 30);
+        uint8_t* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, sz);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Fail{BJ_ERR_OOM, "device arena: cudaMalloc of " + std::to_string(sz) + " bytes failed"};
+        }
+        chunks_.push_back(Chunk{p, sz, bytes});
+        cur_ = chunks_.size() - 1;
+        return p;
+    }
+    void reset() {
+        for (auto& c : chunks_) c.used = 0;
+        cur_ = 0;
+    }
+    size_t used_total() const {
+        size_t u = 0;
+        for (auto& c : chunks_) u += c.used;
+        return u;
+    }
+
+    private:
+    struct Chunk {
+        uint8_t* p;
+        size_t size;
+        size_t used;
+    };
+    std::vector<Chunk> chunks_;
+    size_t cur_ = 0, high_ = 0;
+};
+
+// Persistent allocations (resident tables): plain cudaMalloc, freed together.
+class PersistentAlloc : public Scratch {
+    public:
+    ~PersistentAlloc() override { release(); }
+    void* alloc(size_t bytes) override {
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 256));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Fail{BJ_ERR_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed"};
+        }
+        ptrs_.push_back(p);
+        return p;
+    }
+    void release() {
+        for (void* p : ptrs_) cudaFree(p);
+        ptrs_.clear();
+    }
+
+    private:
+    std::vector<void*> ptrs_;
+};
+
+struct PinnedBlock {
+    uint8_t* p = nullptr;
+    size_t size = 0;
+};
+
+// One column resident on the device.
+struct DevTable {
+    uint64_t rows = 0;
+    std::vector<DevColumn> cols;
+    std::vector<uint8_t> present;
+};
+
+const char* dev_error_text(uint32_t code) {
+    switch (code) {
+    case kErrPageHeader: return "a page header contradicts the page format";
+    case kErrRowRange: return "a row index beyond its column (malformed pages)";
+    case kErrCapacity: return "an internal buffer overflowed";
+    case kErrLongString: return "a long-string page run is malformed";
+    default: return "unknown device error";
+    }
+}
+
+} // namespace
+} // namespace bj
+
+using namespace bj;
+
+struct bj_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    Arena arena;
+    PinnedBlock stage;                 // upload staging
+    std::vector<PinnedBlock> pinned_free;
+    std::unique_ptr<ThreadPool> pool;
+    std::string last_error;
+    uint32_t* d_err = nullptr;         // device error word
+    uint64_t* h_small = nullptr;       // pinned readback slots
+    uint64_t* d_small = nullptr;       // device readback slots
+    uint64_t launches = 0;
+    uint64_t live_results = 0;
+
+    PinnedBlock take_pinned(size_t bytes) {
+        for (size_t i = 0; i < pinned_free.size(); i++)
+            if (pinned_free[i].size >= bytes) {
+                PinnedBlock b = pinned_free[i];
+                pinned_free.erase(pinned_free.begin() + i);
+                return b;
+            }
+        PinnedBlock b;
+        b.size = std::max<size_t>(bytes, 1 << 20);
+        cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&b.p), b.size, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Fail{BJ_ERR_OOM, "pinned host allocation failed"};
+        }
+        return b;
+    }
+    void give_pinned(PinnedBlock b) {
+        if (!b.p) return;
+        pinned_free.push_back(b);
+        while (pinned_free.size() > 4) {
+            cudaFreeHost(pinned_free.front().p);
+            pinned_free.erase(pinned_free.begin());
+        }
+    }
+};
+
+struct bj_resident {
+    PersistentAlloc mem;
+    DevTable table;
+};
+
+struct bj_result {
+    bj_context* ctx = nullptr;
+    uint64_t rows = 0;
+    std::vector<int32_t> types;
+    std::vector<uint64_t> npages;
+    std::vector<uint64_t> page_base;
+    uint64_t total_pages = 0;
+    PinnedBlock host;
+    uint8_t* dev = nullptr;
+    bj_stats stats{};
+};
+
+namespace bj {
+namespace {
+
+// Reads back `n` u64 slots of ctx->d_small after the stream drains; checks the
+// device error word.
+void readback(bj_context* ctx, int n) {
+    BJ_CK(cudaMemcpyAsync(ctx->h_small, ctx->d_small, sizeof(uint64_t) * 64, cudaMemcpyDeviceToHost, ctx->stream));
+    BJ_CK(cudaStreamSynchronize(ctx->stream));
+    (void)n;
+    uint32_t code = uint32_t(ctx->h_small[63]);
+    if (code) throw Fail{BJ_ERR_INVALID, std::string("device check failed: ") + dev_error_text(code)};
+}
+
+// Queue a copy of a device u32/u64 value into readback slot i.
+void stash_u32(bj_context* ctx, const uint32_t* src, int i) {
+    BJ_CK(cudaMemsetAsync(ctx->d_small + i, 0, sizeof(uint64_t), ctx->stream));
+    BJ_CK(cudaMemcpyAsync(ctx->d_small + i, src, sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+}
+void stash_u64(bj_context* ctx, const uint64_t* src, int i) {
+    BJ_CK(cudaMemcpyAsync(ctx->d_small + i, src, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
+}
+void stash_err(bj_context* ctx) {
+    BJ_CK(cudaMemsetAsync(ctx->d_small + 63, 0, sizeof(uint64_t), ctx->stream));
+    BJ_CK(cudaMemcpyAsync(ctx->d_small + 63, ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+// ---------------------------------------------------------------------------
+// Page upload and indexing.
+
+struct ColumnJob {
+    const bj_column* src;  // host pages (null for already-resident pages)
+    uint8_t* dpages;       // device destination
+    uint64_t rows;         // rows the table claims
+    DevColumn* out;
+};
+
+// Copies host pages into `dst` on the device: pages are gathered into pinned
+// staging by the thread pool, chunk by chunk, each chunk's DMA overlapping
+// the next chunk's gathering.
+uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs) {
+    uint64_t total = 0;
+    for (auto& j : jobs) total += j.src->num_pages;
+    if (!total) return 0;
+    size_t bytes = total * kPageSize;
+    if (ctx->stage.size < bytes) {
+        if (ctx->stage.p) {
+            BJ_CK(cudaStreamSynchronize(ctx->stream));
+            cudaFreeHost(ctx->stage.p);
+            ctx->stage = PinnedBlock{};
+        }
+        size_t sz = bytes + bytes / 4;
+        cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&ctx->stage.p), sz, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ctx->stage = PinnedBlock{};
+            throw Fail{BJ_ERR_OOM, "pinned staging allocation failed"};
+        }
+        ctx->stage.size = sz;
+    }
+    // Flatten (column, page) pairs.
+    struct Src {
+        const void* page;
+        uint8_t* dst;
+    };
+    std::vector<Src> all;
+    all.reserve(total);
+    for (auto& j : jobs)
+        for (uint64_t p = 0; p < j.src->num_pages; p++) {
+            if (!j.src->pages[p]) throw Fail{BJ_ERR_INVALID, "null page pointer"};
+            all.push_back(Src{j.src->pages[p], j.dpages + p * kPageSize});
+        }
+    const size_t chunk = 2048;  // pages per DMA
+    uint8_t* stage = ctx->stage.p;
+    for (size_t c0 = 0; c0 < all.size(); c0 += chunk) {
+        size_t c1 = std::min(all.size(), c0 + chunk);
+        size_t per = 64;
+        ctx->pool->parallel_for((c1 - c0 + per - 1) / per, [&](size_t t) {
+            for (size_t i = c0 + t * per; i < std::min(c1, c0 + (t + 1) * per); i++)
+                std::memcpy(stage + i * kPageSize, all[i].page, kPageSize);
+        });
+        // Contiguous destinations within one column become one copy.
+        size_t i = c0;
+        while (i < c1) {
+            size_t k = i + 1;
+            while (k < c1 && all[k].dst == all[k - 1].dst + kPageSize) k++;
+            BJ_CK(cudaMemcpyAsync(all[i].dst, stage + i * kPageSize, (k - i) * kPageSize, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+            i = k;
+        }
+    }
+    return bytes;
+}
+
+// Builds the page index of every job's column (pages already on the device).
+void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem) {
+    struct Tmp {
+        PageIndexBufs b;
+        uint32_t npages;
+    };
+    std::vector<Tmp> tmp(jobs.size());
+    Arena& sc = ctx->arena;
+    for (size_t i = 0; i < jobs.size(); i++) {
+        uint32_t np = uint32_t(jobs[i].src ? jobs[i].src->num_pages : 0);
+        Tmp& t = tmp[i];
+        t.npages = np;
+        t.b.rows = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
+        t.b.chunks = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
+        t.b.row_start = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * (np + 1)));
+        t.b.chunk_base = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * (np + 1)));
+        t.b.flags = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t)));
+        ctx->launches += page_index_pass1(jobs[i].dpages, np, jobs[i].out->type, t.b, ctx->d_err, sc, ctx->stream);
+    }
+    // Read back row totals, chunk totals and flags, a few columns at a time.
+    std::vector<uint64_t> rows(jobs.size()), chunks(jobs.size()), flags(jobs.size());
+    for (size_t i0 = 0; i0 < jobs.size(); i0 += 20) {
+        size_t i1 = std::min(jobs.size(), i0 + 20);
+        for (size_t i = i0; i < i1; i++) {
+            int s = int(3 * (i - i0));
+            stash_u32(ctx, tmp[i].b.row_start + tmp[i].npages, s);
+            stash_u32(ctx, tmp[i].b.chunk_base + tmp[i].npages, s + 1);
+            stash_u32(ctx, tmp[i].b.flags, s + 2);
+        }
+        stash_err(ctx);
+        readback(ctx, 0);
+        for (size_t i = i0; i < i1; i++) {
+            int s = int(3 * (i - i0));
+            rows[i] = ctx->h_small[s];
+            chunks[i] = ctx->h_small[s + 1];
+            flags[i] = ctx->h_small[s + 2];
+        }
+    }
+    for (size_t i = 0; i < jobs.size(); i++) {
+        if (rows[i] != jobs[i].rows)
+            throw Fail{BJ_ERR_INVALID, "a column's pages hold " + std::to_string(rows[i]) + " rows but its table has " +
+                                           std::to_string(jobs[i].rows)};
+        DevColumn& c = *jobs[i].out;
+        c.pages = jobs[i].dpages;
+        c.npages = tmp[i].npages;
+        c.nrows = uint32_t(rows[i]);
+        c.flags = uint32_t(flags[i]);
+        c.row_start = tmp[i].b.row_start;
+        c.chunk_base = tmp[i].b.chunk_base;
+        uint32_t* dense = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * std::max<uint64_t>(chunks[i], 1)));
+        uint32_t nblk = (c.nrows >> kBlkShift) + 2;
+        uint32_t* pob = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * nblk));
+        c.dense_base = dense;
+        c.page_of_blk = pob;
+        ctx->launches += page_index_pass2(c.pages, c.npages, c.nrows, c.row_start, c.chunk_base, dense, pob, ctx->stream);
+    }
+}
+
+// Device copies of the columns of `t` that the plan's scans of `table_id` read.
+void collect_columns(const ExecPlan& ex, uint32_t table_id, uint64_t ncols, std::vector<uint8_t>& used) {
+    used.assign(ncols, 0);
+    for (const PlanAttr& a : ex.attrs)
+        if (ex.inputs[a.input].table == table_id && a.column < ncols) used[a.column] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Pipeline execution.
+
+struct BuiltHT {
+    HTView view{};
+    bool empty = true;
+};
+
+class Executor {
+    public:
+    Executor(bj_context* ctx, const ExecPlan& ex, std::vector<const DevTable*> tables)
+        : ctx_(ctx), ex_(ex), tables_(std::move(tables)), st_(ctx->stream), A_(ctx->arena) {}
+
+    // Runs every pipeline; returns false if the result is empty.
+    bool run(bj_result& res, int flags) {
+        hts_.resize(ex_.pipelines.size());
+        for (size_t p = 0; p + 1 < ex_.pipelines.size(); p++) {
+            if (!run_pipeline(p, nullptr, 0)) return false;
+        }
+        return run_pipeline(ex_.pipelines.size() - 1, &res, flags);
+    }
+    uint64_t pipelines_run() const { return pipes_; }
+
+    private:
+    const DevColumn& col(uint32_t attr) const {
+        const PlanAttr& a = ex_.attrs[attr];
+        const DevTable* t = tables_[ex_.inputs[a.input].table];
+        return t->cols[a.column];
+    }
+    template <typename T>
+    T* alloc(size_t n) {
+        return static_cast<T*>(A_.alloc(sizeof(T) * std::max<size_t>(n, 1)));
+    }
+    void launched(int n) { ctx_->launches += uint64_t(n); }
+
+    // Exclusive scan of tile counts; returns the total (synchronises).
+    uint32_t scan_total_u32(const uint32_t* in, uint32_t* out, size_t n) {
+        launched(scan_exclusive_u32(in, out, n, A_, st_));
+        stash_u32(ctx_, out + n, 0);
+        stash_err(ctx_);
+        readback(ctx_, 1);
+        return uint32_t(ctx_->h_small[0]);
+    }
+    uint64_t scan_total_u64(const uint64_t* in, uint64_t* out, size_t n) {
+        launched(scan_exclusive_u64(in, out, n, A_, st_));
+        stash_u64(ctx_, out + n, 0);
+        stash_err(ctx_);
+        readback(ctx_, 1);
+        return ctx_->h_small[0];
+    }
+
+    bool run_pipeline(size_t pi, bj_result* res, int flags) {
+        pipes_++;
+        const PipelinePlan& pp = ex_.pipelines[pi];
+        const PlanInput& in = ex_.inputs[pp.input];
+        Items items{};
+        items.count = uint32_t(in.rows);
+        items.nprobes = 0;
+
+        // Probe order: ascending sampled hit rate (most selective first).
+        size_t np = pp.probes.size();
+        std::vector<uint32_t> order(np);
+        std::iota(order.begin(), order.end(), 0u);
+        std::vector<double> rate(np, 1.0);
+        if (np) {
+            uint32_t nsample = uint32_t(std::min<uint64_t>(in.rows, 4096));
+            uint32_t* hits = alloc<uint32_t>(np);
+            for (size_t k = 0; k < np; k++) {
+                launched(sample_probe(col(pp.probes[k].probe_attr), nsample, hts_[pp.probes[k].child].view,
+                                      hits + k, st_));
+                stash_u32(ctx_, hits + k, int(k));
+            }
+            stash_err(ctx_);
+            readback(ctx_, int(np));
+            for (size_t k = 0; k < np; k++) rate[k] = nsample ? double(ctx_->h_small[k]) / nsample : 1.0;
+            std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return rate[a] < rate[b]; });
+        }
+        std::vector<uint32_t> stage_of(np);
+        std::vector<HTView> by_stage(np);
+        for (size_t s = 0; s < np; s++) {
+            uint32_t k = order[s];
+            stage_of[k] = uint32_t(s);
+            by_stage[s] = hts_[pp.probes[k].child].view;
+            const HTView& ht = by_stage[s];
+            uint32_t tiles = (items.count + kTile - 1) / kTile;
+            uint32_t* tc = alloc<uint32_t>(tiles);
+            uint32_t* toff = alloc<uint32_t>(tiles + 1);
+            bool bloom = ht.bloom && rate[k] < 0.5;
+            const DevColumn& key = col(pp.probes[k].probe_attr);
+            ItemsOut none{};
+            launched(probe_stage(items, key, ht, 0, tc, nullptr, none, bloom, ctx_->d_err, st_));
+            uint32_t total = scan_total_u32(tc, toff, tiles);
+            if (total == 0) return false;
+            ItemsOut out{};
+            out.rows = alloc<uint32_t>(total);
+            for (size_t j = 0; j <= s; j++) out.ents[j] = alloc<uint32_t>(total);
+            out.mult = alloc<uint64_t>(total);
+            launched(probe_stage(items, key, ht, 1, nullptr, toff, out, bloom, ctx_->d_err, st_));
+            Items next{};
+            next.rows = out.rows;
+            for (size_t j = 0; j <= s; j++) next.ents[j] = out.ents[j];
+            next.mult = out.mult;
+            next.count = total;
+            next.nprobes = int(s + 1);
+            items = next;
+        }
+        if (items.count == 0) return false;
+
+        SlotSources src{};
+        src.n = int(pp.slots.size());
+        for (size_t j = 0; j < pp.slots.size(); j++) {
+            const SlotPlan& sp = pp.slots[j];
+            SlotSource& s = src.s[j];
+            s.kind = sp.kind;
+            if (sp.kind == 0) {
+                s.col = col(sp.attr);
+            } else {
+                s.probe = int(stage_of[sp.probe]);
+                s.slot = int(sp.slot);
+            }
+        }
+        if (pp.build_key >= 0) return build(pi, items, src, by_stage);
+        output(items, src, by_stage, *res, flags);
+        return true;
+    }
+
+    bool build(size_t pi, const Items& items, const SlotSources& src, const std::vector<HTView>& probes) {
+        const PipelinePlan& pp = ex_.pipelines[pi];
+        uint32_t n = items.count;
+        uint32_t width = uint32_t(src.n);
+        TupleBuf tb{};
+        tb.keys = alloc<uint32_t>(n);
+        tb.mult = alloc<uint64_t>(n);
+        tb.pay = alloc<uint64_t>(size_t(n) * std::max<uint32_t>(width, 1));
+        tb.pnull = alloc<uint32_t>(n);
+        tb.count = n;
+        tb.width = width;
+        launched(emit_tuples(items, col(uint32_t(pp.build_key)), src, probes.data(), tb, ctx_->d_err, st_));
+        // Eager aggregation of identical tuples.
+        uint32_t tlog2 = std::max<uint32_t>(1, bit_width(uint64_t(n) * 2));
+        uint32_t* table = alloc<uint32_t>(size_t(1) << tlog2);
+        uint32_t* is_rep = alloc<uint32_t>(n);
+        launched(aggregate_tuples(tb, table, tlog2, is_rep, ctx_->d_err, st_));
+        uint32_t* rep_off = alloc<uint32_t>(n + 1);
+        uint32_t nrep = scan_total_u32(is_rep, rep_off, n);
+        if (nrep == 0) return false;
+        // Buckets: 2^max(bit_width(n), 4) (engine/op/Hashtable.cpp:94-104).
+        uint32_t blog2 = std::max<uint32_t>(bit_width(nrep), 4);
+        uint32_t shift = 64 - blog2;
+        size_t nb = size_t(1) << blog2;
+        uint32_t* counts = alloc<uint32_t>(nb);
+        BJ_CK(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * nb, st_));
+        launched(bucket_count(tb, is_rep, shift, counts, st_));
+        uint32_t* off = alloc<uint32_t>(nb + 1);
+        launched(scan_exclusive_u32(counts, off, nb, A_, st_));
+        uint32_t* cursor = alloc<uint32_t>(nb);
+        BJ_CK(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * nb, st_));
+        HTView ht{};
+        ht.bucket_off = off;
+        ht.keys = alloc<uint32_t>(nrep);
+        ht.mult = alloc<uint64_t>(nrep);
+        ht.pay = alloc<uint64_t>(size_t(nrep) * std::max<uint32_t>(width, 1));
+        ht.pnull = alloc<uint32_t>(nrep);
+        ht.shift = shift;
+        ht.nentries = nrep;
+        ht.width = width;
+        launched(bucket_scatter(tb, is_rep, shift, off, cursor, ht, ctx_->d_err, st_));
+        // Bloom filter: about 16 bits per key.
+        uint32_t wlog2 = std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1));
+        uint32_t* bloom = alloc<uint32_t>(size_t(1) << wlog2);
+        launched(bloom_build(ht.keys, nrep, bloom, wlog2, st_));
+        ht.bloom = bloom;
+        ht.bloom_log2 = wlog2;
+        hts_[pi].view = ht;
+        hts_[pi].empty = false;
+        return true;
+    }
+
+    void output(const Items& items, const SlotSources& src, const std::vector<HTView>& probes, bj_result& res,
+                int flags) {
+        uint32_t n = items.count;
+        uint64_t* mult = alloc<uint64_t>(n);
+        launched(items_mult(items, mult, st_));
+        uint64_t* off = alloc<uint64_t>(size_t(n) + 1);
+        uint64_t N = scan_total_u64(mult, off, n);
+        res.rows = N;
+        FlatOut fo{};
+        fo.n = src.n;
+        for (int j = 0; j < src.n; j++) {
+            fo.vals[j] = alloc<uint64_t>(N);
+            fo.valid[j] = alloc<uint8_t>(N);
+        }
+        launched(emit_output(items, off, src, probes.data(), fo, ctx_->d_err, st_));
+        // Page counts per result column.
+        size_t ncol = ex_.out_slot.size();
+        res.npages.assign(ncol, 0);
+        struct StrPlan {
+            uint32_t* lens = nullptr;
+            uint32_t* block_off = nullptr;
+            size_t nblocks = 0;
+        };
+        std::vector<StrPlan> sp(ncol);
+        for (size_t c = 0; c < ncol; c++) {
+            int32_t t = ex_.out_types[c];
+            uint32_t j = ex_.out_slot[c];
+            if (t != BJ_VARCHAR) {
+                size_t rpp = full_page_rows(t == BJ_INT32 ? 4 : 8);
+                res.npages[c] = (N + rpp - 1) / rpp;
+                continue;
+            }
+            const DevColumn& scol = src.s[j].kind == 0 ? src.s[j].col : col(ex_.pipelines.back().slots[j].attr);
+            sp[c].lens = alloc<uint32_t>(N);
+            launched(string_lengths(fo.vals[j], fo.valid[j], N, StrSource{scol}, sp[c].lens, ctx_->d_err, st_));
+            sp[c].nblocks = (N + kStrBlock - 1) / kStrBlock;
+            uint32_t* bp = alloc<uint32_t>(sp[c].nblocks);
+            sp[c].block_off = alloc<uint32_t>(sp[c].nblocks + 1);
+            launched(string_pack(sp[c].lens, fo.valid[j], N, 0, bp, nullptr, nullptr, st_));
+            res.npages[c] = scan_total_u32(bp, sp[c].block_off, sp[c].nblocks);
+        }
+        res.page_base.assign(ncol, 0);
+        uint64_t total = 0;
+        for (size_t c = 0; c < ncol; c++) {
+            res.page_base[c] = total;
+            total += res.npages[c];
+        }
+        res.total_pages = total;
+        uint8_t* dst = nullptr;
+        if (flags & BJ_RESULT_DEVICE) {
+            if (total) BJ_CK(cudaMallocAsync(reinterpret_cast<void**>(&res.dev), total * kPageSize, st_));
+            dst = res.dev;
+        } else {
+            dst = alloc<uint8_t>(total * kPageSize);
+        }
+        for (size_t c = 0; c < ncol; c++) {
+            int32_t t = ex_.out_types[c];
+            uint32_t j = ex_.out_slot[c];
+            uint8_t* pages = dst + res.page_base[c] * kPageSize;
+            if (t != BJ_VARCHAR) {
+                uint32_t rpp = uint32_t(full_page_rows(t == BJ_INT32 ? 4 : 8));
+                launched(write_fixed_pages(fo.vals[j], fo.valid[j], N, t, rpp, pages, st_));
+                continue;
+            }
+            const DevColumn& scol = src.s[j].kind == 0 ? src.s[j].col : col(ex_.pipelines.back().slots[j].attr);
+            StrPageDesc* descs = alloc<StrPageDesc>(res.npages[c]);
+            launched(string_pack(sp[c].lens, fo.valid[j], N, 1, nullptr, sp[c].block_off, descs, st_));
+            launched(write_string_pages(fo.vals[j], fo.valid[j], sp[c].lens, StrSource{scol}, descs,
+                                        uint32_t(res.npages[c]), pages, ctx_->d_err, st_));
+        }
+        if (!(flags & BJ_RESULT_DEVICE) && total) {
+            res.host = ctx_->take_pinned(total * kPageSize);
+            BJ_CK(cudaMemcpyAsync(res.host.p, dst, total * kPageSize, cudaMemcpyDeviceToHost, st_));
+            res.stats.d2h_bytes += total * kPageSize;
+        }
+        res.stats.output_pages = total;
+    }
+
+    bj_context* ctx_;
+    const ExecPlan& ex_;
+    std::vector<const DevTable*> tables_;
+    cudaStream_t st_;
+    Arena& A_;
+    std::vector<BuiltHT> hts_;
+    uint64_t pipes_ = 0;
+};
+
+void set_empty_result(bj_result& r, const ExecPlan& ex) {
+    r.rows = 0;
+    r.types = ex.out_types;
+    r.npages.assign(ex.out_types.size(), 0);
+    r.page_base.assign(ex.out_types.size(), 0);
+    r.total_pages = 0;
+}
+
+int fail_to_status(bj_context* ctx, const Fail& f) {
+    ctx->last_error = f.msg;
+    // Leave the stream idle and the arena reusable after a failure.
+    cudaStreamSynchronize(ctx->stream);
+    cudaGetLastError();
+    uint32_t zero = 0;
+    cudaMemcpy(ctx->d_err, &zero, sizeof(zero), cudaMemcpyHostToDevice);
+    ctx->arena.reset();
+    return f.status;
+}
+
+// Shared tail of bj_execute / bj_execute_resident.
+int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* resident, int flags, bj_result** out) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!ctx || !plan || !out) return BJ_ERR_INVALID;
+    *out = nullptr;
+    std::unique_ptr<bj_result> res(new bj_result);
+    res->ctx = ctx;
+    try {
+        ExecPlan ex;
+        std::string err;
+        int st = make_exec_plan(*plan, ex, err);
+        if (st != BJ_OK) throw Fail{st, err};
+        res->types = ex.out_types;
+        uint64_t launches0 = ctx->launches;
+        BJ_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(uint32_t), ctx->stream));
+        BJ_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        std::vector<DevTable> owned;
+        std::vector<const DevTable*> tables(plan->num_inputs, nullptr);
+        if (resident) {
+            for (uint64_t i = 0; i < plan->num_inputs; i++) {
+                if (!resident[i]) throw Fail{BJ_ERR_INVALID, "missing resident table"};
+                tables[i] = &resident[i]->table;
+            }
+        } else {
+            // Upload only the columns the scans read.
+            owned.resize(plan->num_inputs);
+            std::vector<ColumnJob> jobs;
+            for (uint64_t i = 0; i < plan->num_inputs; i++) {
+                const bj_table& t = plan->inputs[i];
+                DevTable& d = owned[i];
+                d.rows = t.num_rows;
+                d.cols.assign(t.num_columns, DevColumn{});
+                collect_columns(ex, uint32_t(i), t.num_columns, d.present);
+                tables[i] = &d;
+                if (t.num_rows == 0) continue;
+                if (t.num_columns && !t.columns) throw Fail{BJ_ERR_INVALID, "table without column array"};
+                for (uint64_t c = 0; c < t.num_columns; c++) {
+                    if (!d.present[c]) continue;
+                    const bj_column& hc = t.columns[c];
+                    if (hc.num_pages && !hc.pages) throw Fail{BJ_ERR_INVALID, "column without page array"};
+                    d.cols[c].type = hc.type;
+                    uint8_t* dp = static_cast<uint8_t*>(ctx->arena.alloc(std::max<uint64_t>(hc.num_pages, 1) * kPageSize));
+                    jobs.push_back(ColumnJob{&hc, dp, t.num_rows, &d.cols[c]});
+                    res->stats.input_pages += hc.num_pages;
+                }
+            }
+            if (!ex.empty) {
+                res->stats.h2d_bytes += upload_pages(ctx, jobs);
+                index_columns(ctx, jobs, ctx->arena);
+            }
+        }
+        if (resident) {
+            for (uint64_t i = 0; i < plan->num_inputs; i++) {
+                std::vector<uint8_t> used;
+                collect_columns(ex, uint32_t(i), tables[i]->cols.size(), used);
+                for (size_t c = 0; c < used.size(); c++)
+                    if (used[c]) {
+                        if (!tables[i]->present[c]) throw Fail{BJ_ERR_INVALID, "resident table lacks a scanned column"};
+                        res->stats.input_pages += tables[i]->cols[c].npages;
+                    }
+            }
+        }
+        bool nonempty = false;
+        uint64_t pipes = 0;
+        if (!ex.empty) {
+            Executor exe(ctx, ex, tables);
+            nonempty = exe.run(*res, flags);
+            pipes = exe.pipelines_run();
+        }
+        if (!nonempty) {
+            if (res->dev) cudaFreeAsync(res->dev, ctx->stream);
+            res->dev = nullptr;
+            ctx->give_pinned(res->host);
+            res->host = PinnedBlock{};
+            set_empty_result(*res, ex);
+        }
+        BJ_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+        stash_err(ctx);
+        readback(ctx, 0);
+        float ms = 0;
+        BJ_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        res->stats.device_ms = ms;
+        res->stats.kernel_launches = ctx->launches - launches0;
+        res->stats.pipelines = pipes;
+        ctx->arena.reset();
+    } catch (const Fail& f) {
+        if (res->dev) cudaFree(res->dev);
+        res->dev = nullptr;
+        ctx->give_pinned(res->host);
+        res->host = PinnedBlock{};
+        return fail_to_status(ctx, f);
+    } catch (const std::bad_alloc&) {
+        return fail_to_status(ctx, Fail{BJ_ERR_OOM, "host allocation failed"});
+    } catch (const std::exception& e) {
+        return fail_to_status(ctx, Fail{BJ_ERR_INTERNAL, e.what()});
+    }
+    res->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    ctx->live_results++;
+    ctx->last_error.clear();
+    *out = res.release();
+    return BJ_OK;
+}
+
+} // namespace
+} // namespace bj
+
+extern "C" {
+
+BJ_API const char* bj_version(void) { return "b200join 0.1 (sm_100a)"; }
+
+BJ_API int bj_context_create(int device, bj_context** out) {
+    if (!out) return BJ_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return BJ_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) return BJ_ERR_INVALID;
+    if (cudaSetDevice(device) != cudaSuccess) return BJ_ERR_CUDA;
+    auto ctx = std::make_unique<bj_context>();
+    ctx->device = device;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return BJ_ERR_CUDA;
+    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) return BJ_ERR_CUDA;
+    if (cudaMalloc(&ctx->d_err, 256) != cudaSuccess) return BJ_ERR_OOM;
+    if (cudaMalloc(&ctx->d_small, sizeof(uint64_t) * 64) != cudaSuccess) return BJ_ERR_OOM;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_small), sizeof(uint64_t) * 64, cudaHostAllocDefault) != cudaSuccess)
+        return BJ_ERR_OOM;
+    cudaMemset(ctx->d_err, 0, 256);
+    cudaMemset(ctx->d_small, 0, sizeof(uint64_t) * 64);
+    // Keep freed result buffers cached in the stream-ordered pool.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t threshold = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    ctx->pool = std::make_unique<ThreadPool>(std::min(hw, 16u) - 1);
+    *out = ctx.release();
+    return BJ_OK;
+}
+
+BJ_API void bj_context_destroy(bj_context* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& b : ctx->pinned_free) cudaFreeHost(b.p);
+    if (ctx->stage.p) cudaFreeHost(ctx->stage.p);
+    if (ctx->h_small) cudaFreeHost(ctx->h_small);
+    if (ctx->d_small) cudaFree(ctx->d_small);
+    if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+BJ_API const char* bj_last_error(const bj_context* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+
+BJ_API void* bj_context_stream(bj_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+BJ_API int bj_execute(bj_context* ctx, const bj_plan* plan, bj_result** out) {
+    if (!ctx) return BJ_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    return execute_common(ctx, plan, nullptr, BJ_RESULT_HOST, out);
+}
+
+BJ_API int bj_execute_resident(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int flags,
+                               bj_result** out) {
+    if (!ctx || !tables) return BJ_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    return execute_common(ctx, plan, tables, flags, out);
+}
+
+BJ_API int bj_resident_upload(bj_context* ctx, const bj_table* table, bj_resident** out) {
+    if (!ctx || !table || !out) return BJ_ERR_INVALID;
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    auto r = std::make_unique<bj_resident>();
+    try {
+        DevTable& d = r->table;
+        d.rows = table->num_rows;
+        d.cols.assign(table->num_columns, DevColumn{});
+        d.present.assign(table->num_columns, 0);
+        if (table->num_rows >= (1ull << 32) - 2) throw Fail{BJ_ERR_UNSUPPORTED, "tables are limited to 2^32-2 rows"};
+        std::vector<ColumnJob> jobs;
+        if (table->num_rows) {
+            if (table->num_columns && !table->columns) throw Fail{BJ_ERR_INVALID, "table without column array"};
+            for (uint64_t c = 0; c < table->num_columns; c++) {
+                const bj_column& hc = table->columns[c];
+                if (hc.type < BJ_INT32 || hc.type > BJ_VARCHAR) throw Fail{BJ_ERR_INVALID, "unknown column type"};
+                if (hc.num_pages && !hc.pages) throw Fail{BJ_ERR_INVALID, "column without page array"};
+                d.cols[c].type = hc.type;
+                d.present[c] = 1;
+                uint8_t* dp = static_cast<uint8_t*>(r->mem.alloc(std::max<uint64_t>(hc.num_pages, 1) * kPageSize));
+                jobs.push_back(ColumnJob{&hc, dp, table->num_rows, &d.cols[c]});
+            }
+        } else {
+            for (uint64_t c = 0; c < table->num_columns; c++) d.present[c] = 1;
+        }
+        BJ_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(uint32_t), ctx->stream));
+        upload_pages(ctx, jobs);
+        index_columns(ctx, jobs, r->mem);
+        BJ_CK(cudaStreamSynchronize(ctx->stream));
+        ctx->arena.reset();
+    } catch (const Fail& f) {
+        return fail_to_status(ctx, f);
+    } catch (const std::exception& e) {
+        return fail_to_status(ctx, Fail{BJ_ERR_INTERNAL, e.what()});
+    }
+    *out = r.release();
+    return BJ_OK;
+}
+
+BJ_API void bj_resident_free(bj_context* ctx, bj_resident* t) {
+    if (!t) return;
+    if (ctx) cudaStreamSynchronize(ctx->stream);
+    delete t;
+}
+
+BJ_API uint64_t bj_result_num_rows(const bj_result* r) { return r ? r->rows : 0; }
+BJ_API uint64_t bj_result_num_columns(const bj_result* r) { return r ? r->types.size() : 0; }
+BJ_API int32_t bj_result_column_type(const bj_result* r, uint64_t c) {
+    return r && c < r->types.size() ? r->types[c] : -1;
+}
+BJ_API uint64_t bj_result_column_num_pages(const bj_result* r, uint64_t c) {
+    return r && c < r->npages.size() ? r->npages[c] : 0;
+}
+BJ_API const void* bj_result_page(const bj_result* r, uint64_t c, uint64_t p) {
+    if (!r || !r->host.p || c >= r->npages.size() || p >= r->npages[c]) return nullptr;
+    return r->host.p + (r->page_base[c] + p) * kPageSize;
+}
+BJ_API const void* bj_result_device_page(const bj_result* r, uint64_t c, uint64_t p) {
+    if (!r || !r->dev || c >= r->npages.size() || p >= r->npages[c]) return nullptr;
+    return r->dev + (r->page_base[c] + p) * kPageSize;
+}
+BJ_API int bj_result_copy_pages(const bj_result* r, uint64_t c, void* const* dst) {
+    if (!r || c >= r->npages.size() || (r->npages[c] && !dst)) return BJ_ERR_INVALID;
+    for (uint64_t p = 0; p < r->npages[c]; p++) {
+        if (!dst[p]) return BJ_ERR_INVALID;
+        if (r->host.p) {
+            std::memcpy(dst[p], r->host.p + (r->page_base[c] + p) * kPageSize, kPageSize);
+        } else if (r->dev) {
+            if (cudaMemcpy(dst[p], r->dev + (r->page_base[c] + p) * kPageSize, kPageSize, cudaMemcpyDeviceToHost) !=
+                cudaSuccess)
+                return BJ_ERR_CUDA;
+        } else {
+            return BJ_ERR_INVALID;
+        }
+    }
+    return BJ_OK;
+}
+BJ_API int bj_result_stats(const bj_result* r, bj_stats* out) {
+    if (!r || !out) return BJ_ERR_INVALID;
+    *out = r->stats;
+    return BJ_OK;
+}
+BJ_API void bj_result_free(bj_result* r) {
+    if (!r) return;
+    if (r->ctx) {
+        if (r->dev) {
+            cudaFreeAsync(r->dev, r->ctx->stream);
+            r->dev = nullptr;
+        }
+        if (r->host.p) r->ctx->give_pinned(r->host);
+        r->ctx->live_results--;
+    }
+    delete r;
+}
+
+} // extern "C"

@@ -1,0 +1,323 @@
+// K7: materialisation of result rows into contest pages.
+//
+// Replaces the reference's output writers (impl::WriterT, engine/op/
+// TableTarget.cpp:111-391, and the long-string page copy :243-250). The
+// reference fills pages greedily per worker thread; here every page is built
+// by one CTA in shared memory and stored with 16-byte writes:
+//  * fixed width: a page holds a fixed number of rows (the most that fit when
+//    none is NULL: 1984 for INT32, 1007 for INT64/FP64), so page p covers
+//    rows [p*R, p*R+R) and all pages are independent. A block scan of the
+//    validity flags places the non-null values densely, as the format wants.
+//  * VARCHAR: per-row lengths first; then a greedy packer walks blocks of 4096
+//    rows (one thread per block, same fill rule as the contest's converter,
+//    src/build_table.cpp:640-660) and emits page descriptors; a string longer
+//    than PAGE_SIZE-7 gets its own 0xffff/0xfffe page run. Finally one CTA
+//    per descriptor gathers the strings from the source pages.
+// Any packing that respects the format is a valid result: the harnesses
+// compare row multisets (tests/read_sql.cpp:1208-1213).
+#include "launch.h"
+
+namespace bj {
+namespace {
+
+constexpr uint32_t kMaxShort = kPageSize - 7;  // longest string stored inline
+constexpr uint32_t kLongChunk = kPageSize - 4; // bytes per long-string page
+
+__device__ __forceinline__ uint32_t block_excl_u32(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t ws[32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        int nw = blockDim.x >> 5;
+        uint32_t w = lane < nw ? ws[lane] : 0;
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t u = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += u;
+        }
+        ws[lane] = wi - w;
+        if (lane == nw - 1) *total = wi;
+    }
+    __syncthreads();
+    uint32_t r = ws[warp] + inc - v;
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ void zero_smem_page(uint8_t* page) {
+    uint4* p4 = reinterpret_cast<uint4*>(page);
+    for (uint32_t i = threadIdx.x; i < kPageSize / 16; i += blockDim.x) p4[i] = make_uint4(0, 0, 0, 0);
+}
+
+__device__ __forceinline__ void store_page(const uint8_t* page, uint8_t* dst) {
+    const uint4* s = reinterpret_cast<const uint4*>(page);
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    for (uint32_t i = threadIdx.x; i < kPageSize / 16; i += blockDim.x) d[i] = s[i];
+}
+
+// One CTA of 256 threads per page; each thread owns 8 consecutive rows.
+__global__ void __launch_bounds__(256) k_write_fixed(const uint64_t* __restrict__ vals,
+                                                     const uint8_t* __restrict__ valid, uint64_t n, int32_t type,
+                                                     uint32_t rpp, uint8_t* __restrict__ out) {
+    __shared__ __align__(16) uint8_t page[kPageSize];
+    __shared__ uint32_t total;
+    uint64_t r0 = uint64_t(blockIdx.x) * rpp;
+    uint32_t nr = uint32_t(n - r0 < rpp ? n - r0 : rpp);
+    zero_smem_page(page);
+    uint32_t t = threadIdx.x;
+    uint32_t lo = t * 8, hi = min(nr, lo + 8);
+    uint32_t bits = 0, cnt = 0;
+    for (uint32_t i = lo; i < hi; i++)
+        if (valid[r0 + i]) {
+            bits |= 1u << (i - lo);
+            cnt++;
+        }
+    uint32_t dense = block_excl_u32(cnt, &total);
+    uint32_t w = type == kInt32 ? 4 : 8;
+    uint8_t* data = page + (type == kInt32 ? 4 : 8);
+    for (uint32_t i = lo; i < hi; i++) {
+        if (!((bits >> (i - lo)) & 1)) continue;
+        uint64_t v = vals[r0 + i];
+        if (w == 4)
+            *reinterpret_cast<uint32_t*>(data + 4 * dense) = uint32_t(v);
+        else
+            *reinterpret_cast<uint64_t*>(data + 8 * dense) = v;
+        dense++;
+    }
+    uint32_t nbytes = (nr + 7) / 8;
+    if (lo < nr) page[kPageSize - nbytes + t] = uint8_t(bits);
+    if (t == 0) {
+        *reinterpret_cast<uint16_t*>(page) = uint16_t(nr);
+        *reinterpret_cast<uint16_t*>(page + 2) = uint16_t(total);
+    }
+    __syncthreads();
+    store_page(page, out + size_t(blockIdx.x) * kPageSize);
+}
+
+// Byte range of a short string (page p, value d) in its source page.
+__device__ __forceinline__ void short_string(const DevColumn& c, uint64_t h, const uint8_t*& bytes, uint32_t& len) {
+    uint32_t p = str_handle_page(h), d = str_handle_dense(h);
+    const uint8_t* pg = c.pages + size_t(p) * kPageSize;
+    uint32_t nn = ld16(pg + 2);
+    uint32_t end = ld16(pg + 4 + 2 * d);
+    uint32_t begin = d ? ld16(pg + 4 + 2 * (d - 1)) : 0;
+    bytes = pg + 4 + 2 * nn + begin;
+    len = end - begin;
+}
+
+__device__ __forceinline__ uint32_t long_string_length(const DevColumn& c, uint32_t p, uint32_t* err) {
+    uint32_t len = 0;
+    for (uint32_t q = p; q < c.npages; q++) {
+        const uint8_t* pg = c.pages + size_t(q) * kPageSize;
+        uint32_t n = ld16(pg);
+        if (q > p && n != 0xfffe) break;
+        if (q == p && n != 0xffff) {
+            record_error(err, kErrLongString);
+            return 0;
+        }
+        len += ld16(pg + 2);
+    }
+    return len;
+}
+
+__global__ void k_string_lengths(const uint64_t* __restrict__ handles, const uint8_t* __restrict__ valid, uint64_t n,
+                                 DevColumn c, uint32_t* __restrict__ lens, uint32_t* __restrict__ err) {
+    uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    if (!valid[i]) {
+        lens[i] = 0;
+        return;
+    }
+    uint64_t h = handles[i];
+    if (str_handle_page(h) >= c.npages) {
+        record_error(err, kErrRowRange);
+        lens[i] = 0;
+        return;
+    }
+    if (str_handle_dense(h) == 0xffff) {
+        lens[i] = long_string_length(c, str_handle_page(h), err);
+        return;
+    }
+    const uint8_t* b;
+    uint32_t len;
+    short_string(c, h, b, len);
+    lens[i] = len;
+}
+
+// One thread per block of kStrBlock rows: greedy page packing.
+__global__ void k_string_pack(const uint32_t* __restrict__ lens, const uint8_t* __restrict__ valid, uint64_t n,
+                              int pass, uint32_t* __restrict__ block_pages, const uint32_t* __restrict__ block_off,
+                              StrPageDesc* __restrict__ descs) {
+    uint64_t blk = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    uint64_t r0 = blk * kStrBlock;
+    if (r0 >= n) return;
+    uint64_t r1 = n < r0 + kStrBlock ? n : r0 + kStrBlock;
+    uint32_t pages = 0;
+    uint32_t out = pass ? block_off[blk] : 0;
+    uint32_t rows = 0, nv = 0, bytes = 0;
+    uint64_t first = r0;
+    auto close = [&](uint64_t next_first) {
+        if (rows) {
+            if (pass) descs[out + pages] = StrPageDesc{first, rows, 0xffffffffu};
+            pages++;
+        }
+        rows = nv = bytes = 0;
+        first = next_first;
+    };
+    for (uint64_t r = r0; r < r1; r++) {
+        bool v = valid[r];
+        uint32_t len = v ? lens[r] : 0;
+        if (v && len > kMaxShort) {
+            close(r);
+            uint32_t chunks = (len + kLongChunk - 1) / kLongChunk;
+            for (uint32_t c = 0; c < chunks; c++) {
+                if (pass) descs[out + pages] = StrPageDesc{r, 1, c};
+                pages++;
+            }
+            first = r + 1;
+            continue;
+        }
+        uint32_t need = v ? 4 + (nv + 1) * 2 + bytes + len + (rows / 8 + 1) : 4 + nv * 2 + bytes + (rows / 8 + 1);
+        if (need > kPageSize) close(r);
+        if (rows == 0) first = r;
+        rows++;
+        if (v) {
+            nv++;
+            bytes += len;
+        }
+    }
+    close(r1);
+    if (!pass) block_pages[blk] = pages;
+}
+
+__global__ void __launch_bounds__(256) k_write_string_pages(const uint64_t* __restrict__ handles,
+                                                            const uint8_t* __restrict__ valid,
+                                                            const uint32_t* __restrict__ lens, DevColumn c,
+                                                            const StrPageDesc* __restrict__ descs,
+                                                            uint8_t* __restrict__ out, uint32_t* __restrict__ err) {
+    __shared__ __align__(16) uint8_t page[kPageSize];
+    __shared__ uint32_t tot_valid, tot_bytes, carry_valid, carry_bytes;
+    StrPageDesc d = descs[blockIdx.x];
+    zero_smem_page(page);
+    __syncthreads();
+    if (d.chunk != 0xffffffffu) {
+        // Long-string page: chunk d.chunk of the string of row d.first_row.
+        uint64_t h = handles[d.first_row];
+        uint32_t len = lens[d.first_row];
+        uint32_t off = d.chunk * kLongChunk;
+        uint32_t cnt = min(kLongChunk, len - off);
+        if (threadIdx.x == 0) {
+            *reinterpret_cast<uint16_t*>(page) = d.chunk == 0 ? 0xffff : 0xfffe;
+            *reinterpret_cast<uint16_t*>(page + 2) = uint16_t(cnt);
+        }
+        if (str_handle_dense(h) == 0xffff) {
+            // Source is itself a long-string run: copy byte range [off, off+cnt).
+            uint32_t p = str_handle_page(h), pos = 0;
+            for (uint32_t q = p; q < c.npages && pos < off + cnt; q++) {
+                const uint8_t* pg = c.pages + size_t(q) * kPageSize;
+                uint32_t n = ld16(pg + 2);
+                uint32_t a = max(pos, off), b = min(pos + n, off + cnt);
+                for (uint32_t k = a + threadIdx.x; k < b; k += blockDim.x) page[4 + (k - off)] = pg[4 + (k - pos)];
+                pos += n;
+            }
+        } else {
+            record_error(err, kErrLongString);
+        }
+        __syncthreads();
+        store_page(page, out + size_t(blockIdx.x) * kPageSize);
+        return;
+    }
+    // Normal page: first pass counts valid rows (offset array size), second places data.
+    if (threadIdx.x == 0) carry_valid = carry_bytes = 0;
+    __syncthreads();
+    uint32_t nv_total = 0;
+    for (uint32_t base = 0; base < d.nrows; base += blockDim.x) {
+        uint32_t i = base + threadIdx.x;
+        uint32_t v = i < d.nrows ? valid[d.first_row + i] : 0;
+        block_excl_u32(v, &tot_valid);
+        nv_total += tot_valid;
+    }
+    uint8_t* chars = page + 4 + 2 * nv_total;
+    uint32_t nbytes = (d.nrows + 7) / 8;
+    uint8_t* bm = page + kPageSize - nbytes;
+    for (uint32_t base = 0; base < d.nrows; base += blockDim.x) {
+        uint32_t i = base + threadIdx.x;
+        bool v = i < d.nrows && valid[d.first_row + i];
+        uint32_t len = v ? lens[d.first_row + i] : 0;
+        uint32_t dv = block_excl_u32(v ? 1u : 0u, &tot_valid);
+        uint32_t db = block_excl_u32(len, &tot_bytes);
+        dv += carry_valid;
+        db += carry_bytes;
+        if (v) {
+            const uint8_t* src;
+            uint32_t slen;
+            short_string(c, handles[d.first_row + i], src, slen);
+            for (uint32_t k = 0; k < len; k++) chars[db + k] = src[k];
+            *reinterpret_cast<uint16_t*>(page + 4 + 2 * dv) = uint16_t(db + len);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            carry_valid += tot_valid;
+            carry_bytes += tot_bytes;
+        }
+        __syncthreads();
+    }
+    // Bitmap: one thread per byte.
+    for (uint32_t byte = threadIdx.x; byte < nbytes; byte += blockDim.x) {
+        uint32_t b = 0;
+        for (uint32_t k = 0; k < 8; k++) {
+            uint32_t i = byte * 8 + k;
+            if (i < d.nrows && valid[d.first_row + i]) b |= 1u << k;
+        }
+        bm[byte] = uint8_t(b);
+    }
+    if (threadIdx.x == 0) {
+        *reinterpret_cast<uint16_t*>(page) = uint16_t(d.nrows);
+        *reinterpret_cast<uint16_t*>(page + 2) = uint16_t(nv_total);
+    }
+    __syncthreads();
+    store_page(page, out + size_t(blockIdx.x) * kPageSize);
+}
+
+} // namespace
+
+int write_fixed_pages(const uint64_t* vals, const uint8_t* valid, uint64_t n, int32_t type, uint32_t rpp,
+                      uint8_t* out_pages, cudaStream_t st) {
+    uint64_t npages = (n + rpp - 1) / rpp;
+    if (!npages) return 0;
+    k_write_fixed<<<unsigned(npages), 256, 0, st>>>(vals, valid, n, type, rpp, out_pages);
+    return 1;
+}
+
+int string_lengths(const uint64_t* handles, const uint8_t* valid, uint64_t n, StrSource src, uint32_t* lens,
+                   uint32_t* err, cudaStream_t st) {
+    if (!n) return 0;
+    k_string_lengths<<<unsigned((n + 255) / 256), 256, 0, st>>>(handles, valid, n, src.col, lens, err);
+    return 1;
+}
+
+int string_pack(const uint32_t* lens, const uint8_t* valid, uint64_t n, int pass, uint32_t* block_pages,
+                const uint32_t* block_page_off, StrPageDesc* descs, cudaStream_t st) {
+    uint64_t blocks = (n + kStrBlock - 1) / kStrBlock;
+    if (!blocks) return 0;
+    k_string_pack<<<unsigned((blocks + 63) / 64), 64, 0, st>>>(lens, valid, n, pass, block_pages, block_page_off,
+                                                               descs);
+    return 1;
+}
+
+int write_string_pages(const uint64_t* handles, const uint8_t* valid, const uint32_t* lens, StrSource src,
+                       const StrPageDesc* descs, uint32_t npages, uint8_t* out_pages, uint32_t* err, cudaStream_t st) {
+    if (!npages) return 0;
+    k_write_string_pages<<<npages, 256, 0, st>>>(handles, valid, lens, src.col, descs, out_pages, err);
+    return 1;
+}
+
+} // namespace bj

@@ -1,0 +1,165 @@
+// K1: page index of a resident column.
+//
+// Replaces the reference's per-query column preparation
+// (TableScan::prepareColumn / makeSearchVector, engine/op/TableScan.cpp:546-582:
+// an exclusive prefix of rows per page used by the readers' exponential page
+// search) and the popcount-to-dense-index step of its readers
+// (TableScan.cpp:113-238, 287-292). Pass 1 reads every page header (one
+// thread per page), validates it against the page format and writes the
+// page's contained rows and 64-row chunk count; two scans turn those into
+// row_start / chunk_base. Pass 2 writes the dense-value base of every chunk
+// and the page of every 1024-row block.
+#include "launch.h"
+
+namespace bj {
+namespace {
+
+__global__ void k_page_headers(const uint8_t* __restrict__ pages, uint32_t npages, int32_t type,
+                               uint32_t* __restrict__ rows, uint32_t* __restrict__ chunks,
+                               uint32_t* __restrict__ flags, uint32_t* __restrict__ err) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npages) return;
+    const uint8_t* pg = pages + size_t(p) * kPageSize;
+    uint32_t n = ld16(pg), nn = ld16(pg + 2);
+    uint32_t r = n, c = (n + 63) >> 6;
+    uint32_t f = 0;
+    if (type == kVarchar && n >= 0xfffe) {
+        // Long-string page: 1 row for the first page of the run, 0 for the rest.
+        r = n == 0xffff ? 1 : 0;
+        c = 0;
+        f |= 2;
+        if (nn > kPageSize - 4) record_error(err, kErrLongString);
+        if (n == 0xfffe && (p == 0 || ld16(pg - kPageSize) < 0xfffe)) record_error(err, kErrLongString);
+    } else {
+        // Every later read of this page (values by dense index, string offsets)
+        // stays inside it once these hold: bitmap and header fit, the bitmap's
+        // population equals the non-null count, values / offsets / bytes fit.
+        uint32_t nbytes = (n + 7) >> 3;
+        bool ok = nn <= n && 4 + nbytes <= kPageSize;
+        if (ok && nn != n) {
+            f |= 1;
+            const uint8_t* bm = pg + kPageSize - nbytes;
+            uint32_t pop = 0;
+            for (uint32_t b = 0; b < nbytes; b++) {
+                uint32_t byte = bm[b];
+                if (b == nbytes - 1 && (n & 7)) byte &= (1u << (n & 7)) - 1;
+                pop += __popc(byte);
+            }
+            ok = pop == nn;
+        }
+        if (ok && type == kVarchar) {
+            ok = 4 + 2 * nn + nbytes <= kPageSize;
+            uint32_t prev = 0;
+            for (uint32_t k = 0; ok && k < nn; k++) {
+                uint32_t e = ld16(pg + 4 + 2 * k);
+                ok = e >= prev;
+                prev = e;
+            }
+            ok = ok && 4 + 2 * nn + prev + nbytes <= kPageSize;
+        } else if (ok) {
+            uint32_t w = type == kInt32 ? 4 : 8;
+            uint32_t begin = type == kInt32 ? 4 : 8;
+            ok = begin + nn * w + nbytes <= kPageSize;
+        }
+        if (!ok) {
+            record_error(err, kErrPageHeader);
+            r = 0;
+            c = 0;
+        }
+    }
+    rows[p] = r;
+    chunks[p] = c;
+    if (f) atomicOr(flags, f);
+}
+
+// One warp per page: dense base of each 64-row chunk (a running popcount of
+// the page's null bitmap).
+__global__ void k_page_dense(const uint8_t* __restrict__ pages, uint32_t npages,
+                             const uint32_t* __restrict__ chunk_base, uint32_t* __restrict__ dense_base) {
+    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t lane = threadIdx.x & 31;
+    if (warp >= npages) return;
+    uint32_t p = warp;
+    uint32_t c0 = chunk_base[p], nc = chunk_base[p + 1] - c0;
+    if (!nc) return;
+    const uint8_t* pg = pages + size_t(p) * kPageSize;
+    uint32_t n = ld16(pg), nn = ld16(pg + 2);
+    uint32_t nbytes = (n + 7) >> 3;
+    const uint8_t* bm = pg + kPageSize - nbytes;
+    uint32_t carry = 0;
+    for (uint32_t k0 = 0; k0 < nc; k0 += 32) {
+        uint32_t k = k0 + lane;
+        uint32_t cnt = 0;
+        if (k < nc) {
+            if (nn == n) {
+                cnt = min(64u, n - k * 64);
+            } else {
+                uint64_t w = load_bits64(bm, k, nbytes);
+                uint32_t valid_bits = min(64u, n - k * 64);
+                if (valid_bits < 64) w &= (1ull << valid_bits) - 1;
+                cnt = __popcll(w);
+            }
+        }
+        // exclusive warp scan of cnt
+        uint32_t inc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= uint32_t(o)) inc += u;
+        }
+        if (k < nc) dense_base[c0 + k] = carry + inc - cnt;
+        carry += __shfl_sync(0xffffffffu, inc, 31);
+    }
+}
+
+// Page containing row b * 1024, for every block b (and the terminal entry).
+__global__ void k_page_of_blk(const uint32_t* __restrict__ row_start, uint32_t npages, uint32_t nrows,
+                              uint32_t nblk, uint32_t* __restrict__ page_of_blk) {
+    uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblk) return;
+    uint64_t row = uint64_t(b) << kBlkShift;
+    uint32_t res;
+    if (row >= nrows) {
+        res = npages ? npages - 1 : 0;
+    } else {
+        uint32_t lo = 0, hi = npages - 1;
+        while (lo < hi) {
+            uint32_t mid = (lo + hi + 1) >> 1;
+            if (row_start[mid] <= row)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        res = lo;
+    }
+    page_of_blk[b] = res;
+}
+
+} // namespace
+
+int page_index_pass1(const uint8_t* pages, uint32_t npages, int32_t type, PageIndexBufs b, uint32_t* err, Scratch& s,
+                     cudaStream_t st) {
+    int launches = 0;
+    cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), st);
+    if (npages) {
+        k_page_headers<<<(npages + 255) / 256, 256, 0, st>>>(pages, npages, type, b.rows, b.chunks, b.flags, err);
+        launches++;
+    }
+    launches += scan_exclusive_u32(b.rows, b.row_start, npages, s, st);
+    launches += scan_exclusive_u32(b.chunks, b.chunk_base, npages, s, st);
+    return launches;
+}
+
+int page_index_pass2(const uint8_t* pages, uint32_t npages, uint32_t nrows, const uint32_t* row_start,
+                     const uint32_t* chunk_base, uint32_t* dense_base, uint32_t* page_of_blk, cudaStream_t st) {
+    int launches = 0;
+    if (npages) {
+        k_page_dense<<<(npages * 32 + 255) / 256, 256, 0, st>>>(pages, npages, chunk_base, dense_base);
+        launches++;
+    }
+    uint32_t nblk = (nrows >> kBlkShift) + 2;
+    k_page_of_blk<<<(nblk + 255) / 256, 256, 0, st>>>(row_start, npages, nrows, nblk, page_of_blk);
+    return launches + 1;
+}
+
+} // namespace bj

@@ -1,0 +1,209 @@
+// Pipeline kernels: probe stages, build-side tuple emit, output emit.
+//
+// Replaces the fused push pipeline of the reference
+// (engine/pipeline/JoinPipeline.hpp:46-203: scan -> probe_0 -> probe_1 ->
+// target, multiplicity = product of the matched tuples' multiplicities,
+// :111-131) with stage kernels over item lists. An item is a row of the
+// scanned input plus the hash-table entry matched by every probe so far.
+// Each stage runs twice over the same tiles of 2048 items: once counting
+// matches per tile, once writing at the tile's offset (an exclusive scan of
+// the counts in between), so the output order is deterministic and no
+// capacity has to be guessed.
+//
+// The probe itself follows HashtableProbe::operator() (engine/op/Hashtable.hpp:
+// 228-241): hash the 32-bit key, find its bucket, compare every key in the
+// bucket. Buckets here are contiguous runs of entries (CSR), not chains.
+#include "launch.h"
+
+namespace bj {
+namespace {
+
+struct ProbeSet {
+    HTView ht[kMaxProbes];
+};
+
+__device__ __forceinline__ uint32_t item_row(const Items& in, uint32_t i) { return in.rows ? in.rows[i] : i; }
+__device__ __forceinline__ uint64_t item_mult(const Items& in, uint32_t i) { return in.mult ? in.mult[i] : 1ull; }
+
+// Entries of `ht` whose key equals `key`: calls fn(entry) for each.
+template <typename Fn>
+__device__ __forceinline__ uint32_t for_matches(const HTView& ht, uint32_t key, bool use_bloom, Fn&& fn) {
+    if (use_bloom && ht.bloom && !bloom_may_contain(ht.bloom, ht.bloom_log2, key)) return 0;
+    uint64_t h = key_hash(key);
+    uint32_t b = uint32_t(h >> ht.shift);
+    uint32_t s = ht.bucket_off[b], e = ht.bucket_off[b + 1];
+    uint32_t n = 0;
+    for (uint32_t j = s; j < e; j++) {
+        if (ht.keys[j] == key) {
+            fn(j);
+            n++;
+        }
+    }
+    return n;
+}
+
+template <typename T>
+__device__ __forceinline__ T block_exclusive_sum(T v, T* total) {
+    __shared__ T warp_sums[32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) warp_sums[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        int nw = blockDim.x >> 5;
+        T w = lane < nw ? warp_sums[lane] : T(0);
+        T wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T u = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += u;
+        }
+        warp_sums[lane] = wi - w;
+        if (lane == nw - 1) *total = wi;
+    }
+    __syncthreads();
+    T r = warp_sums[warp] + inc - v;
+    __syncthreads();
+    return r;
+}
+
+template <int kMode>
+__global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HTView ht, uint32_t* tile_counts,
+                                                     const uint32_t* tile_offsets, ItemsOut out, int use_bloom,
+                                                     uint32_t* err) {
+    uint32_t t0 = blockIdx.x * kTile;
+    uint32_t t1 = min(in.count, t0 + kTile);
+    uint32_t mine = 0;
+    for (uint32_t i = t0 + threadIdx.x; i < t1; i += blockDim.x) {
+        uint32_t row = item_row(in, i);
+        if (row >= key.nrows) {
+            record_error(err, kErrRowRange);
+            continue;
+        }
+        uint64_t v;
+        if (!col_get(key, row, v)) continue;
+        mine += for_matches(ht, uint32_t(v), use_bloom != 0, [](uint32_t) {});
+    }
+    __shared__ uint32_t total;
+    uint32_t base = block_exclusive_sum<uint32_t>(mine, &total);
+    if (kMode == 0) {
+        if (threadIdx.x == 0) tile_counts[blockIdx.x] = total;
+        return;
+    }
+    uint32_t o = tile_offsets[blockIdx.x] + base;
+    for (uint32_t i = t0 + threadIdx.x; i < t1; i += blockDim.x) {
+        uint32_t row = item_row(in, i);
+        if (row >= key.nrows) continue;
+        uint64_t v;
+        if (!col_get(key, row, v)) continue;
+        uint64_t m = item_mult(in, i);
+        for_matches(ht, uint32_t(v), use_bloom != 0, [&](uint32_t e) {
+            out.rows[o] = row;
+            for (int p = 0; p < in.nprobes; p++) out.ents[p][o] = in.ents[p][i];
+            out.ents[in.nprobes][o] = e;
+            out.mult[o] = m * ht.mult[e];
+            o++;
+        });
+    }
+}
+
+// Value of one slot for item i (row `row`): returns false for NULL.
+__device__ __forceinline__ bool slot_value(const SlotSource& s, const Items& in, uint32_t i, uint32_t row,
+                                           const ProbeSet& ps, uint64_t& v) {
+    if (s.kind == 0) return col_get(s.col, row, v);
+    uint32_t e = in.ents[s.probe][i];
+    const HTView& ht = ps.ht[s.probe];
+    if ((ht.pnull[e] >> s.slot) & 1) return false;
+    v = ht.pay[size_t(e) * ht.width + s.slot];
+    return true;
+}
+
+__global__ void __launch_bounds__(256) k_emit_tuples(Items in, DevColumn key, SlotSources src, ProbeSet ps,
+                                                     TupleBuf out, uint32_t* err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= in.count) return;
+    uint32_t row = item_row(in, i);
+    uint64_t kv = 0;
+    bool key_ok = row < key.nrows && col_get(key, row, kv);
+    if (row >= key.nrows) record_error(err, kErrRowRange);
+    out.keys[i] = uint32_t(kv);
+    out.mult[i] = key_ok ? item_mult(in, i) : 0ull;
+    uint32_t nulls = 0;
+    for (int j = 0; j < src.n; j++) {
+        uint64_t v = 0;
+        if (!slot_value(src.s[j], in, i, row, ps, v)) {
+            nulls |= 1u << j;
+            v = 0;
+        }
+        out.pay[size_t(i) * out.width + j] = v;
+    }
+    out.pnull[i] = nulls;
+}
+
+__global__ void k_items_mult(Items in, uint64_t* mult_out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < in.count) mult_out[i] = item_mult(in, i);
+}
+
+__global__ void __launch_bounds__(256) k_emit_output(Items in, const uint64_t* out_off, SlotSources src, ProbeSet ps,
+                                                     FlatOut out, uint32_t* err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= in.count) return;
+    uint32_t row = item_row(in, i);
+    uint64_t o0 = out_off[i], o1 = out_off[i + 1];
+    for (int j = 0; j < src.n; j++) {
+        uint64_t v = 0;
+        bool ok = slot_value(src.s[j], in, i, row, ps, v);
+        for (uint64_t o = o0; o < o1; o++) {
+            out.vals[j][o] = ok ? v : 0;
+            out.valid[j][o] = ok;
+        }
+    }
+}
+
+ProbeSet make_probe_set(const HTView* probes, int n) {
+    ProbeSet ps{};
+    for (int i = 0; i < n && i < kMaxProbes; i++) ps.ht[i] = probes[i];
+    return ps;
+}
+
+} // namespace
+
+int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mode, uint32_t* tile_counts,
+                const uint32_t* tile_offsets, ItemsOut out, bool use_bloom, uint32_t* err, cudaStream_t st) {
+    uint32_t tiles = (in.count + kTile - 1) / kTile;
+    if (!tiles) return 0;
+    if (mode == 0)
+        k_probe_stage<0><<<tiles, 256, 0, st>>>(in, key, ht, tile_counts, tile_offsets, out, use_bloom, err);
+    else
+        k_probe_stage<1><<<tiles, 256, 0, st>>>(in, key, ht, tile_counts, tile_offsets, out, use_bloom, err);
+    return 1;
+}
+
+int emit_tuples(const Items& in, const DevColumn& key, const SlotSources& src, const HTView* probes, TupleBuf out,
+                uint32_t* err, cudaStream_t st) {
+    if (!in.count) return 0;
+    k_emit_tuples<<<(in.count + 255) / 256, 256, 0, st>>>(in, key, src, make_probe_set(probes, in.nprobes), out, err);
+    return 1;
+}
+
+int items_mult(const Items& in, uint64_t* mult_out, cudaStream_t st) {
+    if (!in.count) return 0;
+    k_items_mult<<<(in.count + 255) / 256, 256, 0, st>>>(in, mult_out);
+    return 1;
+}
+
+int emit_output(const Items& in, const uint64_t* out_off, const SlotSources& src, const HTView* probes, FlatOut out,
+                uint32_t* err, cudaStream_t st) {
+    if (!in.count) return 0;
+    k_emit_output<<<(in.count + 255) / 256, 256, 0, st>>>(in, out_off, src, make_probe_set(probes, in.nprobes), out,
+                                                          err);
+    return 1;
+}
+
+} // namespace bj

@@ -1,0 +1,150 @@
+// Host-side launch wrappers for the engine's kernels. Each wrapper enqueues
+// its kernels on `st` and returns how many kernels it launched, so the host
+// can account for every launch (bj_stats.kernel_launches).
+#pragma once
+
+#include "device.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace bj {
+
+// Scratch allocator handed to wrappers that need temporary device memory.
+struct Scratch {
+    virtual void* alloc(size_t bytes) = 0;
+    virtual ~Scratch() = default;
+};
+
+// ---- prefix sums (k_util.cu) ----
+// Exclusive scan of n values into out[0..n]; out[n] receives the total.
+int scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, Scratch& s, cudaStream_t st);
+int scan_exclusive_u64(const uint64_t* in, uint64_t* out, size_t n, Scratch& s, cudaStream_t st);
+int fill_u32(uint32_t* p, uint32_t v, size_t n, cudaStream_t st);
+
+// ---- page index (k_pages.cu) ----
+// Builds row_start / chunk_base / dense_base / page_of_blk for a column whose
+// pages are resident at c.pages; checks every page header. Writes the column's
+// row total to *rows_out (device) and flags to *flags_out (device).
+struct PageIndexBufs {
+    uint32_t* rows;          // npages (scratch)
+    uint32_t* chunks;        // npages (scratch)
+    uint32_t* row_start;     // npages + 1
+    uint32_t* chunk_base;    // npages + 1
+    uint32_t* flags;         // 1 word
+};
+int page_index_pass1(const uint8_t* pages, uint32_t npages, int32_t type, PageIndexBufs b, uint32_t* err,
+                     Scratch& s, cudaStream_t st);
+// After pass 1 the host knows the chunk total and row total.
+int page_index_pass2(const uint8_t* pages, uint32_t npages, uint32_t nrows, const uint32_t* row_start,
+                     const uint32_t* chunk_base, uint32_t* dense_base, uint32_t* page_of_blk, cudaStream_t st);
+
+// ---- pipelines (k_probe.cu) ----
+// Items flowing through a pipeline: a row of the scanned input plus, per
+// probe done so far, the index of the matching hash-table entry, and the
+// product of the matched entries' multiplicities.
+struct Items {
+    const uint32_t* rows;                // null: implicit rows 0..count-1
+    const uint32_t* ents[kMaxProbes];
+    const uint64_t* mult;                // null: all 1
+    uint32_t count;
+    int nprobes;
+};
+struct ItemsOut {
+    uint32_t* rows;
+    uint32_t* ents[kMaxProbes];
+    uint64_t* mult;
+};
+constexpr uint32_t kTile = 2048;  // items per CTA tile in stage kernels
+
+// Probe stage: for each item, read the key `key` at its row, probe `ht`,
+// and emit one item per matching entry. mode 0 counts matches per tile into
+// tile_counts; mode 1 writes items at tile_offsets (exclusive scan of counts).
+int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mode, uint32_t* tile_counts,
+                const uint32_t* tile_offsets, ItemsOut out, bool use_bloom, uint32_t* err, cudaStream_t st);
+
+// Source of one value slot: a column of the scanned input read at the item's
+// row, or payload slot `slot` of the entry matched by probe `probe`.
+struct SlotSource {
+    int32_t kind;  // 0: column, 1: probe payload
+    int32_t probe;
+    int32_t slot;
+    int32_t pad;
+    DevColumn col;
+};
+constexpr int kMaxOut = 32;
+struct SlotSources {
+    SlotSource s[kMaxOut];
+    int n;
+};
+
+// Build-side emit: one tuple per item: key from `key` (NULL key -> mult 0),
+// payload from `src`, mult from the item.
+struct TupleBuf {
+    uint32_t* keys;
+    uint64_t* mult;
+    uint64_t* pay;     // count * width
+    uint32_t* pnull;
+    uint32_t count;
+    uint32_t width;
+};
+int emit_tuples(const Items& in, const DevColumn& key, const SlotSources& src, const HTView* probes, TupleBuf out,
+                uint32_t* err, cudaStream_t st);
+
+// Output emit: item multiplicities are expanded; out_off[i] = first output row
+// of item i (exclusive scan of multiplicities). Values go to flat columns.
+struct FlatOut {
+    uint64_t* vals[kMaxOut];
+    uint8_t* valid[kMaxOut];
+    int n;
+};
+int emit_output(const Items& in, const uint64_t* out_off, const SlotSources& src, const HTView* probes, FlatOut out,
+                uint32_t* err, cudaStream_t st);
+// mult of implicit/explicit items as a u64 array (for the scan of output offsets)
+int items_mult(const Items& in, uint64_t* mult_out, cudaStream_t st);
+
+// ---- hash table build (k_build.cu) ----
+struct BuildResult {
+    uint32_t nentries;
+    uint32_t nbuckets_log2;
+};
+// Eager aggregation: representative flags (1 for the first copy of each
+// distinct tuple with mult > 0; duplicates add their mult to it).
+int aggregate_tuples(TupleBuf t, uint32_t* slot_table, uint32_t table_log2, uint32_t* is_rep, uint32_t* err,
+                     cudaStream_t st);
+// Scatter representatives into buckets (CSR). rep_pos = exclusive scan of is_rep.
+int bucket_count(TupleBuf t, const uint32_t* is_rep, uint32_t shift, uint32_t* counts, cudaStream_t st);
+int bucket_scatter(TupleBuf t, const uint32_t* is_rep, uint32_t shift, const uint32_t* bucket_off, uint32_t* cursor,
+                   HTView ht_mut, uint32_t* err, cudaStream_t st);
+int bloom_build(const uint32_t* keys, uint32_t n, uint32_t* bloom, uint32_t log2w, cudaStream_t st);
+// Flags of a built table: [0] = 1 if some key repeats, [1] = 1 if some mult > 1.
+int ht_flags(HTView ht, uint32_t* flags, cudaStream_t st);
+// Counts, for n sampled rows of `key` (evenly spaced), how many hit `ht`.
+int sample_probe(const DevColumn& key, uint32_t nsample, HTView ht, uint32_t* hits, cudaStream_t st);
+
+// ---- output pages (k_output.cu) ----
+// Fixed-width page writer: rows_per_page rows per page.
+int write_fixed_pages(const uint64_t* vals, const uint8_t* valid, uint64_t n, int32_t type, uint32_t rows_per_page,
+                      uint8_t* out_pages, cudaStream_t st);
+// VARCHAR: per-row byte lengths (NULL -> 0, long strings flagged).
+struct StrSource {
+    DevColumn col;  // the source column the handles point into
+};
+int string_lengths(const uint64_t* handles, const uint8_t* valid, uint64_t n, StrSource src, uint32_t* lens,
+                   uint32_t* err, cudaStream_t st);
+// Greedy page packing per block of kStrBlock rows: pass 0 counts pages per
+// block, pass 1 writes page descriptors at block_page_off.
+constexpr uint32_t kStrBlock = 4096;
+struct StrPageDesc {
+    uint64_t first_row;
+    uint32_t nrows;     // rows on the page (1 for a long-string page)
+    uint32_t chunk;     // long string: chunk index, else 0xffffffff
+};
+int string_pack(const uint32_t* lens, const uint8_t* valid, uint64_t n, int pass, uint32_t* block_pages,
+                const uint32_t* block_page_off, StrPageDesc* descs, cudaStream_t st);
+int write_string_pages(const uint64_t* handles, const uint8_t* valid, const uint32_t* lens, StrSource src,
+                       const StrPageDesc* descs, uint32_t npages, uint8_t* out_pages, uint32_t* err, cudaStream_t st);
+
+} // namespace bj

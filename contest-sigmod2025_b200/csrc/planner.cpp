@@ -1,0 +1,241 @@
+// Host planner (see planner.h).
+#include "planner.h"
+
+#include <algorithm>
+#include <functional>
+#include <numeric>
+#include <queue>
+
+namespace bj {
+namespace {
+
+struct UnionFind {
+    std::vector<uint32_t> p;
+    uint32_t add() {
+        p.push_back(uint32_t(p.size()));
+        return p.back();
+    }
+    uint32_t find(uint32_t x) {
+        while (p[x] != x) x = p[x] = p[p[x]];
+        return x;
+    }
+    void merge(uint32_t a, uint32_t b) { p[find(a)] = find(b); }
+};
+
+struct Edge {
+    uint32_t a, b;            // inputs
+    uint32_t attr_a, attr_b;  // attrs of a and b
+};
+
+struct Importer {
+    const bj_plan& plan;
+    ExecPlan& ex;
+    UnionFind uf;
+    std::vector<Edge> edges;
+    std::string err;
+    int status = BJ_OK;
+
+    bool fail(int st, std::string msg) {
+        if (status == BJ_OK) {
+            status = st;
+            err = std::move(msg);
+        }
+        return false;
+    }
+
+    // Output attribute list of a node, as global attr ids
+    // (engine/query/PlanImport.cpp:24-57 walks the tree the same way).
+    bool rec(uint64_t id, std::vector<uint32_t>& out, int depth) {
+        if (id >= plan.num_nodes) return fail(BJ_ERR_INVALID, "plan node index out of range");
+        if (depth > 1024) return fail(BJ_ERR_INVALID, "plan is too deep or cyclic");
+        const bj_node& n = plan.nodes[id];
+        if (n.num_output_attrs && !n.output_attrs) return fail(BJ_ERR_INVALID, "missing output attributes");
+        if (n.kind == BJ_NODE_SCAN) {
+            if (n.base_table_id >= plan.num_inputs) return fail(BJ_ERR_INVALID, "scan of a missing input table");
+            const bj_table& t = plan.inputs[n.base_table_id];
+            if (t.num_rows >= (1ull << 32) - 2) return fail(BJ_ERR_UNSUPPORTED, "tables are limited to 2^32-2 rows");
+            uint32_t in = uint32_t(ex.inputs.size());
+            ex.inputs.push_back(PlanInput{uint32_t(n.base_table_id), t.num_rows, {}});
+            for (uint64_t a = 0; a < n.num_output_attrs; a++) {
+                const bj_attr& at = n.output_attrs[a];
+                if (at.type < BJ_INT32 || at.type > BJ_VARCHAR) return fail(BJ_ERR_INVALID, "unknown attribute type");
+                if (t.num_rows) {
+                    if (at.index >= t.num_columns) return fail(BJ_ERR_INVALID, "scan attribute beyond the table's columns");
+                    if (t.columns[at.index].type != at.type)
+                        return fail(BJ_ERR_INVALID, "scan attribute type differs from the column type");
+                }
+                uint32_t gid = uint32_t(ex.attrs.size());
+                ex.attrs.push_back(PlanAttr{in, uint32_t(at.index), at.type, uf.add()});
+                ex.inputs[in].attrs.push_back(gid);
+                out.push_back(gid);
+            }
+            return true;
+        }
+        if (n.kind != BJ_NODE_JOIN) return fail(BJ_ERR_INVALID, "unknown plan node kind");
+        std::vector<uint32_t> l, r;
+        if (!rec(n.left, l, depth + 1) || !rec(n.right, r, depth + 1)) return false;
+        if (n.left_attr >= l.size() || n.right_attr >= r.size()) return fail(BJ_ERR_INVALID, "join attribute out of range");
+        uint32_t la = l[n.left_attr], ra = r[n.right_attr];
+        // Join keys are 32-bit integers in the reference (engine/op/TableScan.cpp:328,
+        // engine/op/Hashtable.hpp:35-39); it would misread any other type.
+        if (ex.attrs[la].type != BJ_INT32 || ex.attrs[ra].type != BJ_INT32)
+            return fail(BJ_ERR_UNSUPPORTED, "join keys must be INT32");
+        uf.merge(la, ra);
+        edges.push_back(Edge{ex.attrs[la].input, ex.attrs[ra].input, la, ra});
+        for (uint64_t a = 0; a < n.num_output_attrs; a++) {
+            uint64_t idx = n.output_attrs[a].index;
+            if (idx >= l.size() + r.size()) return fail(BJ_ERR_INVALID, "join output attribute out of range");
+            uint32_t g = idx < l.size() ? l[idx] : r[idx - l.size()];
+            if (ex.attrs[g].type != n.output_attrs[a].type)
+                return fail(BJ_ERR_INVALID, "join output attribute type mismatch");
+            out.push_back(g);
+        }
+        return true;
+    }
+};
+
+} // namespace
+
+int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err) {
+    ex = ExecPlan{};
+    if (plan.num_nodes == 0 || !plan.nodes) {
+        err = "empty plan";
+        return BJ_ERR_INVALID;
+    }
+    if (plan.num_inputs && !plan.inputs) {
+        err = "missing input tables";
+        return BJ_ERR_INVALID;
+    }
+    Importer im{plan, ex, {}, {}, {}, BJ_OK};
+    std::vector<uint32_t> root_attrs;
+    if (!im.rec(plan.root, root_attrs, 0)) {
+        err = im.err;
+        return im.status;
+    }
+    // Equivalence classes.
+    for (auto& a : ex.attrs) a.eq = im.uf.find(a.eq);
+    const uint32_t ni = uint32_t(ex.inputs.size());
+    for (uint32_t i = 0; i < ni; i++)
+        if (ex.inputs[i].rows == 0) ex.empty = true;
+    ex.out_types.clear();
+    for (uint32_t a : root_attrs) ex.out_types.push_back(ex.attrs[a].type);
+    if (ex.empty) return BJ_OK;
+
+    // Root the join tree at the largest input.
+    uint32_t driver = 0;
+    for (uint32_t i = 1; i < ni; i++)
+        if (ex.inputs[i].rows > ex.inputs[driver].rows) driver = i;
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> adj(ni);  // (neighbour, edge)
+    for (uint32_t e = 0; e < im.edges.size(); e++) {
+        adj[im.edges[e].a].push_back({im.edges[e].b, e});
+        adj[im.edges[e].b].push_back({im.edges[e].a, e});
+    }
+    std::vector<int64_t> parent(ni, -1), parent_edge(ni, -1), depth(ni, -1);
+    std::vector<uint32_t> order;
+    std::queue<uint32_t> q;
+    q.push(driver);
+    depth[driver] = 0;
+    while (!q.empty()) {
+        uint32_t x = q.front();
+        q.pop();
+        order.push_back(x);
+        for (auto [y, e] : adj[x]) {
+            if (depth[y] >= 0) continue;
+            depth[y] = depth[x] + 1;
+            parent[y] = x;
+            parent_edge[y] = e;
+            q.push(y);
+        }
+    }
+    if (order.size() != ni) {
+        err = "plan's joins do not connect all scans";
+        return BJ_ERR_INVALID;
+    }
+    // Subtree membership: input -> root-ward chain.
+    auto in_subtree = [&](uint32_t node, uint32_t top) {
+        for (int64_t x = node; x >= 0; x = parent[x])
+            if (uint32_t(x) == top) return true;
+        return false;
+    };
+    // Output sources: for each result column, the member of its class whose
+    // input is nearest the driver (all members are equal on result rows).
+    std::vector<uint32_t> out_src;
+    for (uint32_t a : root_attrs) {
+        uint32_t eq = ex.attrs[a].eq, best = a;
+        for (uint32_t g = 0; g < ex.attrs.size(); g++) {
+            if (ex.attrs[g].eq != eq || ex.attrs[g].type != ex.attrs[a].type) continue;
+            if (depth[ex.attrs[g].input] < depth[ex.attrs[best].input] ||
+                (depth[ex.attrs[g].input] == depth[ex.attrs[best].input] && g < best))
+                best = g;
+        }
+        out_src.push_back(best);
+    }
+    std::vector<uint32_t> distinct_src = out_src;
+    std::sort(distinct_src.begin(), distinct_src.end());
+    distinct_src.erase(std::unique(distinct_src.begin(), distinct_src.end()), distinct_src.end());
+
+    // Pipelines in reverse BFS order: children before parents, driver last.
+    std::vector<int64_t> pipe_of(ni, -1);
+    for (auto it = order.rbegin(); it != order.rend(); ++it) {
+        uint32_t x = *it;
+        PipelinePlan pp;
+        pp.input = x;
+        if (parent[x] >= 0) {
+            const Edge& e = im.edges[parent_edge[x]];
+            pp.build_key = e.a == x ? e.attr_a : e.attr_b;
+        }
+        for (auto [y, ei] : adj[x]) {
+            if (parent[y] != int64_t(x) || parent_edge[y] != int64_t(ei)) continue;
+            const Edge& e = im.edges[ei];
+            pp.probes.push_back({uint32_t(pipe_of[y]), e.a == x ? e.attr_a : e.attr_b});
+        }
+        for (uint32_t s : distinct_src) {
+            uint32_t si = ex.attrs[s].input;
+            if (!in_subtree(si, x)) continue;
+            if (si == x) {
+                pp.slots.push_back(SlotPlan{0, s, 0, 0});
+                continue;
+            }
+            bool found = false;
+            for (uint32_t k = 0; k < pp.probes.size(); k++) {
+                const PipelinePlan& child = ex.pipelines[pp.probes[k].child];
+                if (!in_subtree(si, child.input)) continue;
+                for (uint32_t j = 0; j < child.slots.size(); j++)
+                    if (child.slots[j].attr == s) {
+                        pp.slots.push_back(SlotPlan{1, s, k, j});
+                        found = true;
+                    }
+                break;
+            }
+            if (!found) {
+                err = "internal: payload source not found in children";
+                return BJ_ERR_INTERNAL;
+            }
+        }
+        if (pp.probes.size() > 16) {
+            err = "a scan joins more than 16 inputs";
+            return BJ_ERR_UNSUPPORTED;
+        }
+        if (pp.slots.size() > 32) {
+            err = "more than 32 distinct result columns";
+            return BJ_ERR_UNSUPPORTED;
+        }
+        pipe_of[x] = int64_t(ex.pipelines.size());
+        ex.pipelines.push_back(std::move(pp));
+    }
+    const PipelinePlan& root = ex.pipelines.back();
+    for (uint32_t s : out_src) {
+        for (uint32_t j = 0; j < root.slots.size(); j++)
+            if (root.slots[j].attr == s) {
+                ex.out_slot.push_back(j);
+                break;
+            }
+    }
+    if (ex.out_slot.size() != out_src.size()) {
+        err = "internal: result column without a source";
+        return BJ_ERR_INTERNAL;
+    }
+    return BJ_OK;
+}
+
+} // namespace bj

@@ -1,0 +1,71 @@
+// Host planner: turns a contest plan into device pipelines.
+//
+// The reference imports the plan into attribute equivalence classes
+// (engine/query/PlanImport.cpp:24-89), ignores the given join order and build
+// sides, and re-plans incrementally with DPccp over sampled cardinalities,
+// running at most three operators per pipeline (engine/query/QueryPlan.cpp:
+// 748-794, QueryGraph.cpp:107-216). Here the same equivalence classes are
+// built, then the join tree over the scans is rooted at the largest input
+// (the driver): every other input becomes one build pipeline whose hash table
+// is keyed on the class that links it to its parent, carrying the payload
+// columns its ancestors still need; the driver's pipeline probes its children
+// and writes the result. A pipeline may probe any number of children (the
+// GPU has no reason to cap it at two) and the probe order inside a pipeline
+// is chosen at run time from sampled hit rates (engine/query/QueryPlan.cpp:
+// 719-746 samples 64 rows per table for the same purpose).
+#pragma once
+
+#include "../../include/b200join.h"
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace bj {
+
+struct PlanAttr {
+    uint32_t input;   // scan index
+    uint32_t column;  // base column
+    int32_t type;
+    uint32_t eq;      // equivalence class
+};
+
+struct PlanInput {
+    uint32_t table;                // base table id
+    uint64_t rows;
+    std::vector<uint32_t> attrs;   // global attribute ids of this scan
+};
+
+// One value slot of a pipeline: a column of the scanned input, or a payload
+// slot of a probed child's hash table.
+struct SlotPlan {
+    int kind;         // 0: attr of the scanned input, 1: child payload
+    uint32_t attr;    // source attribute (global id), for both kinds
+    uint32_t probe;   // kind 1: index into Pipeline::probes
+    uint32_t slot;    // kind 1: slot in that child's table
+};
+
+struct PipelinePlan {
+    uint32_t input;
+    int64_t build_key = -1;  // attr id of the hash key; -1 for the output pipeline
+    struct Probe {
+        uint32_t child;       // pipeline index of the child
+        uint32_t probe_attr;  // attr of `input` probing the child's table
+    };
+    std::vector<Probe> probes;
+    std::vector<SlotPlan> slots;  // payload (build) or output sources (root)
+};
+
+struct ExecPlan {
+    std::vector<PlanInput> inputs;
+    std::vector<PlanAttr> attrs;
+    std::vector<PipelinePlan> pipelines;  // children before parents; last = root
+    std::vector<uint32_t> out_slot;       // result column -> slot of the root pipeline
+    std::vector<int32_t> out_types;
+    bool empty = false;                   // some input has no rows
+};
+
+// Builds the execution plan; returns BJ_OK or a status with `err` set.
+int make_exec_plan(const bj_plan& plan, ExecPlan& out, std::string& err);
+
+} // namespace bj

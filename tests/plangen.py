@@ -1,0 +1,93 @@
+"""Seeded random plans for parity tests.
+
+Random join trees over 1-6 tables: INT32 join keys drawn from small domains
+(so keys repeat and chains fan out), NULL keys, INT32/INT64/FP64/VARCHAR
+payloads with NULLs, empty and long (>8185 byte) strings, intermediate
+projections that drop attributes, and root outputs that repeat or reorder
+attributes. Table sizes span empty, one row and multi-page columns.
+"""
+import random
+
+INT32, INT64, FP64, VARCHAR = 0, 1, 2, 3
+
+
+def _value(rng, ty, dom, null_p, long_p):
+    if rng.random() < null_p:
+        return None
+    if ty == INT32:
+        return rng.randrange(dom)
+    if ty == INT64:
+        return rng.randrange(-(1 << 62), 1 << 62)
+    if ty == FP64:
+        return rng.choice([0.0, -0.0, 1.5, -2.25, 1e300, rng.random() * 1e6])
+    if rng.random() < long_p:
+        return "L" * rng.randrange(8186, 20000)
+    return "".join(chr(32 + rng.randrange(95)) for _ in range(rng.randrange(0, 24)))
+
+
+def random_case(seed, max_tables=5, max_rows=3000, min_tables=1, max_width=None):
+    """max_width caps the attributes a join node outputs (the reference only
+    instantiates pipelines carrying a few attributes, engine/genpipelines.py:15-49)."""
+    """Returns (tables, nodes, root) in the form tests/golden/make_golden.py uses."""
+    rng = random.Random(seed)
+    ntables = rng.randint(min_tables, max_tables)
+    tables = []
+    for _ in range(ntables):
+        r = rng.random()
+        nrows = 0 if r < 0.04 else 1 if r < 0.1 else rng.randint(2, 40) if r < 0.5 else rng.randint(41, max_rows)
+        nkeys = rng.randint(1, 2)
+        npay = rng.randint(0, 3)
+        types = [INT32] * nkeys + [rng.choice([INT32, INT64, FP64, VARCHAR]) for _ in range(npay)]
+        dom = max(1, int(nrows * rng.choice([0.2, 0.5, 1.0, 3.0])))
+        null_p = rng.choice([0.0, 0.0, 0.05, 0.3])
+        long_p = 0.002 if rng.random() < 0.3 else 0.0
+        rows = [[_value(rng, ty, dom, null_p, long_p) for ty in types] for _ in range(nrows)]
+        tables.append({"types": types, "rows": rows})
+    nodes = []
+    subtrees = []  # (node id, [type per output attr])
+    for t, tab in enumerate(tables):
+        cols = list(range(len(tab["types"])))
+        rng.shuffle(cols)
+        keep = cols[:rng.randint(1, len(cols))]
+        if not any(tab["types"][c] == INT32 for c in keep):
+            keep.append(next(c for c in cols if tab["types"][c] == INT32))
+        attrs = [[c, tab["types"][c]] for c in keep]
+        nodes.append({"kind": "scan", "table": t, "attrs": attrs})
+        subtrees.append((len(nodes) - 1, [a[1] for a in attrs]))
+    while len(subtrees) > 1:
+        a = subtrees.pop(rng.randrange(len(subtrees)))
+        b = subtrees.pop(rng.randrange(len(subtrees)))
+        la = rng.choice([i for i, ty in enumerate(a[1]) if ty == INT32])
+        ra = rng.choice([i for i, ty in enumerate(b[1]) if ty == INT32])
+        both = a[1] + b[1]
+        idx = list(range(len(both)))
+        if rng.random() < 0.5 or (max_width and len(idx) > max_width):
+            rng.shuffle(idx)
+            idx = idx[:rng.randint(1, min(len(idx), max_width or len(idx)))]
+        if not any(both[i] == INT32 for i in idx):
+            idx.append(next(i for i in range(len(both)) if both[i] == INT32))
+        attrs = [[i, both[i]] for i in idx]
+        nodes.append({"kind": "join", "build_left": rng.random() < 0.5, "left": a[0], "right": b[0], "left_attr": la,
+                      "right_attr": ra, "attrs": attrs})
+        subtrees.append((len(nodes) - 1, [x[1] for x in attrs]))
+    root, rtypes = subtrees[0]
+    if rng.random() < 0.3 and nodes[root]["kind"] == "join":
+        # Root output repeating / reordering attributes.
+        n = nodes[root]
+        base = n["attrs"]
+        n["attrs"] = [rng.choice(base) for _ in range(rng.randint(1, min(len(base) + 2, max_width or 99)))]
+    return tables, nodes, root
+
+
+def to_plan(pkg, tables, nodes, root):
+    plan = pkg.Plan()
+    for t in tables:
+        plan.new_input(pkg.table_from_rows(t["rows"], t["types"]))
+    for n in nodes:
+        attrs = [tuple(a) for a in n["attrs"]]
+        if n["kind"] == "scan":
+            plan.new_scan_node(n["table"], attrs)
+        else:
+            plan.new_join_node(n["build_left"], n["left"], n["right"], n["left_attr"], n["right_attr"], attrs)
+    plan.root = root
+    return plan

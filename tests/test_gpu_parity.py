@@ -1,0 +1,170 @@
+"""Parity of the CUDA engine with the oracle, through the C ABI.
+
+Bar: the result row multiset equals the oracle's exactly (integer, string and
+index work is bit-exact), and every result page obeys the page format.
+"""
+import ctypes
+
+import pytest
+
+import oracle_lib
+import plangen
+from golden.make_golden import canon, to_plan
+
+pytestmark = pytest.mark.gpu
+
+
+def check_against_oracle(pkg, ctx, oracle, plan_ref, label):
+    with ctx.execute_raw(plan_ref) as r:
+        st = r.stats()
+        assert st.kernel_launches > 0 or r.num_rows == 0
+        got, keep = r.table_struct()
+        want = oracle.execute(plan_ref.ref() if hasattr(plan_ref, "ref") else plan_ref)
+        return oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), label)
+
+
+def test_golden_cases(pkg, ctx, golden):
+    """The reference's API cases (tests/unit_tests.cpp:19-663) through bj_execute."""
+    for case in golden:
+        out = ctx.execute(to_plan(case, pkg))
+        assert [c.type for c in out.columns] == case["expected_types"], case["name"]
+        assert out.num_rows == len(case["expected"]), case["name"]
+        assert canon(pkg.rows_of(out)) == canon(case["expected"]), case["name"]
+
+
+@pytest.mark.parametrize("seed", range(60))
+def test_random_plans(pkg, ctx, oracle, seed):
+    tables, nodes, root = plangen.random_case(1000 + seed, max_rows=3000)
+    cp = pkg.CPlan(plangen.to_plan(pkg, tables, nodes, root))
+    check_against_oracle(pkg, ctx, oracle, cp, f"seed {1000 + seed}")
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_random_plans_wide_tables(pkg, ctx, oracle, seed):
+    """Larger inputs: columns of many pages, long chains of duplicates."""
+    tables, nodes, root = plangen.random_case(5000 + seed, max_tables=3, max_rows=40000)
+    cp = pkg.CPlan(plangen.to_plan(pkg, tables, nodes, root))
+    check_against_oracle(pkg, ctx, oracle, cp, f"seed {5000 + seed}")
+
+
+@pytest.mark.parametrize("name,seed,scale", [("join2", 1, 0.02), ("snowflake", 2, 0.02), ("snowflake", 7, 0.1)])
+def test_workloads_small(pkg, ctx, oracle, name, seed, scale):
+    w = pkg.Workload(name, seed, scale)
+    n = check_against_oracle(pkg, ctx, oracle, w.plan_ptr(), f"{name} x{scale}")
+    assert n > 0
+
+
+def test_join2_full_size(pkg, ctx, oracle):
+    """The two-table join at its benchmark size (R 1M, S 8M), compared exactly."""
+    w = pkg.Workload("join2", 1, 1.0)
+    n = check_against_oracle(pkg, ctx, oracle, w.plan_ptr(), "join2 full")
+    assert 7_000_000 < n < 7_400_000
+
+
+def test_snowflake_full_size(pkg, ctx, oracle):
+    """The five-way snowflake at its benchmark size (50M-row fact), compared exactly."""
+    w = pkg.Workload("snowflake", 2, 1.0)
+    check_against_oracle(pkg, ctx, oracle, w.plan_ptr(), "snowflake full")
+
+
+def test_resident_equals_host_path(pkg, ctx, oracle):
+    w = pkg.Workload("snowflake", 3, 0.05)
+    plan = w.plan_ptr().contents
+    res = [ctx.upload(plan.inputs[i]) for i in range(plan.num_inputs)]
+    try:
+        with ctx.execute_resident(w.plan_ptr(), res) as r:
+            got, keep = r.table_struct()
+            want = oracle.execute(w.plan_ptr())
+            oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), "resident")
+        # Device-only result: same page counts, pages readable by copy.
+        with ctx.execute_resident(w.plan_ptr(), res, flags=pkg.RESULT_DEVICE) as r:
+            t = r.to_table()
+            assert t.num_rows == r.num_rows
+    finally:
+        for x in res:
+            x.free()
+
+
+def test_repeated_calls_reuse_context(pkg, ctx, oracle):
+    w = pkg.Workload("join2", 4, 0.01)
+    for _ in range(3):
+        check_against_oracle(pkg, ctx, oracle, w.plan_ptr(), "repeat")
+
+
+def test_non_int32_join_key_is_rejected(pkg, ctx):
+    plan = pkg.Plan()
+    t = pkg.table_from_rows([[1], [2]], [pkg.INT64])
+    plan.new_input(t)
+    plan.new_input(t)
+    plan.new_scan_node(0, [(0, pkg.INT64)])
+    plan.new_scan_node(1, [(0, pkg.INT64)])
+    plan.new_join_node(True, 0, 1, 0, 0, [(0, pkg.INT64)])
+    plan.root = 2
+    with pytest.raises(pkg.EngineError) as e:
+        ctx.execute(plan)
+    assert e.value.status == 4
+    # The context stays usable after an error.
+    plan2 = pkg.Plan()
+    t2 = pkg.table_from_rows([[1], [2]], [pkg.INT32])
+    plan2.new_input(t2)
+    plan2.new_input(t2)
+    plan2.new_scan_node(0, [(0, pkg.INT32)])
+    plan2.new_scan_node(1, [(0, pkg.INT32)])
+    plan2.new_join_node(True, 0, 1, 0, 0, [(0, pkg.INT32), (1, pkg.INT32)])
+    plan2.root = 2
+    assert sorted(pkg.rows_of(ctx.execute(plan2))) == [(1, 1), (2, 2)]
+
+
+def test_row_count_mismatch_is_rejected(pkg, ctx):
+    """Pages holding fewer rows than the table claims: caught by the page index."""
+    plan = pkg.Plan()
+    t = pkg.table_from_rows([[1], [2], [3]], [pkg.INT32])
+    t.num_rows = 5
+    plan.new_input(t)
+    plan.new_input(pkg.table_from_rows([[1]], [pkg.INT32]))
+    plan.new_scan_node(0, [(0, pkg.INT32)])
+    plan.new_scan_node(1, [(0, pkg.INT32)])
+    plan.new_join_node(True, 0, 1, 0, 0, [(0, pkg.INT32)])
+    plan.root = 2
+    with pytest.raises(pkg.EngineError) as e:
+        ctx.execute(plan)
+    assert e.value.status == 1
+
+
+def test_inconsistent_bitmap_is_rejected(pkg, ctx):
+    """A page whose non-null count contradicts its bitmap (checked on device
+    before any value is read)."""
+    plan = pkg.Plan()
+    t = pkg.table_from_rows([[1], [None], [3]], [pkg.INT32])
+    bad = bytearray(t.columns[0].data)
+    bad[2] = 1  # header says 1 non-null, bitmap has 2
+    t.columns[0] = pkg.Column(pkg.INT32, bytes(bad))
+    plan.new_input(t)
+    plan.new_input(pkg.table_from_rows([[1]], [pkg.INT32]))
+    plan.new_scan_node(0, [(0, pkg.INT32)])
+    plan.new_scan_node(1, [(0, pkg.INT32)])
+    plan.new_join_node(True, 0, 1, 0, 0, [(0, pkg.INT32)])
+    plan.root = 2
+    with pytest.raises(pkg.EngineError) as e:
+        ctx.execute(plan)
+    assert e.value.status == 1
+
+
+def test_empty_and_single_table_plans(pkg, ctx, oracle):
+    # A table with no rows and no columns (engine/query/PlanImport.cpp:43-49).
+    plan = pkg.Plan()
+    plan.new_input(pkg.ColumnarTable(0, []))
+    plan.new_input(pkg.table_from_rows([[1, "a"]], [pkg.INT32, pkg.VARCHAR]))
+    plan.new_scan_node(0, [(0, pkg.INT32)])
+    plan.new_scan_node(1, [(0, pkg.INT32), (1, pkg.VARCHAR)])
+    plan.new_join_node(True, 0, 1, 0, 0, [(0, pkg.INT32), (2, pkg.VARCHAR)])
+    plan.root = 2
+    out = ctx.execute(plan)
+    assert out.num_rows == 0 and [c.type for c in out.columns] == [pkg.INT32, pkg.VARCHAR]
+    # A lone scan returns its rows, NULLs included.
+    plan = pkg.Plan()
+    rows = [[i if i % 3 else None, "s" * (i % 5), float(i)] for i in range(5000)]
+    plan.new_input(pkg.table_from_rows(rows, [pkg.INT32, pkg.VARCHAR, pkg.FP64]))
+    plan.new_scan_node(0, [(2, pkg.FP64), (0, pkg.INT32), (1, pkg.VARCHAR)])
+    plan.root = 0
+    check_against_oracle(pkg, ctx, oracle, pkg.CPlan(plan), "lone scan")
