@@ -1,0 +1,310 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 join engine on the five-way snowflake join.
+
+Workload (seeded synthetic data of the benchmark's shapes; no public dataset):
+fact table of 50M rows with four INT32 foreign keys, Zipf(s=1.1) over the
+keys of four dimensions of 5M / 1M / 200K / 20K rows; the dimensions arrive
+pre-filtered to 1% / 5% / 30% / 60% of their rows and carry a VARCHAR of 1-64
+bytes; the plan joins all five and outputs two dimension strings and two
+fact keys. The fact's key columns are 206 MB each, far larger than L2, so no
+L2 flush is needed between steps.
+
+One step = one execution of the query.
+  value : queries/s with the tables resident in HBM (bj_execute_resident,
+          result pages left in HBM), timed with CUDA events on the engine's
+          stream, max over ranks, all ranks' queries / time.
+  e2e   : queries/s through the drop-in path (bj_execute: host pages in,
+          host pages out), host->device page copies and the device->host copy
+          of the result pages inside the timed region.
+  roofline: the scan-side probe stage (the kernel that streams the fact's key
+          pages), its page bytes per launch / its CUDA-event duration, against
+          the measured HBM copy bandwidth.
+  cpu_baseline: the reference CPU engine (oracle/_ref/ref_runner, built from
+          the reference's sources) on this host's cores, a bounded sample.
+
+--impl reference times the reference CPU engine alone (rank 0; other ranks
+exit at once). --gpus N > 1 runs N independent replicas (the query does not
+shard: every rank runs the whole query on its own GPU), launched by torchrun.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "queries/s & p99 latency, learned+batched vs plain GPU path (exact rows); GB/s"
+REF_RUNNER = os.path.join(REPO, "oracle", "_ref", "ref_runner")
+WORKLOAD_DESC = ("snowflake-5way: fact 50M rows x 4 INT32 FKs (Zipf 1.1); dims 5M/1M/200K/20K rows "
+                 "pre-filtered 1%/5%/30%/60%, VARCHAR 1-64 B; output 2 VARCHAR + 2 INT32")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="snowflake")
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--cpu-steps", type=int, default=3, help="0 skips the CPU baseline")
+    return ap.parse_args()
+
+
+def config(args, world):
+    return {"workload": WORKLOAD_DESC if args.workload == "snowflake" else args.workload,
+            "name": args.workload, "seed": args.seed, "scale": args.scale,
+            "l2": "inputs larger than L2 (each fact key column 206 MB > 126 MB L2); no flush",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+def run_reference(args, steps, warmup):
+    """The reference CPU engine: wall-clock per execute(), all host cores."""
+    if not os.path.exists(REF_RUNNER):
+        return None, "oracle/_ref/ref_runner is not built (the reference sources were not available at build time)"
+    p = subprocess.run([REF_RUNNER, "bench", args.workload, str(args.seed), str(args.scale), str(warmup), str(steps)],
+                       capture_output=True, text=True, timeout=1800)
+    if p.returncode != 0:
+        return None, f"ref_runner failed: {p.stderr.strip()[-300:]}"
+    line = [l for l in p.stdout.splitlines() if l.startswith("{")][-1]
+    return json.loads(line), None
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    res, err = run_reference(args, args.steps, args.warmup)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return 0
+    times = res["times_ms"]
+    mean_ms = statistics.fmean(times)
+    qps = 1000.0 / mean_ms
+    out = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": config(args, 1),
+        "p50_ms": statistics.median(times), "p99_ms": sorted(times)[min(len(times) - 1, int(0.99 * len(times)))],
+        "rows": res["rows"],
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": res["threads"], "kind": "reference",
+                         "sample": f"{args.steps} timed executions (+{args.warmup} warm-up) of the full query"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "50"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.1)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the scan-side probe stage from the committed
+    ncu summary, if one exists."""
+    try:
+        with open(os.path.join(REPO, "profiles", "scan_probe_traffic.json")) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+
+    import importlib
+    import torch
+
+    pkg = importlib.import_module("contest-sigmod2025_b200")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = pkg.Workload(args.workload, args.seed, args.scale)
+    plan = w.plan_ptr()
+    ctx = pkg.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+    inputs = plan.contents
+    residents = [ctx.upload(inputs.inputs[i]) for i in range(inputs.num_inputs)]
+
+    # ---- value: tables resident in HBM ----
+    for _ in range(args.warmup):
+        ctx.execute_resident(plan, residents, flags=pkg.RESULT_DEVICE).free()
+    ctx.profile(True)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lat = []
+    launches = 0
+    scan_ms = scan_bytes = scan_n = 0
+    rows = 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = ctx.execute_resident(plan, residents, flags=pkg.RESULT_DEVICE)
+        lat.append((time.perf_counter() - t0) * 1e3)
+        s = r.stats()
+        launches += s.kernel_launches
+        scan_ms += s.scan_kernel_ms
+        scan_bytes += s.scan_kernel_bytes
+        scan_n += s.scan_kernel_launches
+        rows = r.num_rows
+        r.free()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ctx.profile(False)
+    elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = args.steps * world / (elapsed_ms / 1e3)
+
+    # ---- e2e: drop-in path, host pages in and out ----
+    e2e_steps = args.e2e_steps or max(3, min(args.steps, 20))
+    for _ in range(2):
+        ctx.execute_raw(plan).free()
+    barrier()
+    h2d = d2h = 0
+    e2e_lat = []
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        t0 = time.perf_counter()
+        r = ctx.execute_raw(plan)
+        e2e_lat.append((time.perf_counter() - t0) * 1e3)
+        s = r.stats()
+        h2d, d2h = s.h2d_bytes, s.d2h_bytes
+        r.free()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    e2e_value = e2e_steps * world / (e2e_ms / 1e3)
+
+    for x in residents:
+        x.free()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    peak, peak_kind = measured_peak()
+    achieved = (scan_bytes / scan_n) / (scan_ms / scan_n / 1e3) / 1e9 if scan_n and scan_ms > 0 else None
+    traffic = profiled_traffic()
+    out = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": config(args, world),
+        "p50_ms": statistics.median(lat), "p99_ms": sorted(lat)[min(len(lat) - 1, int(0.99 * len(lat)))],
+        "rows": rows,
+        "scan_bytes_per_query": w.scan_bytes(),
+        "input_gbs": w.scan_bytes() * value / world / 1e9,
+        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "p50_ms": statistics.median(e2e_lat)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "traffic": traffic,
+                     "kernel": "k_probe_stage over the fact's key pages",
+                     "launches": scan_n, "bytes_per_launch": scan_bytes / scan_n if scan_n else None,
+                     "peak_kind": f"{peak_kind} HBM copy bandwidth"},
+        "clocks": clk,
+    }
+    if world == 1 and args.cpu_steps > 0:
+        res, err = run_reference(args, args.cpu_steps, 1)
+        if res:
+            mean = statistics.fmean(res["times_ms"])
+            out["cpu_baseline"] = {"value": 1000.0 / mean, "unit": "queries/s", "cores": res["threads"],
+                                   "kind": "reference",
+                                   "sample": f"{args.cpu_steps} executions (+1 warm-up) of the full query by the "
+                                             f"reference engine, wall clock"}
+        else:
+            out["cpu_baseline"] = {"value": None, "unit": "queries/s", "cores": None, "kind": "reference",
+                                   "sample": err}
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -69,7 +69,9 @@ class BjPlan(ctypes.Structure):
 class BjStats(ctypes.Structure):
     _fields_ = [("kernel_launches", ctypes.c_uint64), ("pipelines", ctypes.c_uint64), ("h2d_bytes", ctypes.c_uint64),
                 ("d2h_bytes", ctypes.c_uint64), ("input_pages", ctypes.c_uint64), ("output_pages", ctypes.c_uint64),
-                ("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+                ("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("scan_kernel_ms", ctypes.c_double), ("scan_kernel_launches", ctypes.c_uint64),
+                ("scan_kernel_bytes", ctypes.c_uint64)]
 
 
 # Every symbol include/b200join.h declares, with its ctypes signature.
@@ -93,6 +95,7 @@ ABI = {
     "bj_result_stats": (_INT, [_VP, ctypes.POINTER(BjStats)]),
     "bj_result_free": (None, [_VP]),
     "bj_context_stream": (_VP, [_VP]),
+    "bj_context_profile": (None, [_VP, _INT]),
 }
 
 WORKLOAD_ABI = {
@@ -515,6 +518,9 @@ class Context:
 
     def stream(self) -> int:
         return lib().bj_context_stream(self.handle) or 0
+
+    def profile(self, on: bool) -> None:
+        lib().bj_context_profile(self.handle, 1 if on else 0)
 
     def close(self):
         if self.handle:

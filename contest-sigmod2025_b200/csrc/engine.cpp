@@ -241,6 +241,9 @@ struct bj_context {
     uint64_t* d_small = nullptr;       // device readback slots
     uint64_t launches = 0;
     uint64_t live_results = 0;
+    bool profile = false;
+    std::vector<cudaEvent_t> prof_events;  // pairs around timed launches
+    uint64_t prof_bytes = 0;
 
     PinnedBlock take_pinned(size_t bytes) {
         for (size_t i = 0; i < pinned_free.size(); i++)
@@ -348,14 +351,17 @@ uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs) {
     struct Src {
         const void* page;
         uint8_t* dst;
+        size_t job;
     };
     std::vector<Src> all;
     all.reserve(total);
-    for (auto& j : jobs)
+    for (size_t ji = 0; ji < jobs.size(); ji++) {
+        const ColumnJob& j = jobs[ji];
         for (uint64_t p = 0; p < j.src->num_pages; p++) {
             if (!j.src->pages[p]) throw Fail{BJ_ERR_INVALID, "null page pointer"};
-            all.push_back(Src{j.src->pages[p], j.dpages + p * kPageSize});
+            all.push_back(Src{j.src->pages[p], j.dpages + p * kPageSize, ji});
         }
+    }
     const size_t chunk = 2048;  // pages per DMA
     uint8_t* stage = ctx->stage.p;
     for (size_t c0 = 0; c0 < all.size(); c0 += chunk) {
@@ -365,11 +371,12 @@ uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs) {
             for (size_t i = c0 + t * per; i < std::min(c1, c0 + (t + 1) * per); i++)
                 std::memcpy(stage + i * kPageSize, all[i].page, kPageSize);
         });
-        // Contiguous destinations within one column become one copy.
+        // Consecutive pages of one column (one device allocation) become one
+        // copy; a copy never spans two allocations.
         size_t i = c0;
         while (i < c1) {
             size_t k = i + 1;
-            while (k < c1 && all[k].dst == all[k - 1].dst + kPageSize) k++;
+            while (k < c1 && all[k].job == all[i].job && all[k].dst == all[k - 1].dst + kPageSize) k++;
             BJ_CK(cudaMemcpyAsync(all[i].dst, stage + i * kPageSize, (k - i) * kPageSize, cudaMemcpyHostToDevice,
                                   ctx->stream));
             i = k;
@@ -477,6 +484,19 @@ class Executor {
         return static_cast<T*>(A_.alloc(sizeof(T) * std::max<size_t>(n, 1)));
     }
     void launched(int n) { ctx_->launches += uint64_t(n); }
+    void begin_timed() {
+        cudaEvent_t e;
+        BJ_CK(cudaEventCreate(&e));
+        ctx_->prof_events.push_back(e);
+        BJ_CK(cudaEventRecord(e, st_));
+    }
+    void end_timed(uint64_t bytes) {
+        cudaEvent_t e;
+        BJ_CK(cudaEventCreate(&e));
+        ctx_->prof_events.push_back(e);
+        BJ_CK(cudaEventRecord(e, st_));
+        ctx_->prof_bytes += bytes;
+    }
 
     // Exclusive scan of tile counts; returns the total (synchronises).
     uint32_t scan_total_u32(const uint32_t* in, uint32_t* out, size_t n) {
@@ -533,14 +553,19 @@ class Executor {
             bool bloom = ht.bloom && rate[k] < 0.5;
             const DevColumn& key = col(pp.probes[k].probe_attr);
             ItemsOut none{};
+            bool timed = ctx_->profile && items.rows == nullptr;
+            if (timed) begin_timed();
             launched(probe_stage(items, key, ht, 0, tc, nullptr, none, bloom, ctx_->d_err, st_));
+            if (timed) end_timed(uint64_t(key.npages) * kPageSize);
             uint32_t total = scan_total_u32(tc, toff, tiles);
             if (total == 0) return false;
             ItemsOut out{};
             out.rows = alloc<uint32_t>(total);
             for (size_t j = 0; j <= s; j++) out.ents[j] = alloc<uint32_t>(total);
             out.mult = alloc<uint64_t>(total);
+            if (timed) begin_timed();
             launched(probe_stage(items, key, ht, 1, nullptr, toff, out, bloom, ctx_->d_err, st_));
+            if (timed) end_timed(uint64_t(key.npages) * kPageSize);
             Items next{};
             next.rows = out.rows;
             for (size_t j = 0; j <= s; j++) next.ents[j] = out.ents[j];
@@ -718,6 +743,9 @@ void set_empty_result(bj_result& r, const ExecPlan& ex) {
 
 int fail_to_status(bj_context* ctx, const Fail& f) {
     ctx->last_error = f.msg;
+    for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
+    ctx->prof_events.clear();
+    ctx->prof_bytes = 0;
     // Leave the stream idle and the arena reusable after a failure.
     cudaStreamSynchronize(ctx->stream);
     cudaGetLastError();
@@ -809,6 +837,16 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
         float ms = 0;
         BJ_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
         res->stats.device_ms = ms;
+        for (size_t i = 0; i + 1 < ctx->prof_events.size(); i += 2) {
+            float k = 0;
+            BJ_CK(cudaEventElapsedTime(&k, ctx->prof_events[i], ctx->prof_events[i + 1]));
+            res->stats.scan_kernel_ms += k;
+            res->stats.scan_kernel_launches++;
+        }
+        res->stats.scan_kernel_bytes = ctx->prof_bytes;
+        for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
+        ctx->prof_events.clear();
+        ctx->prof_bytes = 0;
         res->stats.kernel_launches = ctx->launches - launches0;
         res->stats.pipelines = pipes;
         ctx->arena.reset();
@@ -887,6 +925,10 @@ BJ_API void bj_context_destroy(bj_context* ctx) {
 BJ_API const char* bj_last_error(const bj_context* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
 
 BJ_API void* bj_context_stream(bj_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+BJ_API void bj_context_profile(bj_context* ctx, int on) {
+    if (ctx) ctx->profile = on != 0;
+}
 
 BJ_API int bj_execute(bj_context* ctx, const bj_plan* plan, bj_result** out) {
     if (!ctx) return BJ_ERR_INVALID;

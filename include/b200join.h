@@ -117,6 +117,11 @@ typedef struct bj_stats {
     uint64_t output_pages;      /* pages written to the result */
     double device_ms;           /* device time of the call, CUDA events */
     double total_ms;            /* host wall time of the call */
+    /* The scan-side probe stage (the kernel that streams a base table's key
+     * pages), timed with CUDA events when profiling is on (bj_context_profile). */
+    double scan_kernel_ms;      /* summed duration of its launches */
+    uint64_t scan_kernel_launches;
+    uint64_t scan_kernel_bytes; /* page bytes those launches had to read */
 } bj_stats;
 
 /* Replaces Contest::build_context (engine/Execute.cpp:42-46). Creates the CUDA
@@ -164,6 +169,10 @@ BJ_API const void* bj_result_device_page(const bj_result* r, uint64_t column, ui
 BJ_API int bj_result_copy_pages(const bj_result* r, uint64_t column, void* const* dst);
 BJ_API int bj_result_stats(const bj_result* r, bj_stats* out);
 BJ_API void bj_result_free(bj_result* r);
+
+/* Turns per-kernel event timing of the scan-side probe stage on (1) or off (0).
+ * Adds two event records per timed launch; off by default. */
+BJ_API void bj_context_profile(bj_context* ctx, int on);
 
 /* The context's CUDA stream (a cudaStream_t), for callers timing with events. */
 BJ_API void* bj_context_stream(bj_context* ctx);
