@@ -96,6 +96,7 @@ ABI = {
     "bj_result_free": (None, [_VP]),
     "bj_context_stream": (_VP, [_VP]),
     "bj_context_profile": (None, [_VP, _INT]),
+    "bj_join_count_static": (_INT, [_VP, _U64, _U64, _VP, _U64, _VP, _VP]),
 }
 
 WORKLOAD_ABI = {

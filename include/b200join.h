@@ -180,6 +180,27 @@ BJ_API void* bj_context_stream(bj_context* ctx);
 /* Library version string. */
 BJ_API const char* bj_version(void);
 
+/* Row count of the inner equi-join of two INT32 page columns, computed without
+ * allocating any memory. No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc (their device memory belongs to another
+ * allocator, or cudaMalloc's implicit device synchronisation is not allowed
+ * where they run). The result equals bj_result_num_rows of bj_execute on
+ * Scan(A) JOIN Scan(B) over these columns; NULL keys never match.
+ *
+ * build_pages / probe_pages: device addresses of the columns' 8 KiB pages,
+ * back to back. build_rows: rows the build pages hold, at most 262144 (the
+ * fixed scratch's capacity; larger counts return BJ_ERR_INVALID).
+ * out_count: a device u64 that receives the count; stream: a cudaStream_t
+ * (NULL = default stream). The call only enqueues work on `stream`.
+ *
+ * Scratch: a 4 MiB array compiled into the library, held by every GPU that
+ * loads it until the process exits. The first call on a device looks up its
+ * device address; make that first call before any stream capture. All calls
+ * share the array: calls that overlap on the GPU race and give wrong counts. */
+BJ_API int bj_join_count_static(const void* build_pages, uint64_t build_num_pages, uint64_t build_rows,
+                                const void* probe_pages, uint64_t probe_num_pages,
+                                unsigned long long* out_count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
