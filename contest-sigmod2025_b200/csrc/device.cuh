@@ -37,6 +37,7 @@ enum DevError : uint32_t {
     kErrRowRange = 2,     // a row id beyond the column
     kErrCapacity = 3,     // an output buffer would overflow
     kErrLongString = 4,   // a long-string page run is malformed
+    kErrTimeout = 5,      // a bounded wait (mbarrier) ran out
 };
 
 struct DevColumn {
@@ -135,12 +136,26 @@ BJ_HD uint64_t mix64(uint64_t x) {
     return x;
 }
 
-// Blocked bloom filter: one 32-bit word per key, four bits set in it.
-BJ_HD uint32_t bloom_bits(uint64_t g) {
+// Blocked bloom filter: one 32-bit word per key with up to four bits set.
+// The word comes from the key hash's top bits (at most 14 of them, so a
+// filter is at most 64 KiB); the bit mask is entry (h >> 32) & 2047 of a
+// 2048-entry mask table. The table is arithmetic (bloom_mask below), so
+// scans can tabulate it in shared memory and replace the bit arithmetic by
+// one lookup. (The reference also draws 4-of-16 masks from a 2048-entry
+// table, engine/infra/JoinFilter.hpp:9-14; ours is 4-of-32 and generated.)
+constexpr uint32_t kBloomMaxLog2 = 14;
+constexpr uint32_t kBloomMasks = 2048;
+BJ_HD uint32_t bloom_mask(uint32_t idx) {
+    uint32_t g = idx * 2654435761u;
+    g ^= g >> 15;
+    g *= 0x2c1b3c6du;
+    g ^= g >> 12;
     return (1u << (g & 31)) | (1u << ((g >> 5) & 31)) | (1u << ((g >> 10) & 31)) | (1u << ((g >> 15) & 31));
 }
-BJ_HD uint32_t bloom_word(uint64_t g, uint32_t log2_words) {
-    return log2_words ? uint32_t(g >> (64 - log2_words)) : 0u;
+BJ_HD uint32_t bloom_mask_index(uint64_t h) { return uint32_t(h >> 32) & (kBloomMasks - 1); }
+BJ_HD uint32_t bloom_bits(uint64_t h) { return bloom_mask(bloom_mask_index(h)); }
+BJ_HD uint32_t bloom_word(uint64_t h, uint32_t log2_words) {
+    return log2_words ? uint32_t(h >> (64 - log2_words)) : 0u;
 }
 
 // A built hash table: entries grouped by bucket (CSR), keys 32-bit, a
@@ -162,9 +177,9 @@ struct HTView {
 
 #if defined(__CUDACC__)
 __device__ __forceinline__ bool bloom_may_contain(const uint32_t* bloom, uint32_t log2w, uint32_t key) {
-    uint64_t g = mix64(key);
-    uint32_t bits = bloom_bits(g);
-    return (bloom[bloom_word(g, log2w)] & bits) == bits;
+    uint64_t h = key_hash(key);
+    uint32_t bits = bloom_bits(h);
+    return (bloom[bloom_word(h, log2w)] & bits) == bits;
 }
 
 __device__ __forceinline__ void record_error(uint32_t* err, uint32_t code) {

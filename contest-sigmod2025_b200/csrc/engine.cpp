@@ -241,6 +241,7 @@ struct bj_context {
     uint64_t* d_small = nullptr;       // device readback slots
     uint64_t launches = 0;
     uint64_t live_results = 0;
+    int num_sms = 148;
     bool profile = false;
     std::vector<cudaEvent_t> prof_events;  // pairs around timed launches
     uint64_t prof_bytes = 0;
@@ -456,6 +457,9 @@ void collect_columns(const ExecPlan& ex, uint32_t table_id, uint64_t ncols, std:
 struct BuiltHT {
     HTView view{};
     bool empty = true;
+    uint32_t* dflags = nullptr;  // device: [0] some key repeats, [1] some multiplicity > 1
+    bool unique = false;         // host copies, valid once the parent pipeline read them back
+    bool unit_mult = false;
 };
 
 class Executor {
@@ -514,6 +518,16 @@ class Executor {
         return ctx_->h_small[0];
     }
 
+    // Replaces a device-side item count by the exact count (one read-back).
+    void resolve(Items& items) {
+        if (!items.dcount) return;
+        stash_u32(ctx_, items.dcount, 0);
+        stash_err(ctx_);
+        readback(ctx_, 1);
+        items.count = uint32_t(ctx_->h_small[0]);
+        items.dcount = nullptr;
+    }
+
     bool run_pipeline(size_t pi, bj_result* res, int flags) {
         pipes_++;
         const PipelinePlan& pp = ex_.pipelines[pi];
@@ -531,13 +545,20 @@ class Executor {
             uint32_t nsample = uint32_t(std::min<uint64_t>(in.rows, 4096));
             uint32_t* hits = alloc<uint32_t>(np);
             for (size_t k = 0; k < np; k++) {
-                launched(sample_probe(col(pp.probes[k].probe_attr), nsample, hts_[pp.probes[k].child].view,
-                                      hits + k, st_));
+                BuiltHT& child = hts_[pp.probes[k].child];
+                launched(sample_probe(col(pp.probes[k].probe_attr), nsample, child.view, hits + k, st_));
                 stash_u32(ctx_, hits + k, int(k));
+                stash_u32(ctx_, child.dflags, int(16 + 2 * k));
+                stash_u32(ctx_, child.dflags + 1, int(17 + 2 * k));
             }
             stash_err(ctx_);
             readback(ctx_, int(np));
-            for (size_t k = 0; k < np; k++) rate[k] = nsample ? double(ctx_->h_small[k]) / nsample : 1.0;
+            for (size_t k = 0; k < np; k++) {
+                rate[k] = nsample ? double(ctx_->h_small[k]) / nsample : 1.0;
+                BuiltHT& child = hts_[pp.probes[k].child];
+                child.unique = ctx_->h_small[16 + 2 * k] == 0;
+                child.unit_mult = ctx_->h_small[17 + 2 * k] == 0;
+            }
             std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return rate[a] < rate[b]; });
         }
         std::vector<uint32_t> stage_of(np);
@@ -547,25 +568,101 @@ class Executor {
             stage_of[k] = uint32_t(s);
             by_stage[s] = hts_[pp.probes[k].child].view;
             const HTView& ht = by_stage[s];
+            if (items.rows == nullptr) {
+                // Scan stage: stream the key pages of the scanned table.
+                const BuiltHT& bh = hts_[pp.probes[k].child];
+                const DevColumn& key = col(pp.probes[k].probe_attr);
+                bool bloom = ht.bloom && rate[k] < 0.5;
+                uint64_t page_bytes = uint64_t(key.npages) * kPageSize;
+                ItemsOut out{};
+                uint32_t total = 0;
+                if (bh.unique) {
+                    uint32_t cap = key.nrows;
+                    out.rows = alloc<uint32_t>(cap);
+                    out.ents[0] = alloc<uint32_t>(cap);
+                    out.mult = bh.unit_mult ? nullptr : alloc<uint64_t>(cap);
+                    uint32_t* cursor = alloc<uint32_t>(1);
+                    BJ_CK(cudaMemsetAsync(cursor, 0, sizeof(uint32_t), st_));
+                    bool timed = ctx_->profile;
+                    if (timed) begin_timed();
+                    launched(scan_probe(key, ht, 2, bloom, nullptr, nullptr, cursor, out.rows, out.ents[0], out.mult,
+                                        cap, ctx_->d_err, ctx_->num_sms, st_));
+                    if (timed) end_timed(page_bytes);
+                    // The next stage reads the count on the device.
+                    Items next{};
+                    next.rows = out.rows;
+                    next.ents[0] = out.ents[0];
+                    next.mult = out.mult;
+                    next.count = cap;
+                    next.dcount = cursor;
+                    next.nprobes = 1;
+                    items = next;
+                    continue;
+                } else {
+                    uint32_t* pc = alloc<uint32_t>(key.npages);
+                    uint32_t* poff = alloc<uint32_t>(size_t(key.npages) + 1);
+                    bool timed = ctx_->profile;
+                    if (timed) begin_timed();
+                    launched(scan_probe(key, ht, 0, bloom, pc, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
+                                        ctx_->d_err, ctx_->num_sms, st_));
+                    if (timed) end_timed(page_bytes);
+                    total = scan_total_u32(pc, poff, key.npages);
+                    if (total) {
+                        out.rows = alloc<uint32_t>(total);
+                        out.ents[0] = alloc<uint32_t>(total);
+                        out.mult = bh.unit_mult ? nullptr : alloc<uint64_t>(total);
+                        if (timed) begin_timed();
+                        launched(scan_probe(key, ht, 1, bloom, nullptr, poff, nullptr, out.rows, out.ents[0],
+                                            out.mult, total, ctx_->d_err, ctx_->num_sms, st_));
+                        if (timed) end_timed(page_bytes);
+                    }
+                }
+                if (total == 0) return false;
+                Items next{};
+                next.rows = out.rows;
+                next.ents[0] = out.ents[0];
+                next.mult = out.mult;
+                next.count = total;
+                next.nprobes = 1;
+                items = next;
+                continue;
+            }
+            const BuiltHT& bh = hts_[pp.probes[k].child];
+            bool bloom = ht.bloom && rate[k] < 0.5;
+            const DevColumn& key = col(pp.probes[k].probe_attr);
+            if (bh.unique) {
+                uint32_t cap = items.count;
+                ItemsOut out{};
+                out.rows = alloc<uint32_t>(cap);
+                for (size_t j = 0; j <= s; j++) out.ents[j] = alloc<uint32_t>(cap);
+                out.mult = (items.mult == nullptr && bh.unit_mult) ? nullptr : alloc<uint64_t>(cap);
+                uint32_t* cursor = alloc<uint32_t>(1);
+                BJ_CK(cudaMemsetAsync(cursor, 0, sizeof(uint32_t), st_));
+                launched(probe_stage_unique(items, key, ht, out, cursor, cap, bloom, ctx_->d_err, ctx_->num_sms, st_));
+                Items next{};
+                next.rows = out.rows;
+                for (size_t j = 0; j <= s; j++) next.ents[j] = out.ents[j];
+                next.mult = out.mult;
+                next.count = cap;
+                next.dcount = cursor;
+                next.nprobes = int(s + 1);
+                items = next;
+                continue;
+            }
+            resolve(items);
+            if (items.count == 0) return false;
             uint32_t tiles = (items.count + kTile - 1) / kTile;
             uint32_t* tc = alloc<uint32_t>(tiles);
             uint32_t* toff = alloc<uint32_t>(tiles + 1);
-            bool bloom = ht.bloom && rate[k] < 0.5;
-            const DevColumn& key = col(pp.probes[k].probe_attr);
             ItemsOut none{};
-            bool timed = ctx_->profile && items.rows == nullptr;
-            if (timed) begin_timed();
             launched(probe_stage(items, key, ht, 0, tc, nullptr, none, bloom, ctx_->d_err, st_));
-            if (timed) end_timed(uint64_t(key.npages) * kPageSize);
             uint32_t total = scan_total_u32(tc, toff, tiles);
             if (total == 0) return false;
             ItemsOut out{};
             out.rows = alloc<uint32_t>(total);
             for (size_t j = 0; j <= s; j++) out.ents[j] = alloc<uint32_t>(total);
             out.mult = alloc<uint64_t>(total);
-            if (timed) begin_timed();
             launched(probe_stage(items, key, ht, 1, nullptr, toff, out, bloom, ctx_->d_err, st_));
-            if (timed) end_timed(uint64_t(key.npages) * kPageSize);
             Items next{};
             next.rows = out.rows;
             for (size_t j = 0; j <= s; j++) next.ents[j] = out.ents[j];
@@ -574,6 +671,7 @@ class Executor {
             next.nprobes = int(s + 1);
             items = next;
         }
+        resolve(items);
         if (items.count == 0) return false;
 
         SlotSources src{};
@@ -611,10 +709,10 @@ class Executor {
         uint32_t* table = alloc<uint32_t>(size_t(1) << tlog2);
         uint32_t* is_rep = alloc<uint32_t>(n);
         launched(aggregate_tuples(tb, table, tlog2, is_rep, ctx_->d_err, st_));
-        uint32_t* rep_off = alloc<uint32_t>(n + 1);
-        uint32_t nrep = scan_total_u32(is_rep, rep_off, n);
-        if (nrep == 0) return false;
-        // Buckets: 2^max(bit_width(n), 4) (engine/op/Hashtable.cpp:94-104).
+        // Buckets: 2^max(bit_width(n), 4) (engine/op/Hashtable.cpp:94-104), sized by
+        // the tuple count n, an upper bound of the distinct tuples, so the build
+        // needs no host round trip.
+        uint32_t nrep = n;
         uint32_t blog2 = std::max<uint32_t>(bit_width(nrep), 4);
         uint32_t shift = 64 - blog2;
         size_t nb = size_t(1) << blog2;
@@ -635,14 +733,17 @@ class Executor {
         ht.nentries = nrep;
         ht.width = width;
         launched(bucket_scatter(tb, is_rep, shift, off, cursor, ht, ctx_->d_err, st_));
-        // Bloom filter: about 16 bits per key.
-        uint32_t wlog2 = std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1));
+        // Bloom filter: about 16 bits per key, at most 64 KiB (shared-memory staging).
+        uint32_t wlog2 = std::min<uint32_t>(kBloomMaxLog2,
+                                            std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1)));
         uint32_t* bloom = alloc<uint32_t>(size_t(1) << wlog2);
-        launched(bloom_build(ht.keys, nrep, bloom, wlog2, st_));
+        launched(bloom_build(tb.keys, is_rep, n, bloom, wlog2, st_));
         ht.bloom = bloom;
         ht.bloom_log2 = wlog2;
         hts_[pi].view = ht;
         hts_[pi].empty = false;
+        hts_[pi].dflags = alloc<uint32_t>(2);
+        launched(ht_flags(ht, uint32_t(nb), hts_[pi].dflags, ctx_->num_sms, st_));
         return true;
     }
 
@@ -666,21 +767,62 @@ class Executor {
         res.npages.assign(ncol, 0);
         struct StrPlan {
             uint32_t* lens = nullptr;
+            uint64_t* start = nullptr;   // exclusive scan of row costs
+            uint32_t* stats = nullptr;   // [0] max cost, [1] long string present
             uint32_t* block_off = nullptr;
             size_t nblocks = 0;
+            bool floor = false;
+            uint64_t cp = 0;
         };
         std::vector<StrPlan> sp(ncol);
+        // Lengths and costs of every VARCHAR column, then one read-back.
+        std::vector<size_t> strcols;
         for (size_t c = 0; c < ncol; c++) {
             int32_t t = ex_.out_types[c];
-            uint32_t j = ex_.out_slot[c];
             if (t != BJ_VARCHAR) {
                 size_t rpp = full_page_rows(t == BJ_INT32 ? 4 : 8);
                 res.npages[c] = (N + rpp - 1) / rpp;
                 continue;
             }
-            const DevColumn& scol = src.s[j].kind == 0 ? src.s[j].col : col(ex_.pipelines.back().slots[j].attr);
+            uint32_t j = ex_.out_slot[c];
+            const DevColumn& scol = col(ex_.pipelines.back().slots[j].attr);
             sp[c].lens = alloc<uint32_t>(N);
             launched(string_lengths(fo.vals[j], fo.valid[j], N, StrSource{scol}, sp[c].lens, ctx_->d_err, st_));
+            uint64_t* cost = alloc<uint64_t>(N);
+            sp[c].stats = alloc<uint32_t>(2);
+            launched(string_cost(sp[c].lens, fo.valid[j], N, cost, sp[c].stats, st_));
+            sp[c].start = alloc<uint64_t>(N + 1);
+            launched(scan_exclusive_u64(cost, sp[c].start, N, A_, st_));
+            strcols.push_back(c);
+        }
+        for (size_t i0 = 0; i0 < strcols.size(); i0 += 20) {
+            size_t i1 = std::min(strcols.size(), i0 + 20);
+            for (size_t i = i0; i < i1; i++) {
+                const StrPlan& q = sp[strcols[i]];
+                int slot = int(3 * (i - i0));
+                if (N) stash_u64(ctx_, q.start + (N - 1), slot);
+                stash_u32(ctx_, q.stats, slot + 1);
+                stash_u32(ctx_, q.stats + 1, slot + 2);
+            }
+            stash_err(ctx_);
+            readback(ctx_, 0);
+            for (size_t i = i0; i < i1; i++) {
+                StrPlan& q = sp[strcols[i]];
+                int slot = int(3 * (i - i0));
+                uint64_t last_start = N ? ctx_->h_small[slot] : 0;
+                uint64_t maxc = ctx_->h_small[slot + 1];
+                bool has_long = ctx_->h_small[slot + 2] != 0;
+                // Floor packing while the longest string keeps pages at least ~87% full.
+                if (!has_long && maxc <= kStrPageUnits / 8) {
+                    q.floor = true;
+                    q.cp = kStrPageUnits - maxc;
+                    res.npages[strcols[i]] = N ? last_start / q.cp + 1 : 0;
+                }
+            }
+        }
+        for (size_t c : strcols) {
+            if (sp[c].floor) continue;
+            uint32_t j = ex_.out_slot[c];
             sp[c].nblocks = (N + kStrBlock - 1) / kStrBlock;
             uint32_t* bp = alloc<uint32_t>(sp[c].nblocks);
             sp[c].block_off = alloc<uint32_t>(sp[c].nblocks + 1);
@@ -710,9 +852,12 @@ class Executor {
                 launched(write_fixed_pages(fo.vals[j], fo.valid[j], N, t, rpp, pages, st_));
                 continue;
             }
-            const DevColumn& scol = src.s[j].kind == 0 ? src.s[j].col : col(ex_.pipelines.back().slots[j].attr);
+            const DevColumn& scol = col(ex_.pipelines.back().slots[j].attr);
             StrPageDesc* descs = alloc<StrPageDesc>(res.npages[c]);
-            launched(string_pack(sp[c].lens, fo.valid[j], N, 1, nullptr, sp[c].block_off, descs, st_));
+            if (sp[c].floor)
+                launched(string_floor_pages(sp[c].start, N, sp[c].cp, uint32_t(res.npages[c]), descs, st_));
+            else
+                launched(string_pack(sp[c].lens, fo.valid[j], N, 1, nullptr, sp[c].block_off, descs, st_));
             launched(write_string_pages(fo.vals[j], fo.valid[j], sp[c].lens, StrSource{scol}, descs,
                                         uint32_t(res.npages[c]), pages, ctx_->d_err, st_));
         }
@@ -901,6 +1046,7 @@ BJ_API int bj_context_create(int device, bj_context** out) {
         uint64_t threshold = ~0ull;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
     }
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     ctx->pool = std::make_unique<ThreadPool>(std::min(hw, 16u) - 1);
     *out = ctx.release();

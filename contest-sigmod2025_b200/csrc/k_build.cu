@@ -17,8 +17,9 @@
 //  2. bucket counts with atomicAdd, an exclusive scan, and a scatter of the
 //     representatives into their bucket's contiguous range (K4). The same
 //     bucket index as the reference: key_hash(key) >> shift.
-//  3. a blocked bloom filter, one 32-bit word per key with 4 bits set (K3);
-//     probes consult it before touching the buckets.
+//  3. a blocked bloom filter, one 32-bit word per key with 4 bits set (K3),
+//     at most 64 KiB so scans can stage it in shared memory; probes consult
+//     it before touching the buckets.
 #include "launch.h"
 
 namespace bj {
@@ -99,30 +100,31 @@ __global__ void k_bucket_scatter(TupleBuf t, const uint32_t* __restrict__ is_rep
     for (uint32_t j = 0; j < t.width; j++) dst[j] = src[j];
 }
 
-__global__ void k_bloom_build(const uint32_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ bloom,
-                              uint32_t log2w) {
+__global__ void k_bloom_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ mask, uint32_t n,
+                              uint32_t* __restrict__ bloom, uint32_t log2w) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    uint64_t g = mix64(keys[i]);
-    atomicOr(&bloom[bloom_word(g, log2w)], bloom_bits(g));
+    if (i >= n || (mask && !mask[i])) return;
+    uint64_t h = key_hash(keys[i]);
+    atomicOr(&bloom[bloom_word(h, log2w)], bloom_bits(h));
 }
 
-__global__ void k_ht_flags(HTView ht, uint32_t* __restrict__ flags) {
-    uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= ht.nentries) return;
-    if (ht.mult[e] > 1) flags[1] = 1;
-    uint32_t key = ht.keys[e];
-    uint32_t b = uint32_t(key_hash(key) >> ht.shift);
-    uint32_t s = ht.bucket_off[b];
-    if (e - s > 256) {
-        flags[0] = 1;  // long bucket: assume repeats (only steers capacity choices)
-        return;
-    }
-    for (uint32_t j = s; j < e; j++)
-        if (ht.keys[j] == key) {
-            flags[0] = 1;
-            return;
+__global__ void k_ht_flags(HTView ht, uint32_t nbuckets, uint32_t* __restrict__ flags) {
+    const uint32_t n = ht.bucket_off[nbuckets];  // entries actually stored
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        if (ht.mult[e] > 1) flags[1] = 1;
+        uint32_t key = ht.keys[e];
+        uint32_t b = uint32_t(key_hash(key) >> ht.shift);
+        uint32_t s = ht.bucket_off[b];
+        if (e - s > 256) {
+            flags[0] = 1;  // long bucket: assume repeats (only steers capacity choices)
+            continue;
         }
+        for (uint32_t j = s; j < e; j++)
+            if (ht.keys[j] == key) {
+                flags[0] = 1;
+                break;
+            }
+    }
 }
 
 __global__ void k_sample_probe(DevColumn key, uint32_t nsample, HTView ht, uint32_t* hits) {
@@ -164,17 +166,20 @@ int bucket_scatter(TupleBuf t, const uint32_t* is_rep, uint32_t shift, const uin
     return 1;
 }
 
-int bloom_build(const uint32_t* keys, uint32_t n, uint32_t* bloom, uint32_t log2w, cudaStream_t st) {
+int bloom_build(const uint32_t* keys, const uint32_t* mask, uint32_t n, uint32_t* bloom, uint32_t log2w,
+                cudaStream_t st) {
     cudaMemsetAsync(bloom, 0, sizeof(uint32_t) << log2w, st);
     if (!n) return 0;
-    k_bloom_build<<<(n + 255) / 256, 256, 0, st>>>(keys, n, bloom, log2w);
+    k_bloom_build<<<(n + 255) / 256, 256, 0, st>>>(keys, mask, n, bloom, log2w);
     return 1;
 }
 
-int ht_flags(HTView ht, uint32_t* flags, cudaStream_t st) {
+int ht_flags(HTView ht, uint32_t nbuckets, uint32_t* flags, int num_sms, cudaStream_t st) {
     cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), st);
     if (!ht.nentries) return 0;
-    k_ht_flags<<<(ht.nentries + 255) / 256, 256, 0, st>>>(ht, flags);
+    uint32_t blocks = (ht.nentries + 255) / 256;
+    if (blocks > uint32_t(num_sms) * 8) blocks = uint32_t(num_sms) * 8;
+    k_ht_flags<<<blocks, 256, 0, st>>>(ht, nbuckets, flags);
     return 1;
 }
 

@@ -287,7 +287,58 @@ __global__ void __launch_bounds__(256) k_write_string_pages(const uint64_t* __re
     store_page(page, out + size_t(blockIdx.x) * kPageSize);
 }
 
+// Parallel page assignment for VARCHAR columns ("floor packing"). Row i costs
+// 8 * (2 + len) + 1 eighth-bytes if non-null (offset, bytes, bitmap bit) or 1
+// if NULL. With S_i the exclusive prefix of costs, row i goes to page
+// floor(S_i / Cp), Cp = 65496 - max cost: a page then holds less than 65496
+// eighth-bytes, i.e. 4 + 2 nv + bytes + ceil(rows / 8) <= 8192, and consecutive
+// rows advance by at most one page, so no page is empty. Used when no string
+// is long (> PAGE_SIZE-7) and the longest is short enough to keep pages ~full.
+__global__ void k_string_cost(const uint32_t* __restrict__ lens, const uint8_t* __restrict__ valid, uint64_t n,
+                              uint64_t* __restrict__ cost, uint32_t* __restrict__ stats) {
+    uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    bool v = valid[i];
+    uint32_t len = v ? lens[i] : 0;
+    uint32_t c = v ? 8 * (2 + min(len, kPageSize)) + 1 : 1;
+    cost[i] = c;
+    atomicMax(&stats[0], c);
+    if (v && len > kMaxShort) stats[1] = 1;
+}
+
+__global__ void k_floor_first(const uint64_t* __restrict__ start, uint64_t n, uint64_t cp,
+                              StrPageDesc* __restrict__ descs) {
+    uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    uint64_t pg = start[i] / cp;
+    if (i == 0 || start[i - 1] / cp != pg) descs[pg].first_row = i;
+}
+
+__global__ void k_floor_desc(StrPageDesc* __restrict__ descs, uint32_t npages, uint64_t n) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npages) return;
+    uint64_t next = p + 1 < npages ? descs[p + 1].first_row : n;
+    descs[p].nrows = uint32_t(next - descs[p].first_row);
+    descs[p].chunk = 0xffffffffu;
+}
+
 } // namespace
+
+int string_cost(const uint32_t* lens, const uint8_t* valid, uint64_t n, uint64_t* cost, uint32_t* stats,
+                cudaStream_t st) {
+    cudaMemsetAsync(stats, 0, 2 * sizeof(uint32_t), st);
+    if (!n) return 0;
+    k_string_cost<<<unsigned((n + 255) / 256), 256, 0, st>>>(lens, valid, n, cost, stats);
+    return 1;
+}
+
+int string_floor_pages(const uint64_t* start, uint64_t n, uint64_t cp, uint32_t npages, StrPageDesc* descs,
+                       cudaStream_t st) {
+    if (!n || !npages) return 0;
+    k_floor_first<<<unsigned((n + 255) / 256), 256, 0, st>>>(start, n, cp, descs);
+    k_floor_desc<<<(npages + 255) / 256, 256, 0, st>>>(descs, npages, n);
+    return 2;
+}
 
 int write_fixed_pages(const uint64_t* vals, const uint8_t* valid, uint64_t n, int32_t type, uint32_t rpp,
                       uint8_t* out_pages, cudaStream_t st) {

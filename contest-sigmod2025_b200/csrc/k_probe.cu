@@ -5,15 +5,19 @@
 // target, multiplicity = product of the matched tuples' multiplicities,
 // :111-131) with stage kernels over item lists. An item is a row of the
 // scanned input plus the hash-table entry matched by every probe so far.
-// Each stage runs twice over the same tiles of 2048 items: once counting
-// matches per tile, once writing at the tile's offset (an exclusive scan of
-// the counts in between), so the output order is deterministic and no
-// capacity has to be guessed.
+// Against a table with unique keys a stage makes at most one item per input
+// item, so it runs once, appending with warp-aggregated atomics and reading
+// its input count on the device (no host round trip between stages).
+// Otherwise it runs twice over tiles of 256 items: once counting matches per
+// tile, once writing at the tile's offset (an exclusive scan of the counts in
+// between).
 //
 // The probe itself follows HashtableProbe::operator() (engine/op/Hashtable.hpp:
 // 228-241): hash the 32-bit key, find its bucket, compare every key in the
 // bucket. Buckets here are contiguous runs of entries (CSR), not chains.
 #include "launch.h"
+
+#include <algorithm>
 
 namespace bj {
 namespace {
@@ -112,6 +116,49 @@ __global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HT
     }
 }
 
+// Unique-key probe stage: persistent grid-stride loop, at most one match per
+// item, warp-aggregated reservation of output slots.
+__global__ void __launch_bounds__(256) k_probe_unique(Items in, DevColumn key, HTView ht, ItemsOut out,
+                                                      uint32_t* cursor, uint32_t capacity, int use_bloom,
+                                                      uint32_t* err) {
+    const uint32_t n = in.dcount ? *in.dcount : in.count;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t lane = threadIdx.x & 31;
+    // Whole warps iterate together so the ballot sees every lane.
+    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
+        uint32_t i = base + lane;
+        bool hit = false;
+        uint32_t row = 0, e = 0;
+        if (i < n) {
+            row = item_row(in, i);
+            uint64_t v;
+            if (row >= key.nrows) {
+                record_error(err, kErrRowRange);
+            } else if (col_get(key, row, v)) {
+                for_matches(ht, uint32_t(v), use_bloom != 0, [&](uint32_t j) {
+                    if (!hit) e = j;
+                    hit = true;
+                });
+            }
+        }
+        uint32_t mask = __ballot_sync(0xffffffffu, hit);
+        if (!mask) continue;
+        uint32_t wbase = 0;
+        if (lane == 0) wbase = atomicAdd(cursor, __popc(mask));
+        wbase = __shfl_sync(0xffffffffu, wbase, 0);
+        if (!hit) continue;
+        uint32_t o = wbase + __popc(mask & ((1u << lane) - 1));
+        if (o >= capacity) {
+            record_error(err, kErrCapacity);
+            continue;
+        }
+        out.rows[o] = row;
+        for (int p = 0; p < in.nprobes; p++) out.ents[p][o] = in.ents[p][i];
+        out.ents[in.nprobes][o] = e;
+        if (out.mult) out.mult[o] = item_mult(in, i) * ht.mult[e];
+    }
+}
+
 // Value of one slot for item i (row `row`): returns false for NULL.
 __device__ __forceinline__ bool slot_value(const SlotSource& s, const Items& in, uint32_t i, uint32_t row,
                                            const ProbeSet& ps, uint64_t& v) {
@@ -182,6 +229,14 @@ int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mod
         k_probe_stage<0><<<tiles, 256, 0, st>>>(in, key, ht, tile_counts, tile_offsets, out, use_bloom, err);
     else
         k_probe_stage<1><<<tiles, 256, 0, st>>>(in, key, ht, tile_counts, tile_offsets, out, use_bloom, err);
+    return 1;
+}
+
+int probe_stage_unique(const Items& in, const DevColumn& key, const HTView& ht, ItemsOut out, uint32_t* cursor,
+                       uint32_t capacity, bool use_bloom, uint32_t* err, int num_sms, cudaStream_t st) {
+    if (!in.count) return 0;
+    uint32_t blocks = std::min<uint32_t>((in.count + 255) / 256, uint32_t(num_sms) * 8);
+    k_probe_unique<<<blocks, 256, 0, st>>>(in, key, ht, out, cursor, capacity, use_bloom, err);
     return 1;
 }
 

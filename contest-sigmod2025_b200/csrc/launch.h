@@ -49,21 +49,30 @@ struct Items {
     const uint32_t* rows;                // null: implicit rows 0..count-1
     const uint32_t* ents[kMaxProbes];
     const uint64_t* mult;                // null: all 1
-    uint32_t count;
+    uint32_t count;                      // item count, or an upper bound when dcount is set
     int nprobes;
+    const uint32_t* dcount;              // device-side item count (null: `count` is exact)
 };
 struct ItemsOut {
     uint32_t* rows;
     uint32_t* ents[kMaxProbes];
     uint64_t* mult;
 };
-constexpr uint32_t kTile = 2048;  // items per CTA tile in stage kernels
+constexpr uint32_t kTile = 256;  // items per CTA tile in stage kernels (one per thread)
 
 // Probe stage: for each item, read the key `key` at its row, probe `ht`,
 // and emit one item per matching entry. mode 0 counts matches per tile into
 // tile_counts; mode 1 writes items at tile_offsets (exclusive scan of counts).
 int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mode, uint32_t* tile_counts,
                 const uint32_t* tile_offsets, ItemsOut out, bool use_bloom, uint32_t* err, cudaStream_t st);
+
+// Probe stage against a table with unique keys (at most one match per item):
+// a persistent grid-stride pass appends items with warp-aggregated atomics at
+// *cursor; reads the input count from in.dcount when set, so no host
+// round trip is needed between stages. out.mult may be null when both the
+// input and the table carry only multiplicity 1.
+int probe_stage_unique(const Items& in, const DevColumn& key, const HTView& ht, ItemsOut out, uint32_t* cursor,
+                       uint32_t capacity, bool use_bloom, uint32_t* err, int num_sms, cudaStream_t st);
 
 // Source of one value slot: a column of the scanned input read at the item's
 // row, or payload slot `slot` of the entry matched by probe `probe`.
@@ -105,6 +114,17 @@ int emit_output(const Items& in, const uint64_t* out_off, const SlotSources& src
 // mult of implicit/explicit items as a u64 array (for the scan of output offsets)
 int items_mult(const Items& in, uint64_t* mult_out, cudaStream_t st);
 
+// ---- scan-side probe stage (k_scan.cu) ----
+// Streams the pages of `key` (a column of the scanned table) through shared
+// memory and probes `ht`. mode 0: per-page match counts into page_counts;
+// mode 1: items written at page_off[p]; mode 2: items appended at *cursor
+// (requires at most one match per row). bloom_smem: test ht.bloom, staged in
+// shared memory (ignored if larger than scan_probe_bloom_limit()).
+size_t scan_probe_bloom_limit();
+int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem, uint32_t* page_counts,
+               const uint32_t* page_off, uint32_t* cursor, uint32_t* out_rows, uint32_t* out_ents, uint64_t* out_mult,
+               uint32_t capacity, uint32_t* err, int num_sms, cudaStream_t st);
+
 // ---- hash table build (k_build.cu) ----
 struct BuildResult {
     uint32_t nentries;
@@ -118,9 +138,12 @@ int aggregate_tuples(TupleBuf t, uint32_t* slot_table, uint32_t table_log2, uint
 int bucket_count(TupleBuf t, const uint32_t* is_rep, uint32_t shift, uint32_t* counts, cudaStream_t st);
 int bucket_scatter(TupleBuf t, const uint32_t* is_rep, uint32_t shift, const uint32_t* bucket_off, uint32_t* cursor,
                    HTView ht_mut, uint32_t* err, cudaStream_t st);
-int bloom_build(const uint32_t* keys, uint32_t n, uint32_t* bloom, uint32_t log2w, cudaStream_t st);
+// Bloom filter over keys[i] for every i with mask[i] != 0 (mask may be null).
+int bloom_build(const uint32_t* keys, const uint32_t* mask, uint32_t n, uint32_t* bloom, uint32_t log2w,
+                cudaStream_t st);
 // Flags of a built table: [0] = 1 if some key repeats, [1] = 1 if some mult > 1.
-int ht_flags(HTView ht, uint32_t* flags, cudaStream_t st);
+// The entry count is read on the device from bucket_off[nbuckets].
+int ht_flags(HTView ht, uint32_t nbuckets, uint32_t* flags, int num_sms, cudaStream_t st);
 // Counts, for n sampled rows of `key` (evenly spaced), how many hit `ht`.
 int sample_probe(const DevColumn& key, uint32_t nsample, HTView ht, uint32_t* hits, cudaStream_t st);
 
@@ -144,6 +167,14 @@ struct StrPageDesc {
 };
 int string_pack(const uint32_t* lens, const uint8_t* valid, uint64_t n, int pass, uint32_t* block_pages,
                 const uint32_t* block_page_off, StrPageDesc* descs, cudaStream_t st);
+// Parallel packing: per-row costs (stats[0] = max cost, stats[1] = 1 if some
+// string is longer than PAGE_SIZE-7), then page descriptors from the
+// exclusive scan `start` of the costs for page capacity cp.
+constexpr uint64_t kStrPageUnits = 65496;  // eighth-bytes a page may hold
+int string_cost(const uint32_t* lens, const uint8_t* valid, uint64_t n, uint64_t* cost, uint32_t* stats,
+                cudaStream_t st);
+int string_floor_pages(const uint64_t* start, uint64_t n, uint64_t cp, uint32_t npages, StrPageDesc* descs,
+                       cudaStream_t st);
 int write_string_pages(const uint64_t* handles, const uint8_t* valid, const uint32_t* lens, StrSource src,
                        const StrPageDesc* descs, uint32_t npages, uint8_t* out_pages, uint32_t* err, cudaStream_t st);
 
