@@ -14,8 +14,10 @@ One step = one execution of the query.
           result pages left in HBM), timed with CUDA events on the engine's
           stream, max over ranks, all ranks' queries / time.
   e2e   : queries/s through the drop-in path (bj_execute: host pages in,
-          host pages out), host->device page copies and the device->host copy
-          of the result pages inside the timed region.
+          host pages out), with the input pages in pinned host memory (read in
+          place by the kernels over the host link) and the device->host copy of
+          the result pages inside the timed region. e2e_pageable is the same
+          with pageable input pages (staged and copied to HBM every step).
   roofline: the scan-side probe stage (the kernel that streams the fact's key
           pages), its page bytes per launch / its CUDA-event duration, against
           the measured HBM copy bandwidth.
@@ -241,25 +243,44 @@ def main():
     elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1))
     value = args.steps * world / (elapsed_ms / 1e3)
 
-    # ---- e2e: drop-in path, host pages in and out ----
+    # ---- e2e: drop-in path (bj_execute), host pages in and out ----
     e2e_steps = args.e2e_steps or max(3, min(args.steps, 20))
-    for _ in range(2):
-        ctx.execute_raw(plan).free()
-    barrier()
-    h2d = d2h = 0
-    e2e_lat = []
-    ev0.record(stream)
-    for _ in range(e2e_steps):
-        t0 = time.perf_counter()
-        r = ctx.execute_raw(plan)
-        e2e_lat.append((time.perf_counter() - t0) * 1e3)
-        s = r.stats()
-        h2d, d2h = s.h2d_bytes, s.d2h_bytes
-        r.free()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    e2e_value = e2e_steps * world / (e2e_ms / 1e3)
+
+    def e2e_run():
+        for _ in range(2):
+            ctx.execute_raw(plan).free()
+        barrier()
+        stats, lat_ms = None, []
+        ev0.record(stream)
+        for _ in range(e2e_steps):
+            t0 = time.perf_counter()
+            r = ctx.execute_raw(plan)
+            lat_ms.append((time.perf_counter() - t0) * 1e3)
+            stats = r.stats()
+            r.free()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(ev0.elapsed_time(ev1))
+        return e2e_steps * world / (ms / 1e3), stats, lat_ms
+
+    # (a) pages in pageable memory: gathered into pinned staging and copied.
+    pageable_value, pageable_stats, pageable_lat = e2e_run()
+    # (b) pages in pinned host memory (registered once, outside the timed
+    # region, as a serving process keeps its host tables): read in place.
+    registered = []
+    for i in range(inputs.num_inputs):
+        t = inputs.inputs[i]
+        for c in range(t.num_columns):
+            col = t.columns[c]
+            if col.num_pages:
+                ptr, size = col.pages[0], col.num_pages * pkg.PAGE_SIZE
+                if torch._C._cudart.cudaHostRegister(ptr, size, 3) == 0:  # portable | mapped
+                    registered.append(ptr)
+    e2e_value, e2e_stats, e2e_lat = e2e_run()
+    for ptr in registered:
+        torch._C._cudart.cudaHostUnregister(ptr)
+    h2d = e2e_stats.h2d_bytes + e2e_stats.mapped_input_bytes
+    d2h = e2e_stats.d2h_bytes
 
     for x in residents:
         x.free()
@@ -282,7 +303,13 @@ def main():
         "scan_bytes_per_query": w.scan_bytes(),
         "input_gbs": w.scan_bytes() * value / world / 1e9,
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "p50_ms": statistics.median(e2e_lat)},
+                "p50_ms": statistics.median(e2e_lat),
+                "inputs": "pinned host pages read in place by the kernels (h2d = page bytes available to them)",
+                "dma_bytes_per_step": e2e_stats.h2d_bytes, "mapped_bytes_per_step": e2e_stats.mapped_input_bytes},
+        "e2e_pageable": {"value": pageable_value, "unit": "queries/s", "p50_ms": statistics.median(pageable_lat),
+                         "h2d_bytes_per_step": pageable_stats.h2d_bytes,
+                         "d2h_bytes_per_step": pageable_stats.d2h_bytes,
+                         "inputs": "pageable host pages, gathered into pinned staging and copied to HBM"},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "traffic": traffic,

@@ -21,6 +21,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <memory>
@@ -243,6 +244,7 @@ struct bj_context {
     uint64_t live_results = 0;
     int num_sms = 148;
     bool profile = false;
+    bool zero_copy = true;  // read pinned, contiguous input columns in place
     std::vector<cudaEvent_t> prof_events;  // pairs around timed launches
     uint64_t prof_bytes = 0;
 
@@ -319,18 +321,40 @@ void stash_err(bj_context* ctx) {
 // Page upload and indexing.
 
 struct ColumnJob {
-    const bj_column* src;  // host pages (null for already-resident pages)
-    uint8_t* dpages;       // device destination
+    const bj_column* src;  // host pages
+    uint8_t* dpages;       // device-accessible address of the pages
     uint64_t rows;         // rows the table claims
     DevColumn* out;
+    bool in_place = false; // pages are read where they are (pinned host memory): no copy
 };
+
+// Device address of a column whose pages lie back to back in one pinned,
+// mapped host allocation; nullptr otherwise (pageable pages are copied).
+uint8_t* mapped_base(const bj_column& hc) {
+    if (!hc.num_pages || !hc.pages || !hc.pages[0]) return nullptr;
+    const uint8_t* p0 = static_cast<const uint8_t*>(hc.pages[0]);
+    for (uint64_t k = 1; k < hc.num_pages; k++)
+        if (hc.pages[k] != p0 + k * kPageSize) return nullptr;
+    cudaPointerAttributes a0{}, a1{};
+    if (cudaPointerGetAttributes(&a0, p0) != cudaSuccess ||
+        cudaPointerGetAttributes(&a1, p0 + hc.num_pages * kPageSize - 1) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a0.type != cudaMemoryTypeHost || a1.type != cudaMemoryTypeHost || !a0.devicePointer || !a1.devicePointer)
+        return nullptr;
+    uint8_t* d0 = static_cast<uint8_t*>(a0.devicePointer);
+    if (static_cast<uint8_t*>(a1.devicePointer) != d0 + hc.num_pages * kPageSize - 1) return nullptr;
+    return d0;
+}
 
 // Copies host pages into `dst` on the device: pages are gathered into pinned
 // staging by the thread pool, chunk by chunk, each chunk's DMA overlapping
 // the next chunk's gathering.
 uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs) {
     uint64_t total = 0;
-    for (auto& j : jobs) total += j.src->num_pages;
+    for (auto& j : jobs)
+        if (!j.in_place) total += j.src->num_pages;
     if (!total) return 0;
     size_t bytes = total * kPageSize;
     if (ctx->stage.size < bytes) {
@@ -358,6 +382,7 @@ uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs) {
     all.reserve(total);
     for (size_t ji = 0; ji < jobs.size(); ji++) {
         const ColumnJob& j = jobs[ji];
+        if (j.in_place) continue;
         for (uint64_t p = 0; p < j.src->num_pages; p++) {
             if (!j.src->pages[p]) throw Fail{BJ_ERR_INVALID, "null page pointer"};
             all.push_back(Src{j.src->pages[p], j.dpages + p * kPageSize, ji});
@@ -941,9 +966,14 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
                     const bj_column& hc = t.columns[c];
                     if (hc.num_pages && !hc.pages) throw Fail{BJ_ERR_INVALID, "column without page array"};
                     d.cols[c].type = hc.type;
+                    res->stats.input_pages += hc.num_pages;
+                    if (uint8_t* mapped = ctx->zero_copy ? mapped_base(hc) : nullptr) {
+                        jobs.push_back(ColumnJob{&hc, mapped, t.num_rows, &d.cols[c], true});
+                        res->stats.mapped_input_bytes += hc.num_pages * kPageSize;
+                        continue;
+                    }
                     uint8_t* dp = static_cast<uint8_t*>(ctx->arena.alloc(std::max<uint64_t>(hc.num_pages, 1) * kPageSize));
                     jobs.push_back(ColumnJob{&hc, dp, t.num_rows, &d.cols[c]});
-                    res->stats.input_pages += hc.num_pages;
                 }
             }
             if (!ex.empty) {
@@ -1047,6 +1077,7 @@ BJ_API int bj_context_create(int device, bj_context** out) {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
     }
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (const char* zc = std::getenv("B200JOIN_ZERO_COPY")) ctx->zero_copy = std::atoi(zc) != 0;
     unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     ctx->pool = std::make_unique<ThreadPool>(std::min(hw, 16u) - 1);
     *out = ctx.release();

@@ -122,6 +122,7 @@ typedef struct bj_stats {
     double scan_kernel_ms;      /* summed duration of its launches */
     uint64_t scan_kernel_launches;
     uint64_t scan_kernel_bytes; /* page bytes those launches had to read */
+    uint64_t mapped_input_bytes; /* input page bytes read in place from pinned host memory */
 } bj_stats;
 
 /* Replaces Contest::build_context (engine/Execute.cpp:42-46). Creates the CUDA
@@ -138,7 +139,13 @@ BJ_API const char* bj_last_error(const bj_context* ctx);
 /* Replaces Contest::execute (engine/Execute.cpp:28-40): runs `plan` on its host
  * input pages and returns the joined rows as host pages. The result's row
  * multiset equals the reference engine's; row order and page packing are free
- * (the contest harnesses sort rows before comparing, tests/read_sql.cpp:1208-1213). */
+ * (the contest harnesses sort rows before comparing, tests/read_sql.cpp:1208-1213).
+ *
+ * Input pages in pageable memory are gathered into pinned staging and copied
+ * to HBM. A column whose pages lie back to back in one pinned, mapped host
+ * allocation (cudaHostAlloc / cudaHostRegister) is instead read in place by
+ * the kernels over the host link, so only the bytes a query touches cross it
+ * (set B200JOIN_ZERO_COPY=0 to always copy). */
 BJ_API int bj_execute(bj_context* ctx, const bj_plan* plan, bj_result** out);
 
 /* Resident tables (no reference counterpart: the reference re-reads host pages

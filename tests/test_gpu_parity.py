@@ -168,3 +168,31 @@ def test_empty_and_single_table_plans(pkg, ctx, oracle):
     plan.new_scan_node(0, [(2, pkg.FP64), (0, pkg.INT32), (1, pkg.VARCHAR)])
     plan.root = 0
     check_against_oracle(pkg, ctx, oracle, pkg.CPlan(plan), "lone scan")
+
+
+@pytest.mark.parametrize("name,seed,scale", [("join2", 5, 0.05), ("snowflake", 6, 0.05)])
+def test_pinned_inputs_read_in_place(pkg, ctx, oracle, name, seed, scale):
+    """Columns in pinned host memory are read in place (no staging copy) and
+    give the same rows."""
+    import torch
+
+    w = pkg.Workload(name, seed, scale)
+    plan = w.plan_ptr().contents
+    regs = []
+    for i in range(plan.num_inputs):
+        t = plan.inputs[i]
+        for c in range(t.num_columns):
+            col = t.columns[c]
+            if col.num_pages:
+                assert torch._C._cudart.cudaHostRegister(col.pages[0], col.num_pages * pkg.PAGE_SIZE, 3) == 0
+                regs.append(col.pages[0])
+    try:
+        with ctx.execute_raw(w.plan_ptr()) as r:
+            st = r.stats()
+            assert st.mapped_input_bytes > 0 and st.h2d_bytes == 0
+            got, keep = r.table_struct()
+            want = oracle.execute(w.plan_ptr())
+            oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), f"{name} pinned")
+    finally:
+        for p in regs:
+            torch._C._cudart.cudaHostUnregister(p)
