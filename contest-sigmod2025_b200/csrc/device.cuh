@@ -4,6 +4,8 @@
 // to back (page p at pages + p * 8192). Nothing is decoded ahead of time: the
 // kernels read values straight out of the pages, helped by three small index
 // arrays built once per column (k_pages.cu):
+//   hdr[p]           page p's header (row count, non-null count), so row
+//                    lookups never touch the page for it
 //   row_start[p]     first row of page p (exclusive prefix of contained rows)
 //   page_of_blk[b]   page holding row b * 1024 (shortcut for the page search)
 //   dense_base[c]    non-null values before 64-row chunk c of a page, with
@@ -42,6 +44,7 @@ enum DevError : uint32_t {
 
 struct DevColumn {
     const uint8_t* pages;
+    const uint32_t* hdr;          // npages: each page's first 4 bytes (row count | non-null count << 16)
     const uint32_t* row_start;    // npages + 1
     const uint32_t* page_of_blk;  // (nrows >> kBlkShift) + 1
     const uint32_t* dense_base;   // per 64-row chunk
@@ -95,12 +98,13 @@ __device__ __forceinline__ bool col_get(const DevColumn& c, uint32_t row, uint64
     uint32_t p = locate_page(c, row);
     uint32_t i = row - c.row_start[p];
     const uint8_t* pg = c.pages + size_t(p) * kPageSize;
-    uint32_t nrows = ld16(pg);
+    const uint32_t h = c.hdr[p];  // header from the device-side cache (pages may be in host memory)
+    uint32_t nrows = h & 0xffff;
     if (c.type == kVarchar && nrows >= 0xfffe) {
         v = make_str_handle(p, 0xffff);
         return true;
     }
-    uint32_t nn = ld16(pg + 2);
+    uint32_t nn = h >> 16;
     uint32_t dense = i;
     if (nn != nrows) {
         uint32_t nbytes = (nrows + 7) >> 3;
@@ -153,6 +157,12 @@ BJ_HD uint32_t bloom_mask(uint32_t idx) {
     return (1u << (g & 31)) | (1u << ((g >> 5) & 31)) | (1u << ((g >> 10) & 31)) | (1u << ((g >> 15) & 31));
 }
 BJ_HD uint32_t bloom_mask_index(uint64_t h) { return uint32_t(h >> 32) & (kBloomMasks - 1); }
+// High 32 bits of key_hash(key) (all the bloom filter uses), in two multiplies.
+#if defined(__CUDACC__)
+__device__ __forceinline__ uint32_t key_hash_hi(uint32_t key) {
+    return __umulhi(key, 0x7F4A7C15u) + key * 0x9E3779B9u;
+}
+#endif
 BJ_HD uint32_t bloom_bits(uint64_t h) { return bloom_mask(bloom_mask_index(h)); }
 BJ_HD uint32_t bloom_word(uint64_t h, uint32_t log2_words) {
     return log2_words ? uint32_t(h >> (64 - log2_words)) : 0u;

@@ -245,6 +245,26 @@ struct bj_context {
     int num_sms = 148;
     bool profile = false;
     bool zero_copy = true;  // read pinned, contiguous input columns in place
+    static constexpr int kSideStreams = 4;
+    cudaStream_t side[kSideStreams] = {};  // independent build pipelines run here
+    std::vector<cudaEvent_t> pipe_events;  // one per pipeline, reused across calls
+
+    cudaEvent_t pipe_event(size_t i) {
+        while (pipe_events.size() <= i) {
+            cudaEvent_t e;
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+            pipe_events.push_back(e);
+        }
+        return pipe_events[i];
+    }
+    void sync_all() {
+        cudaStreamSynchronize(stream);
+        for (cudaStream_t s : side)
+            if (s) cudaStreamSynchronize(s);
+    }
     std::vector<cudaEvent_t> prof_events;  // pairs around timed launches
     uint64_t prof_bytes = 0;
 
@@ -330,8 +350,13 @@ struct ColumnJob {
 
 // Device address of a column whose pages lie back to back in one pinned,
 // mapped host allocation; nullptr otherwise (pageable pages are copied).
+// Columns smaller than this are copied even from pinned memory: a copy is
+// cheap, while reading them in place would pay a host-link round trip per
+// random access.
+constexpr uint64_t kInPlaceMinPages = 2048;  // 16 MiB
+
 uint8_t* mapped_base(const bj_column& hc) {
-    if (!hc.num_pages || !hc.pages || !hc.pages[0]) return nullptr;
+    if (hc.num_pages < kInPlaceMinPages || !hc.pages || !hc.pages[0]) return nullptr;
     const uint8_t* p0 = static_cast<const uint8_t*>(hc.pages[0]);
     for (uint64_t k = 1; k < hc.num_pages; k++)
         if (hc.pages[k] != p0 + k * kPageSize) return nullptr;
@@ -423,6 +448,7 @@ void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem) 
         uint32_t np = uint32_t(jobs[i].src ? jobs[i].src->num_pages : 0);
         Tmp& t = tmp[i];
         t.npages = np;
+        t.b.hdr = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
         t.b.rows = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
         t.b.chunks = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
         t.b.row_start = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * (np + 1)));
@@ -458,6 +484,7 @@ void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem) 
         c.npages = tmp[i].npages;
         c.nrows = uint32_t(rows[i]);
         c.flags = uint32_t(flags[i]);
+        c.hdr = tmp[i].b.hdr;
         c.row_start = tmp[i].b.row_start;
         c.chunk_base = tmp[i].b.chunk_base;
         uint32_t* dense = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * std::max<uint64_t>(chunks[i], 1)));
@@ -465,7 +492,8 @@ void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem) 
         uint32_t* pob = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * nblk));
         c.dense_base = dense;
         c.page_of_blk = pob;
-        ctx->launches += page_index_pass2(c.pages, c.npages, c.nrows, c.row_start, c.chunk_base, dense, pob, ctx->stream);
+        ctx->launches += page_index_pass2(c.pages, c.hdr, c.npages, c.nrows, c.row_start, c.chunk_base, dense, pob,
+                                          ctx->stream);
     }
 }
 
@@ -492,13 +520,40 @@ class Executor {
     Executor(bj_context* ctx, const ExecPlan& ex, std::vector<const DevTable*> tables)
         : ctx_(ctx), ex_(ex), tables_(std::move(tables)), st_(ctx->stream), A_(ctx->arena) {}
 
-    // Runs every pipeline; returns false if the result is empty.
+    // Runs every pipeline; returns false if the result is empty. Pipelines
+    // without probes (leaf builds) need no host round trip, so they run on
+    // side streams and overlap; a pipeline that probes waits for its
+    // children's events and runs on the main stream.
     bool run(bj_result& res, int flags) {
-        hts_.resize(ex_.pipelines.size());
-        for (size_t p = 0; p + 1 < ex_.pipelines.size(); p++) {
-            if (!run_pipeline(p, nullptr, 0)) return false;
+        const size_t np = ex_.pipelines.size();
+        hts_.resize(np);
+        cudaStream_t main = ctx_->stream;
+        cudaEvent_t start = ctx_->pipe_event(np);
+        if (!start) throw Fail{BJ_ERR_CUDA, "event creation failed"};
+        BJ_CK(cudaEventRecord(start, main));
+        int next_side = 0;
+        for (size_t p = 0; p < np; p++) {
+            const PipelinePlan& pp = ex_.pipelines[p];
+            bool leaf = pp.probes.empty() && p + 1 < np;
+            cudaEvent_t done = ctx_->pipe_event(p);
+            if (!done) throw Fail{BJ_ERR_CUDA, "event creation failed"};
+            if (leaf) {
+                st_ = ctx_->side[next_side++ % bj_context::kSideStreams];
+                BJ_CK(cudaStreamWaitEvent(st_, start, 0));
+            } else {
+                st_ = main;
+                for (const auto& pr : pp.probes) BJ_CK(cudaStreamWaitEvent(main, ctx_->pipe_event(pr.child), 0));
+            }
+            bool ok = p + 1 < np ? run_pipeline(p, nullptr, 0) : run_pipeline(p, &res, flags);
+            BJ_CK(cudaEventRecord(done, st_));
+            if (!ok) {
+                st_ = main;
+                for (size_t q = 0; q <= p; q++) BJ_CK(cudaStreamWaitEvent(main, ctx_->pipe_event(q), 0));
+                return false;
+            }
         }
-        return run_pipeline(ex_.pipelines.size() - 1, &res, flags);
+        st_ = main;
+        return true;
     }
     uint64_t pipelines_run() const { return pipes_; }
 
@@ -916,8 +971,8 @@ int fail_to_status(bj_context* ctx, const Fail& f) {
     for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
     ctx->prof_events.clear();
     ctx->prof_bytes = 0;
-    // Leave the stream idle and the arena reusable after a failure.
-    cudaStreamSynchronize(ctx->stream);
+    // Leave every stream idle and the arena reusable after a failure.
+    ctx->sync_all();
     cudaGetLastError();
     uint32_t zero = 0;
     cudaMemcpy(ctx->d_err, &zero, sizeof(zero), cudaMemcpyHostToDevice);
@@ -1063,6 +1118,8 @@ BJ_API int bj_context_create(int device, bj_context** out) {
     auto ctx = std::make_unique<bj_context>();
     ctx->device = device;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return BJ_ERR_CUDA;
+    for (auto& s : ctx->side)
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return BJ_ERR_CUDA;
     if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) return BJ_ERR_CUDA;
     if (cudaMalloc(&ctx->d_err, 256) != cudaSuccess) return BJ_ERR_OOM;
     if (cudaMalloc(&ctx->d_small, sizeof(uint64_t) * 64) != cudaSuccess) return BJ_ERR_OOM;
@@ -1087,7 +1144,10 @@ BJ_API int bj_context_create(int device, bj_context** out) {
 BJ_API void bj_context_destroy(bj_context* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
+    ctx->sync_all();
+    for (cudaEvent_t e : ctx->pipe_events) cudaEventDestroy(e);
+    for (cudaStream_t s : ctx->side)
+        if (s) cudaStreamDestroy(s);
     for (auto& b : ctx->pinned_free) cudaFreeHost(b.p);
     if (ctx->stage.p) cudaFreeHost(ctx->stage.p);
     if (ctx->h_small) cudaFreeHost(ctx->h_small);

@@ -15,12 +15,15 @@ namespace bj {
 namespace {
 
 __global__ void k_page_headers(const uint8_t* __restrict__ pages, uint32_t npages, int32_t type,
-                               uint32_t* __restrict__ rows, uint32_t* __restrict__ chunks,
-                               uint32_t* __restrict__ flags, uint32_t* __restrict__ err) {
+                               uint32_t* __restrict__ hdr, uint32_t* __restrict__ rows,
+                               uint32_t* __restrict__ chunks, uint32_t* __restrict__ flags,
+                               uint32_t* __restrict__ err) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npages) return;
     const uint8_t* pg = pages + size_t(p) * kPageSize;
-    uint32_t n = ld16(pg), nn = ld16(pg + 2);
+    const uint32_t h = *reinterpret_cast<const uint32_t*>(pg);
+    hdr[p] = h;
+    uint32_t n = h & 0xffff, nn = h >> 16;
     uint32_t r = n, c = (n + 63) >> 6;
     uint32_t f = 0;
     if (type == kVarchar && n >= 0xfffe) {
@@ -29,7 +32,7 @@ __global__ void k_page_headers(const uint8_t* __restrict__ pages, uint32_t npage
         c = 0;
         f |= 2;
         if (nn > kPageSize - 4) record_error(err, kErrLongString);
-        if (n == 0xfffe && (p == 0 || ld16(pg - kPageSize) < 0xfffe)) record_error(err, kErrLongString);
+        if (n == 0xfffe && (p == 0 || ld16(pages + size_t(p - 1) * kPageSize) < 0xfffe)) record_error(err, kErrLongString);
     } else {
         // Every later read of this page (values by dense index, string offsets)
         // stays inside it once these hold: bitmap and header fit, the bitmap's
@@ -74,7 +77,7 @@ __global__ void k_page_headers(const uint8_t* __restrict__ pages, uint32_t npage
 
 // One warp per page: dense base of each 64-row chunk (a running popcount of
 // the page's null bitmap).
-__global__ void k_page_dense(const uint8_t* __restrict__ pages, uint32_t npages,
+__global__ void k_page_dense(const uint8_t* __restrict__ pages, const uint32_t* __restrict__ hdr, uint32_t npages,
                              const uint32_t* __restrict__ chunk_base, uint32_t* __restrict__ dense_base) {
     uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t lane = threadIdx.x & 31;
@@ -83,7 +86,7 @@ __global__ void k_page_dense(const uint8_t* __restrict__ pages, uint32_t npages,
     uint32_t c0 = chunk_base[p], nc = chunk_base[p + 1] - c0;
     if (!nc) return;
     const uint8_t* pg = pages + size_t(p) * kPageSize;
-    uint32_t n = ld16(pg), nn = ld16(pg + 2);
+    uint32_t n = hdr[p] & 0xffff, nn = hdr[p] >> 16;
     uint32_t nbytes = (n + 7) >> 3;
     const uint8_t* bm = pg + kPageSize - nbytes;
     uint32_t carry = 0;
@@ -142,7 +145,8 @@ int page_index_pass1(const uint8_t* pages, uint32_t npages, int32_t type, PageIn
     int launches = 0;
     cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), st);
     if (npages) {
-        k_page_headers<<<(npages + 255) / 256, 256, 0, st>>>(pages, npages, type, b.rows, b.chunks, b.flags, err);
+        k_page_headers<<<(npages + 255) / 256, 256, 0, st>>>(pages, npages, type, b.hdr, b.rows, b.chunks, b.flags,
+                                                             err);
         launches++;
     }
     launches += scan_exclusive_u32(b.rows, b.row_start, npages, s, st);
@@ -150,11 +154,12 @@ int page_index_pass1(const uint8_t* pages, uint32_t npages, int32_t type, PageIn
     return launches;
 }
 
-int page_index_pass2(const uint8_t* pages, uint32_t npages, uint32_t nrows, const uint32_t* row_start,
-                     const uint32_t* chunk_base, uint32_t* dense_base, uint32_t* page_of_blk, cudaStream_t st) {
+int page_index_pass2(const uint8_t* pages, const uint32_t* hdr, uint32_t npages, uint32_t nrows,
+                     const uint32_t* row_start, const uint32_t* chunk_base, uint32_t* dense_base,
+                     uint32_t* page_of_blk, cudaStream_t st) {
     int launches = 0;
     if (npages) {
-        k_page_dense<<<(npages * 32 + 255) / 256, 256, 0, st>>>(pages, npages, chunk_base, dense_base);
+        k_page_dense<<<(npages * 32 + 255) / 256, 256, 0, st>>>(pages, hdr, npages, chunk_base, dense_base);
         launches++;
     }
     uint32_t nblk = (nrows >> kBlkShift) + 2;

@@ -165,11 +165,13 @@ __device__ __forceinline__ void push4(const ScanArgs& a, WarpState& w, uint32_t 
     w.n += total;
 }
 
-__device__ __forceinline__ bool bloom_pass(const uint32_t* bloom, const uint32_t* masks, uint32_t log2w,
+// Bloom test with the high half of the key hash: the mask index is its low
+// 11 bits (bits 32-42 of the hash), the word its top log2w bits.
+__device__ __forceinline__ bool bloom_pass(const uint32_t* bloom, const uint32_t* masks, uint32_t wshift,
                                            uint32_t key) {
-    uint64_t h = key_hash(key);
-    uint32_t m = masks[bloom_mask_index(h)];
-    return (bloom[bloom_word(h, log2w)] & m) == m;
+    uint32_t hh = key_hash_hi(key);
+    uint32_t m = masks[hh & (kBloomMasks - 1)];
+    return (bloom[hh >> wshift] & m) == m;
 }
 
 __global__ void __launch_bounds__(kCtaThreads, 2) k_scan_probe(ScanArgs a) {
@@ -189,7 +191,7 @@ __global__ void __launch_bounds__(kCtaThreads, 2) k_scan_probe(ScanArgs a) {
     const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
     const uint32_t total_warps = gridDim.x * kWarpsPerCta;
     WarpState w{bufs[warp], 0, 0};
-    const uint32_t log2w = a.ht.bloom_log2;
+    const uint32_t wshift = 32 - a.ht.bloom_log2;  // bloom_log2 >= 5 whenever the bloom is used
 
     for (uint32_t p = blockIdx.x * kWarpsPerCta + warp; p < a.key.npages; p += total_warps) {
         const uint8_t* pg = a.key.pages + size_t(p) * kPageSize;
@@ -215,13 +217,20 @@ __global__ void __launch_bounds__(kCtaThreads, 2) k_scan_probe(ScanArgs a) {
                     uint32_t m = m0 + lane + 32 * u;
                     uint32_t vals[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
                     int vi0 = int(4 * m) - 1;
-                    uint32_t take4 = 0;
+                    // Words strictly inside the value range need no bounds test.
+                    uint32_t valid4 = (m >= 1 && 4 * m + 3 <= n) ? 0xfu : 0u;
+                    if (!valid4) {
 #pragma unroll
-                    for (int c = 0; c < 4; c++) {
-                        int vi = vi0 + c;
-                        bool valid = vi >= 0 && uint32_t(vi) < n;
-                        bool take = valid && (!use_bloom || bloom_pass(bloom, masks, log2w, vals[c]));
-                        take4 |= uint32_t(take) << c;
+                        for (int c = 0; c < 4; c++) {
+                            int vi = vi0 + c;
+                            valid4 |= uint32_t(vi >= 0 && uint32_t(vi) < n) << c;
+                        }
+                    }
+                    uint32_t take4 = valid4;
+                    if (use_bloom) {
+#pragma unroll
+                        for (int c = 0; c < 4; c++)
+                            if (!bloom_pass(bloom, masks, wshift, vals[c])) take4 &= ~(1u << c);
                     }
                     push4(a, w, take4, vi0, vals, p, row0);
                 }
@@ -244,7 +253,7 @@ __global__ void __launch_bounds__(kCtaThreads, 2) k_scan_probe(ScanArgs a) {
                 uint32_t d = running + __popc(wbits & ((1u << lane) - 1));
                 uint32_t key = valid ? *reinterpret_cast<const uint32_t*>(pg + 4 + 4 * d) : 0;
                 running += __popc(wbits);
-                bool take = valid && (!use_bloom || bloom_pass(bloom, masks, log2w, key));
+                bool take = valid && (!use_bloom || bloom_pass(bloom, masks, wshift, key));
                 push(a, w, take, r0 + lane, key, p, row0);
             }
         }

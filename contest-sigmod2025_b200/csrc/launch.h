@@ -29,6 +29,7 @@ int fill_u32(uint32_t* p, uint32_t v, size_t n, cudaStream_t st);
 // pages are resident at c.pages; checks every page header. Writes the column's
 // row total to *rows_out (device) and flags to *flags_out (device).
 struct PageIndexBufs {
+    uint32_t* hdr;           // npages: page headers (kept)
     uint32_t* rows;          // npages (scratch)
     uint32_t* chunks;        // npages (scratch)
     uint32_t* row_start;     // npages + 1
@@ -38,8 +39,9 @@ struct PageIndexBufs {
 int page_index_pass1(const uint8_t* pages, uint32_t npages, int32_t type, PageIndexBufs b, uint32_t* err,
                      Scratch& s, cudaStream_t st);
 // After pass 1 the host knows the chunk total and row total.
-int page_index_pass2(const uint8_t* pages, uint32_t npages, uint32_t nrows, const uint32_t* row_start,
-                     const uint32_t* chunk_base, uint32_t* dense_base, uint32_t* page_of_blk, cudaStream_t st);
+int page_index_pass2(const uint8_t* pages, const uint32_t* hdr, uint32_t npages, uint32_t nrows,
+                     const uint32_t* row_start, const uint32_t* chunk_base, uint32_t* dense_base,
+                     uint32_t* page_of_blk, cudaStream_t st);
 
 // ---- pipelines (k_probe.cu) ----
 // Items flowing through a pipeline: a row of the scanned input plus, per
