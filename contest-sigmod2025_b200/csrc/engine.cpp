@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -223,10 +224,34 @@ const char* dev_error_text(uint32_t code) {
     }
 }
 
+// Host read-backs of one query, in order: recorded on the first run of a
+// repeated resident query and replayed while that query is captured into a
+// CUDA graph (the capture must not synchronise).
+struct ReadbackTape {
+    std::vector<std::array<uint64_t, 64>> slots;
+    size_t pos = 0;
+};
+
 } // namespace
 } // namespace bj
 
 using namespace bj;
+
+// A repeated resident query captured into a CUDA graph.
+struct GraphEntry {
+    std::vector<uint64_t> key;               // plan, resident handles, flags
+    std::vector<bj_resident*> tables;
+    ReadbackTape tape;
+    cudaGraphExec_t exec = nullptr;
+    bool failed = false;                     // capture failed: always run normally
+    uint64_t rows = 0;
+    std::vector<uint64_t> npages, page_base;
+    uint64_t total_pages = 0;
+    uint8_t* pages = nullptr;                // arena pages the graph writes the result to
+    bj_stats stats{};                        // launches, pipelines, input pages of one run
+    std::vector<cudaEvent_t> prof;           // timed-kernel event pairs inside the graph
+    uint64_t prof_bytes = 0;
+};
 
 struct bj_context {
     int device = 0;
@@ -244,6 +269,11 @@ struct bj_context {
     uint64_t live_results = 0;
     int num_sms = 148;
     bool profile = false;
+    int tape_mode = 0;               // 0 off, 1 record read-backs, 2 replay them (graph capture)
+    ReadbackTape* tape = nullptr;
+    bool graph_output = false;       // result pages stay in the arena (graph capture)
+    bool graphs = true;              // replay repeated resident queries as CUDA graphs
+    std::vector<std::unique_ptr<GraphEntry>> graph_cache;
     bool zero_copy = true;  // read pinned, contiguous input columns in place
     static constexpr int kSideStreams = 4;
     cudaStream_t side[kSideStreams] = {};  // independent build pipelines run here
@@ -308,6 +338,8 @@ struct bj_result {
     uint64_t total_pages = 0;
     PinnedBlock host;
     uint8_t* dev = nullptr;
+    uint8_t* arena_pages = nullptr;  // capture only: where the graph leaves the result pages
+    bool nonempty = false;
     bj_stats stats{};
 };
 
@@ -317,22 +349,36 @@ namespace {
 // Reads back `n` u64 slots of ctx->d_small after the stream drains; checks the
 // device error word.
 void readback(bj_context* ctx, int n) {
+    (void)n;
+    if (ctx->tape_mode == 2) {
+        ReadbackTape& t = *ctx->tape;
+        if (t.pos >= t.slots.size()) throw Fail{BJ_ERR_INTERNAL, "graph capture diverged from its recording"};
+        std::memcpy(ctx->h_small, t.slots[t.pos++].data(), sizeof(uint64_t) * 64);
+        return;
+    }
     BJ_CK(cudaMemcpyAsync(ctx->h_small, ctx->d_small, sizeof(uint64_t) * 64, cudaMemcpyDeviceToHost, ctx->stream));
     BJ_CK(cudaStreamSynchronize(ctx->stream));
-    (void)n;
     uint32_t code = uint32_t(ctx->h_small[63]);
     if (code) throw Fail{BJ_ERR_INVALID, std::string("device check failed: ") + dev_error_text(code)};
+    if (ctx->tape_mode == 1) {
+        std::array<uint64_t, 64> snap;
+        std::memcpy(snap.data(), ctx->h_small, sizeof(snap));
+        ctx->tape->slots.push_back(snap);
+    }
 }
 
 // Queue a copy of a device u32/u64 value into readback slot i.
 void stash_u32(bj_context* ctx, const uint32_t* src, int i) {
+    if (ctx->tape_mode == 2) return;
     BJ_CK(cudaMemsetAsync(ctx->d_small + i, 0, sizeof(uint64_t), ctx->stream));
     BJ_CK(cudaMemcpyAsync(ctx->d_small + i, src, sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->stream));
 }
 void stash_u64(bj_context* ctx, const uint64_t* src, int i) {
+    if (ctx->tape_mode == 2) return;
     BJ_CK(cudaMemcpyAsync(ctx->d_small + i, src, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
 }
 void stash_err(bj_context* ctx) {
+    if (ctx->tape_mode == 2) return;
     BJ_CK(cudaMemsetAsync(ctx->d_small + 63, 0, sizeof(uint64_t), ctx->stream));
     BJ_CK(cudaMemcpyAsync(ctx->d_small + 63, ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->stream));
 }
@@ -568,17 +614,16 @@ class Executor {
         return static_cast<T*>(A_.alloc(sizeof(T) * std::max<size_t>(n, 1)));
     }
     void launched(int n) { ctx_->launches += uint64_t(n); }
-    void begin_timed() {
+    void record_timed() {
         cudaEvent_t e;
         BJ_CK(cudaEventCreate(&e));
         ctx_->prof_events.push_back(e);
-        BJ_CK(cudaEventRecord(e, st_));
+        // Inside a graph capture the record must become a graph node.
+        BJ_CK(cudaEventRecordWithFlags(e, st_, ctx_->graph_output ? cudaEventRecordExternal : cudaEventRecordDefault));
     }
+    void begin_timed() { record_timed(); }
     void end_timed(uint64_t bytes) {
-        cudaEvent_t e;
-        BJ_CK(cudaEventCreate(&e));
-        ctx_->prof_events.push_back(e);
-        BJ_CK(cudaEventRecord(e, st_));
+        record_timed();
         ctx_->prof_bytes += bytes;
     }
 
@@ -917,7 +962,10 @@ class Executor {
         }
         res.total_pages = total;
         uint8_t* dst = nullptr;
-        if (flags & BJ_RESULT_DEVICE) {
+        if (ctx_->graph_output) {
+            dst = alloc<uint8_t>(total * kPageSize);
+            res.arena_pages = dst;
+        } else if (flags & BJ_RESULT_DEVICE) {
             if (total) BJ_CK(cudaMallocAsync(reinterpret_cast<void**>(&res.dev), total * kPageSize, st_));
             dst = res.dev;
         } else {
@@ -941,7 +989,7 @@ class Executor {
             launched(write_string_pages(fo.vals[j], fo.valid[j], sp[c].lens, StrSource{scol}, descs,
                                         uint32_t(res.npages[c]), pages, ctx_->d_err, st_));
         }
-        if (!(flags & BJ_RESULT_DEVICE) && total) {
+        if (!ctx_->graph_output && !(flags & BJ_RESULT_DEVICE) && total) {
             res.host = ctx_->take_pinned(total * kPageSize);
             BJ_CK(cudaMemcpyAsync(res.host.p, dst, total * kPageSize, cudaMemcpyDeviceToHost, st_));
             res.stats.d2h_bytes += total * kPageSize;
@@ -1098,6 +1146,209 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
     return BJ_OK;
 }
 
+// ---------------------------------------------------------------------------
+// CUDA-graph replay of repeated resident queries.
+//
+// A serving process runs the same query shapes over the same resident tables
+// again and again. The first run of a (plan, tables, flags) key executes
+// normally and records every host read-back (probe hit rates, table flags,
+// counts) on a tape. The second run executes the same host logic under
+// stream capture, answering read-backs from the tape instead of
+// synchronising, so every kernel, copy and cross-stream dependency of the
+// query lands in one CUDA graph. Later runs launch that graph -- all kernels
+// run again, on the same resident inputs -- and copy the result pages out.
+// The tables are immutable once resident, so the recorded counts stay exact;
+// freeing a table drops the graphs that read it.
+
+std::vector<uint64_t> graph_key(const bj_plan& plan, bj_resident* const* tables, int flags, bool profile) {
+    std::vector<uint64_t> k{plan.num_nodes, plan.num_inputs, plan.root, uint64_t(flags), uint64_t(profile)};
+    for (uint64_t i = 0; i < plan.num_nodes; i++) {
+        const bj_node& n = plan.nodes[i];
+        k.insert(k.end(), {uint64_t(n.kind), uint64_t(n.build_left), n.base_table_id, n.left, n.right, n.left_attr,
+                           n.right_attr, n.num_output_attrs});
+        for (uint64_t a = 0; a < n.num_output_attrs; a++) {
+            k.push_back(n.output_attrs[a].index);
+            k.push_back(uint64_t(uint32_t(n.output_attrs[a].type)));
+        }
+    }
+    for (uint64_t i = 0; i < plan.num_inputs; i++) k.push_back(reinterpret_cast<uint64_t>(tables[i]));
+    return k;
+}
+
+void destroy_graph(GraphEntry& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    for (cudaEvent_t e : g.prof) cudaEventDestroy(e);
+    g.prof.clear();
+}
+
+bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resident* const* resident, int flags) {
+    bool capturing = false;
+    bj_result res;
+    res.ctx = ctx;
+    uint64_t launches0 = ctx->launches;
+    try {
+        ExecPlan ex;
+        std::string err;
+        if (make_exec_plan(*plan, ex, err) != BJ_OK || ex.empty) return false;
+        std::vector<const DevTable*> tables(plan->num_inputs);
+        for (uint64_t i = 0; i < plan->num_inputs; i++) tables[i] = &resident[i]->table;
+        g.tape.pos = 0;
+        ctx->tape = &g.tape;
+        ctx->tape_mode = 2;
+        ctx->graph_output = true;
+        BJ_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+        capturing = true;
+        Executor exe(ctx, ex, tables);
+        bool nonempty = exe.run(res, flags);
+        capturing = false;
+        cudaGraph_t graph = nullptr;
+        BJ_CK(cudaStreamEndCapture(ctx->stream, &graph));
+        ctx->tape_mode = 0;
+        ctx->tape = nullptr;
+        ctx->graph_output = false;
+        // The recording ends with the call's final error check, not replayed here.
+        if (!graph || g.tape.pos + 1 != g.tape.slots.size()) {
+            if (graph) cudaGraphDestroy(graph);
+            throw Fail{BJ_ERR_INTERNAL, "graph capture diverged from its recording"};
+        }
+        cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) throw Fail{BJ_ERR_CUDA, "cudaGraphInstantiate failed"};
+        if (nonempty) {
+            g.rows = res.rows;
+            g.npages = res.npages;
+            g.page_base = res.page_base;
+            g.total_pages = res.total_pages;
+            g.pages = res.arena_pages;
+        } else {
+            g.rows = 0;
+            g.npages.assign(ex.out_types.size(), 0);
+            g.page_base.assign(ex.out_types.size(), 0);
+            g.total_pages = 0;
+            g.pages = nullptr;
+        }
+        g.stats = bj_stats{};
+        g.stats.kernel_launches = ctx->launches - launches0;
+        g.stats.pipelines = exe.pipelines_run();
+        for (uint64_t i = 0; i < plan->num_inputs; i++) {
+            std::vector<uint8_t> used;
+            collect_columns(ex, uint32_t(i), tables[i]->cols.size(), used);
+            for (size_t c = 0; c < used.size(); c++)
+                if (used[c]) g.stats.input_pages += tables[i]->cols[c].npages;
+        }
+        g.prof = ctx->prof_events;
+        g.prof_bytes = ctx->prof_bytes;
+        ctx->prof_events.clear();
+        ctx->prof_bytes = 0;
+        ctx->arena.reset();
+        return true;
+    } catch (const Fail&) {
+        if (capturing) {
+            cudaGraph_t gr = nullptr;
+            cudaStreamEndCapture(ctx->stream, &gr);
+            if (gr) cudaGraphDestroy(gr);
+        }
+        cudaGetLastError();
+        ctx->tape_mode = 0;
+        ctx->tape = nullptr;
+        ctx->graph_output = false;
+        for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
+        ctx->prof_events.clear();
+        ctx->prof_bytes = 0;
+        ctx->sync_all();
+        ctx->arena.reset();
+        return false;
+    }
+}
+
+int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& types, int flags, bj_result** out) {
+    auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<bj_result> res(new bj_result);
+    res->ctx = ctx;
+    try {
+        res->types = types;
+        BJ_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(uint32_t), ctx->stream));
+        BJ_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        BJ_CK(cudaGraphLaunch(g.exec, ctx->stream));
+        res->rows = g.rows;
+        res->npages = g.npages;
+        res->page_base = g.page_base;
+        res->total_pages = g.total_pages;
+        size_t bytes = g.total_pages * kPageSize;
+        if (bytes && (flags & BJ_RESULT_DEVICE)) {
+            BJ_CK(cudaMallocAsync(reinterpret_cast<void**>(&res->dev), bytes, ctx->stream));
+            BJ_CK(cudaMemcpyAsync(res->dev, g.pages, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        } else if (bytes) {
+            res->host = ctx->take_pinned(bytes);
+            BJ_CK(cudaMemcpyAsync(res->host.p, g.pages, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+            res->stats.d2h_bytes = bytes;
+        }
+        BJ_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+        stash_err(ctx);
+        readback(ctx, 0);
+        float ms = 0;
+        BJ_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        res->stats.device_ms = ms;
+        for (size_t i = 0; i + 1 < g.prof.size(); i += 2) {
+            float k = 0;
+            BJ_CK(cudaEventElapsedTime(&k, g.prof[i], g.prof[i + 1]));
+            res->stats.scan_kernel_ms += k;
+            res->stats.scan_kernel_launches++;
+        }
+        res->stats.scan_kernel_bytes = g.prof_bytes;
+        res->stats.kernel_launches = g.stats.kernel_launches;
+        res->stats.pipelines = g.stats.pipelines;
+        res->stats.input_pages = g.stats.input_pages;
+        res->stats.output_pages = g.total_pages;
+        ctx->launches += g.stats.kernel_launches;
+    } catch (const Fail& f) {
+        if (res->dev) cudaFree(res->dev);
+        res->dev = nullptr;
+        ctx->give_pinned(res->host);
+        res->host = PinnedBlock{};
+        return fail_to_status(ctx, f);
+    }
+    res->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    ctx->live_results++;
+    ctx->last_error.clear();
+    *out = res.release();
+    return BJ_OK;
+}
+
+int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int flags,
+                           bj_result** out) {
+    std::vector<uint64_t> key = graph_key(*plan, tables, flags, ctx->profile);
+    GraphEntry* g = nullptr;
+    for (auto& e : ctx->graph_cache)
+        if (e->key == key) g = e.get();
+    if (!g) {
+        auto e = std::make_unique<GraphEntry>();
+        e->key = std::move(key);
+        e->tables.assign(tables, tables + plan->num_inputs);
+        ctx->tape = &e->tape;
+        ctx->tape_mode = 1;
+        int st = execute_common(ctx, plan, tables, flags, out);
+        ctx->tape_mode = 0;
+        ctx->tape = nullptr;
+        if (st == BJ_OK) {
+            if (ctx->graph_cache.size() >= 64) {
+                destroy_graph(*ctx->graph_cache.front());
+                ctx->graph_cache.erase(ctx->graph_cache.begin());
+            }
+            ctx->graph_cache.push_back(std::move(e));
+        }
+        return st;
+    }
+    if (!g->failed && !g->exec && !capture_graph(ctx, *g, plan, tables, flags)) g->failed = true;
+    if (g->failed) return execute_common(ctx, plan, tables, flags, out);
+    ExecPlan ex;
+    std::string err;
+    int st = make_exec_plan(*plan, ex, err);
+    if (st != BJ_OK) return st;
+    return replay_graph(ctx, *g, ex.out_types, flags, out);
+}
+
 } // namespace
 } // namespace bj
 
@@ -1135,6 +1386,7 @@ BJ_API int bj_context_create(int device, bj_context** out) {
     }
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (const char* zc = std::getenv("B200JOIN_ZERO_COPY")) ctx->zero_copy = std::atoi(zc) != 0;
+    if (const char* gr = std::getenv("B200JOIN_GRAPHS")) ctx->graphs = std::atoi(gr) != 0;
     unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     ctx->pool = std::make_unique<ThreadPool>(std::min(hw, 16u) - 1);
     *out = ctx.release();
@@ -1145,6 +1397,8 @@ BJ_API void bj_context_destroy(bj_context* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     ctx->sync_all();
+    for (auto& g : ctx->graph_cache) destroy_graph(*g);
+    ctx->graph_cache.clear();
     for (cudaEvent_t e : ctx->pipe_events) cudaEventDestroy(e);
     for (cudaStream_t s : ctx->side)
         if (s) cudaStreamDestroy(s);
@@ -1177,6 +1431,7 @@ BJ_API int bj_execute_resident(bj_context* ctx, const bj_plan* plan, bj_resident
                                bj_result** out) {
     if (!ctx || !tables) return BJ_ERR_INVALID;
     cudaSetDevice(ctx->device);
+    if (ctx->graphs && plan) return execute_resident_graph(ctx, plan, tables, flags, out);
     return execute_common(ctx, plan, tables, flags, out);
 }
 
@@ -1222,7 +1477,20 @@ BJ_API int bj_resident_upload(bj_context* ctx, const bj_table* table, bj_residen
 
 BJ_API void bj_resident_free(bj_context* ctx, bj_resident* t) {
     if (!t) return;
-    if (ctx) cudaStreamSynchronize(ctx->stream);
+    if (ctx) {
+        ctx->sync_all();
+        // Graphs that read this table are no longer valid.
+        auto& gc = ctx->graph_cache;
+        for (size_t i = 0; i < gc.size();) {
+            const auto& tabs = gc[i]->tables;
+            if (std::find(tabs.begin(), tabs.end(), t) != tabs.end()) {
+                destroy_graph(*gc[i]);
+                gc.erase(gc.begin() + i);
+            } else {
+                i++;
+            }
+        }
+    }
     delete t;
 }
 

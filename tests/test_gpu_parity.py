@@ -196,3 +196,46 @@ def test_pinned_inputs_read_in_place(pkg, ctx, oracle, name, seed, scale):
     finally:
         for p in regs:
             torch._C._cudart.cudaHostUnregister(p)
+
+
+@pytest.mark.parametrize("name,seed,scale", [("snowflake", 8, 0.05), ("join2", 9, 0.1)])
+def test_repeated_resident_queries_replay_graphs(pkg, ctx, oracle, name, seed, scale):
+    """A resident query run again and again: the first run records, the second
+    is captured into a CUDA graph, later runs replay it. Every run's rows equal
+    the oracle's; freeing a table drops the graph and the next run records anew."""
+    w = pkg.Workload(name, seed, scale)
+    plan = w.plan_ptr().contents
+    res = [ctx.upload(plan.inputs[i]) for i in range(plan.num_inputs)]
+    want = oracle.execute(w.plan_ptr())
+    try:
+        for _ in range(4):
+            with ctx.execute_resident(w.plan_ptr(), res) as r:
+                got, keep = r.table_struct()
+                oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), f"{name} resident replay")
+                assert r.stats().kernel_launches > 0
+        for _ in range(3):
+            with ctx.execute_resident(w.plan_ptr(), res, flags=pkg.RESULT_DEVICE) as r:
+                t = r.to_table()
+                cols = (pkg.BjColumn * max(len(t.columns), 1))()
+                bufs = []
+                for c, col in enumerate(t.columns):
+                    buf = ctypes.create_string_buffer(col.data, max(len(col.data), 1))
+                    ptrs = (ctypes.c_void_p * max(col.num_pages, 1))(
+                        *[ctypes.addressof(buf) + k * pkg.PAGE_SIZE for k in range(col.num_pages)])
+                    bufs += [buf, ptrs]
+                    cols[c].type, cols[c].num_pages = col.type, col.num_pages
+                    cols[c].pages = ctypes.cast(ptrs, ctypes.POINTER(ctypes.c_void_p))
+                tab = pkg.BjTable(t.num_rows, len(t.columns), ctypes.cast(cols, ctypes.POINTER(pkg.BjColumn)))
+                oracle_lib.assert_same_rows(oracle, ctypes.byref(tab), want.view(), f"{name} device replay")
+    finally:
+        res[-1].free()
+    # A new table in the freed slot: the old graph must not be used.
+    res[-1] = ctx.upload(plan.inputs[plan.num_inputs - 1])
+    try:
+        for _ in range(3):
+            with ctx.execute_resident(w.plan_ptr(), res) as r:
+                got, keep = r.table_struct()
+                oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), f"{name} after free")
+    finally:
+        for x in res:
+            x.free()
