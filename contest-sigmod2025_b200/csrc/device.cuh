@@ -52,8 +52,11 @@ struct DevColumn {
     uint32_t npages;
     uint32_t nrows;
     int32_t type;
-    uint32_t flags;  // bit 0: some page has NULLs; bit 1: long strings present
+    uint32_t flags;  // kColNulls | kColLongStrings | kColHostPages
 };
+constexpr uint32_t kColNulls = 1;        // some page has NULLs
+constexpr uint32_t kColLongStrings = 2;  // long-string page runs present
+constexpr uint32_t kColHostPages = 4;    // pages are read in place from (pinned) host memory
 
 // String handle carried in a value slot: page index << 16 | value index in the
 // page; a long string (its own page run) uses value index 0xffff.

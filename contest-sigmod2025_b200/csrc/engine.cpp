@@ -529,7 +529,7 @@ void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem) 
         c.pages = jobs[i].dpages;
         c.npages = tmp[i].npages;
         c.nrows = uint32_t(rows[i]);
-        c.flags = uint32_t(flags[i]);
+        c.flags = uint32_t(flags[i]) | (jobs[i].in_place ? kColHostPages : 0u);
         c.hdr = tmp[i].b.hdr;
         c.row_start = tmp[i].b.row_start;
         c.chunk_base = tmp[i].b.chunk_base;
