@@ -253,7 +253,10 @@ def main():
             x.free()
         ctx.close()
         if rank == 0:
-            print(json.dumps({"mode": "value", "value": value, "unit": "queries/s", "steps": args.steps}))
+            scan_gbs = (scan_bytes / scan_n) / (scan_ms / scan_n / 1e3) / 1e9 if scan_n and scan_ms > 0 else None
+            print(json.dumps({"mode": "value", "value": value, "unit": "queries/s", "steps": args.steps,
+                              "scan_kernel_us": scan_ms / scan_n * 1e3 if scan_n else None,
+                              "scan_kernel_gbs": scan_gbs, "p50_ms": statistics.median(lat)}))
         return 0
 
     # ---- e2e: drop-in path (bj_execute), host pages in and out ----
@@ -333,7 +336,7 @@ def main():
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "traffic": traffic,
-                     "kernel": "k_probe_stage over the fact's key pages",
+                     "kernel": "k_scan_probe over the fact's key pages",
                      "launches": scan_n, "bytes_per_launch": scan_bytes / scan_n if scan_n else None,
                      "peak_kind": f"{peak_kind} HBM copy bandwidth"},
         "clocks": clk,

@@ -133,7 +133,8 @@ BJ_HD uint64_t key_hash(uint32_t key) {
     return uint64_t(key) * 0x9E3779B97F4A7C15ull;
 }
 
-// Independent mix for the bloom filter (murmur3 fmix64 finaliser).
+// 64-bit mixer for whole-tuple hashing in eager aggregation (the murmur3
+// fmix64 finaliser).
 BJ_HD uint64_t mix64(uint64_t x) {
     x ^= x >> 33;
     x *= 0xff51afd7ed558ccdull;
@@ -144,32 +145,36 @@ BJ_HD uint64_t mix64(uint64_t x) {
 }
 
 // Blocked bloom filter: one 32-bit word per key with up to four bits set.
-// The word comes from the key hash's top bits (at most 14 of them, so a
-// filter is at most 64 KiB); the bit mask is entry (h >> 32) & 2047 of a
-// 2048-entry mask table. The table is arithmetic (bloom_mask below), so
-// scans can tabulate it in shared memory and replace the bit arithmetic by
-// one lookup. (The reference also draws 4-of-16 masks from a 2048-entry
-// table, engine/infra/JoinFilter.hpp:9-14; ours is 4-of-32 and generated.)
-constexpr uint32_t kBloomMaxLog2 = 14;
-constexpr uint32_t kBloomMasks = 2048;
-BJ_HD uint32_t bloom_mask(uint32_t idx) {
-    uint32_t g = idx * 2654435761u;
-    g ^= g >> 15;
-    g *= 0x2c1b3c6du;
-    g ^= g >> 12;
-    return (1u << (g & 31)) | (1u << ((g >> 5) & 31)) | (1u << ((g >> 10) & 31)) | (1u << ((g >> 15) & 31));
+// The word is the top log2w bits (at most 15, so a filter is at most 128 KiB
+// and fits in shared memory) of the high half hh of the key hash. The bits
+// are two rotations of fixed two-bit patterns, P1 rotated by hh mod 32 and
+// P2 by (hh >> 5) mod 32: 1024 masks of three or four bits, each made by one
+// funnel shift per pattern, with no mask table. (The reference uses a 16-bit
+// word per bucket and a 2048-entry mask table, engine/infra/JoinFilter.hpp:
+// 9-23; a bloom only removes probes, never results.)
+constexpr uint32_t kBloomMaxLog2 = 15;
+constexpr uint32_t kBloomP1 = (1u << 0) | (1u << 11);
+constexpr uint32_t kBloomP2 = (1u << 0) | (1u << 19);
+BJ_HD uint32_t rotl32(uint32_t x, uint32_t s) {
+    s &= 31;
+    return s ? (x << s) | (x >> (32 - s)) : x;
 }
-BJ_HD uint32_t bloom_mask_index(uint64_t h) { return uint32_t(h >> 32) & (kBloomMasks - 1); }
+BJ_HD uint32_t bloom_bits_hi(uint32_t hh) { return rotl32(kBloomP1, hh) | rotl32(kBloomP2, hh >> 5); }
+BJ_HD uint32_t bloom_word_hi(uint32_t hh, uint32_t log2_words) { return log2_words ? hh >> (32 - log2_words) : 0u; }
 // High 32 bits of key_hash(key) (all the bloom filter uses), in two multiplies.
 #if defined(__CUDACC__)
 __device__ __forceinline__ uint32_t key_hash_hi(uint32_t key) {
     return __umulhi(key, 0x7F4A7C15u) + key * 0x9E3779B9u;
 }
-#endif
-BJ_HD uint32_t bloom_bits(uint64_t h) { return bloom_mask(bloom_mask_index(h)); }
-BJ_HD uint32_t bloom_word(uint64_t h, uint32_t log2_words) {
-    return log2_words ? uint32_t(h >> (64 - log2_words)) : 0u;
+// bloom_bits_hi given hh and hh >> 5 (or any value with the same low five
+// bits): a funnel shift of a pattern with itself is a rotation by the shift
+// amount mod 32.
+__device__ __forceinline__ uint32_t bloom_bits_fast(uint32_t hh, uint32_t hh5) {
+    return __funnelshift_l(kBloomP1, kBloomP1, hh) | __funnelshift_l(kBloomP2, kBloomP2, hh5);
 }
+#else
+inline uint32_t key_hash_hi(uint32_t key) { return uint32_t(key_hash(key) >> 32); }
+#endif
 
 // A built hash table: entries grouped by bucket (CSR), keys 32-bit, a
 // multiplicity per entry (eager aggregation folds identical tuples into one
@@ -190,9 +195,9 @@ struct HTView {
 
 #if defined(__CUDACC__)
 __device__ __forceinline__ bool bloom_may_contain(const uint32_t* bloom, uint32_t log2w, uint32_t key) {
-    uint64_t h = key_hash(key);
-    uint32_t bits = bloom_bits(h);
-    return (bloom[bloom_word(h, log2w)] & bits) == bits;
+    const uint32_t hh = key_hash_hi(key);
+    const uint32_t bits = bloom_bits_fast(hh, hh >> 5);
+    return (bloom[bloom_word_hi(hh, log2w)] & bits) == bits;
 }
 
 __device__ __forceinline__ void record_error(uint32_t* err, uint32_t code) {

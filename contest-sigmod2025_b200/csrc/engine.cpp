@@ -404,6 +404,7 @@ constexpr uint64_t kInPlaceMinPages = 2048;  // 16 MiB
 uint8_t* mapped_base(const bj_column& hc) {
     if (hc.num_pages < kInPlaceMinPages || !hc.pages || !hc.pages[0]) return nullptr;
     const uint8_t* p0 = static_cast<const uint8_t*>(hc.pages[0]);
+    if (reinterpret_cast<uintptr_t>(p0) % 16) return nullptr;  // kernels read pages with 16-byte loads
     for (uint64_t k = 1; k < hc.num_pages; k++)
         if (hc.pages[k] != p0 + k * kPageSize) return nullptr;
     cudaPointerAttributes a0{}, a1{};
@@ -724,14 +725,16 @@ class Executor {
                     items = next;
                     continue;
                 } else {
-                    uint32_t* pc = alloc<uint32_t>(key.npages);
-                    uint32_t* poff = alloc<uint32_t>(size_t(key.npages) + 1);
+                    // Counts per work unit of the scan (two per page).
+                    const uint32_t units = 2 * key.npages;
+                    uint32_t* pc = alloc<uint32_t>(units);
+                    uint32_t* poff = alloc<uint32_t>(size_t(units) + 1);
                     bool timed = ctx_->profile;
                     if (timed) begin_timed();
                     launched(scan_probe(key, ht, 0, bloom, pc, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
                                         ctx_->d_err, ctx_->num_sms, st_));
                     if (timed) end_timed(page_bytes);
-                    total = scan_total_u32(pc, poff, key.npages);
+                    total = scan_total_u32(pc, poff, units);
                     if (total) {
                         out.rows = alloc<uint32_t>(total);
                         out.ents[0] = alloc<uint32_t>(total);
@@ -858,7 +861,7 @@ class Executor {
         ht.nentries = nrep;
         ht.width = width;
         launched(bucket_scatter(tb, is_rep, shift, off, cursor, ht, ctx_->d_err, st_));
-        // Bloom filter: about 16 bits per key, at most 64 KiB (shared-memory staging).
+        // Bloom filter: about 16 bits per key, at most 128 KiB (shared-memory staging).
         uint32_t wlog2 = std::min<uint32_t>(kBloomMaxLog2,
                                             std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1)));
         uint32_t* bloom = alloc<uint32_t>(size_t(1) << wlog2);

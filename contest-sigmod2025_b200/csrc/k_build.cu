@@ -17,8 +17,8 @@
 //  2. bucket counts with atomicAdd, an exclusive scan, and a scatter of the
 //     representatives into their bucket's contiguous range (K4). The same
 //     bucket index as the reference: key_hash(key) >> shift.
-//  3. a blocked bloom filter, one 32-bit word per key with 4 bits set (K3),
-//     at most 64 KiB so scans can stage it in shared memory; probes consult
+//  3. a blocked bloom filter, one 32-bit word per key with 3-4 bits set (K3),
+//     at most 128 KiB so scans can stage it in shared memory; probes consult
 //     it before touching the buckets.
 #include "launch.h"
 
@@ -104,8 +104,8 @@ __global__ void k_bloom_build(const uint32_t* __restrict__ keys, const uint32_t*
                               uint32_t* __restrict__ bloom, uint32_t log2w) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || (mask && !mask[i])) return;
-    uint64_t h = key_hash(keys[i]);
-    atomicOr(&bloom[bloom_word(h, log2w)], bloom_bits(h));
+    const uint32_t hh = key_hash_hi(keys[i]);
+    atomicOr(&bloom[bloom_word_hi(hh, log2w)], bloom_bits_fast(hh, hh >> 5));
 }
 
 __global__ void k_ht_flags(HTView ht, uint32_t nbuckets, uint32_t* __restrict__ flags) {

@@ -5,25 +5,34 @@
 // evaluates the restrictions (NOT NULL, bloom join filter, Hashtable.hpp:81-85)
 // and hands survivors to the probe (HashtableProbe::operator(), :228-241).
 //
-// Here every warp owns whole pages of the probe key column and works on them
-// without block-level barriers:
-//  * a page without NULLs is read with 128-bit coalesced loads, four per lane
-//    in flight (value v sits in 16-byte word (v+1)/4 because values start at
-//    byte 4); a page with NULLs is read row by row, 32 rows per step, the null
-//    bitmap word of those rows giving validity and (by popcount) the dense
-//    index of each value;
-//  * the hash table's bloom filter and the 2048-entry bloom mask table are
-//    staged once per CTA in shared memory, so a miss costs two shared-memory
-//    loads;
+// Here warps stream the pages of the probe key column without block-level
+// barriers:
+//  * a page is read as two work units of 4 KiB, given to warps round-robin:
+//    eight 128-bit loads per lane, plus the page header and first row, are
+//    issued before any is used (every load stays inside the 8 KiB page;
+//    value v sits in 16-byte word (v+1)/4 because values start at byte 4);
+//  * a unit without NULLs gives each lane 32 values. The bloom test
+//    of a value is four multiplies, one shared-memory load of the filter word,
+//    two funnel shifts and a logic op (bloom_bits_fast), spread over the
+//    multiply and integer pipes; the lane's survivors form a 32-bit mask, so
+//    a unit costs one vote and at most one warp prefix sum;
+//  * a page with NULLs is read row by row, 32 rows per step, the null bitmap
+//    word of those rows giving validity and (by popcount) the dense index of
+//    each value;
+//  * the hash table's bloom filter (up to 128 KiB) is staged once per CTA in
+//    shared memory; one CTA of 32 warps runs per SM;
 //  * survivors (bloom hits, or every non-null row when the probe is not
-//    selective) are pushed into a per-warp buffer in shared memory with
-//    ballots; the buffer is probed 128 entries at a time, four independent
-//    bucket lookups per lane, so the L2 latency of the probes is paid once
-//    per batch instead of once per hit;
+//    selective) are recorded as (key, row) in a per-warp buffer in shared
+//    memory (the key read again from the page just loaded, a cache hit); the
+//    buffer is probed 128 entries at a time, four independent bucket lookups
+//    per lane, so the latency of the probes is paid once per batch instead
+//    of once per hit;
 //  * matches become items (row, entry, mult). With unique build keys a row
 //    has at most one match: items are appended with one atomicAdd per batch
-//    (mode 2). Otherwise a counting pass writes per-page counts (mode 0) and
-//    an emitting pass writes at the scanned page offsets (mode 1).
+//    and the buffer carries over from unit to unit (mode 2). Otherwise a
+//    counting pass writes per-unit counts (mode 0) and an emitting pass
+//    writes at the units' offsets (mode 1); the buffer is emptied at the end
+//    of every unit.
 #include "launch.h"
 
 #include <algorithm>
@@ -32,19 +41,27 @@
 namespace bj {
 namespace {
 
-constexpr int kWarpsPerCta = 16;
+constexpr int kWarpsPerCta = 32;
 constexpr int kCtaThreads = kWarpsPerCta * 32;
-constexpr int kPerLane = 4;                      // buffered candidates per lane
-constexpr int kBatch = 32 * kPerLane;            // buffer entries per warp
-constexpr size_t kBloomSmemMax = size_t(4) << kBloomMaxLog2;  // 64 KiB
+constexpr int kPerLane = 4;                          // buffered candidates per lane
+constexpr int kBatch = 32 * kPerLane;                // buffer entries per warp
+constexpr int kStepWords = 8;                        // 16-byte words per lane per step
+constexpr uint32_t kWordsPerStep = 32 * kStepWords;  // 256 words = 4 KiB
+constexpr size_t kBloomSmemMax = size_t(4) << kBloomMaxLog2;  // 128 KiB
 
 struct ScanArgs {
     DevColumn key;             // probe key column (pages of the scanned table)
     HTView ht;
-    uint32_t mode;             // 0 count per page, 1 emit at page offsets, 2 emit with atomics (unique keys)
+    uint32_t mode;             // 0 count per unit, 1 emit at unit offsets, 2 emit with atomics (unique keys)
     uint32_t use_bloom;        // stage ht.bloom in shared memory and test it
-    uint32_t* page_counts;     // mode 0 output (npages)
-    const uint32_t* page_off;  // mode 1 input (npages + 1)
+    uint32_t prefetch;         // pages ahead of its current one a warp bulk-prefetches into L2 (0-2)
+    // Multipliers for the bloom test, given at run time so that the shifts
+    // they stand for (hh >> (32 - log2w), hh >> 5) run on the multiply pipe
+    // as __umulhi instead of competing with the shifts on the integer pipe.
+    uint32_t word_mul;         // 1 << ht.bloom_log2
+    uint32_t field_mul;        // 1 << 27
+    uint32_t* page_counts;     // mode 0 output: matches per work unit (2 npages; unit u = half u % 2 of page u / 2)
+    const uint32_t* page_off;  // mode 1 input: exclusive scan of page_counts (2 npages + 1)
     uint32_t* cursor;          // mode 2 global item counter
     uint32_t* out_rows;
     uint32_t* out_ents;
@@ -55,49 +72,10 @@ struct ScanArgs {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 
-// ---- TMA bulk copies into shared memory, completed on an mbarrier ----
-constexpr uint32_t kWaitLimit = 1u << 24;  // mbarrier polls before a warp gives up (about a second)
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t done;
-    asm volatile(
-        "{\n"
-        ".reg .pred p;\n"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        "selp.u32 %0, 1, 0, p;\n"
-        "}\n"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-// Bounded wait on one phase; false if the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitLimit; i++)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-// Orders this thread's earlier generic-proxy accesses to shared memory before
-// later async-proxy (TMA) writes to it.
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-// One page (8 KiB, 16-byte aligned source) into shared memory, completing on `bar`.
-__device__ __forceinline__ void bulk_load_page(void* dst, const void* src, uint64_t* bar) {
-    mbar_expect_tx(bar, kPageSize);
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(kPageSize), "r"(smem_u32(bar))
-                 : "memory");
+// Asks the TMA unit to bring `bytes` (a multiple of 16, 16-byte aligned
+// source) into L2; nothing waits for it.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
 // Warp-wide exclusive prefix sum; `total` receives the sum.
@@ -113,27 +91,27 @@ __device__ __forceinline__ uint32_t warp_excl(uint32_t v, uint32_t& total) {
 }
 
 struct WarpState {
-    uint2* buf;         // this warp's candidate buffer: (row within page, key)
+    uint32_t* bkey;     // candidate buffer: key
+    uint32_t* brow;     // row of the scanned table
     uint32_t n;         // entries buffered (warp-uniform)
-    uint32_t page_cnt;  // matches counted / written for the current page
+    uint32_t page_cnt;  // matches counted / written for the current unit (modes 0 and 1)
 };
 
-// Probes every buffered candidate; counts (mode 0) or writes items.
-__device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t page, uint32_t row0) {
+// Probes every buffered candidate; counts (mode 0) or writes items. In modes
+// 0 and 1 every entry belongs to work unit `unit` (half a page).
+__device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t unit) {
     if (w.n == 0) return;
     __syncwarp();
     const uint32_t lane = lane_id();
-    uint32_t key[kPerLane], rowi[kPerLane], lo[kPerLane], hi[kPerLane];
+    uint32_t key[kPerLane], row[kPerLane], lo[kPerLane], hi[kPerLane];
 #pragma unroll
     for (int i = 0; i < kPerLane; i++) {
-        uint32_t h = lane + 32 * i;
-        lo[i] = hi[i] = 0;
-        key[i] = rowi[i] = 0;
+        const uint32_t h = lane + 32 * i;
+        key[i] = row[i] = lo[i] = hi[i] = 0;
         if (h < w.n) {
-            uint2 c = w.buf[h];
-            rowi[i] = c.x;
-            key[i] = c.y;
-            uint32_t b = uint32_t(key_hash(c.y) >> a.ht.shift);
+            key[i] = w.bkey[h];
+            row[i] = w.brow[h];
+            const uint32_t b = uint32_t(key_hash(key[i]) >> a.ht.shift);
             lo[i] = a.ht.bucket_off[b];
             hi[i] = a.ht.bucket_off[b + 1];
         }
@@ -153,7 +131,7 @@ __device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t 
         cnt += c;
     }
     uint32_t total;
-    uint32_t off = warp_excl(cnt, total);
+    const uint32_t off = warp_excl(cnt, total);
     if (a.mode != 0 && total) {
         uint32_t base;
         if (a.mode == 2) {
@@ -161,7 +139,7 @@ __device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t 
             if (lane == 31) b = atomicAdd(a.cursor, total);
             base = __shfl_sync(0xffffffffu, b, 31);
         } else {
-            base = a.page_off[page] + w.page_cnt;
+            base = a.page_off[unit] + w.page_cnt;
         }
         uint32_t o = base + off;
 #pragma unroll
@@ -171,7 +149,7 @@ __device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t 
                 if (a.ht.keys[e] != key[i]) continue;
                 left--;
                 if (o < a.capacity) {
-                    a.out_rows[o] = row0 + rowi[i];
+                    a.out_rows[o] = row[i];
                     a.out_ents[o] = e;
                     if (a.out_mult) a.out_mult[o] = a.ht.mult[e];
                 } else {
@@ -186,188 +164,179 @@ __device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t 
     __syncwarp();
 }
 
-// Pushes the candidates (row i, key) of this ballot round into the buffer.
-__device__ __forceinline__ void push(const ScanArgs& a, WarpState& w, bool take, uint32_t i, uint32_t key,
-                                     uint32_t page, uint32_t row0) {
-    uint32_t mask = __ballot_sync(0xffffffffu, take);
+// Buffers the candidates of one step of a page without NULLs: bit c of
+// `take` is value vi0 + 128 (c / 4) + c % 4 of the page of unit p (values
+// at vals, first row row0). The key is read again from the page, which this warp has just
+// loaded, so the read hits in cache. Candidates are numbered across the warp
+// in lane order; when they do not fit, the buffer is filled, probed and
+// refilled until all are in.
+__device__ __forceinline__ void push_step(const ScanArgs& a, WarpState& w, uint32_t take, int vi0,
+                                          const uint32_t* vals, uint32_t row0, uint32_t p) {
+    if (!__any_sync(0xffffffffu, take != 0)) return;
+    uint32_t total;
+    const uint32_t off = warp_excl(__popc(take), total);
+    for (uint32_t done = 0;;) {
+        const uint32_t room = kBatch - w.n;
+        uint32_t t = take, j = off;
+        while (t) {
+            const uint32_t c = __ffs(t) - 1;
+            t &= t - 1;
+            if (j >= done && j - done < room) {
+                const uint32_t vi = uint32_t(vi0 + 128 * int(c >> 2) + int(c & 3));
+                w.bkey[w.n + j - done] = __ldg(vals + vi);
+                w.brow[w.n + j - done] = row0 + vi;
+            }
+            j++;
+        }
+        const uint32_t took = min(room, total - done);
+        w.n += took;
+        done += took;
+        if (done >= total) break;
+        flush(a, w, p);
+    }
+}
+
+// Buffers one candidate per lane (key, row) of unit p.
+__device__ __forceinline__ void push_one(const ScanArgs& a, WarpState& w, bool take, uint32_t key, uint32_t row,
+                                         uint32_t p) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, take);
     if (!mask) return;
-    if (w.n + 32 > kBatch) flush(a, w, page, row0);
-    if (take) w.buf[w.n + __popc(mask & ((1u << lane_id()) - 1))] = make_uint2(i, key);
+    if (w.n + 32 > kBatch) flush(a, w, p);
+    if (take) {
+        const uint32_t o = w.n + __popc(mask & ((1u << lane_id()) - 1));
+        w.bkey[o] = key;
+        w.brow[o] = row;
+    }
     w.n += __popc(mask);
 }
 
-// Pushes up to four candidates per lane (bits of `take4`; value c has row
-// index vi0 + c and key vals[c]).
-__device__ __forceinline__ void push4(const ScanArgs& a, WarpState& w, uint32_t take4, int vi0, const uint32_t* vals,
-                                      uint32_t page, uint32_t row0) {
-    if (!__any_sync(0xffffffffu, take4 != 0)) return;
-    uint32_t total;
-    uint32_t off = warp_excl(__popc(take4), total);
-    if (w.n + total > kBatch) flush(a, w, page, row0);
-    uint32_t o = w.n + off;
+__device__ __forceinline__ bool bloom_pass(const ScanArgs& a, const uint32_t* bloom, uint32_t key) {
+    const uint32_t hh = key_hash_hi(key);
+    const uint32_t m = bloom_bits_fast(hh, __umulhi(hh, a.field_mul));
+    return (~bloom[__umulhi(hh, a.word_mul)] & m) == 0;
+}
+
+// Values of one step of a page without NULLs that pass the bloom (or all of
+// them without one), as bit 4u + k for value k of word u.
+__device__ __forceinline__ uint32_t step_take(const ScanArgs& a, const uint4 (&q)[kStepWords], const uint32_t* bloom,
+                                              bool use_bloom) {
+    if (!use_bloom) return 0xffffffffu;
+    uint32_t take = 0;
 #pragma unroll
-    for (int c = 0; c < 4; c++)
-        if ((take4 >> c) & 1) w.buf[o++] = make_uint2(uint32_t(vi0 + c), vals[c]);
-    w.n += total;
+    for (int u = 0; u < kStepWords; u++) {
+        const uint32_t v[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (bloom_pass(a, bloom, v[k])) take |= 1u << (4 * u + k);
+    }
+    return take;
 }
 
-// Bloom test with the high half of the key hash: the mask index is its low
-// 11 bits (bits 32-42 of the hash), the word its top log2w bits.
-__device__ __forceinline__ bool bloom_pass(const uint32_t* bloom, const uint32_t* masks, uint32_t wshift,
-                                           uint32_t key) {
-    uint32_t hh = key_hash_hi(key);
-    uint32_t m = masks[hh & (kBloomMasks - 1)];
-    return (bloom[hh >> wshift] & m) == m;
+// Valid-value mask of a step for a lane whose first value is vi0 (bit 4u + k
+// is value vi0 + 128u + k, valid when 0 <= value < n).
+__device__ __forceinline__ uint32_t step_valid(int vi0, uint32_t n) {
+    const int avail = int(n) - vi0;  // values from vi0 to n - 1
+    if (avail <= 0) return 0;
+    const uint32_t t = min(uint32_t(avail), 32u * 32u);
+    const uint32_t full = t >> 7;             // words with all four values valid
+    const uint32_t part = min(t & 127u, 4u);  // valid values of word `full`
+    const uint32_t lowfull = full >= 8 ? 0xffffffffu : (1u << (4 * full)) - 1;
+    const uint32_t partial = full >= 8 ? 0u : ((1u << part) - 1) << (4 * full);
+    uint32_t valid = lowfull | partial;
+    if (vi0 < 0) valid &= ~1u;  // the page header
+    return valid;
 }
 
-// Scans one page of the key column (pg: its bytes, in global or shared
-// memory; p: its index) for one warp: validity, bloom test, candidates,
-// batched probes, items.
-__device__ __forceinline__ void scan_page(const ScanArgs& a, WarpState& w, const uint32_t* bloom,
-                                          const uint32_t* masks, bool use_bloom, uint32_t wshift,
-                                          const uint8_t* pg, uint32_t p) {
+// Rows of a page with NULLs, 32 per step: bitmap word, validity, dense
+// index, value.
+__device__ __forceinline__ void scan_page_nulls(const ScanArgs& a, WarpState& w, const uint32_t* bloom, bool use_bloom,
+                                             uint32_t unit, uint32_t n, uint32_t row0) {
     const uint32_t lane = lane_id();
-    uint32_t hdr = lane == 0 ? *reinterpret_cast<const uint32_t*>(pg) : 0;
-    uint32_t row0 = lane == 0 ? a.key.row_start[p] : 0;
-    hdr = __shfl_sync(0xffffffffu, hdr, 0);
-    row0 = __shfl_sync(0xffffffffu, row0, 0);
-    const uint32_t n = hdr & 0xffff, nn = hdr >> 16;
-    w.page_cnt = 0;
-    if (nn == n) {
-        // 16-byte word m holds values 4m-1 .. 4m+2 (word 0 starts with the header).
-        const uint4* v4 = reinterpret_cast<const uint4*>(pg);
-        const uint32_t M = (4 + 4 * n + 15) / 16;
-        for (uint32_t m0 = 0; m0 < M; m0 += 128) {
-            uint4 q[4];
+    const uint8_t* pg = a.key.pages + size_t(unit >> 1) * kPageSize;
+    const uint32_t nbytes = (n + 7) >> 3;
+    const uint8_t* bm = pg + kPageSize - nbytes;
+    uint32_t running = 0;
+    for (uint32_t r0 = 0; r0 < n; r0 += 32) {
+        uint32_t wbits = 0;
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-                uint32_t m = m0 + lane + 32 * u;
-                q[u] = m < M ? v4[m] : make_uint4(0, 0, 0, 0);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                uint32_t m = m0 + lane + 32 * u;
-                uint32_t vals[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
-                int vi0 = int(4 * m) - 1;
-                // Words strictly inside the value range need no bounds test.
-                uint32_t valid4 = (m >= 1 && 4 * m + 3 <= n) ? 0xfu : 0u;
-                if (!valid4) {
-#pragma unroll
-                    for (int c = 0; c < 4; c++) {
-                        int vi = vi0 + c;
-                        valid4 |= uint32_t(vi >= 0 && uint32_t(vi) < n) << c;
-                    }
-                }
-                uint32_t take4 = valid4;
-                if (use_bloom) {
-#pragma unroll
-                    for (int c = 0; c < 4; c++)
-                        if (!bloom_pass(bloom, masks, wshift, vals[c])) take4 &= ~(1u << c);
-                }
-                push4(a, w, take4, vi0, vals, p, row0);
-            }
+        for (int b = 0; b < 4; b++) {
+            const uint32_t byte = (r0 >> 3) + b;
+            if (byte < nbytes) wbits |= uint32_t(bm[byte]) << (8 * b);
         }
-    } else {
-        // Rows r0 .. r0+31: bitmap word, validity, dense index, value.
-        const uint32_t nbytes = (n + 7) >> 3;
-        const uint8_t* bm = pg + kPageSize - nbytes;
-        uint32_t running = 0;
-        for (uint32_t r0 = 0; r0 < n; r0 += 32) {
-            uint32_t wbits = 0;
-#pragma unroll
-            for (int b = 0; b < 4; b++) {
-                uint32_t byte = (r0 >> 3) + b;
-                if (byte < nbytes) wbits |= uint32_t(bm[byte]) << (8 * b);
-            }
-            uint32_t lim = n - r0 >= 32 ? 0xffffffffu : ((1u << (n - r0)) - 1);
-            wbits &= lim;
-            bool valid = (wbits >> lane) & 1;
-            uint32_t d = running + __popc(wbits & ((1u << lane) - 1));
-            uint32_t key = valid ? *reinterpret_cast<const uint32_t*>(pg + 4 + 4 * d) : 0;
-            running += __popc(wbits);
-            bool take = valid && (!use_bloom || bloom_pass(bloom, masks, wshift, key));
-            push(a, w, take, r0 + lane, key, p, row0);
-        }
+        const uint32_t lim = n - r0 >= 32 ? 0xffffffffu : ((1u << (n - r0)) - 1);
+        wbits &= lim;
+        const uint32_t d = running + __popc(wbits & ((1u << lane) - 1));
+        // An INT32 page holds at most 2047 values; a dense index beyond that
+        // only comes from a malformed page (already reported by the page
+        // index) and is not read.
+        const bool valid = ((wbits >> lane) & 1) && d < 2047;
+        const uint32_t key = valid ? __ldg(reinterpret_cast<const uint32_t*>(pg + 4) + d) : 0;
+        running += __popc(wbits);
+        const bool take = valid && (!use_bloom || bloom_pass(a, bloom, key));
+        push_one(a, w, take, key, row0 + r0 + lane, unit);
     }
-    flush(a, w, p, row0);
-    if (a.mode == 0 && lane == 0) a.page_counts[p] = w.page_cnt;
 }
 
-__global__ void __launch_bounds__(kCtaThreads, 2) k_scan_probe(ScanArgs a) {
+__global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
     extern __shared__ uint4 bloom4[];
-    __shared__ uint2 bufs[kWarpsPerCta][kBatch];
-    __shared__ uint32_t masks[kBloomMasks];
-    const uint32_t* bloom = reinterpret_cast<const uint32_t*>(bloom4);
-    const bool use_bloom = a.use_bloom != 0;
-    if (use_bloom) {
-        const uint4* src = reinterpret_cast<const uint4*>(a.ht.bloom);
-        uint32_t n4 = (1u << a.ht.bloom_log2) / 4;
-        for (uint32_t i = threadIdx.x; i < n4; i += kCtaThreads) bloom4[i] = src[i];
-        for (uint32_t i = threadIdx.x; i < kBloomMasks; i += kCtaThreads) masks[i] = bloom_mask(i);
-    }
-    __syncthreads();
-
-    const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
-    const uint32_t total_warps = gridDim.x * kWarpsPerCta;
-    WarpState w{bufs[warp], 0, 0};
-    const uint32_t wshift = 32 - a.ht.bloom_log2;  // bloom_log2 >= 5 whenever the bloom is used
-
-    for (uint32_t p = blockIdx.x * kWarpsPerCta + warp; p < a.key.npages; p += total_warps)
-        scan_page(a, w, bloom, masks, use_bloom, wshift, a.key.pages + size_t(p) * kPageSize, p);
-}
-
-// Same work, pages staged by TMA: each warp owns one 8 KiB slot of shared
-// memory and a private mbarrier; lane 0 issues the bulk copy of the warp's
-// next page as soon as the warp has finished reading the slot, so sixteen
-// pages per SM are in flight without holding registers. No block-level
-// barrier follows the prologue. Opt-in (see scan_probe below), for pages in
-// device memory only.
-__global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe_tma(ScanArgs a) {
-    extern __shared__ __align__(128) uint8_t dyn[];
-    uint8_t* slots = dyn;                                               // kWarpsPerCta * 8 KiB
-    uint4* bloom4 = reinterpret_cast<uint4*>(dyn + kWarpsPerCta * kPageSize);
-    __shared__ uint2 bufs[kWarpsPerCta][kBatch];
-    __shared__ uint32_t masks[kBloomMasks];
-    __shared__ __align__(8) uint64_t bars[kWarpsPerCta];
+    __shared__ uint32_t bkey[kWarpsPerCta][kBatch];
+    __shared__ uint32_t brow[kWarpsPerCta][kBatch];
     const uint32_t* bloom = reinterpret_cast<const uint32_t*>(bloom4);
     const bool use_bloom = a.use_bloom != 0;
     const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
     const uint32_t total_warps = gridDim.x * kWarpsPerCta;
+    const uint32_t nunits = 2 * a.key.npages;
     const uint32_t first = blockIdx.x * kWarpsPerCta + warp;
-    uint8_t* slot = slots + warp * kPageSize;
-    if (lane == 0) {
-        mbar_init(&bars[warp], 1);
-        mbar_fence_init();
-        if (first < a.key.npages) bulk_load_page(slot, a.key.pages + size_t(first) * kPageSize, &bars[warp]);
-    }
+
+    // Work unit u is half u % 2 (4 KiB, 256 words) of page u / 2; the warp's
+    // units are first, first + total_warps, ... (half pages balance the
+    // warps better than whole pages: 10.6 units per warp against 5.3 pages
+    // on the 50M-row fact). A unit's loads are all issued before any is
+    // used, and every load stays inside its 8 KiB page.
+    auto load_unit = [&](uint32_t u, uint4 (&q)[kStepWords], uint32_t& hdr, uint32_t& row0) {
+        const uint4* pw = reinterpret_cast<const uint4*>(a.key.pages + size_t(u >> 1) * kPageSize);
+#pragma unroll
+        for (int i = 0; i < kStepWords; i++) q[i] = __ldg(pw + (u & 1) * kWordsPerStep + lane + 32 * i);
+        hdr = lane == 0 ? __ldg(reinterpret_cast<const uint32_t*>(pw)) : 0;
+        row0 = lane == 0 ? __ldg(a.key.row_start + (u >> 1)) : 0;
+    };
+    uint4 q[kStepWords];
+    uint32_t hdr_l = 0, row0_l = 0;
+
     if (use_bloom) {
         const uint4* src = reinterpret_cast<const uint4*>(a.ht.bloom);
-        uint32_t n4 = (1u << a.ht.bloom_log2) / 4;
+        const uint32_t n4 = (1u << a.ht.bloom_log2) / 4;
         for (uint32_t i = threadIdx.x; i < n4; i += kCtaThreads) bloom4[i] = src[i];
-        for (uint32_t i = threadIdx.x; i < kBloomMasks; i += kCtaThreads) masks[i] = bloom_mask(i);
     }
     __syncthreads();
-    WarpState w{bufs[warp], 0, 0};
-    const uint32_t wshift = 32 - a.ht.bloom_log2;
-    uint32_t k = 0;
-    for (uint32_t p = first; p < a.key.npages; p += total_warps, k++) {
-        bool ok = mbar_wait(&bars[warp], k & 1);
-        if (!__all_sync(0xffffffffu, ok)) {
-            // Give up on this warp's pages: record it; the copy in flight (if
-            // any) is waited for below, with a limit, before the warp exits.
-            if (lane == 0) record_error(a.err, kErrTimeout);
-            if (lane == 0) mbar_wait(&bars[warp], k & 1);
-            __syncwarp();
-            return;
+
+    WarpState w{bkey[warp], brow[warp], 0, 0};
+    for (uint32_t u = first; u < nunits; u += total_warps) {
+        const uint32_t p = u >> 1, half = u & 1;
+        load_unit(u, q, hdr_l, row0_l);
+        if (a.prefetch && lane == 0 && half == 0) {
+            const uint64_t ahead = uint64_t(p) + uint64_t(a.prefetch) * (total_warps / 2);
+            if (ahead < a.key.npages) prefetch_l2(a.key.pages + size_t(ahead) * kPageSize, kPageSize);
         }
-        scan_page(a, w, bloom, masks, use_bloom, wshift, slot, p);
-        __syncwarp();
-        const uint32_t pn = p + total_warps;
-        if (lane == 0 && pn < a.key.npages) {
-            fence_proxy_async();
-            bulk_load_page(slot, a.key.pages + size_t(pn) * kPageSize, &bars[warp]);
+        const uint32_t hdr = __shfl_sync(0xffffffffu, hdr_l, 0);
+        const uint32_t row0 = __shfl_sync(0xffffffffu, row0_l, 0);
+        const uint32_t n = hdr & 0xffff, nn = hdr >> 16;
+        const uint32_t* vals = reinterpret_cast<const uint32_t*>(a.key.pages + size_t(p) * kPageSize) + 1;
+        w.page_cnt = 0;
+        if (nn == n) {
+            const int vi0 = 4 * int(lane) - 1 + int(half * 4 * kWordsPerStep);
+            if (half == 0 || n >= 4 * kWordsPerStep)
+                push_step(a, w, step_take(a, q, bloom, use_bloom) & step_valid(vi0, n), vi0, vals, row0, u);
+        } else if (half == 0) {
+            // A page with NULLs is read whole by the unit of its first half.
+            scan_page_nulls(a, w, bloom, use_bloom, u, n, row0);
+        }
+        if (a.mode != 2) {
+            flush(a, w, u);
+            if (a.mode == 0 && lane == 0) a.page_counts[u] = w.page_cnt;
         }
     }
+    if (a.mode == 2) flush(a, w, 0);
 }
 
 } // namespace
@@ -380,36 +349,28 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
     if (!key.npages) return 0;
     size_t bloom_bytes = bloom_smem && ht.bloom ? (sizeof(uint32_t) << ht.bloom_log2) : 0;
     if (bloom_bytes > kBloomSmemMax) bloom_bytes = 0;
-    ScanArgs a{key, ht, uint32_t(mode), bloom_bytes ? 1u : 0u, page_counts, page_off, cursor,
-               out_rows, out_ents, out_mult, capacity, err};
-    // TMA staging (opt-in: B200JOIN_SCAN_TMA=1) needs device-memory pages
-    // (not pages read in place from the host) with a 16-byte aligned base.
-    // Measured on snowflake x0.7 it ran at 92 us against 68 us for the
-    // load-based kernel: one 8 KiB slot per warp leaves room for only 16
-    // warps per SM next to the bloom filter, too few to hide page latency.
-    static const bool tma_opt_in = [] {
-        const char* e = std::getenv("B200JOIN_SCAN_TMA");
-        return e && std::atoi(e) != 0;
+    // Bulk prefetch into L2 of the pages ahead of each warp (tuning knob
+    // B200JOIN_SCAN_PREFETCH = 0-2 pages; device-memory pages only). Off by
+    // default: on snowflake x1.0 the kernel took 72 us without it, 81 us one
+    // page ahead and 85 us two pages ahead.
+    static const uint32_t ahead = [] {
+        const char* e = std::getenv("B200JOIN_SCAN_PREFETCH");
+        return e ? uint32_t(std::min(2, std::max(0, std::atoi(e)))) : 0u;
     }();
-    const bool tma = tma_opt_in && !(key.flags & kColHostPages) && (reinterpret_cast<uintptr_t>(key.pages) % 16) == 0;
+    const uint32_t prefetch = (key.flags & kColHostPages) ? 0u : ahead;
+    ScanArgs a{key,      ht,       uint32_t(mode), bloom_bytes ? 1u : 0u, prefetch,
+               ht.bloom_log2 ? (1u << ht.bloom_log2) : 0u, 1u << 27,
+               page_counts, page_off, cursor, out_rows, out_ents, out_mult, capacity, err};
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(k_scan_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBloomSmemMax));
-        cudaFuncSetAttribute(k_scan_probe_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(kWarpsPerCta * kPageSize + kBloomSmemMax));
         configured = true;
-    }
-    if (tma) {
-        size_t smem = kWarpsPerCta * kPageSize + bloom_bytes;
-        uint64_t ctas = std::min<uint64_t>((uint64_t(key.npages) + kWarpsPerCta - 1) / kWarpsPerCta, uint64_t(num_sms));
-        k_scan_probe_tma<<<unsigned(ctas), kCtaThreads, smem, st>>>(a);
-        return 1;
     }
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan_probe, kCtaThreads, bloom_bytes);
     per_sm = std::max(1, per_sm);
-    uint64_t ctas = std::min<uint64_t>((uint64_t(key.npages) + kWarpsPerCta - 1) / kWarpsPerCta,
-                                       uint64_t(num_sms) * per_sm);
+    const uint64_t ctas = std::min<uint64_t>((uint64_t(key.npages) + kWarpsPerCta - 1) / kWarpsPerCta,
+                                             uint64_t(num_sms) * per_sm);
     k_scan_probe<<<unsigned(ctas), kCtaThreads, bloom_bytes, st>>>(a);
     return 1;
 }

@@ -117,11 +117,13 @@ int emit_output(const Items& in, const uint64_t* out_off, const SlotSources& src
 int items_mult(const Items& in, uint64_t* mult_out, cudaStream_t st);
 
 // ---- scan-side probe stage (k_scan.cu) ----
-// Streams the pages of `key` (a column of the scanned table) through shared
-// memory and probes `ht`. mode 0: per-page match counts into page_counts;
-// mode 1: items written at page_off[p]; mode 2: items appended at *cursor
-// (requires at most one match per row). bloom_smem: test ht.bloom, staged in
-// shared memory (ignored if larger than scan_probe_bloom_limit()).
+// Streams the pages of `key` (a column of the scanned table) and probes `ht`,
+// in work units of half a page (unit u = half u % 2 of page u / 2). mode 0:
+// match counts per unit into page_counts[2 npages]; mode 1: items written at
+// page_off[u] (exclusive scan of the counts, 2 npages + 1 entries); mode 2:
+// items appended at *cursor (requires at most one match per row).
+// bloom_smem: test ht.bloom, staged in shared memory (ignored if larger than
+// scan_probe_bloom_limit()).
 size_t scan_probe_bloom_limit();
 int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem, uint32_t* page_counts,
                const uint32_t* page_off, uint32_t* cursor, uint32_t* out_rows, uint32_t* out_ents, uint64_t* out_mult,
