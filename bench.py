@@ -229,6 +229,7 @@ def main():
     lat = []
     launches = 0
     scan_ms = scan_bytes = scan_n = 0
+    phase_sum = [0.0] * 4
     rows = 0
     ev0.record(stream)
     for _ in range(args.steps):
@@ -240,6 +241,8 @@ def main():
         scan_ms += s.scan_kernel_ms
         scan_bytes += s.scan_kernel_bytes
         scan_n += s.scan_kernel_launches
+        for i in range(4):
+            phase_sum[i] += s.phase_ms[i]
         rows = r.num_rows
         r.free()
     ev1.record(stream)
@@ -248,6 +251,8 @@ def main():
     ctx.profile(False)
     elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1))
     value = args.steps * world / (elapsed_ms / 1e3) if args.steps else 0.0
+    phases = {name: phase_sum[i] / max(args.steps, 1) for i, name in
+              enumerate(["build_ms", "probe_order_ms", "scan_probe_stages_ms", "output_ms"])}
     if args.mode == "value":
         for x in residents:
             x.free()
@@ -256,7 +261,8 @@ def main():
             scan_gbs = (scan_bytes / scan_n) / (scan_ms / scan_n / 1e3) / 1e9 if scan_n and scan_ms > 0 else None
             print(json.dumps({"mode": "value", "value": value, "unit": "queries/s", "steps": args.steps,
                               "scan_kernel_us": scan_ms / scan_n * 1e3 if scan_n else None,
-                              "scan_kernel_gbs": scan_gbs, "p50_ms": statistics.median(lat)}))
+                              "scan_kernel_gbs": scan_gbs, "p50_ms": statistics.median(lat),
+                              "phases": phases}))
         return 0
 
     # ---- e2e: drop-in path (bj_execute), host pages in and out ----
@@ -334,6 +340,7 @@ def main():
                          "d2h_bytes_per_step": pageable_stats.d2h_bytes,
                          "inputs": "pageable host pages, gathered into pinned staging and copied to HBM"},
         "gpu_launches": launches,
+        "phases": phases,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "traffic": traffic,
                      "kernel": "k_scan_probe over the fact's key pages",

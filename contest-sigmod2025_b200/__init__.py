@@ -71,7 +71,8 @@ class BjStats(ctypes.Structure):
                 ("d2h_bytes", ctypes.c_uint64), ("input_pages", ctypes.c_uint64), ("output_pages", ctypes.c_uint64),
                 ("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
                 ("scan_kernel_ms", ctypes.c_double), ("scan_kernel_launches", ctypes.c_uint64),
-                ("scan_kernel_bytes", ctypes.c_uint64), ("mapped_input_bytes", ctypes.c_uint64)]
+                ("scan_kernel_bytes", ctypes.c_uint64), ("mapped_input_bytes", ctypes.c_uint64),
+                ("phase_ms", ctypes.c_double * 4)]
 
 
 # Every symbol include/b200join.h declares, with its ctypes signature.

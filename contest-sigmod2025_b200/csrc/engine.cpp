@@ -237,6 +237,19 @@ struct ReadbackTape {
 
 using namespace bj;
 
+// Phase marks of a profiled call (bj_stats.phase_ms).
+constexpr size_t kPhaseMarks = 5;
+
+// Phase durations from the five phase marks of a call (bj_stats.phase_ms).
+void phase_stats(const std::vector<cudaEvent_t>& marks, bj_stats& st) {
+    if (marks.size() != kPhaseMarks) return;
+    for (size_t i = 0; i + 1 < kPhaseMarks; i++) {
+        float ms = 0;
+        BJ_CK(cudaEventElapsedTime(&ms, marks[i], marks[i + 1]));
+        st.phase_ms[i] = ms;
+    }
+}
+
 // A repeated resident query captured into a CUDA graph.
 struct GraphEntry {
     std::vector<uint64_t> key;               // plan, resident handles, flags
@@ -250,6 +263,7 @@ struct GraphEntry {
     uint8_t* pages = nullptr;                // arena pages the graph writes the result to
     bj_stats stats{};                        // launches, pipelines, input pages of one run
     std::vector<cudaEvent_t> prof;           // timed-kernel event pairs inside the graph
+    std::vector<cudaEvent_t> phase;          // phase marks inside the graph
     uint64_t prof_bytes = 0;
 };
 
@@ -296,6 +310,7 @@ struct bj_context {
             if (s) cudaStreamSynchronize(s);
     }
     std::vector<cudaEvent_t> prof_events;  // pairs around timed launches
+    std::vector<cudaEvent_t> phase_events; // phase marks of the call (kPhaseMarks when complete)
     uint64_t prof_bytes = 0;
 
     PinnedBlock take_pinned(size_t bytes) {
@@ -578,6 +593,8 @@ class Executor {
         cudaEvent_t start = ctx_->pipe_event(np);
         if (!start) throw Fail{BJ_ERR_CUDA, "event creation failed"};
         BJ_CK(cudaEventRecord(start, main));
+        st_ = main;
+        mark_phase();
         int next_side = 0;
         for (size_t p = 0; p < np; p++) {
             const PipelinePlan& pp = ex_.pipelines[p];
@@ -623,6 +640,16 @@ class Executor {
         BJ_CK(cudaEventRecordWithFlags(e, st_, ctx_->graph_output ? cudaEventRecordExternal : cudaEventRecordDefault));
     }
     void begin_timed() { record_timed(); }
+    // Phase marks on the main stream (profiling only): the call's start, the
+    // root pipeline's start, its probe order fixed, its stages done, its
+    // output written.
+    void mark_phase() {
+        if (!ctx_->profile) return;
+        cudaEvent_t e;
+        BJ_CK(cudaEventCreate(&e));
+        ctx_->phase_events.push_back(e);
+        BJ_CK(cudaEventRecordWithFlags(e, st_, ctx_->graph_output ? cudaEventRecordExternal : cudaEventRecordDefault));
+    }
     void end_timed(uint64_t bytes) {
         record_timed();
         ctx_->prof_bytes += bytes;
@@ -661,6 +688,8 @@ class Executor {
         Items items{};
         items.count = uint32_t(in.rows);
         items.nprobes = 0;
+        const bool root = res != nullptr;
+        if (root) mark_phase();
 
         // Probe order: ascending sampled hit rate (most selective first).
         size_t np = pp.probes.size();
@@ -670,9 +699,15 @@ class Executor {
         if (np) {
             uint32_t nsample = uint32_t(std::min<uint64_t>(in.rows, 4096));
             uint32_t* hits = alloc<uint32_t>(np);
+            SampleSet set{};
+            set.n = int(np);
+            for (size_t k = 0; k < np; k++) {
+                set.p[k].key = col(pp.probes[k].probe_attr);
+                set.p[k].ht = hts_[pp.probes[k].child].view;
+            }
+            launched(sample_probes(set, nsample, hits, st_));
             for (size_t k = 0; k < np; k++) {
                 BuiltHT& child = hts_[pp.probes[k].child];
-                launched(sample_probe(col(pp.probes[k].probe_attr), nsample, child.view, hits + k, st_));
                 stash_u32(ctx_, hits + k, int(k));
                 stash_u32(ctx_, child.dflags, int(16 + 2 * k));
                 stash_u32(ctx_, child.dflags + 1, int(17 + 2 * k));
@@ -687,12 +722,15 @@ class Executor {
             }
             std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return rate[a] < rate[b]; });
         }
+        if (root) mark_phase();
         std::vector<uint32_t> stage_of(np);
         std::vector<HTView> by_stage(np);
         for (size_t s = 0; s < np; s++) {
+            stage_of[order[s]] = uint32_t(s);
+            by_stage[s] = hts_[pp.probes[order[s]].child].view;
+        }
+        for (size_t s = 0; s < np; s++) {
             uint32_t k = order[s];
-            stage_of[k] = uint32_t(s);
-            by_stage[s] = hts_[pp.probes[k].child].view;
             const HTView& ht = by_stage[s];
             if (items.rows == nullptr) {
                 // Scan stage: stream the key pages of the scanned table.
@@ -725,8 +763,8 @@ class Executor {
                     items = next;
                     continue;
                 } else {
-                    // Counts per work unit of the scan (two per page).
-                    const uint32_t units = 2 * key.npages;
+                    // Counts per work unit of the scan (a few per page).
+                    const uint32_t units = scan_probe_units(key.npages);
                     uint32_t* pc = alloc<uint32_t>(units);
                     uint32_t* poff = alloc<uint32_t>(size_t(units) + 1);
                     bool timed = ctx_->profile;
@@ -759,22 +797,37 @@ class Executor {
             bool bloom = ht.bloom && rate[k] < 0.5;
             const DevColumn& key = col(pp.probes[k].probe_attr);
             if (bh.unique) {
+                // This stage and the unique-key stages right after it run as
+                // one fused chain.
+                ProbeChain ch{};
+                bool unit = items.mult == nullptr;
+                size_t s2 = s;
+                while (s2 < np && ch.n < kMaxChain && hts_[pp.probes[order[s2]].child].unique) {
+                    const uint32_t k2 = order[s2];
+                    ChainStage& c = ch.st[ch.n++];
+                    c.key = col(pp.probes[k2].probe_attr);
+                    c.ht = by_stage[s2];
+                    c.use_bloom = (c.ht.bloom && rate[k2] < 0.5) ? 1 : 0;
+                    unit = unit && hts_[pp.probes[k2].child].unit_mult;
+                    s2++;
+                }
                 uint32_t cap = items.count;
                 ItemsOut out{};
                 out.rows = alloc<uint32_t>(cap);
-                for (size_t j = 0; j <= s; j++) out.ents[j] = alloc<uint32_t>(cap);
-                out.mult = (items.mult == nullptr && bh.unit_mult) ? nullptr : alloc<uint64_t>(cap);
+                for (size_t j = 0; j < s2; j++) out.ents[j] = alloc<uint32_t>(cap);
+                out.mult = unit ? nullptr : alloc<uint64_t>(cap);
                 uint32_t* cursor = alloc<uint32_t>(1);
                 BJ_CK(cudaMemsetAsync(cursor, 0, sizeof(uint32_t), st_));
-                launched(probe_stage_unique(items, key, ht, out, cursor, cap, bloom, ctx_->d_err, ctx_->num_sms, st_));
+                launched(probe_chain_unique(items, ch, out, cursor, cap, ctx_->d_err, ctx_->num_sms, st_));
                 Items next{};
                 next.rows = out.rows;
-                for (size_t j = 0; j <= s; j++) next.ents[j] = out.ents[j];
+                for (size_t j = 0; j < s2; j++) next.ents[j] = out.ents[j];
                 next.mult = out.mult;
                 next.count = cap;
                 next.dcount = cursor;
-                next.nprobes = int(s + 1);
+                next.nprobes = int(s2);
                 items = next;
+                s = s2 - 1;
                 continue;
             }
             resolve(items);
@@ -816,7 +869,9 @@ class Executor {
             }
         }
         if (pp.build_key >= 0) return build(pi, items, src, by_stage);
+        mark_phase();
         output(items, src, by_stage, *res, flags);
+        mark_phase();
         return true;
     }
 
@@ -1124,9 +1179,12 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
             res->stats.scan_kernel_ms += k;
             res->stats.scan_kernel_launches++;
         }
+        phase_stats(ctx->phase_events, res->stats);
         res->stats.scan_kernel_bytes = ctx->prof_bytes;
         for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
         ctx->prof_events.clear();
+        for (cudaEvent_t e : ctx->phase_events) cudaEventDestroy(e);
+        ctx->phase_events.clear();
         ctx->prof_bytes = 0;
         res->stats.kernel_launches = ctx->launches - launches0;
         res->stats.pipelines = pipes;
@@ -1183,6 +1241,8 @@ void destroy_graph(GraphEntry& g) {
     g.exec = nullptr;
     for (cudaEvent_t e : g.prof) cudaEventDestroy(e);
     g.prof.clear();
+    for (cudaEvent_t e : g.phase) cudaEventDestroy(e);
+    g.phase.clear();
 }
 
 bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resident* const* resident, int flags) {
@@ -1241,8 +1301,10 @@ bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resid
                 if (used[c]) g.stats.input_pages += tables[i]->cols[c].npages;
         }
         g.prof = ctx->prof_events;
+        g.phase = ctx->phase_events;
         g.prof_bytes = ctx->prof_bytes;
         ctx->prof_events.clear();
+        ctx->phase_events.clear();
         ctx->prof_bytes = 0;
         ctx->arena.reset();
         return true;
@@ -1258,6 +1320,8 @@ bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resid
         ctx->graph_output = false;
         for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
         ctx->prof_events.clear();
+        for (cudaEvent_t e : ctx->phase_events) cudaEventDestroy(e);
+        ctx->phase_events.clear();
         ctx->prof_bytes = 0;
         ctx->sync_all();
         ctx->arena.reset();
@@ -1299,6 +1363,7 @@ int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& typ
             res->stats.scan_kernel_ms += k;
             res->stats.scan_kernel_launches++;
         }
+        phase_stats(g.phase, res->stats);
         res->stats.scan_kernel_bytes = g.prof_bytes;
         res->stats.kernel_launches = g.stats.kernel_launches;
         res->stats.pipelines = g.stats.pipelines;

@@ -22,6 +22,8 @@
 //     it before touching the buckets.
 #include "launch.h"
 
+#include <algorithm>
+
 namespace bj {
 namespace {
 
@@ -127,18 +129,20 @@ __global__ void k_ht_flags(HTView ht, uint32_t nbuckets, uint32_t* __restrict__ 
     }
 }
 
-__global__ void k_sample_probe(DevColumn key, uint32_t nsample, HTView ht, uint32_t* hits) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nsample || key.nrows == 0) return;
-    uint32_t row = uint32_t((uint64_t(i) * key.nrows) / nsample);
+// Hit counts of evenly spaced sample rows against every probe of a pipeline:
+// blockIdx.y selects the probe.
+__global__ void k_sample_probes(SampleSet set, uint32_t nsample, uint32_t* hits) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const SampleProbe& sp = set.p[blockIdx.y];
+    if (i >= nsample || sp.key.nrows == 0) return;
+    const uint32_t row = uint32_t((uint64_t(i) * sp.key.nrows) / nsample);
     uint64_t v;
-    if (!col_get(key, row, v)) return;
-    uint32_t k = uint32_t(v);
-    uint64_t h = key_hash(k);
-    uint32_t b = uint32_t(h >> ht.shift);
-    for (uint32_t j = ht.bucket_off[b]; j < ht.bucket_off[b + 1]; j++)
-        if (ht.keys[j] == k) {
-            atomicAdd(hits, 1u);
+    if (!col_get(sp.key, row, v)) return;
+    const uint32_t k = uint32_t(v);
+    const uint32_t b = uint32_t(key_hash(k) >> sp.ht.shift);
+    for (uint32_t j = sp.ht.bucket_off[b]; j < sp.ht.bucket_off[b + 1]; j++)
+        if (sp.ht.keys[j] == k) {
+            atomicAdd(hits + blockIdx.y, 1u);
             return;
         }
 }
@@ -183,10 +187,10 @@ int ht_flags(HTView ht, uint32_t nbuckets, uint32_t* flags, int num_sms, cudaStr
     return 1;
 }
 
-int sample_probe(const DevColumn& key, uint32_t nsample, HTView ht, uint32_t* hits, cudaStream_t st) {
-    cudaMemsetAsync(hits, 0, sizeof(uint32_t), st);
-    if (!nsample) return 0;
-    k_sample_probe<<<(nsample + 255) / 256, 256, 0, st>>>(key, nsample, ht, hits);
+int sample_probes(const SampleSet& set, uint32_t nsample, uint32_t* hits, cudaStream_t st) {
+    cudaMemsetAsync(hits, 0, sizeof(uint32_t) * std::max(set.n, 1), st);
+    if (!nsample || set.n <= 0) return 0;
+    k_sample_probes<<<dim3((nsample + 255) / 256, unsigned(set.n)), 256, 0, st>>>(set, nsample, hits);
     return 1;
 }
 

@@ -116,46 +116,65 @@ __global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HT
     }
 }
 
-// Unique-key probe stage: persistent grid-stride loop, at most one match per
-// item, warp-aggregated reservation of output slots.
-__global__ void __launch_bounds__(256) k_probe_unique(Items in, DevColumn key, HTView ht, ItemsOut out,
-                                                      uint32_t* cursor, uint32_t capacity, int use_bloom,
-                                                      uint32_t* err) {
+// A chain of consecutive probe stages against tables with unique keys: every
+// item probes stage 0, and while it matches, the next stage, so a row that
+// misses is dropped at its first miss (the fused probe_0 -> probe_1 -> ...
+// of JoinPipeline.hpp:111-131, with early exit). Persistent grid-stride
+// loop, at most one match per stage, warp-aggregated reservation of output
+// slots.
+__global__ void __launch_bounds__(256) k_probe_chain(Items in, ProbeChain ch, ItemsOut out, uint32_t* cursor,
+                                                     uint32_t capacity, uint32_t* err) {
     const uint32_t n = in.dcount ? *in.dcount : in.count;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t lane = threadIdx.x & 31;
     // Whole warps iterate together so the ballot sees every lane.
     for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
-        uint32_t i = base + lane;
-        bool hit = false;
-        uint32_t row = 0, e = 0;
-        if (i < n) {
-            row = item_row(in, i);
+        const uint32_t i = base + lane;
+        bool hit = i < n;
+        uint32_t row = 0;
+        uint32_t e[kMaxChain];
+        if (hit) row = item_row(in, i);
+#pragma unroll
+        for (int t = 0; t < kMaxChain; t++) {
+            e[t] = 0;
+            if (t >= ch.n || !hit) continue;
+            const ChainStage& c = ch.st[t];
             uint64_t v;
-            if (row >= key.nrows) {
+            if (row >= c.key.nrows) {
                 record_error(err, kErrRowRange);
-            } else if (col_get(key, row, v)) {
-                for_matches(ht, uint32_t(v), use_bloom != 0, [&](uint32_t j) {
-                    if (!hit) e = j;
-                    hit = true;
+                hit = false;
+            } else if (!col_get(c.key, row, v)) {
+                hit = false;
+            } else {
+                bool found = false;
+                for_matches(c.ht, uint32_t(v), c.use_bloom != 0, [&](uint32_t j) {
+                    if (!found) e[t] = j;
+                    found = true;
                 });
+                hit = found;
             }
         }
-        uint32_t mask = __ballot_sync(0xffffffffu, hit);
+        const uint32_t mask = __ballot_sync(0xffffffffu, hit);
         if (!mask) continue;
         uint32_t wbase = 0;
         if (lane == 0) wbase = atomicAdd(cursor, __popc(mask));
         wbase = __shfl_sync(0xffffffffu, wbase, 0);
         if (!hit) continue;
-        uint32_t o = wbase + __popc(mask & ((1u << lane) - 1));
+        const uint32_t o = wbase + __popc(mask & ((1u << lane) - 1));
         if (o >= capacity) {
             record_error(err, kErrCapacity);
             continue;
         }
         out.rows[o] = row;
         for (int p = 0; p < in.nprobes; p++) out.ents[p][o] = in.ents[p][i];
-        out.ents[in.nprobes][o] = e;
-        if (out.mult) out.mult[o] = item_mult(in, i) * ht.mult[e];
+        uint64_t m = item_mult(in, i);
+#pragma unroll
+        for (int t = 0; t < kMaxChain; t++) {
+            if (t >= ch.n) continue;
+            out.ents[in.nprobes + t][o] = e[t];
+            m *= ch.st[t].ht.mult[e[t]];
+        }
+        if (out.mult) out.mult[o] = m;
     }
 }
 
@@ -232,11 +251,11 @@ int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mod
     return 1;
 }
 
-int probe_stage_unique(const Items& in, const DevColumn& key, const HTView& ht, ItemsOut out, uint32_t* cursor,
-                       uint32_t capacity, bool use_bloom, uint32_t* err, int num_sms, cudaStream_t st) {
-    if (!in.count) return 0;
+int probe_chain_unique(const Items& in, const ProbeChain& chain, ItemsOut out, uint32_t* cursor, uint32_t capacity,
+                       uint32_t* err, int num_sms, cudaStream_t st) {
+    if (!in.count || chain.n <= 0) return 0;
     uint32_t blocks = std::min<uint32_t>((in.count + 255) / 256, uint32_t(num_sms) * 8);
-    k_probe_unique<<<blocks, 256, 0, st>>>(in, key, ht, out, cursor, capacity, use_bloom, err);
+    k_probe_chain<<<blocks, 256, 0, st>>>(in, chain, out, cursor, capacity, err);
     return 1;
 }
 

@@ -46,7 +46,8 @@ constexpr int kCtaThreads = kWarpsPerCta * 32;
 constexpr int kPerLane = 4;                          // buffered candidates per lane
 constexpr int kBatch = 32 * kPerLane;                // buffer entries per warp
 constexpr int kStepWords = 8;                        // 16-byte words per lane per step
-constexpr uint32_t kWordsPerStep = 32 * kStepWords;  // 256 words = 4 KiB
+constexpr uint32_t kWordsPerStep = 32 * kStepWords;  // 256 words = 4 KiB: one work unit
+constexpr uint32_t kUnitsPerPage = kPageSize / (16 * kWordsPerStep);
 constexpr size_t kBloomSmemMax = size_t(4) << kBloomMaxLog2;  // 128 KiB
 
 struct ScanArgs {
@@ -54,14 +55,14 @@ struct ScanArgs {
     HTView ht;
     uint32_t mode;             // 0 count per unit, 1 emit at unit offsets, 2 emit with atomics (unique keys)
     uint32_t use_bloom;        // stage ht.bloom in shared memory and test it
-    uint32_t prefetch;         // pages ahead of its current one a warp bulk-prefetches into L2 (0-2)
+    uint32_t prefetch;         // work units ahead of its current one a warp prefetches into L2 (0-2)
     // Multipliers for the bloom test, given at run time so that the shifts
     // they stand for (hh >> (32 - log2w), hh >> 5) run on the multiply pipe
     // as __umulhi instead of competing with the shifts on the integer pipe.
     uint32_t word_mul;         // 1 << ht.bloom_log2
     uint32_t field_mul;        // 1 << 27
-    uint32_t* page_counts;     // mode 0 output: matches per work unit (2 npages; unit u = half u % 2 of page u / 2)
-    const uint32_t* page_off;  // mode 1 input: exclusive scan of page_counts (2 npages + 1)
+    uint32_t* page_counts;     // mode 0 output: matches per work unit (scan_probe_units(npages))
+    const uint32_t* page_off;  // mode 1 input: exclusive scan of page_counts (units + 1)
     uint32_t* cursor;          // mode 2 global item counter
     uint32_t* out_rows;
     uint32_t* out_ents;
@@ -72,10 +73,9 @@ struct ScanArgs {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 
-// Asks the TMA unit to bring `bytes` (a multiple of 16, 16-byte aligned
-// source) into L2; nothing waits for it.
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+// Brings the line holding p into L2; nothing waits for it.
+__device__ __forceinline__ void prefetch_line_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
 // Warp-wide exclusive prefix sum; `total` receives the sum.
@@ -285,20 +285,21 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
     const bool use_bloom = a.use_bloom != 0;
     const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
     const uint32_t total_warps = gridDim.x * kWarpsPerCta;
-    const uint32_t nunits = 2 * a.key.npages;
+    const uint32_t nunits = kUnitsPerPage * a.key.npages;
     const uint32_t first = blockIdx.x * kWarpsPerCta + warp;
 
-    // Work unit u is half u % 2 (4 KiB, 256 words) of page u / 2; the warp's
+    // Work unit u is part u % kUnitsPerPage (4 KiB, 256 words) of page
+    // u / kUnitsPerPage; the warp's
     // units are first, first + total_warps, ... (half pages balance the
     // warps better than whole pages: 10.6 units per warp against 5.3 pages
     // on the 50M-row fact). A unit's loads are all issued before any is
     // used, and every load stays inside its 8 KiB page.
     auto load_unit = [&](uint32_t u, uint4 (&q)[kStepWords], uint32_t& hdr, uint32_t& row0) {
-        const uint4* pw = reinterpret_cast<const uint4*>(a.key.pages + size_t(u >> 1) * kPageSize);
+        const uint4* pw = reinterpret_cast<const uint4*>(a.key.pages + size_t(u / kUnitsPerPage) * kPageSize);
 #pragma unroll
-        for (int i = 0; i < kStepWords; i++) q[i] = __ldg(pw + (u & 1) * kWordsPerStep + lane + 32 * i);
+        for (int i = 0; i < kStepWords; i++) q[i] = __ldg(pw + (u % kUnitsPerPage) * kWordsPerStep + lane + 32 * i);
         hdr = lane == 0 ? __ldg(reinterpret_cast<const uint32_t*>(pw)) : 0;
-        row0 = lane == 0 ? __ldg(a.key.row_start + (u >> 1)) : 0;
+        row0 = lane == 0 ? __ldg(a.key.row_start + u / kUnitsPerPage) : 0;
     };
     uint4 q[kStepWords];
     uint32_t hdr_l = 0, row0_l = 0;
@@ -312,11 +313,14 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
 
     WarpState w{bkey[warp], brow[warp], 0, 0};
     for (uint32_t u = first; u < nunits; u += total_warps) {
-        const uint32_t p = u >> 1, half = u & 1;
+        const uint32_t p = u / kUnitsPerPage, part = u % kUnitsPerPage;
         load_unit(u, q, hdr_l, row0_l);
-        if (a.prefetch && lane == 0 && half == 0) {
-            const uint64_t ahead = uint64_t(p) + uint64_t(a.prefetch) * (total_warps / 2);
-            if (ahead < a.key.npages) prefetch_l2(a.key.pages + size_t(ahead) * kPageSize, kPageSize);
+        if (a.prefetch) {
+            // One 128-byte line per lane of the unit a.prefetch units ahead.
+            const uint64_t un = uint64_t(u) + uint64_t(a.prefetch) * total_warps;
+            if (un < nunits)
+                prefetch_line_l2(a.key.pages + size_t(un / kUnitsPerPage) * kPageSize +
+                                 (un % kUnitsPerPage) * (16 * kWordsPerStep) + (lane * 128) % (16 * kWordsPerStep));
         }
         const uint32_t hdr = __shfl_sync(0xffffffffu, hdr_l, 0);
         const uint32_t row0 = __shfl_sync(0xffffffffu, row0_l, 0);
@@ -324,11 +328,11 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
         const uint32_t* vals = reinterpret_cast<const uint32_t*>(a.key.pages + size_t(p) * kPageSize) + 1;
         w.page_cnt = 0;
         if (nn == n) {
-            const int vi0 = 4 * int(lane) - 1 + int(half * 4 * kWordsPerStep);
-            if (half == 0 || n >= 4 * kWordsPerStep)
+            const int vi0 = 4 * int(lane) - 1 + int(part * 4 * kWordsPerStep);
+            if (vi0 - int(lane) * 4 < int(n))  // some value of the unit is below n
                 push_step(a, w, step_take(a, q, bloom, use_bloom) & step_valid(vi0, n), vi0, vals, row0, u);
-        } else if (half == 0) {
-            // A page with NULLs is read whole by the unit of its first half.
+        } else if (part == 0) {
+            // A page with NULLs is read whole by its first unit.
             scan_page_nulls(a, w, bloom, use_bloom, u, n, row0);
         }
         if (a.mode != 2) {
@@ -342,6 +346,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
 } // namespace
 
 size_t scan_probe_bloom_limit() { return kBloomSmemMax; }
+uint32_t scan_probe_units(uint32_t npages) { return kUnitsPerPage * npages; }
 
 int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem, uint32_t* page_counts,
                const uint32_t* page_off, uint32_t* cursor, uint32_t* out_rows, uint32_t* out_ents, uint64_t* out_mult,
@@ -349,10 +354,9 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
     if (!key.npages) return 0;
     size_t bloom_bytes = bloom_smem && ht.bloom ? (sizeof(uint32_t) << ht.bloom_log2) : 0;
     if (bloom_bytes > kBloomSmemMax) bloom_bytes = 0;
-    // Bulk prefetch into L2 of the pages ahead of each warp (tuning knob
-    // B200JOIN_SCAN_PREFETCH = 0-2 pages; device-memory pages only). Off by
-    // default: on snowflake x1.0 the kernel took 72 us without it, 81 us one
-    // page ahead and 85 us two pages ahead.
+    // L2 prefetch of the work unit this many units ahead of each warp's
+    // current one (tuning knob B200JOIN_SCAN_PREFETCH = 0-2; device-memory
+    // pages only).
     static const uint32_t ahead = [] {
         const char* e = std::getenv("B200JOIN_SCAN_PREFETCH");
         return e ? uint32_t(std::min(2, std::max(0, std::atoi(e)))) : 0u;

@@ -68,13 +68,25 @@ constexpr uint32_t kTile = 256;  // items per CTA tile in stage kernels (one per
 int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mode, uint32_t* tile_counts,
                 const uint32_t* tile_offsets, ItemsOut out, bool use_bloom, uint32_t* err, cudaStream_t st);
 
-// Probe stage against a table with unique keys (at most one match per item):
-// a persistent grid-stride pass appends items with warp-aggregated atomics at
-// *cursor; reads the input count from in.dcount when set, so no host
-// round trip is needed between stages. out.mult may be null when both the
-// input and the table carry only multiplicity 1.
-int probe_stage_unique(const Items& in, const DevColumn& key, const HTView& ht, ItemsOut out, uint32_t* cursor,
-                       uint32_t capacity, bool use_bloom, uint32_t* err, int num_sms, cudaStream_t st);
+// Consecutive probe stages against tables with unique keys (at most one
+// match per item and stage), fused: an item probes the stages in order and
+// is dropped at its first miss; survivors are appended with warp-aggregated
+// atomics at *cursor, with one entry per stage after the input's. Reads the
+// input count from in.dcount when set, so no host round trip is needed
+// between stages. out.mult may be null when the input and every table carry
+// only multiplicity 1.
+constexpr int kMaxChain = 8;
+struct ChainStage {
+    DevColumn key;   // probe key column of the scanned input
+    HTView ht;
+    int use_bloom;   // test ht.bloom (in global memory) first
+};
+struct ProbeChain {
+    ChainStage st[kMaxChain];
+    int n;
+};
+int probe_chain_unique(const Items& in, const ProbeChain& chain, ItemsOut out, uint32_t* cursor, uint32_t capacity,
+                       uint32_t* err, int num_sms, cudaStream_t st);
 
 // Source of one value slot: a column of the scanned input read at the item's
 // row, or payload slot `slot` of the entry matched by probe `probe`.
@@ -118,13 +130,14 @@ int items_mult(const Items& in, uint64_t* mult_out, cudaStream_t st);
 
 // ---- scan-side probe stage (k_scan.cu) ----
 // Streams the pages of `key` (a column of the scanned table) and probes `ht`,
-// in work units of half a page (unit u = half u % 2 of page u / 2). mode 0:
-// match counts per unit into page_counts[2 npages]; mode 1: items written at
-// page_off[u] (exclusive scan of the counts, 2 npages + 1 entries); mode 2:
-// items appended at *cursor (requires at most one match per row).
+// in work units of part of a page (scan_probe_units(npages) of them, in page
+// order). mode 0: match counts per unit into page_counts; mode 1: items
+// written at page_off[u] (exclusive scan of the counts, units + 1 entries);
+// mode 2: items appended at *cursor (requires at most one match per row).
 // bloom_smem: test ht.bloom, staged in shared memory (ignored if larger than
 // scan_probe_bloom_limit()).
 size_t scan_probe_bloom_limit();
+uint32_t scan_probe_units(uint32_t npages);
 int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem, uint32_t* page_counts,
                const uint32_t* page_off, uint32_t* cursor, uint32_t* out_rows, uint32_t* out_ents, uint64_t* out_mult,
                uint32_t capacity, uint32_t* err, int num_sms, cudaStream_t st);
@@ -148,8 +161,18 @@ int bloom_build(const uint32_t* keys, const uint32_t* mask, uint32_t n, uint32_t
 // Flags of a built table: [0] = 1 if some key repeats, [1] = 1 if some mult > 1.
 // The entry count is read on the device from bucket_off[nbuckets].
 int ht_flags(HTView ht, uint32_t nbuckets, uint32_t* flags, int num_sms, cudaStream_t st);
-// Counts, for n sampled rows of `key` (evenly spaced), how many hit `ht`.
-int sample_probe(const DevColumn& key, uint32_t nsample, HTView ht, uint32_t* hits, cudaStream_t st);
+// Counts, for nsample evenly spaced rows of each probe's key column, how many
+// hit its table: hits[p] for probe p, all probes in one launch (the role of
+// the reference's 64-row join samples, engine/query/QueryPlan.cpp:719-746).
+struct SampleProbe {
+    DevColumn key;
+    HTView ht;
+};
+struct SampleSet {
+    SampleProbe p[kMaxProbes];
+    int n;
+};
+int sample_probes(const SampleSet& set, uint32_t nsample, uint32_t* hits, cudaStream_t st);
 
 // ---- output pages (k_output.cu) ----
 // Fixed-width page writer: rows_per_page rows per page.

@@ -123,6 +123,12 @@ typedef struct bj_stats {
     uint64_t scan_kernel_launches;
     uint64_t scan_kernel_bytes; /* page bytes those launches had to read */
     uint64_t mapped_input_bytes; /* input page bytes read in place from pinned host memory */
+    /* Device time of the call's phases when profiling is on (0 otherwise, and
+     * for a query whose result is found empty before its output): [0] build
+     * pipelines up to the root pipeline's start, [1] the root pipeline's probe
+     * ordering (hit-rate sampling), [2] its scan and probe stages, [3] its
+     * output (result pages written). */
+    double phase_ms[4];
 } bj_stats;
 
 /* Replaces Contest::build_context (engine/Execute.cpp:42-46). Creates the CUDA
