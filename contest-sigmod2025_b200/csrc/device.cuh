@@ -53,10 +53,15 @@ struct DevColumn {
     uint32_t nrows;
     int32_t type;
     uint32_t flags;  // kColNulls | kColLongStrings | kColHostPages
+    // Rows per page when every page but the last holds exactly rpp rows and
+    // the last at most rpp (pages written full, as the contest's writers do):
+    // row r is then on page r / rpp. 0 otherwise.
+    uint32_t rpp;
 };
 constexpr uint32_t kColNulls = 1;        // some page has NULLs
 constexpr uint32_t kColLongStrings = 2;  // long-string page runs present
 constexpr uint32_t kColHostPages = 4;    // pages are read in place from (pinned) host memory
+constexpr uint32_t kColRaggedPages = 8;  // page row counts are not uniform (rpp = 0)
 
 // String handle carried in a value slot: page index << 16 | value index in the
 // page; a long string (its own page run) uses value index 0xffff.
@@ -98,9 +103,26 @@ __device__ __forceinline__ uint64_t load_bits64(const uint8_t* bm, uint32_t k, u
 // Reads the value of `row` as a 64-bit slot. Returns false for NULL.
 // INT32 is zero-extended, INT64/FP64 are raw bits, VARCHAR yields a handle.
 __device__ __forceinline__ bool col_get(const DevColumn& c, uint32_t row, uint64_t& v) {
-    uint32_t p = locate_page(c, row);
-    uint32_t i = row - c.row_start[p];
+    uint32_t p, i;
+    if (c.rpp) {
+        p = row / c.rpp;
+        i = row - p * c.rpp;
+    } else {
+        p = locate_page(c, row);
+        i = row - c.row_start[p];
+    }
     const uint8_t* pg = c.pages + size_t(p) * kPageSize;
+    if (!(c.flags & (kColNulls | kColLongStrings))) {
+        // No NULLs and no long strings anywhere: the value index is the row's
+        // index in its page, and the header need not be read.
+        switch (c.type) {
+        case kInt32: v = *reinterpret_cast<const uint32_t*>(pg + 4 + 4 * i); break;
+        case kInt64:
+        case kFp64: v = *reinterpret_cast<const uint64_t*>(pg + 8 + 8 * size_t(i)); break;
+        default: v = make_str_handle(p, i); break;
+        }
+        return true;
+    }
     const uint32_t h = c.hdr[p];  // header from the device-side cache (pages may be in host memory)
     uint32_t nrows = h & 0xffff;
     if (c.type == kVarchar && nrows >= 0xfffe) {

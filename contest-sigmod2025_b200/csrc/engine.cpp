@@ -519,22 +519,24 @@ void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem) 
         ctx->launches += page_index_pass1(jobs[i].dpages, np, jobs[i].out->type, t.b, ctx->d_err, sc, ctx->stream);
     }
     // Read back row totals, chunk totals and flags, a few columns at a time.
-    std::vector<uint64_t> rows(jobs.size()), chunks(jobs.size()), flags(jobs.size());
-    for (size_t i0 = 0; i0 < jobs.size(); i0 += 20) {
-        size_t i1 = std::min(jobs.size(), i0 + 20);
+    std::vector<uint64_t> rows(jobs.size()), chunks(jobs.size()), flags(jobs.size()), rows0(jobs.size());
+    for (size_t i0 = 0; i0 < jobs.size(); i0 += 15) {
+        size_t i1 = std::min(jobs.size(), i0 + 15);
         for (size_t i = i0; i < i1; i++) {
-            int s = int(3 * (i - i0));
+            int s = int(4 * (i - i0));
             stash_u32(ctx, tmp[i].b.row_start + tmp[i].npages, s);
             stash_u32(ctx, tmp[i].b.chunk_base + tmp[i].npages, s + 1);
             stash_u32(ctx, tmp[i].b.flags, s + 2);
+            stash_u32(ctx, tmp[i].b.rows, s + 3);  // rows of page 0
         }
         stash_err(ctx);
         readback(ctx, 0);
         for (size_t i = i0; i < i1; i++) {
-            int s = int(3 * (i - i0));
+            int s = int(4 * (i - i0));
             rows[i] = ctx->h_small[s];
             chunks[i] = ctx->h_small[s + 1];
             flags[i] = ctx->h_small[s + 2];
+            rows0[i] = tmp[i].npages ? ctx->h_small[s + 3] : 0;
         }
     }
     for (size_t i = 0; i < jobs.size(); i++) {
@@ -546,6 +548,7 @@ void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem) 
         c.npages = tmp[i].npages;
         c.nrows = uint32_t(rows[i]);
         c.flags = uint32_t(flags[i]) | (jobs[i].in_place ? kColHostPages : 0u);
+        c.rpp = (c.flags & kColRaggedPages) ? 0u : uint32_t(rows0[i]);
         c.hdr = tmp[i].b.hdr;
         c.row_start = tmp[i].b.row_start;
         c.chunk_base = tmp[i].b.chunk_base;
@@ -877,56 +880,74 @@ class Executor {
 
     bool build(size_t pi, const Items& items, const SlotSources& src, const std::vector<HTView>& probes) {
         const PipelinePlan& pp = ex_.pipelines[pi];
-        uint32_t n = items.count;
-        uint32_t width = uint32_t(src.n);
-        TupleBuf tb{};
+        const uint32_t n = items.count;
+        const uint32_t width = uint32_t(src.n);
+        BuildArgs ba{};
+        ba.in = items;
+        ba.key = col(uint32_t(pp.build_key));
+        ba.src = src;
+        ba.ps = make_probe_set(probes.data(), items.nprobes);
+        TupleBuf& tb = ba.tb;
         tb.keys = alloc<uint32_t>(n);
         tb.mult = alloc<uint64_t>(n);
         tb.pay = alloc<uint64_t>(size_t(n) * std::max<uint32_t>(width, 1));
         tb.pnull = alloc<uint32_t>(n);
         tb.count = n;
         tb.width = width;
-        launched(emit_tuples(items, col(uint32_t(pp.build_key)), src, probes.data(), tb, ctx_->d_err, st_));
-        // Eager aggregation of identical tuples.
-        uint32_t tlog2 = std::max<uint32_t>(1, bit_width(uint64_t(n) * 2));
-        uint32_t* table = alloc<uint32_t>(size_t(1) << tlog2);
-        uint32_t* is_rep = alloc<uint32_t>(n);
-        launched(aggregate_tuples(tb, table, tlog2, is_rep, ctx_->d_err, st_));
-        // Buckets: 2^max(bit_width(n), 4) (engine/op/Hashtable.cpp:94-104), sized by
-        // the tuple count n, an upper bound of the distinct tuples, so the build
-        // needs no host round trip.
-        uint32_t nrep = n;
-        uint32_t blog2 = std::max<uint32_t>(bit_width(nrep), 4);
-        uint32_t shift = 64 - blog2;
-        size_t nb = size_t(1) << blog2;
-        uint32_t* counts = alloc<uint32_t>(nb);
-        BJ_CK(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * nb, st_));
-        launched(bucket_count(tb, is_rep, shift, counts, st_));
+        ba.is_rep = alloc<uint32_t>(n);
+        ba.err = ctx_->d_err;
+        // Sizes. Aggregation table: at least 2n slots. Buckets:
+        // 2^max(bit_width(n), 4) (engine/op/Hashtable.cpp:94-104), sized by the
+        // tuple count n, an upper bound of the distinct tuples, so the build
+        // needs no host round trip. Bloom filter: about 16 bits per key, at
+        // most 128 KiB (shared-memory staging).
+        ba.tlog2 = std::max<uint32_t>(1, bit_width(uint64_t(n) * 2));
+        const uint32_t nrep = n;
+        const uint32_t blog2 = std::max<uint32_t>(bit_width(nrep), 4);
+        ba.shift = 64 - blog2;
+        const size_t nb = size_t(1) << blog2;
+        const uint32_t wlog2 =
+            std::min<uint32_t>(kBloomMaxLog2, std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1)));
+        // Everything that must start at zero, cleared by one memset.
+        const size_t zb_table = sizeof(uint32_t) << ba.tlog2, zb_counts = sizeof(uint32_t) * nb,
+                     zb_cursor = sizeof(uint32_t) * nb, zb_bloom = sizeof(uint32_t) << wlog2, zb_flags = 256,
+                     zb_scan = scan_status_bytes(nb);
+        auto round = [](size_t x) { return (x + 255) & ~size_t(255); };
+        const size_t zbytes = round(zb_table) + round(zb_counts) + round(zb_cursor) + round(zb_bloom) + zb_flags +
+                              round(zb_scan);
+        uint8_t* z = alloc<uint8_t>(zbytes);
+        BJ_CK(cudaMemsetAsync(z, 0, zbytes, st_));
+        ba.table = reinterpret_cast<uint32_t*>(z);
+        z += round(zb_table);
+        ba.counts = reinterpret_cast<uint32_t*>(z);
+        z += round(zb_counts);
+        uint32_t* cursor = reinterpret_cast<uint32_t*>(z);
+        z += round(zb_cursor);
+        uint32_t* bloom = reinterpret_cast<uint32_t*>(z);
+        z += round(zb_bloom);
+        uint32_t* dflags = reinterpret_cast<uint32_t*>(z);
+        z += zb_flags;
+        void* scan_status = zb_scan ? z : nullptr;
+
+        launched(emit_aggregate(ba, st_));
         uint32_t* off = alloc<uint32_t>(nb + 1);
-        launched(scan_exclusive_u32(counts, off, nb, A_, st_));
-        uint32_t* cursor = alloc<uint32_t>(nb);
-        BJ_CK(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * nb, st_));
+        launched(scan_exclusive_u32_zeroed(ba.counts, off, nb, scan_status, ctx_->d_err, st_));
         HTView ht{};
         ht.bucket_off = off;
         ht.keys = alloc<uint32_t>(nrep);
         ht.mult = alloc<uint64_t>(nrep);
         ht.pay = alloc<uint64_t>(size_t(nrep) * std::max<uint32_t>(width, 1));
         ht.pnull = alloc<uint32_t>(nrep);
-        ht.shift = shift;
+        ht.shift = ba.shift;
         ht.nentries = nrep;
         ht.width = width;
-        launched(bucket_scatter(tb, is_rep, shift, off, cursor, ht, ctx_->d_err, st_));
-        // Bloom filter: about 16 bits per key, at most 128 KiB (shared-memory staging).
-        uint32_t wlog2 = std::min<uint32_t>(kBloomMaxLog2,
-                                            std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1)));
-        uint32_t* bloom = alloc<uint32_t>(size_t(1) << wlog2);
-        launched(bloom_build(tb.keys, is_rep, n, bloom, wlog2, st_));
+        launched(scatter_bloom(tb, ba.is_rep, ba.shift, off, cursor, ht, bloom, wlog2, ctx_->d_err, st_));
         ht.bloom = bloom;
         ht.bloom_log2 = wlog2;
         hts_[pi].view = ht;
         hts_[pi].empty = false;
-        hts_[pi].dflags = alloc<uint32_t>(2);
-        launched(ht_flags(ht, uint32_t(nb), hts_[pi].dflags, ctx_->num_sms, st_));
+        hts_[pi].dflags = dflags;
+        launched(ht_flags(ht, uint32_t(nb), dflags, ctx_->num_sms, st_));
         return true;
     }
 
@@ -1441,6 +1462,7 @@ BJ_API int bj_context_create(int device, bj_context** out) {
         if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return BJ_ERR_CUDA;
     if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) return BJ_ERR_CUDA;
     if (cudaMalloc(&ctx->d_err, 256) != cudaSuccess) return BJ_ERR_OOM;
+    ctx->arena.err = ctx->d_err;
     if (cudaMalloc(&ctx->d_small, sizeof(uint64_t) * 64) != cudaSuccess) return BJ_ERR_OOM;
     if (cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_small), sizeof(uint64_t) * 64, cudaHostAllocDefault) != cudaSuccess)
         return BJ_ERR_OOM;

@@ -70,6 +70,11 @@ __global__ void k_page_headers(const uint8_t* __restrict__ pages, uint32_t npage
             c = 0;
         }
     }
+    // Uniform pages: every page but the last holds as many rows as page 0,
+    // the last at most that many.
+    const uint32_t h0 = *reinterpret_cast<const uint32_t*>(pages);
+    const uint32_t r0 = (type == kVarchar && (h0 & 0xffff) >= 0xfffe) ? 0u : (h0 & 0xffff);
+    if (r0 == 0 || (r != r0 && (p + 1 < npages || r > r0)) || (f & 2)) f |= kColRaggedPages;
     rows[p] = r;
     chunks[p] = c;
     if (f) atomicOr(flags, f);

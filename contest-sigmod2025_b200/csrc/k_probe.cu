@@ -22,12 +22,6 @@
 namespace bj {
 namespace {
 
-struct ProbeSet {
-    HTView ht[kMaxProbes];
-};
-
-__device__ __forceinline__ uint32_t item_row(const Items& in, uint32_t i) { return in.rows ? in.rows[i] : i; }
-__device__ __forceinline__ uint64_t item_mult(const Items& in, uint32_t i) { return in.mult ? in.mult[i] : 1ull; }
 
 // Entries of `ht` whose key equals `key`: calls fn(entry) for each.
 template <typename Fn>
@@ -178,39 +172,6 @@ __global__ void __launch_bounds__(256) k_probe_chain(Items in, ProbeChain ch, It
     }
 }
 
-// Value of one slot for item i (row `row`): returns false for NULL.
-__device__ __forceinline__ bool slot_value(const SlotSource& s, const Items& in, uint32_t i, uint32_t row,
-                                           const ProbeSet& ps, uint64_t& v) {
-    if (s.kind == 0) return col_get(s.col, row, v);
-    uint32_t e = in.ents[s.probe][i];
-    const HTView& ht = ps.ht[s.probe];
-    if ((ht.pnull[e] >> s.slot) & 1) return false;
-    v = ht.pay[size_t(e) * ht.width + s.slot];
-    return true;
-}
-
-__global__ void __launch_bounds__(256) k_emit_tuples(Items in, DevColumn key, SlotSources src, ProbeSet ps,
-                                                     TupleBuf out, uint32_t* err) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= in.count) return;
-    uint32_t row = item_row(in, i);
-    uint64_t kv = 0;
-    bool key_ok = row < key.nrows && col_get(key, row, kv);
-    if (row >= key.nrows) record_error(err, kErrRowRange);
-    out.keys[i] = uint32_t(kv);
-    out.mult[i] = key_ok ? item_mult(in, i) : 0ull;
-    uint32_t nulls = 0;
-    for (int j = 0; j < src.n; j++) {
-        uint64_t v = 0;
-        if (!slot_value(src.s[j], in, i, row, ps, v)) {
-            nulls |= 1u << j;
-            v = 0;
-        }
-        out.pay[size_t(i) * out.width + j] = v;
-    }
-    out.pnull[i] = nulls;
-}
-
 __global__ void k_items_mult(Items in, uint64_t* mult_out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < in.count) mult_out[i] = item_mult(in, i);
@@ -232,12 +193,6 @@ __global__ void __launch_bounds__(256) k_emit_output(Items in, const uint64_t* o
     }
 }
 
-ProbeSet make_probe_set(const HTView* probes, int n) {
-    ProbeSet ps{};
-    for (int i = 0; i < n && i < kMaxProbes; i++) ps.ht[i] = probes[i];
-    return ps;
-}
-
 } // namespace
 
 int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mode, uint32_t* tile_counts,
@@ -256,13 +211,6 @@ int probe_chain_unique(const Items& in, const ProbeChain& chain, ItemsOut out, u
     if (!in.count || chain.n <= 0) return 0;
     uint32_t blocks = std::min<uint32_t>((in.count + 255) / 256, uint32_t(num_sms) * 8);
     k_probe_chain<<<blocks, 256, 0, st>>>(in, chain, out, cursor, capacity, err);
-    return 1;
-}
-
-int emit_tuples(const Items& in, const DevColumn& key, const SlotSources& src, const HTView* probes, TupleBuf out,
-                uint32_t* err, cudaStream_t st) {
-    if (!in.count) return 0;
-    k_emit_tuples<<<(in.count + 255) / 256, 256, 0, st>>>(in, key, src, make_probe_set(probes, in.nprobes), out, err);
     return 1;
 }
 

@@ -1,8 +1,13 @@
 // Device-wide exclusive prefix sums and fills.
-// Reduce-then-scan over tiles of 4096 values (1024 threads x 4): one pass of
-// per-tile sums, a recursive scan of those sums, and a pass that scans each
-// tile and adds its base. Used for page row offsets, tile offsets of the
-// pipeline stages, bucket offsets of the hash build and output row offsets.
+// A single pass over tiles of 4096 values (1024 threads x 4) with decoupled
+// look-back (Merrill and Garland, "Single-pass Parallel Prefix Scan with
+// Decoupled Look-back", 2016): each CTA takes the next tile by ticket,
+// publishes its tile sum, reads its predecessors' published sums or
+// inclusive prefixes 32 at a time until it meets an inclusive one, and
+// publishes its own inclusive prefix. One launch (plus one memset of the
+// tile status words) for any n. Used for page row offsets, tile offsets of
+// the pipeline stages, bucket offsets of the hash build and output row
+// offsets.
 #include "launch.h"
 
 #include <algorithm>
@@ -13,6 +18,9 @@ namespace {
 constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 4;
 constexpr size_t kScanTile = size_t(kScanThreads) * kScanPer;
+// Polls of a predecessor's status before the scan gives up (error
+// kErrTimeout); predecessors hold earlier tickets, so they are running.
+constexpr uint32_t kLookbackLimit = 1u << 22;
 
 template <typename T>
 __device__ __forceinline__ T warp_inclusive(T v) {
@@ -45,17 +53,85 @@ __device__ __forceinline__ T block_exclusive(T v, T* total) {
     return res;
 }
 
+// Tile status word: sum << 2 | flag, flag 1 = the tile's own sum, 2 = the
+// inclusive prefix through the tile, 0 = not yet published. Sums must stay
+// below 2^62.
+__device__ __forceinline__ unsigned long long ld_status(const unsigned long long* p) {
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+
 template <typename T>
-__global__ void k_tile_reduce(const T* __restrict__ in, size_t n, T* __restrict__ partial) {
-    size_t base = size_t(blockIdx.x) * kScanTile;
-    T s = 0;
-    for (int i = threadIdx.x; i < int(kScanTile); i += kScanThreads) {
-        size_t j = base + i;
-        if (j < n) s += in[j];
+__global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const T* __restrict__ in, T* __restrict__ out,
+                                                                size_t n, unsigned long long* status,
+                                                                uint32_t* ticket, uint32_t* err) {
+    __shared__ uint32_t s_tile;
+    __shared__ T s_prefix;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const size_t base = size_t(tile) * kScanTile + size_t(threadIdx.x) * kScanPer;
+    T v[kScanPer];
+    T local = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        v[k] = base + k < n ? in[base + k] : T(0);
+        local += v[k];
     }
     __shared__ T total;
-    block_exclusive<T>(s, &total);
-    if (threadIdx.x == 0) partial[blockIdx.x] = total;
+    const T ex = block_exclusive<T>(local, &total);
+    if (threadIdx.x < 32) {
+        const uint32_t lane = threadIdx.x;
+        const T agg = total;
+        if (tile == 0) {
+            if (lane == 0) {
+                __threadfence();
+                atomicExch(status, (static_cast<unsigned long long>(agg) << 2) | 2ull);
+                s_prefix = 0;
+            }
+        } else {
+            if (lane == 0) {
+                __threadfence();
+                atomicExch(status + tile, (static_cast<unsigned long long>(agg) << 2) | 1ull);
+            }
+            T prefix = 0;
+            int64_t j = int64_t(tile) - 1 - lane;  // lane 0 reads the nearest predecessor
+            uint32_t polls = 0;
+            for (;;) {
+                unsigned long long st = j >= 0 ? ld_status(status + j) : 2ull;
+                while (__any_sync(0xffffffffu, (st & 3) == 0)) {
+                    if (++polls > kLookbackLimit) {
+                        if (lane == 0) record_error(err, kErrTimeout);
+                        st = 2ull;  // give up: treat as an inclusive zero
+                        break;
+                    }
+                    if ((st & 3) == 0) st = ld_status(status + j);
+                }
+                const uint32_t incl = __ballot_sync(0xffffffffu, (st & 3) == 2);
+                const uint32_t stop = incl ? uint32_t(__ffs(incl) - 1) : 32u;
+                T val = lane <= stop ? T(st >> 2) : T(0);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+                prefix += val;
+                if (incl) break;
+                j -= 32;
+            }
+            if (lane == 0) {
+                __threadfence();
+                atomicExch(status + tile, (static_cast<unsigned long long>(prefix + agg) << 2) | 2ull);
+                s_prefix = prefix;
+            }
+        }
+    }
+    __syncthreads();
+    T run = s_prefix + ex;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        if (base + k < n) {
+            out[base + k] = run;
+            run += v[k];
+            if (base + k == n - 1) out[n] = run;
+        }
+    }
 }
 
 template <typename T>
@@ -85,23 +161,38 @@ __global__ void k_zero_one(T* p) {
     p[0] = 0;
 }
 
+size_t status_bytes(size_t n) {
+    const size_t nt = (n + kScanTile - 1) / kScanTile;
+    return nt > 1 ? (nt + 1) * sizeof(unsigned long long) : 0;  // tile words + ticket
+}
+
+// status: status_bytes(n) zero bytes (null when that is 0).
 template <typename T>
-int scan_impl(const T* in, T* out, size_t n, Scratch& s, cudaStream_t st) {
+int scan_launch(const T* in, T* out, size_t n, void* status, uint32_t* err, cudaStream_t st) {
     if (n == 0) {
         k_zero_one<T><<<1, 1, 0, st>>>(out);
         return 1;
     }
-    size_t nt = (n + kScanTile - 1) / kScanTile;
+    const size_t nt = (n + kScanTile - 1) / kScanTile;
     if (nt == 1) {
         k_tile_scan<T><<<1, kScanThreads, 0, st>>>(in, out, n, nullptr);
         return 1;
     }
-    T* partial = static_cast<T*>(s.alloc(nt * sizeof(T)));
-    T* partial_ex = static_cast<T*>(s.alloc((nt + 1) * sizeof(T)));
-    k_tile_reduce<T><<<unsigned(nt), kScanThreads, 0, st>>>(in, n, partial);
-    int launches = 1 + scan_impl<T>(partial, partial_ex, nt, s, st);
-    k_tile_scan<T><<<unsigned(nt), kScanThreads, 0, st>>>(in, out, n, partial_ex);
-    return launches + 1;
+    auto* words = static_cast<unsigned long long*>(status);
+    k_scan_lookback<T><<<unsigned(nt), kScanThreads, 0, st>>>(in, out, n, words, reinterpret_cast<uint32_t*>(words + nt),
+                                                              err);
+    return 1;
+}
+
+template <typename T>
+int scan_impl(const T* in, T* out, size_t n, Scratch& s, cudaStream_t st) {
+    const size_t bytes = status_bytes(n);
+    void* status = nullptr;
+    if (bytes) {
+        status = s.alloc(bytes);
+        cudaMemsetAsync(status, 0, bytes, st);
+    }
+    return scan_launch<T>(in, out, n, status, s.err, st);
 }
 
 __global__ void k_fill_u32(uint32_t* p, uint32_t v, size_t n) {
@@ -115,6 +206,11 @@ int scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, Scratch& s, 
 }
 int scan_exclusive_u64(const uint64_t* in, uint64_t* out, size_t n, Scratch& s, cudaStream_t st) {
     return scan_impl<uint64_t>(in, out, n, s, st);
+}
+size_t scan_status_bytes(size_t n) { return status_bytes(n); }
+int scan_exclusive_u32_zeroed(const uint32_t* in, uint32_t* out, size_t n, void* status, uint32_t* err,
+                              cudaStream_t st) {
+    return scan_launch<uint32_t>(in, out, n, status, err, st);
 }
 int fill_u32(uint32_t* p, uint32_t v, size_t n, cudaStream_t st) {
     if (!n) return 0;

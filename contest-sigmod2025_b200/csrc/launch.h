@@ -12,16 +12,23 @@
 
 namespace bj {
 
-// Scratch allocator handed to wrappers that need temporary device memory.
+// Scratch allocator handed to wrappers that need temporary device memory;
+// `err` is the device error word kernels launched with it report to.
 struct Scratch {
     virtual void* alloc(size_t bytes) = 0;
     virtual ~Scratch() = default;
+    uint32_t* err = nullptr;
 };
 
 // ---- prefix sums (k_util.cu) ----
 // Exclusive scan of n values into out[0..n]; out[n] receives the total.
 int scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, Scratch& s, cudaStream_t st);
 int scan_exclusive_u64(const uint64_t* in, uint64_t* out, size_t n, Scratch& s, cudaStream_t st);
+// The same scan with its tile status words supplied: scan_status_bytes(n)
+// bytes (possibly 0) that the caller has zeroed, so no memset is issued.
+size_t scan_status_bytes(size_t n);
+int scan_exclusive_u32_zeroed(const uint32_t* in, uint32_t* out, size_t n, void* status, uint32_t* err,
+                              cudaStream_t st);
 int fill_u32(uint32_t* p, uint32_t v, size_t n, cudaStream_t st);
 
 // ---- page index (k_pages.cu) ----
@@ -102,19 +109,30 @@ struct SlotSources {
     SlotSource s[kMaxOut];
     int n;
 };
-
-// Build-side emit: one tuple per item: key from `key` (NULL key -> mult 0),
-// payload from `src`, mult from the item.
-struct TupleBuf {
-    uint32_t* keys;
-    uint64_t* mult;
-    uint64_t* pay;     // count * width
-    uint32_t* pnull;
-    uint32_t count;
-    uint32_t width;
+// The tables probed so far by a pipeline, by stage.
+struct ProbeSet {
+    HTView ht[kMaxProbes];
 };
-int emit_tuples(const Items& in, const DevColumn& key, const SlotSources& src, const HTView* probes, TupleBuf out,
-                uint32_t* err, cudaStream_t st);
+inline ProbeSet make_probe_set(const HTView* probes, int n) {
+    ProbeSet ps{};
+    for (int i = 0; i < n && i < kMaxProbes; i++) ps.ht[i] = probes[i];
+    return ps;
+}
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ uint32_t item_row(const Items& in, uint32_t i) { return in.rows ? in.rows[i] : i; }
+__device__ __forceinline__ uint64_t item_mult(const Items& in, uint32_t i) { return in.mult ? in.mult[i] : 1ull; }
+// Value of one slot for item i (row `row`): returns false for NULL.
+__device__ __forceinline__ bool slot_value(const SlotSource& s, const Items& in, uint32_t i, uint32_t row,
+                                           const ProbeSet& ps, uint64_t& v) {
+    if (s.kind == 0) return col_get(s.col, row, v);
+    const uint32_t e = in.ents[s.probe][i];
+    const HTView& ht = ps.ht[s.probe];
+    if ((ht.pnull[e] >> s.slot) & 1) return false;
+    v = ht.pay[size_t(e) * ht.width + s.slot];
+    return true;
+}
+#endif
 
 // Output emit: item multiplicities are expanded; out_off[i] = first output row
 // of item i (exclusive scan of multiplicities). Values go to flat columns.
@@ -143,23 +161,39 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
                uint32_t capacity, uint32_t* err, int num_sms, cudaStream_t st);
 
 // ---- hash table build (k_build.cu) ----
-struct BuildResult {
-    uint32_t nentries;
-    uint32_t nbuckets_log2;
+// Tuples of a build pipeline, one per item: key from `key` (NULL key ->
+// mult 0), payload from `src`, mult from the item.
+struct TupleBuf {
+    uint32_t* keys;
+    uint64_t* mult;
+    uint64_t* pay;     // count * width
+    uint32_t* pnull;
+    uint32_t count;
+    uint32_t width;
 };
-// Eager aggregation: representative flags (1 for the first copy of each
-// distinct tuple with mult > 0; duplicates add their mult to it).
-int aggregate_tuples(TupleBuf t, uint32_t* slot_table, uint32_t table_log2, uint32_t* is_rep, uint32_t* err,
-                     cudaStream_t st);
-// Scatter representatives into buckets (CSR). rep_pos = exclusive scan of is_rep.
-int bucket_count(TupleBuf t, const uint32_t* is_rep, uint32_t shift, uint32_t* counts, cudaStream_t st);
-int bucket_scatter(TupleBuf t, const uint32_t* is_rep, uint32_t shift, const uint32_t* bucket_off, uint32_t* cursor,
-                   HTView ht_mut, uint32_t* err, cudaStream_t st);
-// Bloom filter over keys[i] for every i with mask[i] != 0 (mask may be null).
-int bloom_build(const uint32_t* keys, const uint32_t* mask, uint32_t n, uint32_t* bloom, uint32_t log2w,
-                cudaStream_t st);
-// Flags of a built table: [0] = 1 if some key repeats, [1] = 1 if some mult > 1.
-// The entry count is read on the device from bucket_off[nbuckets].
+// Emit, eager aggregation and bucket counts of a hash build in one pass.
+// table (1 << tlog2 words) and counts (one per bucket) must be zero.
+struct BuildArgs {
+    Items in;
+    DevColumn key;
+    SlotSources src;
+    ProbeSet ps;
+    TupleBuf tb;
+    uint32_t* table;   // slot: index + 1 of the tuple representing it, 0 = empty
+    uint32_t tlog2;
+    uint32_t* is_rep;  // per tuple: 1 if it represents its distinct tuple
+    uint32_t* counts;  // per bucket: representatives
+    uint32_t shift;    // bucket = key_hash >> shift
+    uint32_t* err;
+};
+int emit_aggregate(const BuildArgs& a, cudaStream_t st);
+// Scatters the representatives into their buckets' ranges (cursor: one zero
+// word per bucket) and sets their bloom bits (bloom: zero, 1 << log2w words).
+int scatter_bloom(TupleBuf t, const uint32_t* is_rep, uint32_t shift, const uint32_t* bucket_off, uint32_t* cursor,
+                  HTView ht_mut, uint32_t* bloom, uint32_t log2w, uint32_t* err, cudaStream_t st);
+// Flags of a built table: [0] = 1 if some key repeats, [1] = 1 if some mult > 1
+// (both words must be zero before). The entry count is read on the device
+// from bucket_off[nbuckets].
 int ht_flags(HTView ht, uint32_t nbuckets, uint32_t* flags, int num_sms, cudaStream_t st);
 // Counts, for nsample evenly spaced rows of each probe's key column, how many
 // hit its table: hits[p] for probe p, all probes in one launch (the role of
