@@ -269,24 +269,36 @@ def main():
     e2e_steps = args.e2e_steps or max(3, min(args.steps, 20))
 
     def e2e_run():
+        # Profiling (CUDA events at the executor's phase boundaries) is on, so
+        # the line can say where a drop-in call spends its time.
+        ctx.profile(True)
         for _ in range(2):
             ctx.execute_raw(plan).free()
         barrier()
         stats, lat_ms = None, []
+        split = {"device_ms": 0.0, "phases": [0.0] * 4}
         ev0.record(stream)
         for _ in range(e2e_steps):
             t0 = time.perf_counter()
             r = ctx.execute_raw(plan)
             lat_ms.append((time.perf_counter() - t0) * 1e3)
             stats = r.stats()
+            split["device_ms"] += stats.device_ms / e2e_steps
+            for i in range(4):
+                split["phases"][i] += stats.phase_ms[i] / e2e_steps
             r.free()
         ev1.record(stream)
         torch.cuda.synchronize()
+        ctx.profile(False)
         ms = max_over_ranks(ev0.elapsed_time(ev1))
-        return e2e_steps * world / (ms / 1e3), stats, lat_ms
+        ph = split["phases"]
+        split = {"device_ms": split["device_ms"],
+                 "inputs_ms": split["device_ms"] - sum(ph),
+                 "build_ms": ph[0], "probe_order_ms": ph[1], "scan_probe_stages_ms": ph[2], "output_ms": ph[3]}
+        return e2e_steps * world / (ms / 1e3), stats, lat_ms, split
 
     # (a) pages in pageable memory: gathered into pinned staging and copied.
-    pageable_value, pageable_stats, pageable_lat = e2e_run()
+    pageable_value, pageable_stats, pageable_lat, pageable_split = e2e_run()
     # (b) pages in pinned host memory (registered once, outside the timed
     # region, as a serving process keeps its host tables): read in place.
     registered = []
@@ -298,7 +310,7 @@ def main():
                 ptr, size = col.pages[0], col.num_pages * pkg.PAGE_SIZE
                 if torch._C._cudart.cudaHostRegister(ptr, size, 3) == 0:  # portable | mapped
                     registered.append(ptr)
-    e2e_value, e2e_stats, e2e_lat = e2e_run()
+    e2e_value, e2e_stats, e2e_lat, e2e_split = e2e_run()
     for ptr in registered:
         torch._C._cudart.cudaHostUnregister(ptr)
     if args.mode == "e2e":
@@ -306,7 +318,9 @@ def main():
             x.free()
         ctx.close()
         if rank == 0:
-            print(json.dumps({"mode": "e2e", "e2e": e2e_value, "e2e_pageable": pageable_value, "unit": "queries/s"}))
+            print(json.dumps({"mode": "e2e", "e2e": e2e_value, "e2e_pageable": pageable_value, "unit": "queries/s",
+                              "e2e_split": e2e_split, "e2e_pageable_split": pageable_split,
+                              "e2e_p50_ms": statistics.median(e2e_lat)}))
         return 0
     h2d = e2e_stats.h2d_bytes + e2e_stats.mapped_input_bytes
     d2h = e2e_stats.d2h_bytes
@@ -334,11 +348,13 @@ def main():
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "p50_ms": statistics.median(e2e_lat),
                 "inputs": "pinned host pages read in place by the kernels (h2d = page bytes available to them)",
-                "dma_bytes_per_step": e2e_stats.h2d_bytes, "mapped_bytes_per_step": e2e_stats.mapped_input_bytes},
+                "dma_bytes_per_step": e2e_stats.h2d_bytes, "mapped_bytes_per_step": e2e_stats.mapped_input_bytes,
+                "split_ms": e2e_split},
         "e2e_pageable": {"value": pageable_value, "unit": "queries/s", "p50_ms": statistics.median(pageable_lat),
                          "h2d_bytes_per_step": pageable_stats.h2d_bytes,
                          "d2h_bytes_per_step": pageable_stats.d2h_bytes,
-                         "inputs": "pageable host pages, gathered into pinned staging and copied to HBM"},
+                         "inputs": "pageable host pages, gathered into pinned staging and copied to HBM",
+                         "split_ms": pageable_split},
         "gpu_launches": launches,
         "phases": phases,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -708,7 +708,10 @@ class Executor {
                 set.p[k].key = col(pp.probes[k].probe_attr);
                 set.p[k].ht = hts_[pp.probes[k].child].view;
             }
-            launched(sample_probes(set, nsample, hits, st_));
+            // The hit counts (and the tables' flags) only steer host decisions;
+            // while a graph is captured those come from the recorded tape, so
+            // the kernels producing them are left out of the graph.
+            if (ctx_->tape_mode != 2) launched(sample_probes(set, nsample, hits, st_));
             for (size_t k = 0; k < np; k++) {
                 BuiltHT& child = hts_[pp.probes[k].child];
                 stash_u32(ctx_, hits + k, int(k));
@@ -947,17 +950,23 @@ class Executor {
         hts_[pi].view = ht;
         hts_[pi].empty = false;
         hts_[pi].dflags = dflags;
-        launched(ht_flags(ht, uint32_t(nb), dflags, ctx_->num_sms, st_));
+        if (ctx_->tape_mode != 2) launched(ht_flags(ht, uint32_t(nb), dflags, ctx_->num_sms, st_));
         return true;
     }
 
     void output(const Items& items, const SlotSources& src, const std::vector<HTView>& probes, bj_result& res,
                 int flags) {
-        uint32_t n = items.count;
-        uint64_t* mult = alloc<uint64_t>(n);
-        launched(items_mult(items, mult, st_));
-        uint64_t* off = alloc<uint64_t>(size_t(n) + 1);
-        uint64_t N = scan_total_u64(mult, off, n);
+        const uint32_t n = items.count;
+        // Output row offsets: the scan of the item multiplicities, or the
+        // identity when every item has multiplicity 1.
+        uint64_t* off = nullptr;
+        uint64_t N = n;
+        if (items.mult) {
+            uint64_t* mult = alloc<uint64_t>(n);
+            launched(items_mult(items, mult, st_));
+            off = alloc<uint64_t>(size_t(n) + 1);
+            N = scan_total_u64(mult, off, n);
+        }
         res.rows = N;
         FlatOut fo{};
         fo.n = src.n;
@@ -967,43 +976,54 @@ class Executor {
         }
         launched(emit_output(items, off, src, probes.data(), fo, ctx_->d_err, st_));
         // Page counts per result column.
-        size_t ncol = ex_.out_slot.size();
+        const size_t ncol = ex_.out_slot.size();
         res.npages.assign(ncol, 0);
         struct StrPlan {
             uint32_t* lens = nullptr;
             uint64_t* start = nullptr;   // exclusive scan of row costs
             uint32_t* stats = nullptr;   // [0] max cost, [1] long string present
             uint32_t* block_off = nullptr;
-            size_t nblocks = 0;
             bool floor = false;
             uint64_t cp = 0;
         };
         std::vector<StrPlan> sp(ncol);
-        // Lengths and costs of every VARCHAR column, then one read-back.
         std::vector<size_t> strcols;
         for (size_t c = 0; c < ncol; c++) {
-            int32_t t = ex_.out_types[c];
-            if (t != BJ_VARCHAR) {
-                size_t rpp = full_page_rows(t == BJ_INT32 ? 4 : 8);
-                res.npages[c] = (N + rpp - 1) / rpp;
+            const int32_t t = ex_.out_types[c];
+            if (t == BJ_VARCHAR) {
+                strcols.push_back(c);
                 continue;
             }
-            uint32_t j = ex_.out_slot[c];
-            const DevColumn& scol = col(ex_.pipelines.back().slots[j].attr);
-            sp[c].lens = alloc<uint32_t>(N);
-            launched(string_lengths(fo.vals[j], fo.valid[j], N, StrSource{scol}, sp[c].lens, ctx_->d_err, st_));
-            uint64_t* cost = alloc<uint64_t>(N);
-            sp[c].stats = alloc<uint32_t>(2);
-            launched(string_cost(sp[c].lens, fo.valid[j], N, cost, sp[c].stats, st_));
-            sp[c].start = alloc<uint64_t>(N + 1);
-            launched(scan_exclusive_u64(cost, sp[c].start, N, A_, st_));
-            strcols.push_back(c);
+            const size_t rpp = full_page_rows(t == BJ_INT32 ? 4 : 8);
+            res.npages[c] = (N + rpp - 1) / rpp;
         }
+        // Lengths, costs and cost scans of every VARCHAR column (batches of up
+        // to kMaxOut columns, one launch each), then one read-back.
         for (size_t i0 = 0; i0 < strcols.size(); i0 += 20) {
-            size_t i1 = std::min(strcols.size(), i0 + 20);
+            const size_t i1 = std::min(strcols.size(), i0 + 20);
+            uint32_t* stats = alloc<uint32_t>(2 * (i1 - i0));
+            BJ_CK(cudaMemsetAsync(stats, 0, sizeof(uint32_t) * 2 * (i1 - i0), st_));
+            StrCols sc{};
+            ScanBatch64 sb{};
+            for (size_t i = i0; i < i1; i++) {
+                const size_t c = strcols[i];
+                const uint32_t j = ex_.out_slot[c];
+                StrCol& x = sc.c[sc.n++];
+                x.handles = fo.vals[j];
+                x.valid = fo.valid[j];
+                x.src = col(ex_.pipelines.back().slots[j].attr);
+                x.lens = sp[c].lens = alloc<uint32_t>(N);
+                x.cost = alloc<uint64_t>(N);
+                x.stats = sp[c].stats = stats + 2 * (i - i0);
+                sp[c].start = alloc<uint64_t>(N + 1);
+                sb.in[sb.n] = x.cost;
+                sb.out[sb.n++] = sp[c].start;
+            }
+            launched(string_len_cost(sc, N, ctx_->d_err, st_));
+            launched(scan_exclusive_u64_batch(sb, N, A_, st_));
             for (size_t i = i0; i < i1; i++) {
                 const StrPlan& q = sp[strcols[i]];
-                int slot = int(3 * (i - i0));
+                const int slot = int(3 * (i - i0));
                 if (N) stash_u64(ctx_, q.start + (N - 1), slot);
                 stash_u32(ctx_, q.stats, slot + 1);
                 stash_u32(ctx_, q.stats + 1, slot + 2);
@@ -1012,10 +1032,10 @@ class Executor {
             readback(ctx_, 0);
             for (size_t i = i0; i < i1; i++) {
                 StrPlan& q = sp[strcols[i]];
-                int slot = int(3 * (i - i0));
-                uint64_t last_start = N ? ctx_->h_small[slot] : 0;
-                uint64_t maxc = ctx_->h_small[slot + 1];
-                bool has_long = ctx_->h_small[slot + 2] != 0;
+                const int slot = int(3 * (i - i0));
+                const uint64_t last_start = N ? ctx_->h_small[slot] : 0;
+                const uint64_t maxc = ctx_->h_small[slot + 1];
+                const bool has_long = ctx_->h_small[slot + 2] != 0;
                 // Floor packing while the longest string keeps pages at least ~87% full.
                 if (!has_long && maxc <= kStrPageUnits / 8) {
                     q.floor = true;
@@ -1026,12 +1046,12 @@ class Executor {
         }
         for (size_t c : strcols) {
             if (sp[c].floor) continue;
-            uint32_t j = ex_.out_slot[c];
-            sp[c].nblocks = (N + kStrBlock - 1) / kStrBlock;
-            uint32_t* bp = alloc<uint32_t>(sp[c].nblocks);
-            sp[c].block_off = alloc<uint32_t>(sp[c].nblocks + 1);
+            const uint32_t j = ex_.out_slot[c];
+            const size_t nblocks = (N + kStrBlock - 1) / kStrBlock;
+            uint32_t* bp = alloc<uint32_t>(nblocks);
+            sp[c].block_off = alloc<uint32_t>(nblocks + 1);
             launched(string_pack(sp[c].lens, fo.valid[j], N, 0, bp, nullptr, nullptr, st_));
-            res.npages[c] = scan_total_u32(bp, sp[c].block_off, sp[c].nblocks);
+            res.npages[c] = scan_total_u32(bp, sp[c].block_off, nblocks);
         }
         res.page_base.assign(ncol, 0);
         uint64_t total = 0;
@@ -1050,23 +1070,51 @@ class Executor {
         } else {
             dst = alloc<uint8_t>(total * kPageSize);
         }
-        for (size_t c = 0; c < ncol; c++) {
-            int32_t t = ex_.out_types[c];
-            uint32_t j = ex_.out_slot[c];
-            uint8_t* pages = dst + res.page_base[c] * kPageSize;
-            if (t != BJ_VARCHAR) {
-                uint32_t rpp = uint32_t(full_page_rows(t == BJ_INT32 ? 4 : 8));
-                launched(write_fixed_pages(fo.vals[j], fo.valid[j], N, t, rpp, pages, st_));
+        // Page descriptors of the VARCHAR columns: floor-packed ones in one
+        // launch, greedy-packed ones per column.
+        std::vector<StrPageDesc*> descs(ncol, nullptr);
+        FloorCols fc{};
+        for (size_t c : strcols) {
+            descs[c] = alloc<StrPageDesc>(std::max<uint64_t>(res.npages[c], 1));
+            const uint32_t j = ex_.out_slot[c];
+            if (!sp[c].floor) {
+                launched(string_pack(sp[c].lens, fo.valid[j], N, 1, nullptr, sp[c].block_off, descs[c], st_));
                 continue;
             }
-            const DevColumn& scol = col(ex_.pipelines.back().slots[j].attr);
-            StrPageDesc* descs = alloc<StrPageDesc>(res.npages[c]);
-            if (sp[c].floor)
-                launched(string_floor_pages(sp[c].start, N, sp[c].cp, uint32_t(res.npages[c]), descs, st_));
-            else
-                launched(string_pack(sp[c].lens, fo.valid[j], N, 1, nullptr, sp[c].block_off, descs, st_));
-            launched(write_string_pages(fo.vals[j], fo.valid[j], sp[c].lens, StrSource{scol}, descs,
-                                        uint32_t(res.npages[c]), pages, ctx_->d_err, st_));
+            fc.start[fc.n] = sp[c].start;
+            fc.descs[fc.n] = descs[c];
+            fc.cp[fc.n++] = sp[c].cp;
+            if (fc.n == kMaxOut) {
+                launched(string_floor_first(fc, N, st_));
+                fc = FloorCols{};
+            }
+        }
+        launched(string_floor_first(fc, N, st_));
+        // Every page of every column, up to kMaxOut columns per launch.
+        for (size_t c0 = 0; c0 < ncol; c0 += kMaxOut) {
+            const size_t c1 = std::min(ncol, c0 + kMaxOut);
+            OutColumns oc{};
+            oc.nrows = N;
+            for (size_t c = c0; c < c1; c++) {
+                const int32_t t = ex_.out_types[c];
+                const uint32_t j = ex_.out_slot[c];
+                OutColumn& o = oc.c[oc.n++];
+                o.type = t;
+                o.vals = fo.vals[j];
+                o.valid = fo.valid[j];
+                o.page_base = uint32_t(res.page_base[c] - res.page_base[c0]);
+                o.npages = uint32_t(res.npages[c]);
+                if (t != BJ_VARCHAR) {
+                    o.rpp = uint32_t(full_page_rows(t == BJ_INT32 ? 4 : 8));
+                } else {
+                    o.floor = sp[c].floor ? 1u : 0u;
+                    o.lens = sp[c].lens;
+                    o.descs = descs[c];
+                    o.src = col(ex_.pipelines.back().slots[j].attr);
+                }
+            }
+            const uint64_t pages = res.page_base[c1 - 1] + res.npages[c1 - 1] - res.page_base[c0];
+            launched(write_pages(oc, uint32_t(pages), dst + res.page_base[c0] * kPageSize, ctx_->d_err, st_));
         }
         if (!ctx_->graph_output && !(flags & BJ_RESULT_DEVICE) && total) {
             res.host = ctx_->take_pinned(total * kPageSize);

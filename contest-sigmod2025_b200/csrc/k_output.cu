@@ -63,13 +63,13 @@ __device__ __forceinline__ void store_page(const uint8_t* page, uint8_t* dst) {
     for (uint32_t i = threadIdx.x; i < kPageSize / 16; i += blockDim.x) d[i] = s[i];
 }
 
-// One CTA of 256 threads per page; each thread owns 8 consecutive rows.
-__global__ void __launch_bounds__(256) k_write_fixed(const uint64_t* __restrict__ vals,
-                                                     const uint8_t* __restrict__ valid, uint64_t n, int32_t type,
-                                                     uint32_t rpp, uint8_t* __restrict__ out) {
-    __shared__ __align__(16) uint8_t page[kPageSize];
+// Page pidx of a fixed-width column, by one CTA of 256 threads; each thread
+// owns 8 consecutive rows.
+__device__ __forceinline__ void write_fixed_page(const uint64_t* __restrict__ vals, const uint8_t* __restrict__ valid,
+                                                 uint64_t n, int32_t type, uint32_t rpp, uint32_t pidx,
+                                                 uint8_t* page, uint8_t* __restrict__ dst) {
     __shared__ uint32_t total;
-    uint64_t r0 = uint64_t(blockIdx.x) * rpp;
+    uint64_t r0 = uint64_t(pidx) * rpp;
     uint32_t nr = uint32_t(n - r0 < rpp ? n - r0 : rpp);
     zero_smem_page(page);
     uint32_t t = threadIdx.x;
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(256) k_write_fixed(const uint64_t* __restrict_
         *reinterpret_cast<uint16_t*>(page + 2) = uint16_t(total);
     }
     __syncthreads();
-    store_page(page, out + size_t(blockIdx.x) * kPageSize);
+    store_page(page, dst);
 }
 
 // Byte range of a short string (page p, value d) in its source page.
@@ -128,28 +128,32 @@ __device__ __forceinline__ uint32_t long_string_length(const DevColumn& c, uint3
     return len;
 }
 
-__global__ void k_string_lengths(const uint64_t* __restrict__ handles, const uint8_t* __restrict__ valid, uint64_t n,
-                                 DevColumn c, uint32_t* __restrict__ lens, uint32_t* __restrict__ err) {
-    uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+// Byte length (NULL -> 0) and packing cost of every row, all VARCHAR columns
+// of the result (blockIdx.y = column). Cost: 8 * (2 + len) + 1 eighth-bytes
+// if non-null (offset, bytes, bitmap bit), 1 if NULL; stats[0] = largest
+// cost, stats[1] = 1 if some string is longer than PAGE_SIZE-7.
+__global__ void k_string_len_cost(StrCols cols, uint64_t n, uint32_t* __restrict__ err) {
+    const uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    const StrCol& sc = cols.c[blockIdx.y];
     if (i >= n) return;
-    if (!valid[i]) {
-        lens[i] = 0;
-        return;
+    uint32_t len = 0;
+    const bool v = sc.valid[i];
+    if (v) {
+        const uint64_t h = sc.handles[i];
+        if (str_handle_page(h) >= sc.src.npages) {
+            record_error(err, kErrRowRange);
+        } else if (str_handle_dense(h) == 0xffff) {
+            len = long_string_length(sc.src, str_handle_page(h), err);
+        } else {
+            const uint8_t* b;
+            short_string(sc.src, h, b, len);
+        }
     }
-    uint64_t h = handles[i];
-    if (str_handle_page(h) >= c.npages) {
-        record_error(err, kErrRowRange);
-        lens[i] = 0;
-        return;
-    }
-    if (str_handle_dense(h) == 0xffff) {
-        lens[i] = long_string_length(c, str_handle_page(h), err);
-        return;
-    }
-    const uint8_t* b;
-    uint32_t len;
-    short_string(c, h, b, len);
-    lens[i] = len;
+    sc.lens[i] = len;
+    const uint32_t c = v ? 8 * (2 + min(len, kPageSize)) + 1 : 1;
+    sc.cost[i] = c;
+    atomicMax(&sc.stats[0], c);
+    if (v && len > kMaxShort) sc.stats[1] = 1;
 }
 
 // One thread per block of kStrBlock rows: greedy page packing.
@@ -198,14 +202,13 @@ __global__ void k_string_pack(const uint32_t* __restrict__ lens, const uint8_t* 
     if (!pass) block_pages[blk] = pages;
 }
 
-__global__ void __launch_bounds__(256) k_write_string_pages(const uint64_t* __restrict__ handles,
-                                                            const uint8_t* __restrict__ valid,
-                                                            const uint32_t* __restrict__ lens, DevColumn c,
-                                                            const StrPageDesc* __restrict__ descs,
-                                                            uint8_t* __restrict__ out, uint32_t* __restrict__ err) {
-    __shared__ __align__(16) uint8_t page[kPageSize];
+// One page of a VARCHAR column described by d, by one CTA.
+__device__ __forceinline__ void write_string_page(const uint64_t* __restrict__ handles,
+                                                  const uint8_t* __restrict__ valid,
+                                                  const uint32_t* __restrict__ lens, const DevColumn& c,
+                                                  StrPageDesc d, uint8_t* page, uint8_t* __restrict__ dst,
+                                                  uint32_t* __restrict__ err) {
     __shared__ uint32_t tot_valid, tot_bytes, carry_valid, carry_bytes;
-    StrPageDesc d = descs[blockIdx.x];
     zero_smem_page(page);
     __syncthreads();
     if (d.chunk != 0xffffffffu) {
@@ -232,7 +235,7 @@ __global__ void __launch_bounds__(256) k_write_string_pages(const uint64_t* __re
             record_error(err, kErrLongString);
         }
         __syncthreads();
-        store_page(page, out + size_t(blockIdx.x) * kPageSize);
+        store_page(page, dst);
         return;
     }
     // Normal page: first pass counts valid rows (offset array size), second places data.
@@ -284,74 +287,59 @@ __global__ void __launch_bounds__(256) k_write_string_pages(const uint64_t* __re
         *reinterpret_cast<uint16_t*>(page + 2) = uint16_t(nv_total);
     }
     __syncthreads();
-    store_page(page, out + size_t(blockIdx.x) * kPageSize);
+    store_page(page, dst);
 }
 
-// Parallel page assignment for VARCHAR columns ("floor packing"). Row i costs
-// 8 * (2 + len) + 1 eighth-bytes if non-null (offset, bytes, bitmap bit) or 1
-// if NULL. With S_i the exclusive prefix of costs, row i goes to page
-// floor(S_i / Cp), Cp = 65496 - max cost: a page then holds less than 65496
-// eighth-bytes, i.e. 4 + 2 nv + bytes + ceil(rows / 8) <= 8192, and consecutive
-// rows advance by at most one page, so no page is empty. Used when no string
-// is long (> PAGE_SIZE-7) and the longest is short enough to keep pages ~full.
-__global__ void k_string_cost(const uint32_t* __restrict__ lens, const uint8_t* __restrict__ valid, uint64_t n,
-                              uint64_t* __restrict__ cost, uint32_t* __restrict__ stats) {
-    uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+// Every page of the result, all columns: CTA g writes output page g.
+__global__ void __launch_bounds__(256) k_write_pages(OutColumns cols, uint8_t* __restrict__ out,
+                                                     uint32_t* __restrict__ err) {
+    __shared__ __align__(16) uint8_t page[kPageSize];
+    const uint32_t g = blockIdx.x;
+    int k = 0;
+    while (k + 1 < cols.n && g >= cols.c[k].page_base + cols.c[k].npages) k++;
+    const OutColumn& oc = cols.c[k];
+    const uint32_t p = g - oc.page_base;
+    uint8_t* dst = out + size_t(g) * kPageSize;
+    if (oc.type != kVarchar) {
+        write_fixed_page(oc.vals, oc.valid, cols.nrows, oc.type, oc.rpp, p, page, dst);
+        return;
+    }
+    StrPageDesc d = oc.descs[p];
+    if (oc.floor) {
+        d.nrows = uint32_t((p + 1 < oc.npages ? oc.descs[p + 1].first_row : cols.nrows) - d.first_row);
+        d.chunk = 0xffffffffu;
+    }
+    write_string_page(oc.vals, oc.valid, oc.lens, oc.src, d, page, dst, err);
+}
+
+// Parallel page assignment for VARCHAR columns ("floor packing"). With S_i
+// the exclusive prefix of row costs, row i goes to page floor(S_i / Cp),
+// Cp = 65496 - max cost: a page then holds less than 65496 eighth-bytes, i.e.
+// 4 + 2 nv + bytes + ceil(rows / 8) <= 8192, and consecutive rows advance by
+// at most one page, so no page is empty. Used when no string is long
+// (> PAGE_SIZE-7) and the longest is short enough to keep pages ~full. This
+// pass records each page's first row (blockIdx.y = column); the page writer
+// takes a page's row count from the next page's first row.
+__global__ void k_floor_first(FloorCols cols, uint64_t n) {
+    const uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
     if (i >= n) return;
-    bool v = valid[i];
-    uint32_t len = v ? lens[i] : 0;
-    uint32_t c = v ? 8 * (2 + min(len, kPageSize)) + 1 : 1;
-    cost[i] = c;
-    atomicMax(&stats[0], c);
-    if (v && len > kMaxShort) stats[1] = 1;
-}
-
-__global__ void k_floor_first(const uint64_t* __restrict__ start, uint64_t n, uint64_t cp,
-                              StrPageDesc* __restrict__ descs) {
-    uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
-    if (i >= n) return;
-    uint64_t pg = start[i] / cp;
-    if (i == 0 || start[i - 1] / cp != pg) descs[pg].first_row = i;
-}
-
-__global__ void k_floor_desc(StrPageDesc* __restrict__ descs, uint32_t npages, uint64_t n) {
-    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npages) return;
-    uint64_t next = p + 1 < npages ? descs[p + 1].first_row : n;
-    descs[p].nrows = uint32_t(next - descs[p].first_row);
-    descs[p].chunk = 0xffffffffu;
+    const uint64_t* start = cols.start[blockIdx.y];
+    const uint64_t cp = cols.cp[blockIdx.y];
+    const uint64_t pg = start[i] / cp;
+    if (i == 0 || start[i - 1] / cp != pg) cols.descs[blockIdx.y][pg].first_row = i;
 }
 
 } // namespace
 
-int string_cost(const uint32_t* lens, const uint8_t* valid, uint64_t n, uint64_t* cost, uint32_t* stats,
-                cudaStream_t st) {
-    cudaMemsetAsync(stats, 0, 2 * sizeof(uint32_t), st);
-    if (!n) return 0;
-    k_string_cost<<<unsigned((n + 255) / 256), 256, 0, st>>>(lens, valid, n, cost, stats);
+int string_len_cost(const StrCols& cols, uint64_t n, uint32_t* err, cudaStream_t st) {
+    if (!n || cols.n <= 0) return 0;
+    k_string_len_cost<<<dim3(unsigned((n + 255) / 256), unsigned(cols.n)), 256, 0, st>>>(cols, n, err);
     return 1;
 }
 
-int string_floor_pages(const uint64_t* start, uint64_t n, uint64_t cp, uint32_t npages, StrPageDesc* descs,
-                       cudaStream_t st) {
-    if (!n || !npages) return 0;
-    k_floor_first<<<unsigned((n + 255) / 256), 256, 0, st>>>(start, n, cp, descs);
-    k_floor_desc<<<(npages + 255) / 256, 256, 0, st>>>(descs, npages, n);
-    return 2;
-}
-
-int write_fixed_pages(const uint64_t* vals, const uint8_t* valid, uint64_t n, int32_t type, uint32_t rpp,
-                      uint8_t* out_pages, cudaStream_t st) {
-    uint64_t npages = (n + rpp - 1) / rpp;
-    if (!npages) return 0;
-    k_write_fixed<<<unsigned(npages), 256, 0, st>>>(vals, valid, n, type, rpp, out_pages);
-    return 1;
-}
-
-int string_lengths(const uint64_t* handles, const uint8_t* valid, uint64_t n, StrSource src, uint32_t* lens,
-                   uint32_t* err, cudaStream_t st) {
-    if (!n) return 0;
-    k_string_lengths<<<unsigned((n + 255) / 256), 256, 0, st>>>(handles, valid, n, src.col, lens, err);
+int string_floor_first(const FloorCols& cols, uint64_t n, cudaStream_t st) {
+    if (!n || cols.n <= 0) return 0;
+    k_floor_first<<<dim3(unsigned((n + 255) / 256), unsigned(cols.n)), 256, 0, st>>>(cols, n);
     return 1;
 }
 
@@ -364,10 +352,9 @@ int string_pack(const uint32_t* lens, const uint8_t* valid, uint64_t n, int pass
     return 1;
 }
 
-int write_string_pages(const uint64_t* handles, const uint8_t* valid, const uint32_t* lens, StrSource src,
-                       const StrPageDesc* descs, uint32_t npages, uint8_t* out_pages, uint32_t* err, cudaStream_t st) {
-    if (!npages) return 0;
-    k_write_string_pages<<<npages, 256, 0, st>>>(handles, valid, lens, src.col, descs, out_pages, err);
+int write_pages(const OutColumns& cols, uint32_t total_pages, uint8_t* out_pages, uint32_t* err, cudaStream_t st) {
+    if (!total_pages || cols.n <= 0) return 0;
+    k_write_pages<<<total_pages, 256, 0, st>>>(cols, out_pages, err);
     return 1;
 }
 

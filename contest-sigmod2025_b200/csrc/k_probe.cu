@@ -182,7 +182,8 @@ __global__ void __launch_bounds__(256) k_emit_output(Items in, const uint64_t* o
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= in.count) return;
     uint32_t row = item_row(in, i);
-    uint64_t o0 = out_off[i], o1 = out_off[i + 1];
+    // Without offsets every item is one output row.
+    uint64_t o0 = out_off ? out_off[i] : i, o1 = out_off ? out_off[i + 1] : i + 1;
     for (int j = 0; j < src.n; j++) {
         uint64_t v = 0;
         bool ok = slot_value(src.s[j], in, i, row, ps, v);

@@ -156,6 +156,30 @@ __global__ void k_tile_scan(const T* __restrict__ in, T* __restrict__ out, size_
     }
 }
 
+// Single-tile scans of several arrays of the same length (blockIdx.x = array).
+__global__ void k_tile_scan_batch(ScanBatch64 b, size_t n) {
+    const uint64_t* in = b.in[blockIdx.x];
+    uint64_t* out = b.out[blockIdx.x];
+    const size_t base = size_t(threadIdx.x) * kScanPer;
+    uint64_t v[kScanPer];
+    uint64_t local = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        v[k] = base + k < n ? in[base + k] : 0ull;
+        local += v[k];
+    }
+    __shared__ uint64_t total;
+    uint64_t run = block_exclusive<uint64_t>(local, &total);
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        if (base + k < n) {
+            out[base + k] = run;
+            run += v[k];
+            if (base + k == n - 1) out[n] = run;
+        }
+    }
+}
+
 template <typename T>
 __global__ void k_zero_one(T* p) {
     p[0] = 0;
@@ -207,6 +231,17 @@ int scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, Scratch& s, 
 int scan_exclusive_u64(const uint64_t* in, uint64_t* out, size_t n, Scratch& s, cudaStream_t st) {
     return scan_impl<uint64_t>(in, out, n, s, st);
 }
+int scan_exclusive_u64_batch(const ScanBatch64& b, size_t n, Scratch& s, cudaStream_t st) {
+    if (b.n <= 0) return 0;
+    if (n == 0 || n > kScanTile) {
+        int launches = 0;
+        for (int i = 0; i < b.n; i++) launches += scan_impl<uint64_t>(b.in[i], b.out[i], n, s, st);
+        return launches;
+    }
+    k_tile_scan_batch<<<unsigned(b.n), kScanThreads, 0, st>>>(b, n);
+    return 1;
+}
+
 size_t scan_status_bytes(size_t n) { return status_bytes(n); }
 int scan_exclusive_u32_zeroed(const uint32_t* in, uint32_t* out, size_t n, void* status, uint32_t* err,
                               cudaStream_t st) {

@@ -29,6 +29,15 @@ int scan_exclusive_u64(const uint64_t* in, uint64_t* out, size_t n, Scratch& s, 
 size_t scan_status_bytes(size_t n);
 int scan_exclusive_u32_zeroed(const uint32_t* in, uint32_t* out, size_t n, void* status, uint32_t* err,
                               cudaStream_t st);
+// Exclusive scans of several u64 arrays of length n (out[i][n] = total):
+// one launch when n fits one tile.
+constexpr int kMaxScanBatch = 32;
+struct ScanBatch64 {
+    const uint64_t* in[kMaxScanBatch];
+    uint64_t* out[kMaxScanBatch];
+    int n;
+};
+int scan_exclusive_u64_batch(const ScanBatch64& b, size_t n, Scratch& s, cudaStream_t st);
 int fill_u32(uint32_t* p, uint32_t v, size_t n, cudaStream_t st);
 
 // ---- page index (k_pages.cu) ----
@@ -135,7 +144,8 @@ __device__ __forceinline__ bool slot_value(const SlotSource& s, const Items& in,
 #endif
 
 // Output emit: item multiplicities are expanded; out_off[i] = first output row
-// of item i (exclusive scan of multiplicities). Values go to flat columns.
+// of item i (exclusive scan of multiplicities; null when every item has
+// multiplicity 1, item i then being row i). Values go to flat columns.
 struct FlatOut {
     uint64_t* vals[kMaxOut];
     uint8_t* valid[kMaxOut];
@@ -209,34 +219,63 @@ struct SampleSet {
 int sample_probes(const SampleSet& set, uint32_t nsample, uint32_t* hits, cudaStream_t st);
 
 // ---- output pages (k_output.cu) ----
-// Fixed-width page writer: rows_per_page rows per page.
-int write_fixed_pages(const uint64_t* vals, const uint8_t* valid, uint64_t n, int32_t type, uint32_t rows_per_page,
-                      uint8_t* out_pages, cudaStream_t st);
-// VARCHAR: per-row byte lengths (NULL -> 0, long strings flagged).
-struct StrSource {
-    DevColumn col;  // the source column the handles point into
-};
-int string_lengths(const uint64_t* handles, const uint8_t* valid, uint64_t n, StrSource src, uint32_t* lens,
-                   uint32_t* err, cudaStream_t st);
-// Greedy page packing per block of kStrBlock rows: pass 0 counts pages per
-// block, pass 1 writes page descriptors at block_page_off.
+// Page descriptors of a VARCHAR column.
 constexpr uint32_t kStrBlock = 4096;
 struct StrPageDesc {
     uint64_t first_row;
     uint32_t nrows;     // rows on the page (1 for a long-string page)
     uint32_t chunk;     // long string: chunk index, else 0xffffffff
 };
+// Byte lengths and packing costs of the rows of every VARCHAR result column
+// in one launch; stats (2 words per column, zero before): [0] largest cost,
+// [1] 1 if some string is longer than PAGE_SIZE-7.
+struct StrCol {
+    const uint64_t* handles;  // string handles into src
+    const uint8_t* valid;
+    DevColumn src;            // the source column the handles point into
+    uint32_t* lens;
+    uint64_t* cost;
+    uint32_t* stats;
+};
+struct StrCols {
+    StrCol c[kMaxOut];
+    int n;
+};
+int string_len_cost(const StrCols& cols, uint64_t n, uint32_t* err, cudaStream_t st);
+// Greedy page packing per block of kStrBlock rows: pass 0 counts pages per
+// block, pass 1 writes page descriptors at block_page_off.
 int string_pack(const uint32_t* lens, const uint8_t* valid, uint64_t n, int pass, uint32_t* block_pages,
                 const uint32_t* block_page_off, StrPageDesc* descs, cudaStream_t st);
-// Parallel packing: per-row costs (stats[0] = max cost, stats[1] = 1 if some
-// string is longer than PAGE_SIZE-7), then page descriptors from the
-// exclusive scan `start` of the costs for page capacity cp.
+// Parallel packing: first row of each page from the exclusive scan `start`
+// of the costs for page capacity cp, every floor-packed column in one launch.
 constexpr uint64_t kStrPageUnits = 65496;  // eighth-bytes a page may hold
-int string_cost(const uint32_t* lens, const uint8_t* valid, uint64_t n, uint64_t* cost, uint32_t* stats,
-                cudaStream_t st);
-int string_floor_pages(const uint64_t* start, uint64_t n, uint64_t cp, uint32_t npages, StrPageDesc* descs,
-                       cudaStream_t st);
-int write_string_pages(const uint64_t* handles, const uint8_t* valid, const uint32_t* lens, StrSource src,
-                       const StrPageDesc* descs, uint32_t npages, uint8_t* out_pages, uint32_t* err, cudaStream_t st);
+struct FloorCols {
+    const uint64_t* start[kMaxOut];
+    StrPageDesc* descs[kMaxOut];
+    uint64_t cp[kMaxOut];
+    int n;
+};
+int string_floor_first(const FloorCols& cols, uint64_t n, cudaStream_t st);
+// Every page of the result in one launch: column k owns output pages
+// [page_base, page_base + npages). Fixed width: rpp rows per page. VARCHAR:
+// pages from descs (floor: first rows only, row counts from the next page).
+struct OutColumn {
+    int32_t type;
+    uint32_t floor;
+    const uint64_t* vals;       // values, or string handles into src
+    const uint8_t* valid;
+    const uint32_t* lens;       // VARCHAR
+    const StrPageDesc* descs;   // VARCHAR
+    DevColumn src;              // VARCHAR source column
+    uint32_t rpp;               // fixed width: rows per page
+    uint32_t page_base;
+    uint32_t npages;
+};
+struct OutColumns {
+    OutColumn c[kMaxOut];
+    int n;
+    uint64_t nrows;
+};
+int write_pages(const OutColumns& cols, uint32_t total_pages, uint8_t* out_pages, uint32_t* err, cudaStream_t st);
 
 } // namespace bj
