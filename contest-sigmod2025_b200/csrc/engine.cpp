@@ -22,6 +22,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -31,6 +32,8 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <future>
+#include <atomic>
 #include <vector>
 
 namespace bj {
@@ -279,6 +282,7 @@ struct bj_context {
     uint32_t* d_err = nullptr;         // device error word
     uint64_t* h_small = nullptr;       // pinned readback slots
     uint64_t* d_small = nullptr;       // device readback slots
+    GatherList gather{};               // values queued for the next read-back
     uint64_t launches = 0;
     uint64_t live_results = 0;
     int num_sms = 148;
@@ -363,6 +367,28 @@ namespace {
 
 // Reads back `n` u64 slots of ctx->d_small after the stream drains; checks the
 // device error word.
+// Host-side trace of a call (B200JOIN_TRACE=1): milliseconds since the call
+// began and since the previous mark, to stderr.
+bool trace_on() {
+    static const bool on = [] {
+        const char* e = std::getenv("B200JOIN_TRACE");
+        return e && std::atoi(e) != 0;
+    }();
+    return on;
+}
+thread_local std::chrono::steady_clock::time_point g_trace_t0, g_trace_last;
+void trace_begin() {
+    if (trace_on()) g_trace_t0 = g_trace_last = std::chrono::steady_clock::now();
+}
+void trace(const char* what) {
+    if (!trace_on()) return;
+    auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[b200join] %8.3f ms (+%7.3f) %s\n",
+                 std::chrono::duration<double, std::milli>(now - g_trace_t0).count(),
+                 std::chrono::duration<double, std::milli>(now - g_trace_last).count(), what);
+    g_trace_last = now;
+}
+
 void readback(bj_context* ctx, int n) {
     (void)n;
     if (ctx->tape_mode == 2) {
@@ -371,8 +397,12 @@ void readback(bj_context* ctx, int n) {
         std::memcpy(ctx->h_small, t.slots[t.pos++].data(), sizeof(uint64_t) * 64);
         return;
     }
+    ctx->launches += uint64_t(gather_values(ctx->gather, ctx->d_small, ctx->stream));
+    ctx->gather.n = 0;
     BJ_CK(cudaMemcpyAsync(ctx->h_small, ctx->d_small, sizeof(uint64_t) * 64, cudaMemcpyDeviceToHost, ctx->stream));
+    trace("read-back issued");
     BJ_CK(cudaStreamSynchronize(ctx->stream));
+    trace("read-back done");
     uint32_t code = uint32_t(ctx->h_small[63]);
     if (code) throw Fail{BJ_ERR_INVALID, std::string("device check failed: ") + dev_error_text(code)};
     if (ctx->tape_mode == 1) {
@@ -382,21 +412,19 @@ void readback(bj_context* ctx, int n) {
     }
 }
 
-// Queue a copy of a device u32/u64 value into readback slot i.
-void stash_u32(bj_context* ctx, const uint32_t* src, int i) {
+// Queue a device u32/u64 value for the next read-back, into slot i; the
+// queued values are gathered by one kernel when the read-back is issued.
+void stash_value(bj_context* ctx, const void* src, int i, bool wide) {
     if (ctx->tape_mode == 2) return;
-    BJ_CK(cudaMemsetAsync(ctx->d_small + i, 0, sizeof(uint64_t), ctx->stream));
-    BJ_CK(cudaMemcpyAsync(ctx->d_small + i, src, sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+    GatherList& g = ctx->gather;
+    if (g.n >= kMaxGather) throw Fail{BJ_ERR_INTERNAL, "too many read-back values"};
+    g.src[g.n] = src;
+    g.slot[g.n] = uint8_t(i);
+    g.wide[g.n++] = wide ? 1 : 0;
 }
-void stash_u64(bj_context* ctx, const uint64_t* src, int i) {
-    if (ctx->tape_mode == 2) return;
-    BJ_CK(cudaMemcpyAsync(ctx->d_small + i, src, sizeof(uint64_t), cudaMemcpyDeviceToDevice, ctx->stream));
-}
-void stash_err(bj_context* ctx) {
-    if (ctx->tape_mode == 2) return;
-    BJ_CK(cudaMemsetAsync(ctx->d_small + 63, 0, sizeof(uint64_t), ctx->stream));
-    BJ_CK(cudaMemcpyAsync(ctx->d_small + 63, ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->stream));
-}
+void stash_u32(bj_context* ctx, const uint32_t* src, int i) { stash_value(ctx, src, i, false); }
+void stash_u64(bj_context* ctx, const uint64_t* src, int i) { stash_value(ctx, src, i, true); }
+void stash_err(bj_context* ctx) { stash_value(ctx, ctx->d_err, 63, false); }
 
 // ---------------------------------------------------------------------------
 // Page upload and indexing.
@@ -500,65 +528,63 @@ uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs) {
 
 // Builds the page index of every job's column (pages already on the device).
 void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem) {
-    struct Tmp {
-        PageIndexBufs b;
-        uint32_t npages;
-    };
-    std::vector<Tmp> tmp(jobs.size());
     Arena& sc = ctx->arena;
-    for (size_t i = 0; i < jobs.size(); i++) {
-        uint32_t np = uint32_t(jobs[i].src ? jobs[i].src->num_pages : 0);
-        Tmp& t = tmp[i];
-        t.npages = np;
-        t.b.hdr = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
-        t.b.rows = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
-        t.b.chunks = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
-        t.b.row_start = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * (np + 1)));
-        t.b.chunk_base = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * (np + 1)));
-        t.b.flags = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t)));
-        ctx->launches += page_index_pass1(jobs[i].dpages, np, jobs[i].out->type, t.b, ctx->d_err, sc, ctx->stream);
-    }
-    // Read back row totals, chunk totals and flags, a few columns at a time.
-    std::vector<uint64_t> rows(jobs.size()), chunks(jobs.size()), flags(jobs.size()), rows0(jobs.size());
+    // Batches of up to 15 columns: one launch per pass, one read-back
+    // (4 slots per column) between the passes.
     for (size_t i0 = 0; i0 < jobs.size(); i0 += 15) {
-        size_t i1 = std::min(jobs.size(), i0 + 15);
+        const size_t i1 = std::min(jobs.size(), i0 + 15);
+        PageIndexBatch b{};
+        uint32_t* flags = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t) * (i1 - i0)));
+        BJ_CK(cudaMemsetAsync(flags, 0, sizeof(uint32_t) * (i1 - i0), ctx->stream));
         for (size_t i = i0; i < i1; i++) {
-            int s = int(4 * (i - i0));
-            stash_u32(ctx, tmp[i].b.row_start + tmp[i].npages, s);
-            stash_u32(ctx, tmp[i].b.chunk_base + tmp[i].npages, s + 1);
-            stash_u32(ctx, tmp[i].b.flags, s + 2);
-            stash_u32(ctx, tmp[i].b.rows, s + 3);  // rows of page 0
+            const uint32_t np = uint32_t(jobs[i].src ? jobs[i].src->num_pages : 0);
+            PageIndexCol& c = b.c[b.n++];
+            c.pages = jobs[i].dpages;
+            c.npages = np;
+            c.type = jobs[i].out->type;
+            c.hdr = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
+            c.rows = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
+            c.chunks = static_cast<uint32_t*>(sc.alloc(sizeof(uint32_t) * std::max<size_t>(np, 1)));
+            c.row_start = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * (np + 1)));
+            c.chunk_base = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * (np + 1)));
+            c.flags = flags + (i - i0);
+        }
+        ctx->launches += page_index_pass1(b, ctx->d_err, sc, ctx->stream);
+        // Row totals, chunk totals, flags and the rows of page 0.
+        for (size_t i = i0; i < i1; i++) {
+            const PageIndexCol& c = b.c[i - i0];
+            const int s = int(4 * (i - i0));
+            stash_u32(ctx, c.row_start + c.npages, s);
+            stash_u32(ctx, c.chunk_base + c.npages, s + 1);
+            stash_u32(ctx, c.flags, s + 2);
+            stash_u32(ctx, c.rows, s + 3);
         }
         stash_err(ctx);
         readback(ctx, 0);
         for (size_t i = i0; i < i1; i++) {
-            int s = int(4 * (i - i0));
-            rows[i] = ctx->h_small[s];
-            chunks[i] = ctx->h_small[s + 1];
-            flags[i] = ctx->h_small[s + 2];
-            rows0[i] = tmp[i].npages ? ctx->h_small[s + 3] : 0;
+            PageIndexCol& pc = b.c[i - i0];
+            const int s = int(4 * (i - i0));
+            const uint64_t rows = ctx->h_small[s], chunks = ctx->h_small[s + 1], flg = ctx->h_small[s + 2];
+            const uint64_t rows0 = pc.npages ? ctx->h_small[s + 3] : 0;
+            if (rows != jobs[i].rows)
+                throw Fail{BJ_ERR_INVALID, "a column's pages hold " + std::to_string(rows) + " rows but its table has " +
+                                               std::to_string(jobs[i].rows)};
+            DevColumn& c = *jobs[i].out;
+            c.pages = jobs[i].dpages;
+            c.npages = pc.npages;
+            c.nrows = uint32_t(rows);
+            c.flags = uint32_t(flg) | (jobs[i].in_place ? kColHostPages : 0u);
+            c.rpp = (c.flags & kColRaggedPages) ? 0u : uint32_t(rows0);
+            c.hdr = pc.hdr;
+            c.row_start = pc.row_start;
+            c.chunk_base = pc.chunk_base;
+            pc.nrows = c.nrows;
+            pc.dense_base = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * std::max<uint64_t>(chunks, 1)));
+            pc.page_of_blk = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * ((c.nrows >> kBlkShift) + 2)));
+            c.dense_base = pc.dense_base;
+            c.page_of_blk = pc.page_of_blk;
         }
-    }
-    for (size_t i = 0; i < jobs.size(); i++) {
-        if (rows[i] != jobs[i].rows)
-            throw Fail{BJ_ERR_INVALID, "a column's pages hold " + std::to_string(rows[i]) + " rows but its table has " +
-                                           std::to_string(jobs[i].rows)};
-        DevColumn& c = *jobs[i].out;
-        c.pages = jobs[i].dpages;
-        c.npages = tmp[i].npages;
-        c.nrows = uint32_t(rows[i]);
-        c.flags = uint32_t(flags[i]) | (jobs[i].in_place ? kColHostPages : 0u);
-        c.rpp = (c.flags & kColRaggedPages) ? 0u : uint32_t(rows0[i]);
-        c.hdr = tmp[i].b.hdr;
-        c.row_start = tmp[i].b.row_start;
-        c.chunk_base = tmp[i].b.chunk_base;
-        uint32_t* dense = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * std::max<uint64_t>(chunks[i], 1)));
-        uint32_t nblk = (c.nrows >> kBlkShift) + 2;
-        uint32_t* pob = static_cast<uint32_t*>(mem.alloc(sizeof(uint32_t) * nblk));
-        c.dense_base = dense;
-        c.page_of_blk = pob;
-        ctx->launches += page_index_pass2(c.pages, c.hdr, c.npages, c.nrows, c.row_start, c.chunk_base, dense, pob,
-                                          ctx->stream);
+        ctx->launches += page_index_pass2(b, ctx->stream);
     }
 }
 
@@ -612,6 +638,7 @@ class Executor {
                 for (const auto& pr : pp.probes) BJ_CK(cudaStreamWaitEvent(main, ctx_->pipe_event(pr.child), 0));
             }
             bool ok = p + 1 < np ? run_pipeline(p, nullptr, 0) : run_pipeline(p, &res, flags);
+            trace(leaf ? "leaf pipeline enqueued" : "pipeline done");
             BJ_CK(cudaEventRecord(done, st_));
             if (!ok) {
                 st_ = main;
@@ -1143,8 +1170,11 @@ void set_empty_result(bj_result& r, const ExecPlan& ex) {
 
 int fail_to_status(bj_context* ctx, const Fail& f) {
     ctx->last_error = f.msg;
+    ctx->gather.n = 0;
     for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
     ctx->prof_events.clear();
+    for (cudaEvent_t e : ctx->phase_events) cudaEventDestroy(e);
+    ctx->phase_events.clear();
     ctx->prof_bytes = 0;
     // Leave every stream idle and the arena reusable after a failure.
     ctx->sync_all();
@@ -1155,13 +1185,69 @@ int fail_to_status(bj_context* ctx, const Fail& f) {
     return f.status;
 }
 
+// Speculative layout of a host-resident fixed-width column read in place:
+// page 0 and the last page (read directly, they are in host memory) both
+// without NULLs, page 0 holding rpp rows that fit the page format, the last
+// at most rpp, and (pages - 1) * rpp + last rows = the table's rows. The
+// column then runs without a device page index (row r is on page r / rpp);
+// every other page's header must equal page 0's, which host threads check
+// while the GPU works (SpecCheck); a mismatch reruns the call with the full
+// index. Reads stay inside pages either way.
+bool guess_uniform(const bj_column& hc, uint64_t rows, uint32_t& h0_out) {
+    if ((hc.type != BJ_INT32 && hc.type != BJ_INT64 && hc.type != BJ_FP64) || hc.num_pages == 0) return false;
+    const uint32_t h0 = *static_cast<const uint32_t*>(hc.pages[0]);
+    const uint32_t hl = *static_cast<const uint32_t*>(hc.pages[hc.num_pages - 1]);
+    const uint32_t n0 = h0 & 0xffff, nl = hl & 0xffff;
+    const uint32_t w = hc.type == BJ_INT32 ? 4 : 8;
+    if (n0 == 0 || (h0 >> 16) != n0 || w + uint64_t(w) * n0 + (n0 + 7) / 8 > kPageSize) return false;
+    if (nl == 0 || nl > n0 || (hl >> 16) != nl) return false;
+    if (uint64_t(hc.num_pages - 1) * n0 + nl != rows) return false;
+    h0_out = h0;
+    return true;
+}
+
+struct SpecMiss {};  // a speculative page layout was wrong: rerun with the page index
+
+// Asynchronous check of the speculated columns' page headers.
+struct SpecCheck {
+    std::vector<std::pair<const bj_column*, uint32_t>> cols;  // column, expected header
+    std::future<bool> ok;
+    void start(ThreadPool* pool) {
+        if (cols.empty()) return;
+        ok = std::async(std::launch::async, [this, pool] {
+            std::atomic<bool> good{true};
+            for (const auto& [hc, h0] : cols) {
+                const uint64_t np = hc->num_pages, per = 4096;
+                if (np < 3) continue;
+                pool->parallel_for((np - 2 + per - 1) / per, [&, hc = hc, h0 = h0](size_t t) {
+                    const uint64_t lo = 1 + t * per, hi = std::min<uint64_t>(np - 1, lo + per);
+                    for (uint64_t q = lo; q < hi && good.load(std::memory_order_relaxed); q++)
+                        if (*static_cast<const uint32_t*>(hc->pages[q]) != h0) good = false;
+                });
+            }
+            return good.load();
+        });
+    }
+    int result = -1;  // -1 unknown, 0 a header differs, 1 all match
+    bool passed() {
+        if (result < 0) result = (!ok.valid() || ok.get()) ? 1 : 0;
+        return result == 1;
+    }
+    ~SpecCheck() {
+        if (ok.valid()) ok.wait();
+    }
+};
+
 // Shared tail of bj_execute / bj_execute_resident.
-int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* resident, int flags, bj_result** out) {
+int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* resident, int flags, bj_result** out,
+                   bool speculate = true) {
     auto t0 = std::chrono::steady_clock::now();
     if (!ctx || !plan || !out) return BJ_ERR_INVALID;
+    trace_begin();
     *out = nullptr;
     std::unique_ptr<bj_result> res(new bj_result);
     res->ctx = ctx;
+    SpecCheck spec;
     try {
         ExecPlan ex;
         std::string err;
@@ -1198,17 +1284,32 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
                     d.cols[c].type = hc.type;
                     res->stats.input_pages += hc.num_pages;
                     if (uint8_t* mapped = ctx->zero_copy ? mapped_base(hc) : nullptr) {
-                        jobs.push_back(ColumnJob{&hc, mapped, t.num_rows, &d.cols[c], true});
                         res->stats.mapped_input_bytes += hc.num_pages * kPageSize;
+                        uint32_t h0 = 0;
+                        if (speculate && guess_uniform(hc, t.num_rows, h0)) {
+                            DevColumn& dc = d.cols[c];
+                            dc.pages = mapped;
+                            dc.npages = uint32_t(hc.num_pages);
+                            dc.nrows = uint32_t(t.num_rows);
+                            dc.flags = kColHostPages;
+                            dc.rpp = h0 & 0xffff;
+                            spec.cols.emplace_back(&hc, h0);
+                            continue;
+                        }
+                        jobs.push_back(ColumnJob{&hc, mapped, t.num_rows, &d.cols[c], true});
                         continue;
                     }
                     uint8_t* dp = static_cast<uint8_t*>(ctx->arena.alloc(std::max<uint64_t>(hc.num_pages, 1) * kPageSize));
                     jobs.push_back(ColumnJob{&hc, dp, t.num_rows, &d.cols[c]});
                 }
             }
+            trace("plan and input columns");
             if (!ex.empty) {
                 res->stats.h2d_bytes += upload_pages(ctx, jobs);
+                trace("pages staged");
                 index_columns(ctx, jobs, ctx->arena);
+                trace("pages indexed");
+                spec.start(ctx->pool.get());
             }
         }
         if (resident) {
@@ -1236,9 +1337,12 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
             res->host = PinnedBlock{};
             set_empty_result(*res, ex);
         }
+        trace("executor done");
         BJ_CK(cudaEventRecord(ctx->ev1, ctx->stream));
         stash_err(ctx);
         readback(ctx, 0);
+        if (!spec.passed()) throw SpecMiss{};
+        trace("page layouts confirmed");
         float ms = 0;
         BJ_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
         res->stats.device_ms = ms;
@@ -1258,11 +1362,33 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
         res->stats.kernel_launches = ctx->launches - launches0;
         res->stats.pipelines = pipes;
         ctx->arena.reset();
+    } catch (const SpecMiss&) {
+        // Not an error: the call runs again with a page index for every column.
+        if (res->dev) cudaFree(res->dev);
+        res->dev = nullptr;
+        ctx->give_pinned(res->host);
+        res->host = PinnedBlock{};
+        for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
+        ctx->prof_events.clear();
+        for (cudaEvent_t e : ctx->phase_events) cudaEventDestroy(e);
+        ctx->phase_events.clear();
+        ctx->prof_bytes = 0;
+        ctx->arena.reset();
+        res.reset();
+        return execute_common(ctx, plan, resident, flags, out, false);
     } catch (const Fail& f) {
         if (res->dev) cudaFree(res->dev);
         res->dev = nullptr;
         ctx->give_pinned(res->host);
         res->host = PinnedBlock{};
+        // A device check that failed on a speculated layout that was wrong:
+        // clear the error and run again with the page index.
+        if (!spec.cols.empty() && !spec.passed()) {
+            fail_to_status(ctx, f);
+            ctx->last_error.clear();
+            res.reset();
+            return execute_common(ctx, plan, resident, flags, out, false);
+        }
         return fail_to_status(ctx, f);
     } catch (const std::bad_alloc&) {
         return fail_to_status(ctx, Fail{BJ_ERR_OOM, "host allocation failed"});
@@ -1384,6 +1510,7 @@ bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resid
             if (gr) cudaGraphDestroy(gr);
         }
         cudaGetLastError();
+        ctx->gather.n = 0;
         ctx->tape_mode = 0;
         ctx->tape = nullptr;
         ctx->graph_output = false;

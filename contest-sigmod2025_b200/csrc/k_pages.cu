@@ -1,4 +1,4 @@
-// K1: page index of a resident column.
+// K1: page index of resident columns, every column of a batch per launch.
 //
 // Replaces the reference's per-query column preparation
 // (TableScan::prepareColumn / makeSearchVector, engine/op/TableScan.cpp:546-582:
@@ -11,13 +11,25 @@
 // and the page of every 1024-row block.
 #include "launch.h"
 
+#include <algorithm>
+
 namespace bj {
 namespace {
 
-__global__ void k_page_headers(const uint8_t* __restrict__ pages, uint32_t npages, int32_t type,
-                               uint32_t* __restrict__ hdr, uint32_t* __restrict__ rows,
-                               uint32_t* __restrict__ chunks, uint32_t* __restrict__ flags,
-                               uint32_t* __restrict__ err) {
+__global__ void k_page_headers(PageIndexBatch batch, uint32_t* __restrict__ err) {
+    const PageIndexCol& col = batch.c[blockIdx.y];
+    const uint8_t* __restrict__ pages = col.pages;
+    const uint32_t npages = col.npages;
+    const int32_t type = col.type;
+    uint32_t* __restrict__ hdr = col.hdr;
+    uint32_t* __restrict__ rows = col.rows;
+    uint32_t* __restrict__ chunks = col.chunks;
+    uint32_t* __restrict__ flags = col.flags;
+    if (blockIdx.x * blockDim.x >= npages) return;  // whole CTA beyond this column
+    // Page 0's header, read once per CTA (pages may be in host memory).
+    __shared__ uint32_t s_h0;
+    if (threadIdx.x == 0) s_h0 = *reinterpret_cast<const uint32_t*>(pages);
+    __syncthreads();
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npages) return;
     const uint8_t* pg = pages + size_t(p) * kPageSize;
@@ -72,7 +84,7 @@ __global__ void k_page_headers(const uint8_t* __restrict__ pages, uint32_t npage
     }
     // Uniform pages: every page but the last holds as many rows as page 0,
     // the last at most that many.
-    const uint32_t h0 = *reinterpret_cast<const uint32_t*>(pages);
+    const uint32_t h0 = s_h0;
     const uint32_t r0 = (type == kVarchar && (h0 & 0xffff) >= 0xfffe) ? 0u : (h0 & 0xffff);
     if (r0 == 0 || (r != r0 && (p + 1 < npages || r > r0)) || (f & 2)) f |= kColRaggedPages;
     rows[p] = r;
@@ -82,8 +94,13 @@ __global__ void k_page_headers(const uint8_t* __restrict__ pages, uint32_t npage
 
 // One warp per page: dense base of each 64-row chunk (a running popcount of
 // the page's null bitmap).
-__global__ void k_page_dense(const uint8_t* __restrict__ pages, const uint32_t* __restrict__ hdr, uint32_t npages,
-                             const uint32_t* __restrict__ chunk_base, uint32_t* __restrict__ dense_base) {
+__global__ void k_page_dense(PageIndexBatch batch) {
+    const PageIndexCol& col = batch.c[blockIdx.y];
+    const uint8_t* __restrict__ pages = col.pages;
+    const uint32_t* __restrict__ hdr = col.hdr;
+    const uint32_t npages = col.npages;
+    const uint32_t* __restrict__ chunk_base = col.chunk_base;
+    uint32_t* __restrict__ dense_base = col.dense_base;
     uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t lane = threadIdx.x & 31;
     if (warp >= npages) return;
@@ -121,8 +138,12 @@ __global__ void k_page_dense(const uint8_t* __restrict__ pages, const uint32_t* 
 }
 
 // Page containing row b * 1024, for every block b (and the terminal entry).
-__global__ void k_page_of_blk(const uint32_t* __restrict__ row_start, uint32_t npages, uint32_t nrows,
-                              uint32_t nblk, uint32_t* __restrict__ page_of_blk) {
+__global__ void k_page_of_blk(PageIndexBatch batch) {
+    const PageIndexCol& col = batch.c[blockIdx.y];
+    const uint32_t* __restrict__ row_start = col.row_start;
+    const uint32_t npages = col.npages, nrows = col.nrows;
+    const uint32_t nblk = (nrows >> kBlkShift) + 2;
+    uint32_t* __restrict__ page_of_blk = col.page_of_blk;
     uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nblk) return;
     uint64_t row = uint64_t(b) << kBlkShift;
@@ -145,30 +166,36 @@ __global__ void k_page_of_blk(const uint32_t* __restrict__ row_start, uint32_t n
 
 } // namespace
 
-int page_index_pass1(const uint8_t* pages, uint32_t npages, int32_t type, PageIndexBufs b, uint32_t* err, Scratch& s,
-                     cudaStream_t st) {
+int page_index_pass1(const PageIndexBatch& b, uint32_t* err, Scratch& s, cudaStream_t st) {
+    if (b.n <= 0) return 0;
+    uint32_t max_np = 0;
+    ScanSegs segs{};
+    for (int k = 0; k < b.n; k++) {
+        max_np = std::max(max_np, b.c[k].npages);
+        segs.s[segs.n++] = ScanSeg{b.c[k].rows, b.c[k].row_start, b.c[k].npages};
+        segs.s[segs.n++] = ScanSeg{b.c[k].chunks, b.c[k].chunk_base, b.c[k].npages};
+    }
     int launches = 0;
-    cudaMemsetAsync(b.flags, 0, sizeof(uint32_t), st);
-    if (npages) {
-        k_page_headers<<<(npages + 255) / 256, 256, 0, st>>>(pages, npages, type, b.hdr, b.rows, b.chunks, b.flags,
-                                                             err);
+    if (max_np) {
+        k_page_headers<<<dim3((max_np + 255) / 256, unsigned(b.n)), 256, 0, st>>>(b, err);
         launches++;
     }
-    launches += scan_exclusive_u32(b.rows, b.row_start, npages, s, st);
-    launches += scan_exclusive_u32(b.chunks, b.chunk_base, npages, s, st);
-    return launches;
+    return launches + scan_exclusive_u32_segs(segs, s, st);
 }
 
-int page_index_pass2(const uint8_t* pages, const uint32_t* hdr, uint32_t npages, uint32_t nrows,
-                     const uint32_t* row_start, const uint32_t* chunk_base, uint32_t* dense_base,
-                     uint32_t* page_of_blk, cudaStream_t st) {
+int page_index_pass2(const PageIndexBatch& b, cudaStream_t st) {
+    if (b.n <= 0) return 0;
+    uint32_t max_np = 0, max_blk = 0;
+    for (int k = 0; k < b.n; k++) {
+        max_np = std::max(max_np, b.c[k].npages);
+        max_blk = std::max(max_blk, (b.c[k].nrows >> kBlkShift) + 2);
+    }
     int launches = 0;
-    if (npages) {
-        k_page_dense<<<(npages * 32 + 255) / 256, 256, 0, st>>>(pages, hdr, npages, chunk_base, dense_base);
+    if (max_np) {
+        k_page_dense<<<dim3((max_np * 32 + 255) / 256, unsigned(b.n)), 256, 0, st>>>(b);
         launches++;
     }
-    uint32_t nblk = (nrows >> kBlkShift) + 2;
-    k_page_of_blk<<<(nblk + 255) / 256, 256, 0, st>>>(row_start, npages, nrows, nblk, page_of_blk);
+    k_page_of_blk<<<dim3((max_blk + 255) / 256, unsigned(b.n)), 256, 0, st>>>(b);
     return launches + 1;
 }
 

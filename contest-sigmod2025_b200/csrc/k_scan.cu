@@ -299,7 +299,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
 #pragma unroll
         for (int i = 0; i < kStepWords; i++) q[i] = __ldg(pw + (u % kUnitsPerPage) * kWordsPerStep + lane + 32 * i);
         hdr = lane == 0 ? __ldg(reinterpret_cast<const uint32_t*>(pw)) : 0;
-        row0 = lane == 0 ? __ldg(a.key.row_start + u / kUnitsPerPage) : 0;
+        row0 = lane == 0 ? (a.key.rpp ? (u / kUnitsPerPage) * a.key.rpp : __ldg(a.key.row_start + u / kUnitsPerPage))
+                         : 0;
     };
     uint4 q[kStepWords];
     uint32_t hdr_l = 0, row0_l = 0;

@@ -60,10 +60,10 @@ __device__ __forceinline__ unsigned long long ld_status(const unsigned long long
     return *reinterpret_cast<const volatile unsigned long long*>(p);
 }
 
+// One tile of a single-pass scan (the calling CTA takes its tile by ticket).
 template <typename T>
-__global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const T* __restrict__ in, T* __restrict__ out,
-                                                                size_t n, unsigned long long* status,
-                                                                uint32_t* ticket, uint32_t* err) {
+__device__ __forceinline__ void scan_tile_lookback(const T* __restrict__ in, T* __restrict__ out, size_t n,
+                                                   unsigned long long* status, uint32_t* ticket, uint32_t* err) {
     __shared__ uint32_t s_tile;
     __shared__ T s_prefix;
     if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
@@ -132,6 +132,29 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const T* __restr
             if (base + k == n - 1) out[n] = run;
         }
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const T* __restrict__ in, T* __restrict__ out,
+                                                                size_t n, unsigned long long* status,
+                                                                uint32_t* ticket, uint32_t* err) {
+    scan_tile_lookback<T>(in, out, n, status, ticket, err);
+}
+
+// Independent scans of several u32 arrays (blockIdx.y = array); array k's
+// tile status words start at status + status_off[k], its ticket at
+// tickets + k. An empty array gets out[0] = 0.
+__global__ void __launch_bounds__(kScanThreads) k_scan_segs(ScanSegs segs, unsigned long long* status,
+                                                            uint32_t* tickets, uint32_t* err) {
+    const ScanSeg& sg = segs.s[blockIdx.y];
+    const uint32_t nt = uint32_t((sg.n + kScanTile - 1) / kScanTile);
+    if (sg.n == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) sg.out[0] = 0;
+        return;
+    }
+    if (blockIdx.x >= nt) return;
+    scan_tile_lookback<uint32_t>(sg.in, sg.out, sg.n, status + segs.status_off[blockIdx.y], tickets + blockIdx.y,
+                                 err);
 }
 
 template <typename T>
@@ -219,6 +242,12 @@ int scan_impl(const T* in, T* out, size_t n, Scratch& s, cudaStream_t st) {
     return scan_launch<T>(in, out, n, status, s.err, st);
 }
 
+__global__ void k_gather_values(GatherList g, uint64_t* dst) {
+    const int i = threadIdx.x;
+    if (i >= g.n) return;
+    dst[g.slot[i]] = g.wide[i] ? *static_cast<const uint64_t*>(g.src[i]) : *static_cast<const uint32_t*>(g.src[i]);
+}
+
 __global__ void k_fill_u32(uint32_t* p, uint32_t v, size_t n) {
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) p[i] = v;
 }
@@ -243,6 +272,29 @@ int scan_exclusive_u64_batch(const ScanBatch64& b, size_t n, Scratch& s, cudaStr
 }
 
 size_t scan_status_bytes(size_t n) { return status_bytes(n); }
+
+int scan_exclusive_u32_segs(ScanSegs segs, Scratch& s, cudaStream_t st) {
+    if (segs.n <= 0) return 0;
+    size_t words = 0, max_nt = 1;
+    for (int k = 0; k < segs.n; k++) {
+        const size_t nt = (size_t(segs.s[k].n) + kScanTile - 1) / kScanTile;
+        segs.status_off[k] = uint32_t(words);
+        words += nt;
+        max_nt = std::max(max_nt, nt);
+    }
+    const size_t bytes = words * sizeof(unsigned long long) + segs.n * sizeof(uint32_t);
+    auto* status = static_cast<unsigned long long*>(s.alloc(std::max<size_t>(bytes, 16)));
+    auto* tickets = reinterpret_cast<uint32_t*>(status + words);
+    cudaMemsetAsync(status, 0, bytes, st);
+    k_scan_segs<<<dim3(unsigned(max_nt), unsigned(segs.n)), kScanThreads, 0, st>>>(segs, status, tickets, s.err);
+    return 1;
+}
+
+int gather_values(const GatherList& g, uint64_t* dst, cudaStream_t st) {
+    if (g.n <= 0) return 0;
+    k_gather_values<<<1, kMaxGather, 0, st>>>(g, dst);
+    return 1;
+}
 int scan_exclusive_u32_zeroed(const uint32_t* in, uint32_t* out, size_t n, void* status, uint32_t* err,
                               cudaStream_t st) {
     return scan_launch<uint32_t>(in, out, n, status, err, st);

@@ -29,6 +29,20 @@ int scan_exclusive_u64(const uint64_t* in, uint64_t* out, size_t n, Scratch& s, 
 size_t scan_status_bytes(size_t n);
 int scan_exclusive_u32_zeroed(const uint32_t* in, uint32_t* out, size_t n, void* status, uint32_t* err,
                               cudaStream_t st);
+// Independent exclusive scans of up to kMaxScanSegs u32 arrays of any
+// lengths, in one launch (status_off is filled in by the wrapper).
+constexpr int kMaxScanSegs = 64;
+struct ScanSeg {
+    const uint32_t* in;
+    uint32_t* out;  // n + 1 entries
+    uint32_t n;
+};
+struct ScanSegs {
+    ScanSeg s[kMaxScanSegs];
+    uint32_t status_off[kMaxScanSegs];
+    int n;
+};
+int scan_exclusive_u32_segs(ScanSegs segs, Scratch& s, cudaStream_t st);
 // Exclusive scans of several u64 arrays of length n (out[i][n] = total):
 // one launch when n fits one tile.
 constexpr int kMaxScanBatch = 32;
@@ -39,25 +53,45 @@ struct ScanBatch64 {
 };
 int scan_exclusive_u64_batch(const ScanBatch64& b, size_t n, Scratch& s, cudaStream_t st);
 int fill_u32(uint32_t* p, uint32_t v, size_t n, cudaStream_t st);
+// Gathers device values into dst[slot] (u32 zero-extended, or u64): the
+// values a host read-back needs, in one launch.
+constexpr int kMaxGather = 64;
+struct GatherList {
+    const void* src[kMaxGather];
+    uint8_t slot[kMaxGather];
+    uint8_t wide[kMaxGather];  // 1: u64, 0: u32
+    int n;
+};
+int gather_values(const GatherList& g, uint64_t* dst, cudaStream_t st);
 
 // ---- page index (k_pages.cu) ----
-// Builds row_start / chunk_base / dense_base / page_of_blk for a column whose
-// pages are resident at c.pages; checks every page header. Writes the column's
-// row total to *rows_out (device) and flags to *flags_out (device).
-struct PageIndexBufs {
+// Builds hdr / row_start / chunk_base / dense_base / page_of_blk for columns
+// whose pages are device-accessible at `pages`; checks every page header.
+// Pass 1 (headers, row and chunk offsets) and pass 2 (dense bases and block
+// pages) each take every column of a batch in one launch (blockIdx.y =
+// column); between them the host reads back row and chunk totals.
+constexpr int kMaxIndexBatch = 32;
+struct PageIndexCol {
+    const uint8_t* pages;
+    uint32_t npages;
+    int32_t type;
     uint32_t* hdr;           // npages: page headers (kept)
     uint32_t* rows;          // npages (scratch)
     uint32_t* chunks;        // npages (scratch)
     uint32_t* row_start;     // npages + 1
     uint32_t* chunk_base;    // npages + 1
-    uint32_t* flags;         // 1 word
+    uint32_t* flags;         // 1 word, zero before pass 1
+    // pass 2
+    uint32_t nrows;
+    uint32_t* dense_base;    // chunk total
+    uint32_t* page_of_blk;   // (nrows >> kBlkShift) + 2
 };
-int page_index_pass1(const uint8_t* pages, uint32_t npages, int32_t type, PageIndexBufs b, uint32_t* err,
-                     Scratch& s, cudaStream_t st);
-// After pass 1 the host knows the chunk total and row total.
-int page_index_pass2(const uint8_t* pages, const uint32_t* hdr, uint32_t npages, uint32_t nrows,
-                     const uint32_t* row_start, const uint32_t* chunk_base, uint32_t* dense_base,
-                     uint32_t* page_of_blk, cudaStream_t st);
+struct PageIndexBatch {
+    PageIndexCol c[kMaxIndexBatch];
+    int n;
+};
+int page_index_pass1(const PageIndexBatch& b, uint32_t* err, Scratch& s, cudaStream_t st);
+int page_index_pass2(const PageIndexBatch& b, cudaStream_t st);
 
 // ---- pipelines (k_probe.cu) ----
 // Items flowing through a pipeline: a row of the scanned input plus, per
