@@ -57,7 +57,10 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-steps", type=int, default=3, help="0 skips the CPU baseline")
-    ap.add_argument("--mode", default="all", choices=["all", "value", "e2e"],
+    ap.add_argument("--serve-queries", type=int, default=2000,
+                    help="queries per serving measurement (0 skips serving)")
+    ap.add_argument("--serve-workers", type=int, default=4)
+    ap.add_argument("--mode", default="all", choices=["all", "value", "e2e", "serve"],
                     help="value / e2e run one measurement only (for profiling); all prints the bench line")
     return ap.parse_args()
 
@@ -176,6 +179,89 @@ def profiled_traffic():
         return None
 
 
+def serve_bench(pkg, args, large):
+    """Serving on one GPU: a 9:1 mix of small queries (the 1M-row fact of a
+    second snowflake instance joined with 1 or 2 dimensions) and large ones
+    (the 5-way snowflake on the 50M-row fact), all over resident tables,
+    through a server of 1 worker (the plain path: one query at a time) and of
+    `--serve-workers` workers (queries overlap on the device). Closed loop:
+    every query submitted at once, queries/s = queries / time to the last
+    completion. Open loop: Poisson arrivals at 50% of the plain path's
+    closed-loop rate, p50/p99 of submit-to-completion latency."""
+    import random
+    import threading
+
+    small = pkg.Workload("snowflake", args.seed + 100, 0.02)
+    rng = random.Random(args.seed)
+    mix = [("large", None) if i % 10 == 9 else ("small", 1 + rng.randrange(2)) for i in range(args.serve_queries)]
+    out = {"mix": "9 small (1M-row fact, 2-3 tables) : 1 large (50M-row fact, 5 tables)", "queries": len(mix)}
+    plain_qps = None
+    for label, workers in (("plain", 1), ("batched", args.serve_workers)):
+        with pkg.Server(0, workers=workers) as srv:
+            tabs = {}
+            for name, w in (("small", small), ("large", large)):
+                plan = w.plan_ptr().contents
+                tabs[name] = [srv.upload(plan.inputs[i]) for i in range(plan.num_inputs)]
+            plans = {("large", None): large.plan_ptr(), ("small", 1): small.variant_ptr(1),
+                     ("small", 2): small.variant_ptr(2)}
+
+            def submit(q):
+                p = plans[q]
+                return srv.submit(p, tabs[q[0]][:p.contents.num_inputs], pkg.RESULT_DEVICE)
+
+            try:
+                # Warm every worker's graph cache for every plan.
+                for t in [submit(q) for q in list(plans) * (3 * workers)]:
+                    srv.wait(t)[0].free()
+                # Closed loop.
+                t0 = time.perf_counter()
+                tickets = [submit(q) for q in mix]
+                for t in tickets:
+                    srv.wait(t)[0].free()
+                qps = len(mix) / (time.perf_counter() - t0)
+                plain_qps = plain_qps or qps
+                # Open loop: Poisson arrivals; a waiter thread collects results.
+                rate = 0.5 * plain_qps
+                lat, issued = [], []
+                lock = threading.Lock()
+
+                def waiter():
+                    k = 0
+                    while k < len(mix):
+                        with lock:
+                            t = issued[k] if k < len(issued) else None
+                        if t is None:
+                            time.sleep(0.0001)
+                            continue
+                        r, ms = srv.wait(t)
+                        r.free()
+                        lat.append(ms)
+                        k += 1
+
+                th = threading.Thread(target=waiter)
+                th.start()
+                arrivals = random.Random(args.seed + 1)
+                t_next = time.perf_counter()
+                for q in mix:
+                    t_next += arrivals.expovariate(rate)
+                    while time.perf_counter() < t_next:
+                        pass
+                    t = submit(q)
+                    with lock:
+                        issued.append(t)
+                th.join()
+                lat.sort()
+                out[label] = {"workers": workers, "queries_per_s": qps, "arrival_rate_qps": rate,
+                              "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]}
+            finally:
+                for xs in tabs.values():
+                    for x in xs:
+                        x.free()
+    out["speedup_closed_loop"] = out["batched"]["queries_per_s"] / out["plain"]["queries_per_s"]
+    small.close()
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -214,8 +300,16 @@ def main():
     inputs = plan.contents
     residents = [ctx.upload(inputs.inputs[i]) for i in range(inputs.num_inputs)]
 
-    if args.mode == "e2e":
+    if args.mode in ("e2e", "serve"):
         args.steps = 0
+    if args.mode == "serve":
+        serving = serve_bench(pkg, args, w)
+        for x in residents:
+            x.free()
+        ctx.close()
+        if rank == 0:
+            print(json.dumps({"mode": "serve", "serving": serving}))
+        return 0
     # ---- value: tables resident in HBM ----
     # Kernel timing is on from the first warm-up step, so every timed step
     # runs the same (graph-replayed) query.
@@ -324,6 +418,8 @@ def main():
         return 0
     h2d = e2e_stats.h2d_bytes + e2e_stats.mapped_input_bytes
     d2h = e2e_stats.d2h_bytes
+    # ---- serving: concurrent queries through bj_server (one GPU) ----
+    serving = serve_bench(pkg, args, w) if args.serve_queries > 0 and world == 1 else None
 
     for x in residents:
         x.free()
@@ -357,6 +453,7 @@ def main():
                          "split_ms": pageable_split},
         "gpu_launches": launches,
         "phases": phases,
+        "serving": serving,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "traffic": traffic,
                      "kernel": "k_scan_probe over the fact's key pages",

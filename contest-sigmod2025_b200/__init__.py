@@ -72,7 +72,7 @@ class BjStats(ctypes.Structure):
                 ("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
                 ("scan_kernel_ms", ctypes.c_double), ("scan_kernel_launches", ctypes.c_uint64),
                 ("scan_kernel_bytes", ctypes.c_uint64), ("mapped_input_bytes", ctypes.c_uint64),
-                ("phase_ms", ctypes.c_double * 4)]
+                ("phase_ms", ctypes.c_double * 4), ("arena_bytes", ctypes.c_uint64)]
 
 
 # Every symbol include/b200join.h declares, with its ctypes signature.
@@ -98,6 +98,12 @@ ABI = {
     "bj_context_stream": (_VP, [_VP]),
     "bj_context_profile": (None, [_VP, _INT]),
     "bj_join_count_static": (_INT, [_VP, _U64, _U64, _VP, _U64, _VP, _VP]),
+    "bj_server_create": (_INT, [_INT, _INT, _U64, ctypes.POINTER(_VP)]),
+    "bj_server_destroy": (None, [_VP]),
+    "bj_server_context": (_VP, [_VP, _INT]),
+    "bj_server_submit": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), _INT, ctypes.POINTER(_U64)]),
+    "bj_server_wait": (_INT, [_VP, _U64, ctypes.POINTER(_VP), ctypes.POINTER(ctypes.c_double)]),
+    "bj_server_resident_free": (None, [_VP, _VP]),
 }
 
 WORKLOAD_ABI = {
@@ -105,6 +111,7 @@ WORKLOAD_ABI = {
     "bjw_workload_load": (_INT, [ctypes.c_char_p, ctypes.POINTER(_VP)]),
     "bjw_workload_plan": (ctypes.POINTER(BjPlan), [_VP]),
     "bjw_workload_scan_bytes": (_U64, [_VP]),
+    "bjw_workload_variant": (ctypes.POINTER(BjPlan), [_VP, _INT]),
     "bjw_workload_free": (None, [_VP]),
     "bjw_save_plan": (_INT, [ctypes.c_char_p, ctypes.POINTER(BjPlan)]),
     "bjw_save_table": (_INT, [ctypes.c_char_p, ctypes.POINTER(BjTable)]),
@@ -389,6 +396,14 @@ class Workload:
     def scan_bytes(self) -> int:
         return wlib().bjw_workload_scan_bytes(self.handle)
 
+    def variant_ptr(self, dims: int):
+        """Snowflake: the fact joined with its first `dims` dimensions (its
+        inputs are the workload's first dims + 1 tables)."""
+        p = wlib().bjw_workload_variant(self.handle, dims)
+        if not p:
+            raise EngineError(1, f"no {dims}-dimension variant of {self.name}")
+        return p
+
     def close(self):
         if self.handle:
             wlib().bjw_workload_free(self.handle)
@@ -527,6 +542,69 @@ class Context:
     def close(self):
         if self.handle:
             lib().bj_context_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class ServerResident:
+    """A resident table shared by a server's workers."""
+
+    def __init__(self, server: "Server", handle):
+        self._server, self.handle = server, handle
+
+    def free(self):
+        if self.handle:
+            lib().bj_server_resident_free(self._server.handle, self.handle)
+            self.handle = None
+
+
+class Server:
+    """Concurrent queries over resident tables (bj_server_*): `workers`
+    contexts on one device, admission by estimated device scratch."""
+
+    def __init__(self, device: int = 0, workers: int = 4, scratch_cap_bytes: int = 0):
+        h = ctypes.c_void_p()
+        st = lib().bj_server_create(device, workers, scratch_cap_bytes, ctypes.byref(h))
+        if st != 0:
+            raise EngineError(st, "bj_server_create failed")
+        self.handle = h
+        self._plans = {}
+
+    def upload(self, table_struct) -> ServerResident:
+        ctx0 = lib().bj_server_context(self.handle, 0)
+        r = ctypes.c_void_p()
+        st = lib().bj_resident_upload(ctx0, table_struct, ctypes.byref(r))
+        if st != 0:
+            raise EngineError(st, "bj_resident_upload failed")
+        return ServerResident(self, r)
+
+    def submit(self, plan_ptr, residents: Sequence[ServerResident], flags: int = RESULT_DEVICE) -> int:
+        arr = (ctypes.c_void_p * len(residents))(*[x.handle for x in residents])
+        t = ctypes.c_uint64()
+        st = lib().bj_server_submit(self.handle, plan_ptr, arr, flags, ctypes.byref(t))
+        if st != 0:
+            raise EngineError(st, "bj_server_submit failed")
+        self._plans[t.value] = arr  # the table array must outlive the query
+        return t.value
+
+    def wait(self, ticket: int):
+        """(Result, latency in ms) of a submitted query."""
+        r = ctypes.c_void_p()
+        ms = ctypes.c_double()
+        st = lib().bj_server_wait(self.handle, ticket, ctypes.byref(r), ctypes.byref(ms))
+        self._plans.pop(ticket, None)
+        if st != 0:
+            raise EngineError(st, "query failed")
+        return Result(None, r), ms.value
+
+    def close(self):
+        if self.handle:
+            lib().bj_server_destroy(self.handle)
             self.handle = None
 
     def __enter__(self):

@@ -1361,6 +1361,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
         ctx->prof_bytes = 0;
         res->stats.kernel_launches = ctx->launches - launches0;
         res->stats.pipelines = pipes;
+        res->stats.arena_bytes = ctx->arena.used_total();
         ctx->arena.reset();
     } catch (const SpecMiss&) {
         // Not an error: the call runs again with a page index for every column.
@@ -1489,6 +1490,7 @@ bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resid
         g.stats = bj_stats{};
         g.stats.kernel_launches = ctx->launches - launches0;
         g.stats.pipelines = exe.pipelines_run();
+        g.stats.arena_bytes = ctx->arena.used_total();
         for (uint64_t i = 0; i < plan->num_inputs; i++) {
             std::vector<uint8_t> used;
             collect_columns(ex, uint32_t(i), tables[i]->cols.size(), used);
@@ -1563,6 +1565,7 @@ int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& typ
         res->stats.scan_kernel_bytes = g.prof_bytes;
         res->stats.kernel_launches = g.stats.kernel_launches;
         res->stats.pipelines = g.stats.pipelines;
+        res->stats.arena_bytes = g.stats.arena_bytes;
         res->stats.input_pages = g.stats.input_pages;
         res->stats.output_pages = g.total_pages;
         ctx->launches += g.stats.kernel_launches;
@@ -1614,6 +1617,23 @@ int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* co
 }
 
 } // namespace
+} // namespace bj
+
+namespace bj {
+// Waits for ctx's work, then drops its graphs that read table t.
+void drop_graphs_using(bj_context* ctx, const bj_resident* t) {
+    ctx->sync_all();
+    auto& gc = ctx->graph_cache;
+    for (size_t i = 0; i < gc.size();) {
+        const auto& tabs = gc[i]->tables;
+        if (std::find(tabs.begin(), tabs.end(), t) != tabs.end()) {
+            destroy_graph(*gc[i]);
+            gc.erase(gc.begin() + i);
+        } else {
+            i++;
+        }
+    }
+}
 } // namespace bj
 
 extern "C" {
@@ -1740,22 +1760,11 @@ BJ_API int bj_resident_upload(bj_context* ctx, const bj_table* table, bj_residen
     return BJ_OK;
 }
 
+
 BJ_API void bj_resident_free(bj_context* ctx, bj_resident* t) {
     if (!t) return;
-    if (ctx) {
-        ctx->sync_all();
-        // Graphs that read this table are no longer valid.
-        auto& gc = ctx->graph_cache;
-        for (size_t i = 0; i < gc.size();) {
-            const auto& tabs = gc[i]->tables;
-            if (std::find(tabs.begin(), tabs.end(), t) != tabs.end()) {
-                destroy_graph(*gc[i]);
-                gc.erase(gc.begin() + i);
-            } else {
-                i++;
-            }
-        }
-    }
+    // Graphs that read this table are no longer valid.
+    if (ctx) drop_graphs_using(ctx, t);
     delete t;
 }
 

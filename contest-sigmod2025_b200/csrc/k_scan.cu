@@ -366,11 +366,13 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
     ScanArgs a{key,      ht,       uint32_t(mode), bloom_bytes ? 1u : 0u, prefetch,
                ht.bloom_log2 ? (1u << ht.bloom_log2) : 0u, 1u << 27,
                page_counts, page_off, cursor, out_rows, out_ents, out_mult, capacity, err};
-    static bool configured = false;
-    if (!configured) {
+    // Once per process (thread-safe static initialisation; server workers
+    // launch from several threads).
+    static const bool configured = [] {
         cudaFuncSetAttribute(k_scan_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBloomSmemMax));
-        configured = true;
-    }
+        return true;
+    }();
+    (void)configured;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan_probe, kCtaThreads, bloom_bytes);
     per_sm = std::max(1, per_sm);

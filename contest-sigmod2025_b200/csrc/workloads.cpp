@@ -14,6 +14,7 @@
 #include <exception>
 #include <string>
 #include <thread>
+#include <memory>
 #include <vector>
 
 namespace {
@@ -342,9 +343,19 @@ void make_snowflake(plan_io::OwnedPlan& p, uint64_t seed, double scale) {
 
 } // namespace
 
+// A plan over a prefix of a workload's tables (page arrays shared, not copied).
+struct VariantPlan {
+    std::vector<bj_table> tables;
+    std::vector<std::vector<bj_attr>> attrs;
+    std::vector<bj_node> nodes;
+    bj_plan view{};
+};
+
 struct bjw_workload {
     plan_io::OwnedPlan plan;
     bj_plan view{};
+    std::string name;
+    std::vector<std::unique_ptr<VariantPlan>> variants;  // by dimension count
 };
 
 struct bjw_pages {
@@ -357,6 +368,7 @@ int bjw_workload_create(const char* name, uint64_t seed, double scale, bjw_workl
     try {
         auto w = std::make_unique<bjw_workload>();
         std::string n(name ? name : "");
+        w->name = n;
         if (n == "join2")
             make_join2(w->plan, seed, scale);
         else if (n == "snowflake")
@@ -385,6 +397,39 @@ int bjw_workload_load(const char* path, bjw_workload** out) {
 }
 
 const bj_plan* bjw_workload_plan(bjw_workload* w) { return &w->view; }
+
+const bj_plan* bjw_workload_variant(bjw_workload* w, int dims) {
+    if (!w || w->name != "snowflake" || dims < 1 || dims > 4) return nullptr;
+    if (w->variants.size() <= size_t(dims)) w->variants.resize(dims + 1);
+    auto& v = w->variants[dims];
+    if (!v) {
+        v = std::make_unique<VariantPlan>();
+        for (int t = 0; t <= dims; t++) v->tables.push_back(w->view.inputs[t]);
+        auto add = [&](bj_node n, std::vector<bj_attr> a) {
+            v->nodes.push_back(n);
+            v->attrs.push_back(std::move(a));
+        };
+        // Scans: fact {fk0..fk3}; dimension d {key, name}.
+        add(scan_node(0), {{0, BJ_INT32, 0}, {1, BJ_INT32, 0}, {2, BJ_INT32, 0}, {3, BJ_INT32, 0}});
+        for (int d = 0; d < dims; d++) add(scan_node(1 + d), {{0, BJ_INT32, 0}, {2, BJ_VARCHAR, 0}});
+        // Join d keeps fk0..fk3 and the names so far, and adds dimension d's
+        // name: left has 4 + d attributes, the right's name is 4 + d + 1.
+        uint64_t left = 0;
+        for (int d = 0; d < dims; d++) {
+            std::vector<bj_attr> out;
+            for (uint32_t a = 0; a < uint32_t(4 + d); a++) out.push_back({a, a < 4 ? BJ_INT32 : BJ_VARCHAR, 0});
+            out.push_back({uint32_t(4 + d + 1), BJ_VARCHAR, 0});
+            add(join_node(left, uint64_t(1 + d), uint64_t(d), 0, false), std::move(out));
+            left = v->nodes.size() - 1;
+        }
+        for (size_t i = 0; i < v->nodes.size(); i++) {
+            v->nodes[i].num_output_attrs = v->attrs[i].size();
+            v->nodes[i].output_attrs = v->attrs[i].data();
+        }
+        v->view = bj_plan{v->nodes.size(), v->nodes.data(), v->tables.size(), v->tables.data(), left};
+    }
+    return &v->view;
+}
 
 uint64_t bjw_workload_scan_bytes(bjw_workload* w) {
     // Pages of every column a scan node names (each base column counted once).

@@ -39,6 +39,11 @@ BJ_API int bjw_workload_create(const char* name, uint64_t seed, double scale, bj
 BJ_API int bjw_workload_load(const char* path, bjw_workload** out);
 /* The plan view (valid until bjw_workload_free). */
 BJ_API const bj_plan* bjw_workload_plan(bjw_workload* w);
+/* Snowflake only: the fact table joined with its first `dims` dimensions
+ * (1..4), over the workload's first dims + 1 tables (pages shared); output: the
+ * four fact keys and the joined dimensions' names. NULL for other workloads.
+ * Valid until bjw_workload_free. */
+BJ_API const bj_plan* bjw_workload_variant(bjw_workload* w, int dims);
 /* Total bytes of input pages the plan's scans read. */
 BJ_API uint64_t bjw_workload_scan_bytes(bjw_workload* w);
 BJ_API void bjw_workload_free(bjw_workload* w);

@@ -129,6 +129,7 @@ typedef struct bj_stats {
      * ordering (hit-rate sampling), [2] its scan and probe stages, [3] its
      * output (result pages written). */
     double phase_ms[4];
+    uint64_t arena_bytes;       /* device scratch the call used (the query's intermediates) */
 } bj_stats;
 
 /* Replaces Contest::build_context (engine/Execute.cpp:42-46). Creates the CUDA
@@ -182,6 +183,31 @@ BJ_API const void* bj_result_device_page(const bj_result* r, uint64_t column, ui
 BJ_API int bj_result_copy_pages(const bj_result* r, uint64_t column, void* const* dst);
 BJ_API int bj_result_stats(const bj_result* r, bj_stats* out);
 BJ_API void bj_result_free(bj_result* r);
+
+/* Serving (no reference counterpart: the reference runs one query at a time,
+ * engine/infra/Scheduler.cpp:170-172). A server owns `workers` contexts on one
+ * device, each with its own streams, scratch arena and CUDA-graph cache, and a
+ * worker thread per context. Queries over resident tables wait in arrival
+ * order; the head is admitted when the device scratch of the running queries
+ * (each estimated by what its plan used the last time it ran) plus its own
+ * fits `scratch_cap_bytes` (0: no cap), and runs on the next free worker, so
+ * queries overlap on the device. A query is always admitted when none runs.
+ * Resident tables uploaded through any of the server's contexts
+ * (bj_server_context) serve every worker; free them with
+ * bj_server_resident_free once no submitted query uses them. The plan and
+ * table arrays passed to bj_server_submit must stay valid until
+ * bj_server_wait returns for that ticket. */
+typedef struct bj_server bj_server;
+BJ_API int bj_server_create(int device, int workers, uint64_t scratch_cap_bytes, bj_server** out);
+BJ_API void bj_server_destroy(bj_server* s);
+BJ_API bj_context* bj_server_context(bj_server* s, int worker);
+BJ_API int bj_server_submit(bj_server* s, const bj_plan* plan, bj_resident* const* tables, int flags,
+                            uint64_t* ticket);
+/* Blocks until the query is done; *out receives its result (free it with
+ * bj_result_free), *latency_ms the time from submit to completion. Returns
+ * the query's status. */
+BJ_API int bj_server_wait(bj_server* s, uint64_t ticket, bj_result** out, double* latency_ms);
+BJ_API void bj_server_resident_free(bj_server* s, bj_resident* table);
 
 /* Turns per-kernel event timing of the scan-side probe stage on (1) or off (0).
  * Adds two event records per timed launch; off by default. */
