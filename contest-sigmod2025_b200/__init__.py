@@ -85,6 +85,8 @@ ABI = {
     "bj_execute": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP)]),
     "bj_resident_upload": (_INT, [_VP, ctypes.POINTER(BjTable), ctypes.POINTER(_VP)]),
     "bj_resident_free": (None, [_VP, _VP]),
+    "bj_resident_save": (_INT, [_VP, _VP, ctypes.c_char_p]),
+    "bj_resident_load": (_INT, [_VP, ctypes.c_char_p, ctypes.POINTER(_VP)]),
     "bj_execute_resident": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), _INT, ctypes.POINTER(_VP)]),
     "bj_result_num_rows": (_U64, [_VP]),
     "bj_result_num_columns": (_U64, [_VP]),
@@ -524,6 +526,14 @@ class Context:
         r = ctypes.c_void_p()
         self._check(lib().bj_resident_upload(self.handle, ctypes.byref(table_struct), ctypes.byref(r)),
                     "bj_resident_upload")
+        return Resident(self, r)
+
+    def save_resident(self, resident: Resident, path: str) -> None:
+        self._check(lib().bj_resident_save(self.handle, resident.handle, path.encode()), "bj_resident_save")
+
+    def load_resident(self, path: str) -> Resident:
+        r = ctypes.c_void_p()
+        self._check(lib().bj_resident_load(self.handle, path.encode(), ctypes.byref(r)), "bj_resident_load")
         return Resident(self, r)
 
     def execute_resident(self, plan, residents: Sequence[Resident], flags: int = RESULT_HOST) -> Result:

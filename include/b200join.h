@@ -160,6 +160,12 @@ BJ_API int bj_execute(bj_context* ctx, const bj_plan* plan, bj_result** out);
  * handle instead of re-copying the pages. */
 BJ_API int bj_resident_upload(bj_context* ctx, const bj_table* table, bj_resident** out);
 BJ_API void bj_resident_free(bj_context* ctx, bj_resident* table);
+/* Snapshot of a resident table: its pages and page index written to one file
+ * (replaces the reference's table cache file, engine/infra/DataSource.cpp:
+ * 50-159); loading copies them straight to HBM without re-indexing. Returns
+ * BJ_ERR_INVALID for an unreadable, truncated or foreign file. */
+BJ_API int bj_resident_save(bj_context* ctx, const bj_resident* table, const char* path);
+BJ_API int bj_resident_load(bj_context* ctx, const char* path, bj_resident** out);
 
 /* Flags of bj_execute_resident. */
 #define BJ_RESULT_HOST 0   /* copy result pages to host memory */

@@ -300,3 +300,36 @@ def test_pinned_uniform_column_speculation(pkg, ctx, oracle, break_middle_page):
             assert n > 0
     finally:
         torch._C._cudart.cudaHostUnregister(base)
+
+
+def test_resident_snapshot_round_trip(pkg, ctx, oracle, tmp_path):
+    """Resident tables saved to snapshot files and loaded back (no page index
+    pass) answer the query exactly; truncated or foreign files are rejected."""
+    w = pkg.Workload("snowflake", 14, 0.05)
+    plan = w.plan_ptr().contents
+    res = [ctx.upload(plan.inputs[i]) for i in range(plan.num_inputs)]
+    paths = [str(tmp_path / f"t{i}.bjres") for i in range(len(res))]
+    for r, path in zip(res, paths):
+        ctx.save_resident(r, path)
+        r.free()
+    loaded = [ctx.load_resident(path) for path in paths]
+    try:
+        with ctx.execute_resident(w.plan_ptr(), loaded) as r:
+            got, keep = r.table_struct()
+            want = oracle.execute(w.plan_ptr())
+            assert oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), "snapshot") > 0
+    finally:
+        for x in loaded:
+            x.free()
+    data = open(paths[0], "rb").read()
+    bad = tmp_path / "truncated.bjres"
+    bad.write_bytes(data[: len(data) // 2])
+    with pytest.raises(pkg.EngineError):
+        ctx.load_resident(str(bad))
+    foreign = tmp_path / "foreign.bjres"
+    foreign.write_bytes(b"not a snapshot" * 100)
+    with pytest.raises(pkg.EngineError):
+        ctx.load_resident(str(foreign))
+    # The context is still usable.
+    w2 = pkg.Workload("join2", 15, 0.01)
+    check_against_oracle(pkg, ctx, oracle, w2.plan_ptr(), "after bad snapshots")
