@@ -896,6 +896,15 @@ class Executor {
             s.kind = sp.kind;
             if (sp.kind == 0) {
                 s.col = col(sp.attr);
+                // A probe key column of this input: every item matched an
+                // entry with that key, so the value is the entry's key (one
+                // load, never NULL) instead of a lookup in the column's pages.
+                for (size_t k = 0; k < np; k++)
+                    if (pp.probes[k].probe_attr == sp.attr) {
+                        s.kind = 2;
+                        s.probe = int(stage_of[k]);
+                        break;
+                    }
             } else {
                 s.probe = int(stage_of[sp.probe]);
                 s.slot = int(sp.slot);

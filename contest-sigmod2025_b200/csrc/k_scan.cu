@@ -16,9 +16,10 @@
 //    two funnel shifts and a logic op (bloom_bits_fast), spread over the
 //    multiply and integer pipes; the lane's survivors form a 32-bit mask, so
 //    a unit costs one vote and at most one warp prefix sum;
-//  * a page with NULLs is read row by row, 32 rows per step, the null bitmap
-//    word of those rows giving validity and (by popcount) the dense index of
-//    each value;
+//  * a page with NULLs is read in blocks of 1024 rows, 32 per lane: the null
+//    bitmap word of a lane's rows gives their validity, and the page index's
+//    dense base of their 64-row chunk plus a popcount the value index of
+//    each (units split a page's rows the same way);
 //  * the hash table's bloom filter (up to 128 KiB) is staged once per CTA in
 //    shared memory; one CTA of 32 warps runs per SM;
 //  * survivors (bloom hits, or every non-null row when the probe is not
@@ -116,12 +117,17 @@ __device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t 
             hi[i] = a.ht.bucket_off[b + 1];
         }
     }
+    // The first entry of every bucket is loaded for all candidates at once;
+    // only buckets with more entries (few: about one key per bucket) loop.
+    uint32_t k0[kPerLane];
+#pragma unroll
+    for (int i = 0; i < kPerLane; i++) k0[i] = lo[i] < hi[i] ? a.ht.keys[lo[i]] : ~key[i];
     uint32_t cnt = 0;
     uint32_t cj[kPerLane];
 #pragma unroll
     for (int i = 0; i < kPerLane; i++) {
-        uint32_t c = 0, first = hi[i];
-        for (uint32_t e = lo[i]; e < hi[i]; e++)
+        uint32_t c = k0[i] == key[i] ? 1u : 0u, first = c ? lo[i] : hi[i];
+        for (uint32_t e = lo[i] + 1; e < hi[i]; e++)
             if (a.ht.keys[e] == key[i]) {
                 first = c ? first : e;
                 c++;
@@ -142,20 +148,25 @@ __device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t 
             base = a.page_off[unit] + w.page_cnt;
         }
         uint32_t o = base + off;
+        auto emit = [&](uint32_t r, uint32_t e) {
+            if (o < a.capacity) {
+                a.out_rows[o] = r;
+                a.out_ents[o] = e;
+                if (a.out_mult) a.out_mult[o] = a.ht.mult[e];
+            } else {
+                record_error(a.err, kErrCapacity);
+            }
+            o++;
+        };
 #pragma unroll
         for (int i = 0; i < kPerLane; i++) {
-            uint32_t left = cj[i];
-            for (uint32_t e = lo[i]; left; e++) {
+            if (!cj[i]) continue;
+            emit(row[i], lo[i]);  // the first match, found above
+            uint32_t left = cj[i] - 1;
+            for (uint32_t e = lo[i] + 1; left; e++) {
                 if (a.ht.keys[e] != key[i]) continue;
                 left--;
-                if (o < a.capacity) {
-                    a.out_rows[o] = row[i];
-                    a.out_ents[o] = e;
-                    if (a.out_mult) a.out_mult[o] = a.ht.mult[e];
-                } else {
-                    record_error(a.err, kErrCapacity);
-                }
-                o++;
+                emit(row[i], e);
             }
         }
     }
@@ -164,29 +175,31 @@ __device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t 
     __syncwarp();
 }
 
-// Buffers the candidates of one step of a page without NULLs: bit c of
-// `take` is value vi0 + 128 (c / 4) + c % 4 of the page of unit p (values
-// at vals, first row row0). The key is read again from the page, which this warp has just
-// loaded, so the read hits in cache. Candidates are numbered across the warp
-// in lane order; when they do not fit, the buffer is filled, probed and
+// Buffers the candidates flagged in `take` (up to 32 per lane): map(c, key,
+// row) gives candidate c's key and row. Candidates are numbered across the
+// warp in lane order; when they do not fit, the buffer is filled, probed and
 // refilled until all are in.
-__device__ __forceinline__ void push_step(const ScanArgs& a, WarpState& w, uint32_t take, int vi0,
-                                          const uint32_t* vals, uint32_t row0, uint32_t p) {
+template <typename Map>
+__device__ __forceinline__ void push_bits(const ScanArgs& a, WarpState& w, uint32_t take, uint32_t p, Map&& map) {
     if (!__any_sync(0xffffffffu, take != 0)) return;
     uint32_t total;
-    const uint32_t off = warp_excl(__popc(take), total);
+    const uint32_t cnt = __popc(take);
+    const uint32_t off = warp_excl(cnt, total);
     for (uint32_t done = 0;;) {
         const uint32_t room = kBatch - w.n;
-        uint32_t t = take, j = off;
-        while (t) {
-            const uint32_t c = __ffs(t) - 1;
-            t &= t - 1;
-            if (j >= done && j - done < room) {
-                const uint32_t vi = uint32_t(vi0 + 128 * int(c >> 2) + int(c & 3));
-                w.bkey[w.n + j - done] = __ldg(vals + vi);
-                w.brow[w.n + j - done] = row0 + vi;
+        // This lane's candidates are numbered [off, off + cnt); only those in
+        // the window [done, done + room) go into the buffer this round.
+        if (off + cnt > done && off < done + room) {
+            uint32_t t = take, j = off;
+            for (; j < done; j++) t &= t - 1;  // skip the ones already buffered
+            for (; t && j < done + room; j++) {
+                const uint32_t c = __ffs(t) - 1;
+                t &= t - 1;
+                uint32_t key, row;
+                map(c, key, row);
+                w.bkey[w.n + j - done] = key;
+                w.brow[w.n + j - done] = row;
             }
-            j++;
         }
         const uint32_t took = min(room, total - done);
         w.n += took;
@@ -196,18 +209,16 @@ __device__ __forceinline__ void push_step(const ScanArgs& a, WarpState& w, uint3
     }
 }
 
-// Buffers one candidate per lane (key, row) of unit p.
-__device__ __forceinline__ void push_one(const ScanArgs& a, WarpState& w, bool take, uint32_t key, uint32_t row,
-                                         uint32_t p) {
-    const uint32_t mask = __ballot_sync(0xffffffffu, take);
-    if (!mask) return;
-    if (w.n + 32 > kBatch) flush(a, w, p);
-    if (take) {
-        const uint32_t o = w.n + __popc(mask & ((1u << lane_id()) - 1));
-        w.bkey[o] = key;
-        w.brow[o] = row;
-    }
-    w.n += __popc(mask);
+// Candidates of one step of a page without NULLs: bit c of `take` is value
+// vi0 + 128 (c / 4) + c % 4 of the page of unit p (values at vals, first row
+// row0); the key is read again from the page, which this warp has just loaded.
+__device__ __forceinline__ void push_step(const ScanArgs& a, WarpState& w, uint32_t take, int vi0,
+                                          const uint32_t* vals, uint32_t row0, uint32_t p) {
+    push_bits(a, w, take, p, [&](uint32_t c, uint32_t& key, uint32_t& row) {
+        const uint32_t vi = uint32_t(vi0 + 128 * int(c >> 2) + int(c & 3));
+        key = __ldg(vals + vi);
+        row = row0 + vi;
+    });
 }
 
 __device__ __forceinline__ bool bloom_pass(const ScanArgs& a, const uint32_t* bloom, uint32_t key) {
@@ -247,33 +258,59 @@ __device__ __forceinline__ uint32_t step_valid(int vi0, uint32_t n) {
     return valid;
 }
 
-// Rows of a page with NULLs, 32 per step: bitmap word, validity, dense
-// index, value.
-__device__ __forceinline__ void scan_page_nulls(const ScanArgs& a, WarpState& w, const uint32_t* bloom, bool use_bloom,
-                                             uint32_t unit, uint32_t n, uint32_t row0) {
+// Rows [r_begin, r_end) of page p, which has NULLs, in blocks of 1024 rows:
+// lane l takes 32 rows (one 32-bit bitmap word); the page index's dense base
+// of their 64-row chunk, plus the popcount of the chunk's lower word for an
+// upper half, gives the value index of the first valid row. Without a bloom
+// every valid row is a candidate and no value is read before the probe.
+__device__ __forceinline__ void scan_rows_nulls(const ScanArgs& a, WarpState& w, const uint32_t* bloom,
+                                                bool use_bloom, uint32_t unit, uint32_t p, uint32_t n,
+                                                uint32_t row0, uint32_t r_begin, uint32_t r_end) {
     const uint32_t lane = lane_id();
-    const uint8_t* pg = a.key.pages + size_t(unit >> 1) * kPageSize;
+    if (!a.key.chunk_base || !a.key.dense_base) {
+        // A column run without a page index (its layout speculated to have
+        // no NULLs): the speculation was wrong and the call runs again.
+        if (lane == 0) record_error(a.err, kErrPageHeader);
+        return;
+    }
+    const uint8_t* pg = a.key.pages + size_t(p) * kPageSize;
+    const uint32_t* vals = reinterpret_cast<const uint32_t*>(pg + 4);
     const uint32_t nbytes = (n + 7) >> 3;
     const uint8_t* bm = pg + kPageSize - nbytes;
-    uint32_t running = 0;
-    for (uint32_t r0 = 0; r0 < n; r0 += 32) {
-        uint32_t wbits = 0;
+    const uint32_t cb = __ldg(a.key.chunk_base + p);
+    for (uint32_t blk = r_begin; blk < r_end; blk += 1024) {
+        const uint32_t r = blk + 32 * lane;  // this lane's first row
+        uint32_t wb = 0;
+        if (r < r_end) {
 #pragma unroll
-        for (int b = 0; b < 4; b++) {
-            const uint32_t byte = (r0 >> 3) + b;
-            if (byte < nbytes) wbits |= uint32_t(bm[byte]) << (8 * b);
+            for (int b = 0; b < 4; b++) {
+                const uint32_t byte = (r >> 3) + b;
+                if (byte < nbytes) wb |= uint32_t(bm[byte]) << (8 * b);
+            }
+            if (r_end - r < 32) wb &= (1u << (r_end - r)) - 1;
         }
-        const uint32_t lim = n - r0 >= 32 ? 0xffffffffu : ((1u << (n - r0)) - 1);
-        wbits &= lim;
-        const uint32_t d = running + __popc(wbits & ((1u << lane) - 1));
-        // An INT32 page holds at most 2047 values; a dense index beyond that
-        // only comes from a malformed page (already reported by the page
-        // index) and is not read.
-        const bool valid = ((wbits >> lane) & 1) && d < 2047;
-        const uint32_t key = valid ? __ldg(reinterpret_cast<const uint32_t*>(pg + 4) + d) : 0;
-        running += __popc(wbits);
-        const bool take = valid && (!use_bloom || bloom_pass(a, bloom, key));
-        push_one(a, w, take, key, row0 + r0 + lane, unit);
+        // Lanes pair up into 64-row chunks (blocks start at a multiple of 64).
+        const uint32_t lower = __shfl_up_sync(0xffffffffu, wb, 1);
+        uint32_t d0 = 0;
+        if (r < r_end) d0 = __ldg(a.key.dense_base + cb + (r >> 6)) + ((lane & 1) ? __popc(lower) : 0u);
+        // An INT32 page holds at most 2047 values; a larger dense index only
+        // comes from a malformed page (reported by the page index) and is not read.
+        if (d0 + __popc(wb) > 2047) wb = 0;
+        uint32_t take = wb;
+        if (use_bloom && wb) {
+            take = 0;
+            uint32_t t = wb, d = d0;
+            while (t) {
+                const uint32_t j = __ffs(t) - 1;
+                t &= t - 1;
+                if (bloom_pass(a, bloom, __ldg(vals + d))) take |= 1u << j;
+                d++;
+            }
+        }
+        push_bits(a, w, take, unit, [&](uint32_t c, uint32_t& key, uint32_t& row) {
+            key = __ldg(vals + d0 + __popc(wb & ((1u << c) - 1)));
+            row = row0 + r + c;
+        });
     }
 }
 
@@ -332,9 +369,12 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
             const int vi0 = 4 * int(lane) - 1 + int(part * 4 * kWordsPerStep);
             if (vi0 - int(lane) * 4 < int(n))  // some value of the unit is below n
                 push_step(a, w, step_take(a, q, bloom, use_bloom) & step_valid(vi0, n), vi0, vals, row0, u);
-        } else if (part == 0) {
-            // A page with NULLs is read whole by its first unit.
-            scan_page_nulls(a, w, bloom, use_bloom, u, n, row0);
+        } else {
+            // A page with NULLs: unit k takes rows [1024 k, 1024 (k + 1)), the
+            // last unit every row from there on.
+            const uint32_t r_begin = part * 1024;
+            const uint32_t r_end = part + 1 == kUnitsPerPage ? n : min(n, r_begin + 1024);
+            if (r_begin < r_end) scan_rows_nulls(a, w, bloom, use_bloom, u, p, n, row0, r_begin, r_end);
         }
         if (a.mode != 2) {
             flush(a, w, u);
@@ -376,7 +416,7 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan_probe, kCtaThreads, bloom_bytes);
     per_sm = std::max(1, per_sm);
-    const uint64_t ctas = std::min<uint64_t>((uint64_t(key.npages) + kWarpsPerCta - 1) / kWarpsPerCta,
+    const uint64_t ctas = std::min<uint64_t>((uint64_t(scan_probe_units(key.npages)) + kWarpsPerCta - 1) / kWarpsPerCta,
                                              uint64_t(num_sms) * per_sm);
     k_scan_probe<<<unsigned(ctas), kCtaThreads, bloom_bytes, st>>>(a);
     return 1;

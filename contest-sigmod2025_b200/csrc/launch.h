@@ -141,7 +141,7 @@ int probe_chain_unique(const Items& in, const ProbeChain& chain, ItemsOut out, u
 // Source of one value slot: a column of the scanned input read at the item's
 // row, or payload slot `slot` of the entry matched by probe `probe`.
 struct SlotSource {
-    int32_t kind;  // 0: column, 1: probe payload
+    int32_t kind;  // 0: column, 1: probe payload, 2: key of the entry matched by probe `probe`
     int32_t probe;
     int32_t slot;
     int32_t pad;
@@ -170,6 +170,10 @@ __device__ __forceinline__ bool slot_value(const SlotSource& s, const Items& in,
                                            const ProbeSet& ps, uint64_t& v) {
     if (s.kind == 0) return col_get(s.col, row, v);
     const uint32_t e = in.ents[s.probe][i];
+    if (s.kind == 2) {
+        v = ps.ht[s.probe].keys[e];
+        return true;
+    }
     const HTView& ht = ps.ht[s.probe];
     if ((ht.pnull[e] >> s.slot) & 1) return false;
     v = ht.pay[size_t(e) * ht.width + s.slot];
