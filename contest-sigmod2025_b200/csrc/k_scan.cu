@@ -22,12 +22,12 @@
 //    each (units split a page's rows the same way);
 //  * the hash table's bloom filter (up to 128 KiB) is staged once per CTA in
 //    shared memory; one CTA of 32 warps runs per SM;
-//  * survivors (bloom hits, or every non-null row when the probe is not
-//    selective) are recorded as (key, row) in a per-warp buffer in shared
-//    memory (the key read again from the page just loaded, a cache hit); the
-//    buffer is probed 128 entries at a time, four independent bucket lookups
-//    per lane, so the latency of the probes is paid once per batch instead
-//    of once per hit;
+//  * bloom survivors are recorded as (key, row) in a per-warp buffer in
+//    shared memory (the key read again from the page just loaded, a cache
+//    hit); the buffer is probed 128 entries at a time, four independent
+//    bucket lookups per lane, so the latency of the probes is paid once per
+//    batch instead of once per hit. Without a bloom filter (a probe that is
+//    not selective) every lane probes its own rows directly, four at a time;
 //  * matches become items (row, entry, mult). With unique build keys a row
 //    has at most one match: items are appended with one atomicAdd per batch
 //    and the buffer carries over from unit to unit (mode 2). Otherwise a
@@ -98,20 +98,17 @@ struct WarpState {
     uint32_t page_cnt;  // matches counted / written for the current unit (modes 0 and 1)
 };
 
-// Probes every buffered candidate; counts (mode 0) or writes items. In modes
-// 0 and 1 every entry belongs to work unit `unit` (half a page).
-__device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t unit) {
-    if (w.n == 0) return;
-    __syncwarp();
+// Probes up to kPerLane candidates per lane (candidate i present when bit i
+// of `has` is set) and counts (mode 0) or writes their matches. In modes 0
+// and 1 every candidate belongs to work unit `unit`.
+__device__ __forceinline__ void probe_batch(const ScanArgs& a, WarpState& w, const uint32_t (&key)[kPerLane],
+                                            const uint32_t (&row)[kPerLane], uint32_t has, uint32_t unit) {
     const uint32_t lane = lane_id();
-    uint32_t key[kPerLane], row[kPerLane], lo[kPerLane], hi[kPerLane];
+    uint32_t lo[kPerLane], hi[kPerLane];
 #pragma unroll
     for (int i = 0; i < kPerLane; i++) {
-        const uint32_t h = lane + 32 * i;
-        key[i] = row[i] = lo[i] = hi[i] = 0;
-        if (h < w.n) {
-            key[i] = w.bkey[h];
-            row[i] = w.brow[h];
+        lo[i] = hi[i] = 0;
+        if ((has >> i) & 1) {
             const uint32_t b = uint32_t(key_hash(key[i]) >> a.ht.shift);
             lo[i] = a.ht.bucket_off[b];
             hi[i] = a.ht.bucket_off[b + 1];
@@ -171,8 +168,50 @@ __device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t 
         }
     }
     w.page_cnt += total;
+}
+
+// Probes every buffered candidate.
+__device__ __forceinline__ void flush(const ScanArgs& a, WarpState& w, uint32_t unit) {
+    if (w.n == 0) return;
+    __syncwarp();
+    const uint32_t lane = lane_id();
+    uint32_t key[kPerLane], row[kPerLane], has = 0;
+#pragma unroll
+    for (int i = 0; i < kPerLane; i++) {
+        const uint32_t h = lane + 32 * i;
+        key[i] = row[i] = 0;
+        if (h < w.n) {
+            key[i] = w.bkey[h];
+            row[i] = w.brow[h];
+            has |= 1u << i;
+        }
+    }
+    probe_batch(a, w, key, row, has, unit);
     w.n = 0;
     __syncwarp();
+}
+
+// Probes the candidates flagged in `take` (up to 32 per lane) directly, every
+// lane taking kPerLane of its own per round: for dense candidates (no bloom
+// filter) this keeps all lanes busy, where buffering would fill the buffer
+// from a few lanes at a time. map(c, key, row) gives candidate c.
+template <typename Map>
+__device__ __forceinline__ void probe_bits(const ScanArgs& a, WarpState& w, uint32_t take, uint32_t unit, Map&& map) {
+    uint32_t t = take;
+    while (__any_sync(0xffffffffu, t != 0)) {
+        uint32_t key[kPerLane], row[kPerLane], has = 0;
+#pragma unroll
+        for (int i = 0; i < kPerLane; i++) {
+            key[i] = row[i] = 0;
+            if (t) {
+                const uint32_t c = __ffs(t) - 1;
+                t &= t - 1;
+                map(c, key[i], row[i]);
+                has |= 1u << i;
+            }
+        }
+        probe_batch(a, w, key, row, has, unit);
+    }
 }
 
 // Buffers the candidates flagged in `take` (up to 32 per lane): map(c, key,
@@ -213,12 +252,16 @@ __device__ __forceinline__ void push_bits(const ScanArgs& a, WarpState& w, uint3
 // vi0 + 128 (c / 4) + c % 4 of the page of unit p (values at vals, first row
 // row0); the key is read again from the page, which this warp has just loaded.
 __device__ __forceinline__ void push_step(const ScanArgs& a, WarpState& w, uint32_t take, int vi0,
-                                          const uint32_t* vals, uint32_t row0, uint32_t p) {
-    push_bits(a, w, take, p, [&](uint32_t c, uint32_t& key, uint32_t& row) {
+                                          const uint32_t* vals, uint32_t row0, uint32_t p, bool dense) {
+    auto cand = [&](uint32_t c, uint32_t& key, uint32_t& row) {
         const uint32_t vi = uint32_t(vi0 + 128 * int(c >> 2) + int(c & 3));
         key = __ldg(vals + vi);
         row = row0 + vi;
-    });
+    };
+    if (dense)
+        probe_bits(a, w, take, p, cand);
+    else
+        push_bits(a, w, take, p, cand);
 }
 
 __device__ __forceinline__ bool bloom_pass(const ScanArgs& a, const uint32_t* bloom, uint32_t key) {
@@ -307,10 +350,14 @@ __device__ __forceinline__ void scan_rows_nulls(const ScanArgs& a, WarpState& w,
                 d++;
             }
         }
-        push_bits(a, w, take, unit, [&](uint32_t c, uint32_t& key, uint32_t& row) {
+        auto cand = [&](uint32_t c, uint32_t& key, uint32_t& row) {
             key = __ldg(vals + d0 + __popc(wb & ((1u << c) - 1)));
             row = row0 + r + c;
-        });
+        };
+        if (use_bloom)
+            push_bits(a, w, take, unit, cand);
+        else
+            probe_bits(a, w, take, unit, cand);
     }
 }
 
@@ -368,7 +415,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
         if (nn == n) {
             const int vi0 = 4 * int(lane) - 1 + int(part * 4 * kWordsPerStep);
             if (vi0 - int(lane) * 4 < int(n))  // some value of the unit is below n
-                push_step(a, w, step_take(a, q, bloom, use_bloom) & step_valid(vi0, n), vi0, vals, row0, u);
+                push_step(a, w, step_take(a, q, bloom, use_bloom) & step_valid(vi0, n), vi0, vals, row0, u,
+                          !use_bloom);
         } else {
             // A page with NULLs: unit k takes rows [1024 k, 1024 (k + 1)), the
             // last unit every row from there on.
