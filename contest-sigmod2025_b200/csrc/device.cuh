@@ -16,6 +16,8 @@
 
 #include <cstdint>
 
+#include <vector_types.h>
+
 #if defined(__CUDACC__)
 #define BJ_HD __host__ __device__ __forceinline__
 #else
@@ -203,7 +205,10 @@ inline uint32_t key_hash_hi(uint32_t key) { return uint32_t(key_hash(key) >> 32)
 // entry, engine/op/Hashtable.cpp:236-248), `width` 64-bit payload slots per
 // entry with a NULL mask.
 struct HTView {
-    const uint32_t* bucket_off;  // nbuckets + 1
+    // nbuckets + 1: x = position of the bucket's first entry (the last x is
+    // the entry count), y = that entry's key when the bucket is not empty,
+    // so one 8-byte load answers a probe of a bucket with a single key.
+    const uint2* buckets;
     const uint32_t* keys;        // nentries
     const uint64_t* mult;        // nentries
     const uint64_t* pay;         // nentries * width

@@ -969,10 +969,13 @@ class Executor {
         void* scan_status = zb_scan ? z : nullptr;
 
         launched(emit_aggregate(ba, st_));
-        uint32_t* off = alloc<uint32_t>(nb + 1);
-        launched(scan_exclusive_u32_zeroed(ba.counts, off, nb, scan_status, ctx_->d_err, st_));
+        // Bucket offsets go into the x words of the interleaved bucket array;
+        // the scatter fills each non-empty bucket's y (its first key).
+        uint2* buckets = alloc<uint2>(nb + 1);
+        launched(scan_exclusive_u32_zeroed(ba.counts, reinterpret_cast<uint32_t*>(buckets), nb, scan_status,
+                                           ctx_->d_err, st_, 2));
         HTView ht{};
-        ht.bucket_off = off;
+        ht.buckets = buckets;
         ht.keys = alloc<uint32_t>(nrep);
         ht.mult = alloc<uint64_t>(nrep);
         ht.pay = alloc<uint64_t>(size_t(nrep) * std::max<uint32_t>(width, 1));
@@ -980,7 +983,7 @@ class Executor {
         ht.shift = ba.shift;
         ht.nentries = nrep;
         ht.width = width;
-        launched(scatter_bloom(tb, ba.is_rep, ba.shift, off, cursor, ht, bloom, wlog2, ctx_->d_err, st_));
+        launched(scatter_bloom(tb, ba.is_rep, ba.shift, buckets, cursor, ht, bloom, wlog2, ctx_->d_err, st_));
         ht.bloom = bloom;
         ht.bloom_log2 = wlog2;
         hts_[pi].view = ht;

@@ -98,19 +98,21 @@ __global__ void __launch_bounds__(256) k_emit_aggregate(BuildArgs a) {
 }
 
 __global__ void k_scatter_bloom(TupleBuf t, const uint32_t* __restrict__ is_rep, uint32_t shift,
-                                const uint32_t* __restrict__ bucket_off, uint32_t* __restrict__ cursor, HTView ht,
+                                uint2* __restrict__ buckets, uint32_t* __restrict__ cursor, HTView ht,
                                 uint32_t* __restrict__ bloom, uint32_t log2w, uint32_t* __restrict__ err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= t.count || !is_rep[i]) return;
     const uint32_t key = t.keys[i];
     const uint32_t b = uint32_t(key_hash(key) >> shift);
-    const uint32_t pos = bucket_off[b] + atomicAdd(&cursor[b], 1u);
+    const uint32_t first = buckets[b].x;
+    const uint32_t pos = first + atomicAdd(&cursor[b], 1u);
     const uint32_t hh = key_hash_hi(key);
     atomicOr(&bloom[bloom_word_hi(hh, log2w)], bloom_bits_fast(hh, hh >> 5));
-    if (pos >= bucket_off[b + 1] || pos >= ht.nentries) {
+    if (pos >= buckets[b + 1].x || pos >= ht.nentries) {
         record_error(err, kErrCapacity);
         return;
     }
+    if (pos == first) buckets[b].y = key;  // the bucket's first entry
     const_cast<uint32_t*>(ht.keys)[pos] = key;
     const_cast<uint64_t*>(ht.mult)[pos] = t.mult[i];
     const_cast<uint32_t*>(ht.pnull)[pos] = t.pnull[i];
@@ -120,12 +122,12 @@ __global__ void k_scatter_bloom(TupleBuf t, const uint32_t* __restrict__ is_rep,
 }
 
 __global__ void k_ht_flags(HTView ht, uint32_t nbuckets, uint32_t* __restrict__ flags) {
-    const uint32_t n = ht.bucket_off[nbuckets];  // entries actually stored
+    const uint32_t n = ht.buckets[nbuckets].x;  // entries actually stored
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         if (ht.mult[e] > 1) flags[1] = 1;
         uint32_t key = ht.keys[e];
         uint32_t b = uint32_t(key_hash(key) >> ht.shift);
-        uint32_t s = ht.bucket_off[b];
+        uint32_t s = ht.buckets[b].x;
         if (e - s > 256) {
             flags[0] = 1;  // long bucket: assume repeats (only steers capacity choices)
             continue;
@@ -149,7 +151,7 @@ __global__ void k_sample_probes(SampleSet set, uint32_t nsample, uint32_t* hits)
     if (!col_get(sp.key, row, v)) return;
     const uint32_t k = uint32_t(v);
     const uint32_t b = uint32_t(key_hash(k) >> sp.ht.shift);
-    for (uint32_t j = sp.ht.bucket_off[b]; j < sp.ht.bucket_off[b + 1]; j++)
+    for (uint32_t j = sp.ht.buckets[b].x; j < sp.ht.buckets[b + 1].x; j++)
         if (sp.ht.keys[j] == k) {
             atomicAdd(hits + blockIdx.y, 1u);
             return;
@@ -164,10 +166,10 @@ int emit_aggregate(const BuildArgs& a, cudaStream_t st) {
     return 1;
 }
 
-int scatter_bloom(TupleBuf t, const uint32_t* is_rep, uint32_t shift, const uint32_t* bucket_off, uint32_t* cursor,
+int scatter_bloom(TupleBuf t, const uint32_t* is_rep, uint32_t shift, uint2* buckets, uint32_t* cursor,
                   HTView ht_mut, uint32_t* bloom, uint32_t log2w, uint32_t* err, cudaStream_t st) {
     if (!t.count) return 0;
-    k_scatter_bloom<<<(t.count + 255) / 256, 256, 0, st>>>(t, is_rep, shift, bucket_off, cursor, ht_mut, bloom, log2w,
+    k_scatter_bloom<<<(t.count + 255) / 256, 256, 0, st>>>(t, is_rep, shift, buckets, cursor, ht_mut, bloom, log2w,
                                                            err);
     return 1;
 }

@@ -29,9 +29,14 @@ __device__ __forceinline__ uint32_t for_matches(const HTView& ht, uint32_t key, 
     if (use_bloom && ht.bloom && !bloom_may_contain(ht.bloom, ht.bloom_log2, key)) return 0;
     uint64_t h = key_hash(key);
     uint32_t b = uint32_t(h >> ht.shift);
-    uint32_t s = ht.bucket_off[b], e = ht.bucket_off[b + 1];
+    const uint2 b0 = ht.buckets[b];
+    const uint32_t e = ht.buckets[b + 1].x;
     uint32_t n = 0;
-    for (uint32_t j = s; j < e; j++) {
+    if (b0.x < e && b0.y == key) {
+        fn(b0.x);
+        n++;
+    }
+    for (uint32_t j = b0.x + 1; j < e; j++) {
         if (ht.keys[j] == key) {
             fn(j);
             n++;

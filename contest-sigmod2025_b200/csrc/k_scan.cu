@@ -104,21 +104,24 @@ struct WarpState {
 __device__ __forceinline__ void probe_batch(const ScanArgs& a, WarpState& w, const uint32_t (&key)[kPerLane],
                                             const uint32_t (&row)[kPerLane], uint32_t has, uint32_t unit) {
     const uint32_t lane = lane_id();
-    uint32_t lo[kPerLane], hi[kPerLane];
+    // One load per candidate gives its bucket's range and first key; only
+    // buckets with more entries (few: about one key per bucket) loop.
+    uint32_t lo[kPerLane], hi[kPerLane], k0[kPerLane];
 #pragma unroll
     for (int i = 0; i < kPerLane; i++) {
         lo[i] = hi[i] = 0;
+        k0[i] = ~key[i];
         if ((has >> i) & 1) {
             const uint32_t b = uint32_t(key_hash(key[i]) >> a.ht.shift);
-            lo[i] = a.ht.bucket_off[b];
-            hi[i] = a.ht.bucket_off[b + 1];
+            const uint2 b0 = a.ht.buckets[b];
+            lo[i] = b0.x;
+            hi[i] = a.ht.buckets[b + 1].x;
+            k0[i] = b0.y;
         }
     }
-    // The first entry of every bucket is loaded for all candidates at once;
-    // only buckets with more entries (few: about one key per bucket) loop.
-    uint32_t k0[kPerLane];
 #pragma unroll
-    for (int i = 0; i < kPerLane; i++) k0[i] = lo[i] < hi[i] ? a.ht.keys[lo[i]] : ~key[i];
+    for (int i = 0; i < kPerLane; i++)
+        if (lo[i] >= hi[i]) k0[i] = ~key[i];
     uint32_t cnt = 0;
     uint32_t cj[kPerLane];
 #pragma unroll

@@ -63,7 +63,8 @@ __device__ __forceinline__ unsigned long long ld_status(const unsigned long long
 // One tile of a single-pass scan (the calling CTA takes its tile by ticket).
 template <typename T>
 __device__ __forceinline__ void scan_tile_lookback(const T* __restrict__ in, T* __restrict__ out, size_t n,
-                                                   unsigned long long* status, uint32_t* ticket, uint32_t* err) {
+                                                   unsigned long long* status, uint32_t* ticket, uint32_t* err,
+                                                   uint32_t ostride = 1) {
     __shared__ uint32_t s_tile;
     __shared__ T s_prefix;
     if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
@@ -127,9 +128,9 @@ __device__ __forceinline__ void scan_tile_lookback(const T* __restrict__ in, T* 
 #pragma unroll
     for (int k = 0; k < kScanPer; k++) {
         if (base + k < n) {
-            out[base + k] = run;
+            out[(base + k) * ostride] = run;
             run += v[k];
-            if (base + k == n - 1) out[n] = run;
+            if (base + k == n - 1) out[n * ostride] = run;
         }
     }
 }
@@ -137,8 +138,8 @@ __device__ __forceinline__ void scan_tile_lookback(const T* __restrict__ in, T* 
 template <typename T>
 __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const T* __restrict__ in, T* __restrict__ out,
                                                                 size_t n, unsigned long long* status,
-                                                                uint32_t* ticket, uint32_t* err) {
-    scan_tile_lookback<T>(in, out, n, status, ticket, err);
+                                                                uint32_t* ticket, uint32_t* err, uint32_t ostride) {
+    scan_tile_lookback<T>(in, out, n, status, ticket, err, ostride);
 }
 
 // Independent scans of several u32 arrays (blockIdx.y = array); array k's
@@ -157,8 +158,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_segs(ScanSegs segs, unsig
                                  err);
 }
 
+// Output i goes to out[i * ostride].
 template <typename T>
-__global__ void k_tile_scan(const T* __restrict__ in, T* __restrict__ out, size_t n, const T* __restrict__ base_ex) {
+__global__ void k_tile_scan(const T* __restrict__ in, T* __restrict__ out, size_t n, const T* __restrict__ base_ex,
+                            uint32_t ostride = 1) {
     size_t base = size_t(blockIdx.x) * kScanTile + size_t(threadIdx.x) * kScanPer;
     T v[kScanPer];
     T local = 0;
@@ -172,9 +175,9 @@ __global__ void k_tile_scan(const T* __restrict__ in, T* __restrict__ out, size_
 #pragma unroll
     for (int k = 0; k < kScanPer; k++) {
         if (base + k < n) {
-            out[base + k] = run;
+            out[(base + k) * ostride] = run;
             run += v[k];
-            if (base + k == n - 1) out[n] = run;
+            if (base + k == n - 1) out[n * ostride] = run;
         }
     }
 }
@@ -214,20 +217,21 @@ size_t status_bytes(size_t n) {
 }
 
 // status: status_bytes(n) zero bytes (null when that is 0).
+// Output i goes to out[i * ostride].
 template <typename T>
-int scan_launch(const T* in, T* out, size_t n, void* status, uint32_t* err, cudaStream_t st) {
+int scan_launch(const T* in, T* out, size_t n, void* status, uint32_t* err, cudaStream_t st, uint32_t ostride = 1) {
     if (n == 0) {
         k_zero_one<T><<<1, 1, 0, st>>>(out);
         return 1;
     }
     const size_t nt = (n + kScanTile - 1) / kScanTile;
     if (nt == 1) {
-        k_tile_scan<T><<<1, kScanThreads, 0, st>>>(in, out, n, nullptr);
+        k_tile_scan<T><<<1, kScanThreads, 0, st>>>(in, out, n, nullptr, ostride);
         return 1;
     }
     auto* words = static_cast<unsigned long long*>(status);
     k_scan_lookback<T><<<unsigned(nt), kScanThreads, 0, st>>>(in, out, n, words, reinterpret_cast<uint32_t*>(words + nt),
-                                                              err);
+                                                              err, ostride);
     return 1;
 }
 
@@ -296,8 +300,8 @@ int gather_values(const GatherList& g, uint64_t* dst, cudaStream_t st) {
     return 1;
 }
 int scan_exclusive_u32_zeroed(const uint32_t* in, uint32_t* out, size_t n, void* status, uint32_t* err,
-                              cudaStream_t st) {
-    return scan_launch<uint32_t>(in, out, n, status, err, st);
+                              cudaStream_t st, uint32_t out_stride) {
+    return scan_launch<uint32_t>(in, out, n, status, err, st, out_stride);
 }
 int fill_u32(uint32_t* p, uint32_t v, size_t n, cudaStream_t st) {
     if (!n) return 0;

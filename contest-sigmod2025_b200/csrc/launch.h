@@ -26,9 +26,10 @@ int scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, Scratch& s, 
 int scan_exclusive_u64(const uint64_t* in, uint64_t* out, size_t n, Scratch& s, cudaStream_t st);
 // The same scan with its tile status words supplied: scan_status_bytes(n)
 // bytes (possibly 0) that the caller has zeroed, so no memset is issued.
+// Output i goes to out[i * out_stride].
 size_t scan_status_bytes(size_t n);
 int scan_exclusive_u32_zeroed(const uint32_t* in, uint32_t* out, size_t n, void* status, uint32_t* err,
-                              cudaStream_t st);
+                              cudaStream_t st, uint32_t out_stride = 1);
 // Independent exclusive scans of up to kMaxScanSegs u32 arrays of any
 // lengths, in one launch (status_off is filled in by the wrapper).
 constexpr int kMaxScanSegs = 64;
@@ -237,11 +238,11 @@ struct BuildArgs {
 int emit_aggregate(const BuildArgs& a, cudaStream_t st);
 // Scatters the representatives into their buckets' ranges (cursor: one zero
 // word per bucket) and sets their bloom bits (bloom: zero, 1 << log2w words).
-int scatter_bloom(TupleBuf t, const uint32_t* is_rep, uint32_t shift, const uint32_t* bucket_off, uint32_t* cursor,
+int scatter_bloom(TupleBuf t, const uint32_t* is_rep, uint32_t shift, uint2* buckets, uint32_t* cursor,
                   HTView ht_mut, uint32_t* bloom, uint32_t log2w, uint32_t* err, cudaStream_t st);
 // Flags of a built table: [0] = 1 if some key repeats, [1] = 1 if some mult > 1
 // (both words must be zero before). The entry count is read on the device
-// from bucket_off[nbuckets].
+// from buckets[nbuckets].x.
 int ht_flags(HTView ht, uint32_t nbuckets, uint32_t* flags, int num_sms, cudaStream_t st);
 // Counts, for nsample evenly spaced rows of each probe's key column, how many
 // hit its table: hits[p] for probe p, all probes in one launch (the role of
