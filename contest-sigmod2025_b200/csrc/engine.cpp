@@ -1007,15 +1007,25 @@ class Executor {
             N = scan_total_u64(mult, off, n);
         }
         res.rows = N;
+        const size_t ncol = ex_.out_slot.size();
+        // When every item is one output row, fixed-width columns are written
+        // straight from the items; only the slots VARCHAR columns use (their
+        // lengths are needed first) go through flat arrays.
+        const bool direct = items.mult == nullptr;
+        std::vector<uint8_t> flat(src.n, direct ? 0 : 1);
+        for (size_t c = 0; c < ncol; c++)
+            if (ex_.out_types[c] == BJ_VARCHAR) flat[ex_.out_slot[c]] = 1;
         FlatOut fo{};
         fo.n = src.n;
+        bool any_flat = false;
         for (int j = 0; j < src.n; j++) {
+            if (!flat[j]) continue;
             fo.vals[j] = alloc<uint64_t>(N);
             fo.valid[j] = alloc<uint8_t>(N);
+            any_flat = true;
         }
-        launched(emit_output(items, off, src, probes.data(), fo, ctx_->d_err, st_));
+        if (any_flat) launched(emit_output(items, off, src, probes.data(), fo, ctx_->d_err, st_));
         // Page counts per result column.
-        const size_t ncol = ex_.out_slot.size();
         res.npages.assign(ncol, 0);
         struct StrPlan {
             uint32_t* lens = nullptr;
@@ -1134,6 +1144,8 @@ class Executor {
             const size_t c1 = std::min(ncol, c0 + kMaxOut);
             OutColumns oc{};
             oc.nrows = N;
+            oc.items = items;
+            oc.ps = make_probe_set(probes.data(), items.nprobes);
             for (size_t c = c0; c < c1; c++) {
                 const int32_t t = ex_.out_types[c];
                 const uint32_t j = ex_.out_slot[c];
@@ -1145,6 +1157,10 @@ class Executor {
                 o.npages = uint32_t(res.npages[c]);
                 if (t != BJ_VARCHAR) {
                     o.rpp = uint32_t(full_page_rows(t == BJ_INT32 ? 4 : 8));
+                    if (!flat[j]) {
+                        o.direct = 1;
+                        o.slot = src.s[j];
+                    }
                 } else {
                     o.floor = sp[c].floor ? 1u : 0u;
                     o.lens = sp[c].lens;

@@ -64,35 +64,38 @@ __device__ __forceinline__ void store_page(const uint8_t* page, uint8_t* dst) {
 }
 
 // Page pidx of a fixed-width column, by one CTA of 256 threads; each thread
-// owns 8 consecutive rows.
-__device__ __forceinline__ void write_fixed_page(const uint64_t* __restrict__ vals, const uint8_t* __restrict__ valid,
-                                                 uint64_t n, int32_t type, uint32_t rpp, uint32_t pidx,
+// owns 8 consecutive rows. get(o, v) gives output row o's value (false: NULL).
+template <typename Get>
+__device__ __forceinline__ void write_fixed_page(Get&& get, uint64_t n, int32_t type, uint32_t rpp, uint32_t pidx,
                                                  uint8_t* page, uint8_t* __restrict__ dst) {
     __shared__ uint32_t total;
-    uint64_t r0 = uint64_t(pidx) * rpp;
-    uint32_t nr = uint32_t(n - r0 < rpp ? n - r0 : rpp);
+    const uint64_t r0 = uint64_t(pidx) * rpp;
+    const uint32_t nr = uint32_t(n - r0 < rpp ? n - r0 : rpp);
     zero_smem_page(page);
-    uint32_t t = threadIdx.x;
-    uint32_t lo = t * 8, hi = min(nr, lo + 8);
+    const uint32_t t = threadIdx.x;
+    const uint32_t lo = t * 8;
+    uint64_t v8[8];
     uint32_t bits = 0, cnt = 0;
-    for (uint32_t i = lo; i < hi; i++)
-        if (valid[r0 + i]) {
-            bits |= 1u << (i - lo);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        v8[k] = 0;
+        if (lo + k < nr && get(r0 + lo + k, v8[k])) {
+            bits |= 1u << k;
             cnt++;
         }
+    }
     uint32_t dense = block_excl_u32(cnt, &total);
-    uint32_t w = type == kInt32 ? 4 : 8;
     uint8_t* data = page + (type == kInt32 ? 4 : 8);
-    for (uint32_t i = lo; i < hi; i++) {
-        if (!((bits >> (i - lo)) & 1)) continue;
-        uint64_t v = vals[r0 + i];
-        if (w == 4)
-            *reinterpret_cast<uint32_t*>(data + 4 * dense) = uint32_t(v);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        if (!((bits >> k) & 1)) continue;
+        if (type == kInt32)
+            *reinterpret_cast<uint32_t*>(data + 4 * dense) = uint32_t(v8[k]);
         else
-            *reinterpret_cast<uint64_t*>(data + 8 * dense) = v;
+            *reinterpret_cast<uint64_t*>(data + 8 * dense) = v8[k];
         dense++;
     }
-    uint32_t nbytes = (nr + 7) / 8;
+    const uint32_t nbytes = (nr + 7) / 8;
     if (lo < nr) page[kPageSize - nbytes + t] = uint8_t(bits);
     if (t == 0) {
         *reinterpret_cast<uint16_t*>(page) = uint16_t(nr);
@@ -301,7 +304,23 @@ __global__ void __launch_bounds__(256) k_write_pages(OutColumns cols, uint8_t* _
     const uint32_t p = g - oc.page_base;
     uint8_t* dst = out + size_t(g) * kPageSize;
     if (oc.type != kVarchar) {
-        write_fixed_page(oc.vals, oc.valid, cols.nrows, oc.type, oc.rpp, p, page, dst);
+        if (oc.direct) {
+            // Values straight from the items (every item is one output row).
+            write_fixed_page(
+                [&](uint64_t o, uint64_t& v) {
+                    const uint32_t i = uint32_t(o);
+                    return slot_value(oc.slot, cols.items, i, item_row(cols.items, i), cols.ps, v);
+                },
+                cols.nrows, oc.type, oc.rpp, p, page, dst);
+        } else {
+            write_fixed_page(
+                [&](uint64_t o, uint64_t& v) {
+                    if (!oc.valid[o]) return false;
+                    v = oc.vals[o];
+                    return true;
+                },
+                cols.nrows, oc.type, oc.rpp, p, page, dst);
+        }
         return;
     }
     StrPageDesc d = oc.descs[p];

@@ -190,6 +190,7 @@ __global__ void __launch_bounds__(256) k_emit_output(Items in, const uint64_t* o
     // Without offsets every item is one output row.
     uint64_t o0 = out_off ? out_off[i] : i, o1 = out_off ? out_off[i + 1] : i + 1;
     for (int j = 0; j < src.n; j++) {
+        if (!out.vals[j]) continue;  // a slot the page writer reads from the items
         uint64_t v = 0;
         bool ok = slot_value(src.s[j], in, i, row, ps, v);
         for (uint64_t o = o0; o < o1; o++) {

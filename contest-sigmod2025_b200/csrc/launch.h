@@ -296,11 +296,15 @@ struct FloorCols {
 };
 int string_floor_first(const FloorCols& cols, uint64_t n, cudaStream_t st);
 // Every page of the result in one launch: column k owns output pages
-// [page_base, page_base + npages). Fixed width: rpp rows per page. VARCHAR:
-// pages from descs (floor: first rows only, row counts from the next page).
+// [page_base, page_base + npages). Fixed width: rpp rows per page, values from
+// vals/valid, or (direct) read from the items when each item is one output
+// row. VARCHAR: pages from descs (floor: first rows only, row counts from the
+// next page).
 struct OutColumn {
     int32_t type;
     uint32_t floor;
+    uint32_t direct;            // fixed width: values from `slot` of the items, not vals/valid
+    SlotSource slot;
     const uint64_t* vals;       // values, or string handles into src
     const uint8_t* valid;
     const uint32_t* lens;       // VARCHAR
@@ -314,6 +318,8 @@ struct OutColumns {
     OutColumn c[kMaxOut];
     int n;
     uint64_t nrows;
+    Items items;  // direct columns: item o is output row o
+    ProbeSet ps;
 };
 int write_pages(const OutColumns& cols, uint32_t total_pages, uint8_t* out_pages, uint32_t* err, cudaStream_t st);
 
