@@ -939,17 +939,23 @@ class Executor {
         // 2^max(bit_width(n), 4) (engine/op/Hashtable.cpp:94-104), sized by the
         // tuple count n, an upper bound of the distinct tuples, so the build
         // needs no host round trip. Bloom filter: about 16 bits per key, at
-        // most 128 KiB (shared-memory staging).
+        // most 128 KiB (shared-memory staging); none when that leaves fewer
+        // than 8 bits per key (over 131,072 tuples), where it would pass
+        // most keys and its build would be contended atomics for nothing.
         ba.tlog2 = std::max<uint32_t>(1, bit_width(uint64_t(n) * 2));
         const uint32_t nrep = n;
         const uint32_t blog2 = std::max<uint32_t>(bit_width(nrep), 4);
         ba.shift = 64 - blog2;
         const size_t nb = size_t(1) << blog2;
+        const bool with_bloom = uint64_t(nrep) * 8 <= (uint64_t(32) << kBloomMaxLog2);
         const uint32_t wlog2 =
-            std::min<uint32_t>(kBloomMaxLog2, std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1)));
+            with_bloom
+                ? std::min<uint32_t>(kBloomMaxLog2, std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1)))
+                : 0;
         // Everything that must start at zero, cleared by one memset.
         const size_t zb_table = sizeof(uint32_t) << ba.tlog2, zb_counts = sizeof(uint32_t) * nb,
-                     zb_cursor = sizeof(uint32_t) * nb, zb_bloom = sizeof(uint32_t) << wlog2, zb_flags = 256,
+                     zb_cursor = sizeof(uint32_t) * nb, zb_bloom = with_bloom ? sizeof(uint32_t) << wlog2 : 0,
+                     zb_flags = 256,
                      zb_scan = scan_status_bytes(nb);
         auto round = [](size_t x) { return (x + 255) & ~size_t(255); };
         const size_t zbytes = round(zb_table) + round(zb_counts) + round(zb_cursor) + round(zb_bloom) + zb_flags +
@@ -983,8 +989,9 @@ class Executor {
         ht.shift = ba.shift;
         ht.nentries = nrep;
         ht.width = width;
-        launched(scatter_bloom(tb, ba.is_rep, ba.shift, buckets, cursor, ht, bloom, wlog2, ctx_->d_err, st_));
-        ht.bloom = bloom;
+        launched(scatter_bloom(tb, ba.is_rep, ba.shift, buckets, cursor, ht, with_bloom ? bloom : nullptr, wlog2,
+                               ctx_->d_err, st_));
+        ht.bloom = with_bloom ? bloom : nullptr;
         ht.bloom_log2 = wlog2;
         hts_[pi].view = ht;
         hts_[pi].empty = false;

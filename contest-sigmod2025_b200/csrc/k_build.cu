@@ -107,7 +107,7 @@ __global__ void k_scatter_bloom(TupleBuf t, const uint32_t* __restrict__ is_rep,
     const uint32_t first = buckets[b].x;
     const uint32_t pos = first + atomicAdd(&cursor[b], 1u);
     const uint32_t hh = key_hash_hi(key);
-    atomicOr(&bloom[bloom_word_hi(hh, log2w)], bloom_bits_fast(hh, hh >> 5));
+    if (bloom) atomicOr(&bloom[bloom_word_hi(hh, log2w)], bloom_bits_fast(hh, hh >> 5));
     if (pos >= buckets[b + 1].x || pos >= ht.nentries) {
         record_error(err, kErrCapacity);
         return;

@@ -237,7 +237,8 @@ struct BuildArgs {
 };
 int emit_aggregate(const BuildArgs& a, cudaStream_t st);
 // Scatters the representatives into their buckets' ranges (cursor: one zero
-// word per bucket) and sets their bloom bits (bloom: zero, 1 << log2w words).
+// word per bucket) and sets their bloom bits (bloom: zero, 1 << log2w words;
+// null: no filter).
 int scatter_bloom(TupleBuf t, const uint32_t* is_rep, uint32_t shift, uint2* buckets, uint32_t* cursor,
                   HTView ht_mut, uint32_t* bloom, uint32_t log2w, uint32_t* err, cudaStream_t st);
 // Flags of a built table: [0] = 1 if some key repeats, [1] = 1 if some mult > 1
