@@ -262,6 +262,41 @@ def serve_bench(pkg, args, large):
     return out
 
 
+class Replicas:
+    """The ranks of a multi-GPU run: one process per GPU, each running whole
+    queries on its own replica of the tables (no data exchange). Timing is the
+    max over ranks of each rank's device time, and the job's queries/s counts
+    every rank's queries. `dist` is torch.distributed (None for one rank);
+    `device` holds the reduction tensor ("cuda" with NCCL, "cpu" with gloo)."""
+
+    def __init__(self, dist=None, device="cuda", sync=None):
+        self.dist, self.device, self.sync = dist, device, sync
+
+    @property
+    def world(self):
+        return self.dist.get_world_size() if self.dist else 1
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+        if self.sync:
+            self.sync()
+
+    def max_over_ranks(self, x):
+        if not self.dist:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def job_rate(self, units_per_rank, elapsed_ms):
+        """Whole-job units/s from this rank's units and time (max over ranks)."""
+        ms = self.max_over_ranks(elapsed_ms)
+        return units_per_rank * self.world / (ms / 1e3) if units_per_rank else 0.0, ms
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -281,17 +316,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
 
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    replicas = Replicas(dist, "cuda", torch.cuda.synchronize)
+    barrier, max_over_ranks = replicas.barrier, replicas.max_over_ranks
 
     w = pkg.Workload(args.workload, args.seed, args.scale)
     plan = w.plan_ptr()
@@ -343,8 +369,7 @@ def main():
     torch.cuda.synchronize()
     clk = clocks.stop()
     ctx.profile(False)
-    elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = args.steps * world / (elapsed_ms / 1e3) if args.steps else 0.0
+    value, elapsed_ms = replicas.job_rate(args.steps, ev0.elapsed_time(ev1))
     phases = {name: phase_sum[i] / max(args.steps, 1) for i, name in
               enumerate(["build_ms", "probe_order_ms", "scan_probe_stages_ms", "output_ms"])}
     if args.mode == "value":
@@ -384,12 +409,12 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
         ctx.profile(False)
-        ms = max_over_ranks(ev0.elapsed_time(ev1))
+        rate, ms = replicas.job_rate(e2e_steps, ev0.elapsed_time(ev1))
         ph = split["phases"]
         split = {"device_ms": split["device_ms"],
                  "inputs_ms": split["device_ms"] - sum(ph),
                  "build_ms": ph[0], "probe_order_ms": ph[1], "scan_probe_stages_ms": ph[2], "output_ms": ph[3]}
-        return e2e_steps * world / (ms / 1e3), stats, lat_ms, split
+        return rate, stats, lat_ms, split
 
     # (a) pages in pageable memory: gathered into pinned staging and copied.
     pageable_value, pageable_stats, pageable_lat, pageable_split = e2e_run()
