@@ -295,7 +295,23 @@ struct bj_context {
     bool zero_copy = true;  // read pinned, contiguous input columns in place
     static constexpr int kSideStreams = 4;
     cudaStream_t side[kSideStreams] = {};  // independent build pipelines run here
+    cudaStream_t copy = nullptr;           // host-to-HBM copies of a streamed scan
+    bool stream_scans = true;              // scans of host pages copy them through HBM windows
     std::vector<cudaEvent_t> pipe_events;  // one per pipeline, reused across calls
+    std::vector<cudaEvent_t> window_events;  // a streamed scan's copy and release marks
+
+    // `n` events without timing, created once and reused across calls.
+    cudaEvent_t* events(std::vector<cudaEvent_t>& v, size_t n) {
+        while (v.size() < n) {
+            cudaEvent_t e;
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+            v.push_back(e);
+        }
+        return v.data();
+    }
 
     cudaEvent_t pipe_event(size_t i) {
         while (pipe_events.size() <= i) {
@@ -312,6 +328,7 @@ struct bj_context {
         cudaStreamSynchronize(stream);
         for (cudaStream_t s : side)
             if (s) cudaStreamSynchronize(s);
+        if (copy) cudaStreamSynchronize(copy);
     }
     std::vector<cudaEvent_t> prof_events;  // pairs around timed launches
     std::vector<cudaEvent_t> phase_events; // phase marks of the call (kPhaseMarks when complete)
@@ -368,20 +385,27 @@ namespace {
 // Reads back `n` u64 slots of ctx->d_small after the stream drains; checks the
 // device error word.
 // Host-side trace of a call (B200JOIN_TRACE=1): milliseconds since the call
-// began and since the previous mark, to stderr.
-bool trace_on() {
-    static const bool on = [] {
+// began and since the previous mark, to stderr. B200JOIN_TRACE=2 drains the
+// call's stream at every mark first, so that a mark's delta is the device
+// time of the work enqueued since the previous one (and the call runs
+// serialised: for locating time, not for timing).
+int trace_level() {
+    static const int level = [] {
         const char* e = std::getenv("B200JOIN_TRACE");
-        return e && std::atoi(e) != 0;
+        return e ? std::atoi(e) : 0;
     }();
-    return on;
+    return level;
 }
+bool trace_on() { return trace_level() != 0; }
 thread_local std::chrono::steady_clock::time_point g_trace_t0, g_trace_last;
-void trace_begin() {
+thread_local cudaStream_t g_trace_stream = nullptr;
+void trace_begin(cudaStream_t st) {
+    g_trace_stream = st;
     if (trace_on()) g_trace_t0 = g_trace_last = std::chrono::steady_clock::now();
 }
 void trace(const char* what) {
     if (!trace_on()) return;
+    if (trace_level() >= 2 && g_trace_stream) cudaStreamSynchronize(g_trace_stream);
     auto now = std::chrono::steady_clock::now();
     std::fprintf(stderr, "[b200join] %8.3f ms (+%7.3f) %s\n",
                  std::chrono::duration<double, std::milli>(now - g_trace_t0).count(),
@@ -435,19 +459,17 @@ struct ColumnJob {
     uint64_t rows;         // rows the table claims
     DevColumn* out;
     bool in_place = false; // pages are read where they are (pinned host memory): no copy
+    const uint8_t* pinned = nullptr;  // pages back to back in pinned host memory: one DMA from here
 };
 
-// Device address of a column whose pages lie back to back in one pinned,
-// mapped host allocation; nullptr otherwise (pageable pages are copied).
-// Columns smaller than this are copied even from pinned memory: a copy is
-// cheap, while reading them in place would pay a host-link round trip per
-// random access.
-constexpr uint64_t kInPlaceMinPages = 2048;  // 16 MiB
-
-uint8_t* mapped_base(const bj_column& hc) {
-    if (hc.num_pages < kInPlaceMinPages || !hc.pages || !hc.pages[0]) return nullptr;
+// A column's pages when they lie back to back in pinned host memory (the
+// first and the last byte pinned, both mapped to one device range when
+// mapped): the host address, and in `dev` the device address of the mapping
+// or nullptr. Returns nullptr for pageable or scattered pages.
+const uint8_t* pinned_base(const bj_column& hc, uint8_t*& dev) {
+    dev = nullptr;
+    if (!hc.num_pages || !hc.pages || !hc.pages[0]) return nullptr;
     const uint8_t* p0 = static_cast<const uint8_t*>(hc.pages[0]);
-    if (reinterpret_cast<uintptr_t>(p0) % 16) return nullptr;  // kernels read pages with 16-byte loads
     for (uint64_t k = 1; k < hc.num_pages; k++)
         if (hc.pages[k] != p0 + k * kPageSize) return nullptr;
     cudaPointerAttributes a0{}, a1{};
@@ -456,21 +478,42 @@ uint8_t* mapped_base(const bj_column& hc) {
         cudaGetLastError();
         return nullptr;
     }
-    if (a0.type != cudaMemoryTypeHost || a1.type != cudaMemoryTypeHost || !a0.devicePointer || !a1.devicePointer)
-        return nullptr;
+    if (a0.type != cudaMemoryTypeHost || a1.type != cudaMemoryTypeHost) return nullptr;
     uint8_t* d0 = static_cast<uint8_t*>(a0.devicePointer);
-    if (static_cast<uint8_t*>(a1.devicePointer) != d0 + hc.num_pages * kPageSize - 1) return nullptr;
-    return d0;
+    if (d0 && static_cast<uint8_t*>(a1.devicePointer) == d0 + hc.num_pages * kPageSize - 1) dev = d0;
+    return p0;
+}
+
+// Columns of pinned, mapped pages at least this large are read in place
+// (their device address is `dev` of pinned_base, 16-byte aligned for the
+// kernels' 16-byte loads). Smaller ones are copied even from pinned memory:
+// a copy is cheap, while reading them in place would pay a host-link round
+// trip per random access.
+constexpr uint64_t kInPlaceMinPages = 2048;  // 16 MiB
+
+bool read_in_place(const bj_column& hc, const uint8_t* dev) {
+    return dev && hc.num_pages >= kInPlaceMinPages && reinterpret_cast<uintptr_t>(dev) % 16 == 0;
 }
 
 // Copies host pages into `dst` on the device: pages are gathered into pinned
 // staging by the thread pool, chunk by chunk, each chunk's DMA overlapping
 // the next chunk's gathering.
 uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs) {
-    uint64_t total = 0;
-    for (auto& j : jobs)
-        if (!j.in_place) total += j.src->num_pages;
-    if (!total) return 0;
+    // Pinned pages lying back to back go to the device in one DMA each,
+    // straight from where they are. (DMA out of staging that the host has
+    // just written ran at about a tenth of the link rate on a B200 host.)
+    uint64_t direct = 0, total = 0;
+    for (auto& j : jobs) {
+        if (j.in_place) continue;
+        if (j.pinned) {
+            const size_t b = j.src->num_pages * kPageSize;
+            if (b) BJ_CK(cudaMemcpyAsync(j.dpages, j.pinned, b, cudaMemcpyHostToDevice, ctx->stream));
+            direct += b;
+            continue;
+        }
+        total += j.src->num_pages;
+    }
+    if (!total) return direct;
     size_t bytes = total * kPageSize;
     if (ctx->stage.size < bytes) {
         if (ctx->stage.p) {
@@ -497,7 +540,7 @@ uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs) {
     all.reserve(total);
     for (size_t ji = 0; ji < jobs.size(); ji++) {
         const ColumnJob& j = jobs[ji];
-        if (j.in_place) continue;
+        if (j.in_place || j.pinned) continue;
         for (uint64_t p = 0; p < j.src->num_pages; p++) {
             if (!j.src->pages[p]) throw Fail{BJ_ERR_INVALID, "null page pointer"};
             all.push_back(Src{j.src->pages[p], j.dpages + p * kPageSize, ji});
@@ -523,7 +566,7 @@ uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs) {
             i = k;
         }
     }
-    return bytes;
+    return bytes + direct;
 }
 
 // Builds the page index of every job's column (pages already on the device).
@@ -550,6 +593,7 @@ void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem) 
             c.flags = flags + (i - i0);
         }
         ctx->launches += page_index_pass1(b, ctx->d_err, sc, ctx->stream);
+        trace("page index pass 1 enqueued");
         // Row totals, chunk totals, flags and the rows of page 0.
         for (size_t i = i0; i < i1; i++) {
             const PageIndexCol& c = b.c[i - i0];
@@ -685,6 +729,103 @@ class Executor {
         ctx_->prof_bytes += bytes;
     }
 
+    // A fused chain of the unique-key stages s, s + 1, ... (up to kMaxChain)
+    // over `in`: the stages, the outputs (room for in.count items) and the
+    // items it leaves, whose count is on the device.
+    struct ChainRun {
+        ProbeChain ch{};
+        ItemsOut out{};
+        uint32_t* cursor = nullptr;
+        uint32_t cap = 0;
+        size_t s2 = 0;  // first stage after the chain
+        Items result{};
+    };
+    ChainRun plan_chain(const PipelinePlan& pp, const std::vector<uint32_t>& order,
+                        const std::vector<HTView>& by_stage, const std::vector<double>& rate, size_t s,
+                        const Items& in) {
+        ChainRun r;
+        bool unit = in.mult == nullptr;
+        size_t s2 = s;
+        while (s2 < order.size() && r.ch.n < kMaxChain && hts_[pp.probes[order[s2]].child].unique) {
+            const uint32_t k2 = order[s2];
+            ChainStage& c = r.ch.st[r.ch.n++];
+            c.key = col(pp.probes[k2].probe_attr);
+            c.ht = by_stage[s2];
+            c.use_bloom = (c.ht.bloom && rate[k2] < 0.5) ? 1 : 0;
+            unit = unit && hts_[pp.probes[k2].child].unit_mult;
+            s2++;
+        }
+        r.s2 = s2;
+        r.cap = in.count;
+        r.out.rows = alloc<uint32_t>(r.cap);
+        for (size_t j = 0; j < s2; j++) r.out.ents[j] = alloc<uint32_t>(r.cap);
+        r.out.mult = unit ? nullptr : alloc<uint64_t>(r.cap);
+        r.cursor = alloc<uint32_t>(1);
+        BJ_CK(cudaMemsetAsync(r.cursor, 0, sizeof(uint32_t), st_));
+        r.result.rows = r.out.rows;
+        for (size_t j = 0; j < s2; j++) r.result.ents[j] = r.out.ents[j];
+        r.result.mult = r.out.mult;
+        r.result.count = r.cap;
+        r.result.dcount = r.cursor;
+        r.result.nprobes = int(s2);
+        return r;
+    }
+
+    // Scan-side probe (append mode) of a column whose pages are in pinned
+    // host memory: the pages cross the host link by DMA, a window of
+    // kWindowPages at a time, into a ring of kRing windows in HBM, and each
+    // window is scanned once its copy has landed while the next ones are in
+    // flight. The copy engine moves pages at the link's rate (53.6 GB/s on
+    // a B200 host against 46.5 GB/s for the kernel's own 16-byte loads of
+    // mapped memory), and the scan of a window in HBM takes a few percent of
+    // its copy, so the stage runs at about the link's rate.
+    //
+    // With `chain`, the chain runs after each window's scan over the items
+    // that window appended (from the count the previous chain launch saw to
+    // the cursor), on the main stream while the next copies are in flight.
+    void streamed_scan(const DevColumn& key, const HTView& ht, bool bloom, uint32_t* cursor, const ItemsOut& out,
+                       uint32_t cap, ChainRun* chain, const Items& scanned) {
+        constexpr uint32_t kWindowPages = 2048;  // 16 MiB
+        constexpr uint32_t kRing = 3;
+        const uint32_t nwin = (key.npages + kWindowPages - 1) / kWindowPages;
+        const uint32_t ring = std::min(kRing, nwin);
+        uint8_t* win[kRing] = {};
+        for (uint32_t r = 0; r < ring; r++) win[r] = alloc<uint8_t>(size_t(kWindowPages) * kPageSize);
+        // [0, kRing): window copied; [kRing, 2 kRing): window scanned; last: start.
+        cudaEvent_t* ev = ctx_->events(ctx_->window_events, 2 * kRing + 1);
+        if (!ev) throw Fail{BJ_ERR_CUDA, "event creation failed"};
+        cudaStream_t cp = ctx_->copy;
+        uint32_t* marks = nullptr;  // marks[i]: items appended before window i
+        if (chain) {
+            marks = alloc<uint32_t>(nwin + 1);
+            BJ_CK(cudaMemsetAsync(marks, 0, sizeof(uint32_t), st_));
+        }
+        BJ_CK(cudaEventRecord(ev[2 * kRing], st_));
+        BJ_CK(cudaStreamWaitEvent(cp, ev[2 * kRing], 0));
+        for (uint32_t i = 0; i < nwin; i++) {
+            const uint32_t p0 = i * kWindowPages, np = std::min(kWindowPages, key.npages - p0), r = i % kRing;
+            if (i >= kRing) BJ_CK(cudaStreamWaitEvent(cp, ev[kRing + r], 0));
+            // key.pages is the mapped (unified) address of the pinned pages.
+            BJ_CK(cudaMemcpyAsync(win[r], key.pages + size_t(p0) * kPageSize, size_t(np) * kPageSize,
+                                  cudaMemcpyDefault, cp));
+            BJ_CK(cudaEventRecord(ev[r], cp));
+            BJ_CK(cudaStreamWaitEvent(st_, ev[r], 0));
+            DevColumn w = key;
+            w.pages = win[r];
+            w.npages = np;
+            w.flags &= ~kColHostPages;
+            if (w.hdr) w.hdr += p0;
+            if (w.row_start) w.row_start += p0;
+            if (w.chunk_base) w.chunk_base += p0;
+            launched(scan_probe(w, ht, 2, bloom, nullptr, nullptr, cursor, out.rows, out.ents[0], out.mult, cap,
+                                ctx_->d_err, ctx_->num_sms, st_, key.rpp ? p0 * key.rpp : 0));
+            BJ_CK(cudaEventRecord(ev[kRing + r], st_));
+            if (chain)
+                launched(probe_chain_unique(scanned, chain->ch, chain->out, chain->cursor, chain->cap, ctx_->d_err,
+                                            ctx_->num_sms, st_, marks + i, marks + i + 1));
+        }
+    }
+
     // Exclusive scan of tile counts; returns the total (synchronises).
     uint32_t scan_total_u32(const uint32_t* in, uint32_t* out, size_t n) {
         launched(scan_exclusive_u32(in, out, n, A_, st_));
@@ -780,11 +921,6 @@ class Executor {
                     out.mult = bh.unit_mult ? nullptr : alloc<uint64_t>(cap);
                     uint32_t* cursor = alloc<uint32_t>(1);
                     BJ_CK(cudaMemsetAsync(cursor, 0, sizeof(uint32_t), st_));
-                    bool timed = ctx_->profile;
-                    if (timed) begin_timed();
-                    launched(scan_probe(key, ht, 2, bloom, nullptr, nullptr, cursor, out.rows, out.ents[0], out.mult,
-                                        cap, ctx_->d_err, ctx_->num_sms, st_));
-                    if (timed) end_timed(page_bytes);
                     // The next stage reads the count on the device.
                     Items next{};
                     next.rows = out.rows;
@@ -793,6 +929,31 @@ class Executor {
                     next.count = cap;
                     next.dcount = cursor;
                     next.nprobes = 1;
+                    bool timed = ctx_->profile;
+                    if (timed) begin_timed();
+                    if ((key.flags & kColHostPages) && ctx_->stream_scans && ctx_->tape_mode == 0) {
+                        // Pages in host memory stream through HBM windows; the
+                        // unique-key stages right after the scan run window by
+                        // window too, so their reads of host columns overlap
+                        // the next windows' copies.
+                        const bool fuse = s + 1 < np && hts_[pp.probes[order[s + 1]].child].unique;
+                        ChainRun chain;
+                        if (fuse) chain = plan_chain(pp, order, by_stage, rate, s + 1, next);
+                        streamed_scan(key, ht, bloom, cursor, out, cap, fuse ? &chain : nullptr, next);
+                        if (timed) end_timed(page_bytes);
+                        trace("streamed scan enqueued");
+                        if (fuse) {
+                            items = chain.result;
+                            s = chain.s2 - 1;
+                        } else {
+                            items = next;
+                        }
+                        continue;
+                    }
+                    launched(scan_probe(key, ht, 2, bloom, nullptr, nullptr, cursor, out.rows, out.ents[0], out.mult,
+                                        cap, ctx_->d_err, ctx_->num_sms, st_));
+                    if (timed) end_timed(page_bytes);
+                    trace("scan-side probe enqueued");
                     items = next;
                     continue;
                 } else {
@@ -832,35 +993,12 @@ class Executor {
             if (bh.unique) {
                 // This stage and the unique-key stages right after it run as
                 // one fused chain.
-                ProbeChain ch{};
-                bool unit = items.mult == nullptr;
-                size_t s2 = s;
-                while (s2 < np && ch.n < kMaxChain && hts_[pp.probes[order[s2]].child].unique) {
-                    const uint32_t k2 = order[s2];
-                    ChainStage& c = ch.st[ch.n++];
-                    c.key = col(pp.probes[k2].probe_attr);
-                    c.ht = by_stage[s2];
-                    c.use_bloom = (c.ht.bloom && rate[k2] < 0.5) ? 1 : 0;
-                    unit = unit && hts_[pp.probes[k2].child].unit_mult;
-                    s2++;
-                }
-                uint32_t cap = items.count;
-                ItemsOut out{};
-                out.rows = alloc<uint32_t>(cap);
-                for (size_t j = 0; j < s2; j++) out.ents[j] = alloc<uint32_t>(cap);
-                out.mult = unit ? nullptr : alloc<uint64_t>(cap);
-                uint32_t* cursor = alloc<uint32_t>(1);
-                BJ_CK(cudaMemsetAsync(cursor, 0, sizeof(uint32_t), st_));
-                launched(probe_chain_unique(items, ch, out, cursor, cap, ctx_->d_err, ctx_->num_sms, st_));
-                Items next{};
-                next.rows = out.rows;
-                for (size_t j = 0; j < s2; j++) next.ents[j] = out.ents[j];
-                next.mult = out.mult;
-                next.count = cap;
-                next.dcount = cursor;
-                next.nprobes = int(s2);
-                items = next;
-                s = s2 - 1;
+                ChainRun chain = plan_chain(pp, order, by_stage, rate, s, items);
+                launched(probe_chain_unique(items, chain.ch, chain.out, chain.cursor, chain.cap, ctx_->d_err,
+                                            ctx_->num_sms, st_));
+                trace("probe chain enqueued");
+                items = chain.result;
+                s = chain.s2 - 1;
                 continue;
             }
             resolve(items);
@@ -1278,7 +1416,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
                    bool speculate = true) {
     auto t0 = std::chrono::steady_clock::now();
     if (!ctx || !plan || !out) return BJ_ERR_INVALID;
-    trace_begin();
+    trace_begin(ctx->stream);
     *out = nullptr;
     std::unique_ptr<bj_result> res(new bj_result);
     res->ctx = ctx;
@@ -1318,7 +1456,10 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
                     if (hc.num_pages && !hc.pages) throw Fail{BJ_ERR_INVALID, "column without page array"};
                     d.cols[c].type = hc.type;
                     res->stats.input_pages += hc.num_pages;
-                    if (uint8_t* mapped = ctx->zero_copy ? mapped_base(hc) : nullptr) {
+                    uint8_t* mapped = nullptr;
+                    const uint8_t* pinned = pinned_base(hc, mapped);
+                    if (!ctx->zero_copy || !read_in_place(hc, mapped)) mapped = nullptr;
+                    if (mapped) {
                         res->stats.mapped_input_bytes += hc.num_pages * kPageSize;
                         uint32_t h0 = 0;
                         if (speculate && guess_uniform(hc, t.num_rows, h0)) {
@@ -1335,7 +1476,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
                         continue;
                     }
                     uint8_t* dp = static_cast<uint8_t*>(ctx->arena.alloc(std::max<uint64_t>(hc.num_pages, 1) * kPageSize));
-                    jobs.push_back(ColumnJob{&hc, dp, t.num_rows, &d.cols[c]});
+                    jobs.push_back(ColumnJob{&hc, dp, t.num_rows, &d.cols[c], false, pinned});
                 }
             }
             trace("plan and input columns");
@@ -1690,6 +1831,7 @@ BJ_API int bj_context_create(int device, bj_context** out) {
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return BJ_ERR_CUDA;
     for (auto& s : ctx->side)
         if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return BJ_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking) != cudaSuccess) return BJ_ERR_CUDA;
     if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) return BJ_ERR_CUDA;
     if (cudaMalloc(&ctx->d_err, 256) != cudaSuccess) return BJ_ERR_OOM;
     ctx->arena.err = ctx->d_err;
@@ -1707,6 +1849,7 @@ BJ_API int bj_context_create(int device, bj_context** out) {
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (const char* zc = std::getenv("B200JOIN_ZERO_COPY")) ctx->zero_copy = std::atoi(zc) != 0;
     if (const char* gr = std::getenv("B200JOIN_GRAPHS")) ctx->graphs = std::atoi(gr) != 0;
+    if (const char* ss = std::getenv("B200JOIN_STREAM_SCAN")) ctx->stream_scans = std::atoi(ss) != 0;
     unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     ctx->pool = std::make_unique<ThreadPool>(std::min(hw, 16u) - 1);
     *out = ctx.release();
@@ -1720,8 +1863,10 @@ BJ_API void bj_context_destroy(bj_context* ctx) {
     for (auto& g : ctx->graph_cache) destroy_graph(*g);
     ctx->graph_cache.clear();
     for (cudaEvent_t e : ctx->pipe_events) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->window_events) cudaEventDestroy(e);
     for (cudaStream_t s : ctx->side)
         if (s) cudaStreamDestroy(s);
+    if (ctx->copy) cudaStreamDestroy(ctx->copy);
     for (auto& b : ctx->pinned_free) cudaFreeHost(b.p);
     if (ctx->stage.p) cudaFreeHost(ctx->stage.p);
     if (ctx->h_small) cudaFreeHost(ctx->h_small);
@@ -1776,7 +1921,9 @@ BJ_API int bj_resident_upload(bj_context* ctx, const bj_table* table, bj_residen
                 d.cols[c].type = hc.type;
                 d.present[c] = 1;
                 uint8_t* dp = static_cast<uint8_t*>(r->mem.alloc(std::max<uint64_t>(hc.num_pages, 1) * kPageSize));
-                jobs.push_back(ColumnJob{&hc, dp, table->num_rows, &d.cols[c]});
+                uint8_t* mapped = nullptr;
+                const uint8_t* pinned = pinned_base(hc, mapped);
+                jobs.push_back(ColumnJob{&hc, dp, table->num_rows, &d.cols[c], false, pinned});
             }
         } else {
             for (uint64_t c = 0; c < table->num_columns; c++) d.present[c] = 1;

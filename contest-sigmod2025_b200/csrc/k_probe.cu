@@ -122,12 +122,15 @@ __global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HT
 // loop, at most one match per stage, warp-aggregated reservation of output
 // slots.
 __global__ void __launch_bounds__(256) k_probe_chain(Items in, ProbeChain ch, ItemsOut out, uint32_t* cursor,
-                                                     uint32_t capacity, uint32_t* err) {
+                                                     uint32_t capacity, uint32_t* err, const uint32_t* dfirst,
+                                                     uint32_t* dend) {
     const uint32_t n = in.dcount ? *in.dcount : in.count;
+    const uint32_t first = dfirst ? *dfirst : 0u;
+    if (dend && blockIdx.x == 0 && threadIdx.x == 0) *dend = n;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t lane = threadIdx.x & 31;
     // Whole warps iterate together so the ballot sees every lane.
-    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
+    for (uint32_t base = first + (blockIdx.x * blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
         const uint32_t i = base + lane;
         bool hit = i < n;
         uint32_t row = 0;
@@ -214,10 +217,10 @@ int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mod
 }
 
 int probe_chain_unique(const Items& in, const ProbeChain& chain, ItemsOut out, uint32_t* cursor, uint32_t capacity,
-                       uint32_t* err, int num_sms, cudaStream_t st) {
+                       uint32_t* err, int num_sms, cudaStream_t st, const uint32_t* dfirst, uint32_t* dend) {
     if (!in.count || chain.n <= 0) return 0;
     uint32_t blocks = std::min<uint32_t>((in.count + 255) / 256, uint32_t(num_sms) * 8);
-    k_probe_chain<<<blocks, 256, 0, st>>>(in, chain, out, cursor, capacity, err);
+    k_probe_chain<<<blocks, 256, 0, st>>>(in, chain, out, cursor, capacity, err, dfirst, dend);
     return 1;
 }
 

@@ -70,6 +70,7 @@ struct ScanArgs {
     uint64_t* out_mult;        // may be null when every entry has multiplicity 1
     uint32_t capacity;         // items the outputs can hold
     uint32_t* err;
+    uint32_t row_base;         // row of the first page when rows follow from key.rpp (a window of a column)
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
@@ -386,7 +387,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
 #pragma unroll
         for (int i = 0; i < kStepWords; i++) q[i] = __ldg(pw + (u % kUnitsPerPage) * kWordsPerStep + lane + 32 * i);
         hdr = lane == 0 ? __ldg(reinterpret_cast<const uint32_t*>(pw)) : 0;
-        row0 = lane == 0 ? (a.key.rpp ? (u / kUnitsPerPage) * a.key.rpp : __ldg(a.key.row_start + u / kUnitsPerPage))
+        row0 = lane == 0 ? (a.key.rpp ? a.row_base + (u / kUnitsPerPage) * a.key.rpp
+                                      : __ldg(a.key.row_start + u / kUnitsPerPage))
                          : 0;
     };
     uint4 q[kStepWords];
@@ -442,7 +444,7 @@ uint32_t scan_probe_units(uint32_t npages) { return kUnitsPerPage * npages; }
 
 int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem, uint32_t* page_counts,
                const uint32_t* page_off, uint32_t* cursor, uint32_t* out_rows, uint32_t* out_ents, uint64_t* out_mult,
-               uint32_t capacity, uint32_t* err, int num_sms, cudaStream_t st) {
+               uint32_t capacity, uint32_t* err, int num_sms, cudaStream_t st, uint32_t row_base) {
     if (!key.npages) return 0;
     size_t bloom_bytes = bloom_smem && ht.bloom ? (sizeof(uint32_t) << ht.bloom_log2) : 0;
     if (bloom_bytes > kBloomSmemMax) bloom_bytes = 0;
@@ -456,7 +458,7 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
     const uint32_t prefetch = (key.flags & kColHostPages) ? 0u : ahead;
     ScanArgs a{key,      ht,       uint32_t(mode), bloom_bytes ? 1u : 0u, prefetch,
                ht.bloom_log2 ? (1u << ht.bloom_log2) : 0u, 1u << 27,
-               page_counts, page_off, cursor, out_rows, out_ents, out_mult, capacity, err};
+               page_counts, page_off, cursor, out_rows, out_ents, out_mult, capacity, err, row_base};
     // Once per process (thread-safe static initialisation; server workers
     // launch from several threads).
     static const bool configured = [] {

@@ -136,8 +136,12 @@ struct ProbeChain {
     ChainStage st[kMaxChain];
     int n;
 };
+// dfirst (optional): the items start at index *dfirst instead of 0; dend
+// (optional): receives the item count read from in.dcount, so that the next
+// launch over items appended after this one can start there.
 int probe_chain_unique(const Items& in, const ProbeChain& chain, ItemsOut out, uint32_t* cursor, uint32_t capacity,
-                       uint32_t* err, int num_sms, cudaStream_t st);
+                       uint32_t* err, int num_sms, cudaStream_t st, const uint32_t* dfirst = nullptr,
+                       uint32_t* dend = nullptr);
 
 // Source of one value slot: a column of the scanned input read at the item's
 // row, or payload slot `slot` of the entry matched by probe `probe`.
@@ -202,12 +206,14 @@ int items_mult(const Items& in, uint64_t* mult_out, cudaStream_t st);
 // written at page_off[u] (exclusive scan of the counts, units + 1 entries);
 // mode 2: items appended at *cursor (requires at most one match per row).
 // bloom_smem: test ht.bloom, staged in shared memory (ignored if larger than
-// scan_probe_bloom_limit()).
+// scan_probe_bloom_limit()). `key` may be a window of a column's pages (its
+// row_start / chunk_base / hdr advanced to the window's first page): with
+// uniform pages (key.rpp) the window's first row is row_base.
 size_t scan_probe_bloom_limit();
 uint32_t scan_probe_units(uint32_t npages);
 int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem, uint32_t* page_counts,
                const uint32_t* page_off, uint32_t* cursor, uint32_t* out_rows, uint32_t* out_ents, uint64_t* out_mult,
-               uint32_t capacity, uint32_t* err, int num_sms, cudaStream_t st);
+               uint32_t capacity, uint32_t* err, int num_sms, cudaStream_t st, uint32_t row_base = 0);
 
 // ---- hash table build (k_build.cu) ----
 // Tuples of a build pipeline, one per item: key from `key` (NULL key ->

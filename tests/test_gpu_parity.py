@@ -241,16 +241,21 @@ def test_repeated_resident_queries_replay_graphs(pkg, ctx, oracle, name, seed, s
             x.free()
 
 
-def _uniform_int32_pages(keys, rows_per_page=1984):
+def _uniform_int32_pages(keys, rows_per_page=1984, ragged=False):
     """INT32 pages without NULLs, rows_per_page rows each (the last page the
-    rest), built directly with numpy."""
+    rest), built directly with numpy; ragged: every third page holds 1500
+    rows instead."""
     import numpy as np
 
     keys = np.asarray(keys, dtype=np.int32)
-    npages = (len(keys) + rows_per_page - 1) // rows_per_page
+    starts = [0]
+    while starts[-1] < len(keys):
+        starts.append(starts[-1] + (1500 if ragged and len(starts) % 3 == 0 else rows_per_page))
+    starts[-1] = len(keys)
+    npages = len(starts) - 1
     buf = np.zeros((npages, 8192), dtype=np.uint8)
     for p in range(npages):
-        v = keys[p * rows_per_page:(p + 1) * rows_per_page]
+        v = keys[starts[p]:starts[p + 1]]
         n = len(v)
         buf[p, 0:4] = np.frombuffer(np.array([n | (n << 16)], dtype=np.uint32).tobytes(), dtype=np.uint8)
         buf[p, 4:4 + 4 * n] = np.frombuffer(v.tobytes(), dtype=np.uint8)
@@ -262,20 +267,24 @@ def _uniform_int32_pages(keys, rows_per_page=1984):
     return buf
 
 
-@pytest.mark.parametrize("break_middle_page", [False, True])
-def test_pinned_uniform_column_speculation(pkg, ctx, oracle, break_middle_page):
-    """A large pinned INT32 column read in place whose first and last pages
-    look uniform runs without a device page index; every other header is
-    checked on the host meanwhile. With one middle page changed to hold a
-    NULL (same row count, different header) the check fails and the call
-    reruns with the full index: the rows are right either way."""
+@pytest.mark.parametrize("layout", ["uniform", "null_page", "ragged"])
+def test_pinned_uniform_column_speculation(pkg, ctx, oracle, layout):
+    """A large pinned INT32 column whose first and last pages look uniform
+    runs without a device page index; every other header is checked on the
+    host meanwhile. With one middle page changed to hold a NULL (same row
+    count, different header) the check fails and the call reruns with the
+    full index; ragged pages (row counts differ) take the page index from the
+    start. The scanned column crosses the host link in 16 MiB windows (2101
+    or more pages: two windows, the second partial), so window row offsets
+    come from the uniform row count, the page index's row starts or its
+    chunk bases: the rows are right in every case."""
     import numpy as np
     import torch
 
     rows = 2100 * 1984 + 1000
     keys = np.arange(rows, dtype=np.int64) % 5000
-    pages = _uniform_int32_pages(keys)
-    if break_middle_page:
+    pages = _uniform_int32_pages(keys, ragged=layout == "ragged")
+    if layout == "null_page":
         p, n = 1000, 1984
         pages[p, 0:4] = np.frombuffer(np.array([n | ((n - 1) << 16)], dtype=np.uint32).tobytes(), dtype=np.uint8)
         nbytes = (n + 7) // 8
