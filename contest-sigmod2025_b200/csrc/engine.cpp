@@ -264,6 +264,7 @@ struct GraphEntry {
     std::vector<uint64_t> npages, page_base;
     uint64_t total_pages = 0;
     uint8_t* pages = nullptr;                // arena pages the graph writes the result to
+    std::vector<int32_t> out_types;          // result column types
     bj_stats stats{};                        // launches, pipelines, input pages of one run
     std::vector<cudaEvent_t> prof;           // timed-kernel event pairs inside the graph
     std::vector<cudaEvent_t> phase;          // phase marks inside the graph
@@ -1650,6 +1651,7 @@ bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resid
         cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
         cudaGraphDestroy(graph);
         if (ie != cudaSuccess) throw Fail{BJ_ERR_CUDA, "cudaGraphInstantiate failed"};
+        g.out_types = ex.out_types;
         if (nonempty) {
             g.rows = res.rows;
             g.npages = res.npages;
@@ -1785,11 +1787,7 @@ int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* co
     }
     if (!g->failed && !g->exec && !capture_graph(ctx, *g, plan, tables, flags)) g->failed = true;
     if (g->failed) return execute_common(ctx, plan, tables, flags, out);
-    ExecPlan ex;
-    std::string err;
-    int st = make_exec_plan(*plan, ex, err);
-    if (st != BJ_OK) return st;
-    return replay_graph(ctx, *g, ex.out_types, flags, out);
+    return replay_graph(ctx, *g, g->out_types, flags, out);
 }
 
 } // namespace
