@@ -106,6 +106,7 @@ ABI = {
     "bj_server_submit": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), _INT, ctypes.POINTER(_U64)]),
     "bj_server_wait": (_INT, [_VP, _U64, ctypes.POINTER(_VP), ctypes.POINTER(ctypes.c_double)]),
     "bj_server_resident_free": (None, [_VP, _VP]),
+    "bj_plan_explain": (_INT, [ctypes.POINTER(BjPlan), ctypes.c_char_p, _U64, ctypes.POINTER(_U64)]),
 }
 
 WORKLOAD_ABI = {
@@ -622,6 +623,24 @@ class Server:
 
     def __exit__(self, *a):
         self.close()
+
+
+def explain(plan) -> str:
+    """The pipelines the engine runs for `plan` (Plan, CPlan or POINTER(BjPlan)):
+    the driver and the plan's estimated cost, then one line per pipeline.
+    Needs no GPU."""
+    if isinstance(plan, Plan):
+        plan = CPlan(plan)
+    p = plan.ref() if isinstance(plan, CPlan) else plan
+    n = ctypes.c_uint64(0)
+    st = lib().bj_plan_explain(p, None, 0, ctypes.byref(n))
+    if st != 0:
+        raise EngineError(st, "bj_plan_explain failed")
+    buf = ctypes.create_string_buffer(n.value + 1)
+    st = lib().bj_plan_explain(p, buf, n.value + 1, ctypes.byref(n))
+    if st != 0:
+        raise EngineError(st, "bj_plan_explain failed")
+    return buf.value.decode()
 
 
 def build_context(device: int = 0) -> Context:

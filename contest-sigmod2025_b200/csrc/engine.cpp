@@ -1814,6 +1814,62 @@ extern "C" {
 
 BJ_API const char* bj_version(void) { return "b200join 0.1 (sm_100a)"; }
 
+BJ_API int bj_plan_explain(const bj_plan* plan, char* buf, uint64_t cap, uint64_t* len) {
+    if (!plan || !len || (cap && !buf)) return BJ_ERR_INVALID;
+    try {
+        ExecPlan ex;
+        std::string err;
+        int st = make_exec_plan(*plan, ex, err);
+        if (st != BJ_OK) return st;
+        std::string out;
+        char line[256];
+        auto input_text = [&](uint32_t i) {
+            char t[96];
+            std::snprintf(t, sizeof t, "input %u (table %u, %llu rows)", i, ex.inputs[i].table,
+                          static_cast<unsigned long long>(ex.inputs[i].rows));
+            return std::string(t);
+        };
+        if (ex.empty) {
+            out = "empty: an input has no rows\n";
+        } else {
+            out = "driver: " + input_text(ex.driver);
+            if (ex.est_cost >= 0) {
+                std::snprintf(line, sizeof line, "; estimated cost %.4g (result card + 10 x hashed card per join)",
+                              ex.est_cost);
+                out += line;
+            }
+            out += "\n";
+            for (size_t p = 0; p < ex.pipelines.size(); p++) {
+                const PipelinePlan& pp = ex.pipelines[p];
+                std::snprintf(line, sizeof line, "pipeline %zu: scan ", p);
+                out += line;
+                out += input_text(pp.input);
+                for (size_t k = 0; k < pp.probes.size(); k++) {
+                    std::snprintf(line, sizeof line, "%s pipeline %u on attr %u", k ? "," : ", probe", pp.probes[k].child,
+                                  pp.probes[k].probe_attr);
+                    out += line;
+                }
+                if (pp.build_key >= 0) {
+                    std::snprintf(line, sizeof line, " -> hash table on attr %lld", static_cast<long long>(pp.build_key));
+                    out += line;
+                } else {
+                    out += " -> result";
+                }
+                out += "\n";
+            }
+        }
+        *len = out.size();
+        if (cap) {
+            const size_t n = std::min<size_t>(out.size(), cap - 1);
+            std::memcpy(buf, out.data(), n);
+            buf[n] = '\0';
+        }
+        return BJ_OK;
+    } catch (...) {
+        return BJ_ERR_INTERNAL;
+    }
+}
+
 BJ_API int bj_context_create(int device, bj_context** out) {
     if (!out) return BJ_ERR_INVALID;
     *out = nullptr;

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <functional>
+#include <limits>
 #include <numeric>
 #include <queue>
 
@@ -94,6 +95,87 @@ struct Importer {
     }
 };
 
+// Join order over the plan's join tree, with the reference's cost model
+// (engine/query/QueryGraph.cpp:62-66, 70-87, 120-145: a join costs the
+// cardinality of its result plus 10 x the cardinality of the side hashed,
+// and a result's cardinality is the largest of its inputs'). The plans
+// enumerated are the ones the executor runs: every pipeline is driven by a
+// scan, probes only with its own columns, and builds its table keyed on one
+// of its own columns, so a plan for a connected set S of inputs is fixed by
+// its driver d and the order in which d's pipeline joins the branches
+// hanging off d. cost[S][d] = card(d) for S = {d}; otherwise the minimum over
+// the neighbours v of d in S of
+//     cost[S \ L][d] + cost[L][v] + card(S) + 10 card(L),
+// L being the branch of S behind the edge d-v (joined last, built with
+// driver v). Subsets come in increasing numeric order, so both parts of a
+// split are done before S. The reference enumerates the same connected
+// pairs with DPccp (engine/query/DPccp.hpp:16-56) over equivalence-class
+// neighbourhoods and caps a pipeline at two probes (QueryGraph.hpp:39); the
+// executor probes any number of tables per pipeline, so there is no cap.
+// Returns the driver of the cheapest full plan (ties: the larger input,
+// then the lower index); `cost` receives its cost. Plans over more than
+// kMaxDpInputs inputs take the largest input.
+constexpr uint32_t kMaxDpInputs = 14;
+
+uint32_t choose_driver(const std::vector<double>& card, const std::vector<Edge>& edges, double& cost) {
+    const uint32_t n = uint32_t(card.size());
+    uint32_t largest = 0;
+    for (uint32_t i = 1; i < n; i++)
+        if (card[i] > card[largest]) largest = i;
+    cost = -1;
+    if (n == 1 || n > kMaxDpInputs) return largest;
+    std::vector<uint32_t> nbr(n, 0);
+    for (const Edge& e : edges) {
+        nbr[e.a] |= 1u << e.b;
+        nbr[e.b] |= 1u << e.a;
+    }
+    // Vertices reachable from `v` inside `set`.
+    auto reach = [&](uint32_t v, uint32_t set) {
+        uint32_t seen = 1u << v, frontier = seen;
+        while (frontier) {
+            uint32_t next = 0;
+            for (uint32_t f = frontier; f; f &= f - 1) next |= nbr[__builtin_ctz(f)];
+            next &= set & ~seen;
+            seen |= next;
+            frontier = next;
+        }
+        return seen;
+    };
+    const uint32_t full = n == 32 ? ~0u : (1u << n) - 1;
+    const double inf = std::numeric_limits<double>::infinity();
+    std::vector<double> best(size_t(full + 1) * n, inf);
+    std::vector<double> setcard(full + 1, 0.0);
+    for (uint32_t S = 1; S <= full; S++) {
+        const uint32_t low = __builtin_ctz(S);
+        setcard[S] = std::max(setcard[S & (S - 1)], card[low]);
+        if (S == (1u << low)) {
+            best[size_t(S) * n + low] = card[low];
+            continue;
+        }
+        if (reach(low, S) != S) continue;  // not connected
+        for (uint32_t ds = S; ds; ds &= ds - 1) {
+            const uint32_t d = __builtin_ctz(ds);
+            double c = inf;
+            for (uint32_t vs = nbr[d] & S; vs; vs &= vs - 1) {
+                const uint32_t v = __builtin_ctz(vs);
+                const uint32_t L = reach(v, S & ~(1u << d));
+                const uint32_t R = S & ~L;
+                const double cr = best[size_t(R) * n + d], cl = best[size_t(L) * n + v];
+                if (cr == inf || cl == inf) continue;
+                c = std::min(c, cr + cl + setcard[S] + 10.0 * setcard[L]);
+            }
+            best[size_t(S) * n + d] = c;
+        }
+    }
+    uint32_t driver = largest;
+    for (uint32_t d = 0; d < n; d++) {
+        const double c = best[size_t(full) * n + d], cb = best[size_t(full) * n + driver];
+        if (c < cb || (c == cb && (card[d] > card[driver] || (card[d] == card[driver] && d < driver)))) driver = d;
+    }
+    cost = best[size_t(full) * n + driver];
+    return driver;
+}
+
 } // namespace
 
 int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err) {
@@ -121,10 +203,12 @@ int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err) {
     for (uint32_t a : root_attrs) ex.out_types.push_back(ex.attrs[a].type);
     if (ex.empty) return BJ_OK;
 
-    // Root the join tree at the largest input.
-    uint32_t driver = 0;
-    for (uint32_t i = 1; i < ni; i++)
-        if (ex.inputs[i].rows > ex.inputs[driver].rows) driver = i;
+    // Root the join tree at the driver of the cheapest plan (cardinality of
+    // an input: its row count).
+    std::vector<double> card(ni);
+    for (uint32_t i = 0; i < ni; i++) card[i] = double(ex.inputs[i].rows);
+    const uint32_t driver = choose_driver(card, im.edges, ex.est_cost);
+    ex.driver = driver;
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> adj(ni);  // (neighbour, edge)
     for (uint32_t e = 0; e < im.edges.size(); e++) {
         adj[im.edges[e].a].push_back({im.edges[e].b, e});

@@ -5,8 +5,10 @@
 // sides, and re-plans incrementally with DPccp over sampled cardinalities,
 // running at most three operators per pipeline (engine/query/QueryPlan.cpp:
 // 748-794, QueryGraph.cpp:107-216). Here the same equivalence classes are
-// built, then the join tree over the scans is rooted at the largest input
-// (the driver): every other input becomes one build pipeline whose hash table
+// built, then the join tree over the scans is rooted at the driver of the
+// cheapest plan under the reference's cost model (a dynamic program over
+// connected sets of inputs and their drivers, planner.cpp: choose_driver):
+// every other input becomes one build pipeline whose hash table
 // is keyed on the class that links it to its parent, carrying the payload
 // columns its ancestors still need; the driver's pipeline probes its children
 // and writes the result. A pipeline may probe any number of children (the
@@ -63,6 +65,8 @@ struct ExecPlan {
     std::vector<uint32_t> out_slot;       // result column -> slot of the root pipeline
     std::vector<int32_t> out_types;
     bool empty = false;                   // some input has no rows
+    uint32_t driver = 0;                  // input scanned by the output pipeline
+    double est_cost = -1;                 // cost of the chosen plan (-1: not costed)
 };
 
 // Builds the execution plan; returns BJ_OK or a status with `err` set.

@@ -152,8 +152,19 @@ BJ_API const char* bj_last_error(const bj_context* ctx);
  * to HBM. A column whose pages lie back to back in one pinned, mapped host
  * allocation (cudaHostAlloc / cudaHostRegister) is instead read in place by
  * the kernels over the host link, so only the bytes a query touches cross it
- * (set B200JOIN_ZERO_COPY=0 to always copy). */
+ * (set B200JOIN_ZERO_COPY=0 to always copy); the scan of such a column has
+ * the copy engine stream its pages through HBM windows. */
 BJ_API int bj_execute(bj_context* ctx, const bj_plan* plan, bj_result** out);
+
+/* The pipelines bj_execute runs for `plan`, as text: the driver (the input the
+ * output pipeline scans) with the plan's estimated cost, then one line per
+ * pipeline in execution order (its scan, the pipelines it probes and with
+ * which attribute, the attribute its hash table is keyed on). The role of
+ * the reference's plan printer (printPlanRec, engine/query/QueryPlan.cpp:380-411). Needs no
+ * device. Writes at most `cap` bytes to `buf` (NUL-terminated when cap > 0;
+ * buf may be NULL when cap is 0) and the text's full length, without the NUL,
+ * to *len. */
+BJ_API int bj_plan_explain(const bj_plan* plan, char* buf, uint64_t cap, uint64_t* len);
 
 /* Resident tables (no reference counterpart: the reference re-reads host pages
  * on every call). Uploads a table's pages to HBM once; later calls name it by

@@ -1,0 +1,124 @@
+"""Join ordering (CPU only: the planner needs no device).
+
+The planner roots the join tree at the driver of the cheapest plan under the
+reference's cost model (engine/query/QueryGraph.cpp:62-66, 70-87, 120-145):
+a join costs the cardinality of its result plus 10 x the cardinality of the
+side that is hashed, a result's cardinality is the largest of its inputs',
+and a base input costs its cardinality. The plans it weighs are the ones the
+executor runs: a pipeline scans one input (its driver), probes the tables
+built from the branches hanging off that input, in some order, and each
+branch is planned the same way with the input next to the driver as its own
+driver. Here an exhaustive enumeration of those plans (every driver, every
+order of every pipeline's branches) checks the planner's dynamic program."""
+import itertools
+import random
+import re
+
+import pytest
+
+
+def _tree_plan(pkg, rows, edges):
+    """A plan over inputs with the given row counts whose join nodes link
+    exactly the input pairs in `edges` (a tree, each edge (parent, child)
+    with the parent already joined). Every input has one INT32 column; each
+    join node keeps every attribute, so later joins can use any input's."""
+    plan = pkg.Plan()
+    for r in rows:
+        plan.new_input(pkg.table_from_rows([[i % 7] for i in range(r)], [pkg.INT32]))
+    order = [edges[0][0]] + [c for _, c in edges]
+    node = plan.new_scan_node(order[0], [(0, pkg.INT32)])
+    pos = {order[0]: 0}  # input -> attribute index in the current node's output
+    for parent, child in edges:
+        scan = plan.new_scan_node(child, [(0, pkg.INT32)])
+        width = len(pos)
+        outs = [(i, pkg.INT32) for i in range(width + 1)]
+        node = plan.new_join_node(True, node, scan, pos[parent], 0, outs)
+        pos[child] = width
+    plan.root = node
+    return plan
+
+
+def _exhaustive(card, edges):
+    """Minimum cost and its driver over every plan the executor can run."""
+    n = len(card)
+    nbr = {i: set() for i in range(n)}
+    for a, b in edges:
+        nbr[a].add(b)
+        nbr[b].add(a)
+
+    def branch(v, away):  # inputs reachable from v without passing `away`
+        seen, stack = {v}, [v]
+        while stack:
+            x = stack.pop()
+            for y in nbr[x]:
+                if y != away and y not in seen:
+                    seen.add(y)
+                    stack.append(y)
+        return frozenset(seen)
+
+    def cost(S, d):
+        kids = [v for v in nbr[d] if v in S]
+        best = None
+        for perm in itertools.permutations(kids):
+            c, cur = card[d], {d}
+            for v in perm:
+                L = branch(v, d) & S
+                c += cost(L, v)
+                cur |= L
+                c += max(card[i] for i in cur) + 10 * max(card[i] for i in L)
+            best = c if best is None else min(best, c)
+        return card[d] if best is None else best
+
+    full = frozenset(range(n))
+    costs = [cost(full, d) for d in range(n)]
+    best = min(costs)
+    drivers = [d for d in range(n) if costs[d] == best]
+    drivers.sort(key=lambda d: (-card[d], d))
+    return best, drivers[0]
+
+
+def _explained(pkg, plan):
+    text = pkg.explain(plan)
+    m = re.match(r"driver: input (\d+) \(table (\d+), (\d+) rows\); estimated cost ([0-9.e+]+)", text)
+    assert m, text
+    return int(m.group(1)), float(m.group(4)), text
+
+
+def test_snowflake_is_driven_by_the_fact(pkg):
+    w = pkg.Workload("snowflake", 2, 0.002)
+    text = pkg.explain(w.plan_ptr())
+    lines = text.strip().splitlines()
+    assert re.match(r"driver: input \d+ \(table 0, ", lines[0]), text  # table 0 is the fact
+    # four dimension builds, then the fact's pipeline probing all four
+    assert len(lines) == 6 and lines[-1].endswith("-> result"), text
+    assert lines[-1].count("pipeline") == 5 and all("hash table" in l for l in lines[1:5]), text
+
+
+def test_tie_goes_to_the_larger_input(pkg):
+    """A 10-row hub joined with two 300-row inputs: driving from the hub
+    hashes both large inputs (10 + 300 + 300 + (300 + 3,000) x 2 = 7,210),
+    driving from a large input hashes the other one and the hub's branch
+    (300 + (10 + 300 + 300 + 3,000) + 300 + 3,000 = 7,210). On equal cost the
+    larger input drives (it is never hashed), then the lower index."""
+    plan = _tree_plan(pkg, [300, 10, 300], [(0, 1), (1, 2)])
+    driver, cost, text = _explained(pkg, plan)
+    assert driver == 0, text
+    assert cost == pytest.approx(7210), text
+    lines = text.strip().splitlines()
+    assert lines[-1].startswith("pipeline 2: scan input 0") and lines[-1].endswith("-> result"), text
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_driver_and_cost_match_exhaustive_enumeration(pkg, seed):
+    rng = random.Random(seed)
+    n = rng.randint(2, 6)
+    rows = [rng.choice([1, 3, 10, 40, 100, 250]) for _ in range(n)]
+    edges = []
+    for c in range(1, n):
+        edges.append((rng.randrange(c), c))
+    # input order in the plan differs from the tree's numbering
+    plan = _tree_plan(pkg, rows, edges)
+    driver, cost, text = _explained(pkg, plan)
+    best, want = _exhaustive(rows, edges)
+    assert cost == pytest.approx(best), text
+    assert driver == want, (text, rows, edges)
