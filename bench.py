@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=3, help="0 skips the CPU baseline")
     ap.add_argument("--serve-queries", type=int, default=2000,
                     help="queries per serving measurement (0 skips serving)")
-    ap.add_argument("--serve-workers", type=int, default=4)
+    ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--mode", default="all", choices=["all", "value", "e2e", "serve"],
                     help="value / e2e run one measurement only (for profiling); all prints the bench line")
     return ap.parse_args()
