@@ -298,6 +298,7 @@ struct bj_context {
     cudaStream_t side[kSideStreams] = {};  // independent build pipelines run here
     cudaStream_t copy = nullptr;           // host-to-HBM copies of a streamed scan
     bool stream_scans = true;              // scans of host pages copy them through HBM windows
+    bool leaf_batch = true;                // leaf builds batched (one launch per pass)
     std::vector<cudaEvent_t> pipe_events;  // one per pipeline, reused across calls
     std::vector<cudaEvent_t> window_events;  // a streamed scan's copy and release marks
 
@@ -670,7 +671,26 @@ class Executor {
         st_ = main;
         mark_phase();
         int next_side = 0;
+        // Leaf builds: batched, each pass one launch over all of them, on the
+        // main stream (B200JOIN_LEAF_BATCH=0: one pipeline per side stream).
+        std::vector<uint8_t> batched(np, 0);
+        if (ctx_->leaf_batch) {
+            std::vector<size_t> leaves;
+            for (size_t p = 0; p + 1 < np; p++)
+                if (ex_.pipelines[p].probes.empty()) leaves.push_back(p);
+            if (!leaves.empty()) {
+                build_leaf_batch(leaves);
+                trace("leaf builds enqueued");
+                for (size_t p : leaves) {
+                    cudaEvent_t done = ctx_->pipe_event(p);
+                    if (!done) throw Fail{BJ_ERR_CUDA, "event creation failed"};
+                    BJ_CK(cudaEventRecord(done, main));
+                    batched[p] = 1;
+                }
+            }
+        }
         for (size_t p = 0; p < np; p++) {
+            if (batched[p]) continue;
             const PipelinePlan& pp = ex_.pipelines[p];
             bool leaf = pp.probes.empty() && p + 1 < np;
             cudaEvent_t done = ctx_->pipe_event(p);
@@ -1056,11 +1076,31 @@ class Executor {
         return true;
     }
 
-    bool build(size_t pi, const Items& items, const SlotSources& src, const std::vector<HTView>& probes) {
+    // A build's buffers and sizes; the buffers that must start at zero lie
+    // in one region of zbytes bytes, placed by place_zero.
+    struct PreparedBuild {
+        BuildArgs ba{};
+        HTView ht{};
+        uint2* buckets = nullptr;
+        uint32_t nb = 0;
+        bool with_bloom = false;
+        uint32_t wlog2 = 0;
+        size_t zb_table = 0, zb_counts = 0, zb_cursor = 0, zb_bloom = 0, zb_flags = 256, zb_scan = 0;
+        size_t zbytes = 0;
+        uint32_t* cursor = nullptr;
+        uint32_t* bloom = nullptr;
+        uint32_t* dflags = nullptr;
+        void* scan_status = nullptr;
+    };
+    static size_t round256(size_t x) { return (x + 255) & ~size_t(255); }
+
+    PreparedBuild prepare_build(size_t pi, const Items& items, const SlotSources& src,
+                                const std::vector<HTView>& probes) {
         const PipelinePlan& pp = ex_.pipelines[pi];
+        PreparedBuild pb;
         const uint32_t n = items.count;
         const uint32_t width = uint32_t(src.n);
-        BuildArgs ba{};
+        BuildArgs& ba = pb.ba;
         ba.in = items;
         ba.key = col(uint32_t(pp.build_key));
         ba.src = src;
@@ -1085,42 +1125,23 @@ class Executor {
         const uint32_t nrep = n;
         const uint32_t blog2 = std::max<uint32_t>(bit_width(nrep), 4);
         ba.shift = 64 - blog2;
-        const size_t nb = size_t(1) << blog2;
-        const bool with_bloom = uint64_t(nrep) * 8 <= (uint64_t(32) << kBloomMaxLog2);
-        const uint32_t wlog2 =
-            with_bloom
-                ? std::min<uint32_t>(kBloomMaxLog2, std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1)))
-                : 0;
-        // Everything that must start at zero, cleared by one memset.
-        const size_t zb_table = sizeof(uint32_t) << ba.tlog2, zb_counts = sizeof(uint32_t) * nb,
-                     zb_cursor = sizeof(uint32_t) * nb, zb_bloom = with_bloom ? sizeof(uint32_t) << wlog2 : 0,
-                     zb_flags = 256,
-                     zb_scan = scan_status_bytes(nb);
-        auto round = [](size_t x) { return (x + 255) & ~size_t(255); };
-        const size_t zbytes = round(zb_table) + round(zb_counts) + round(zb_cursor) + round(zb_bloom) + zb_flags +
-                              round(zb_scan);
-        uint8_t* z = alloc<uint8_t>(zbytes);
-        BJ_CK(cudaMemsetAsync(z, 0, zbytes, st_));
-        ba.table = reinterpret_cast<uint32_t*>(z);
-        z += round(zb_table);
-        ba.counts = reinterpret_cast<uint32_t*>(z);
-        z += round(zb_counts);
-        uint32_t* cursor = reinterpret_cast<uint32_t*>(z);
-        z += round(zb_cursor);
-        uint32_t* bloom = reinterpret_cast<uint32_t*>(z);
-        z += round(zb_bloom);
-        uint32_t* dflags = reinterpret_cast<uint32_t*>(z);
-        z += zb_flags;
-        void* scan_status = zb_scan ? z : nullptr;
-
-        launched(emit_aggregate(ba, st_));
+        pb.nb = uint32_t(1) << blog2;
+        pb.with_bloom = uint64_t(nrep) * 8 <= (uint64_t(32) << kBloomMaxLog2);
+        pb.wlog2 = pb.with_bloom ? std::min<uint32_t>(kBloomMaxLog2,
+                                                      std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1)))
+                                 : 0;
+        pb.zb_table = sizeof(uint32_t) << ba.tlog2;
+        pb.zb_counts = sizeof(uint32_t) * pb.nb;
+        pb.zb_cursor = sizeof(uint32_t) * pb.nb;
+        pb.zb_bloom = pb.with_bloom ? sizeof(uint32_t) << pb.wlog2 : 0;
+        pb.zb_scan = scan_status_bytes(pb.nb);
+        pb.zbytes = round256(pb.zb_table) + round256(pb.zb_counts) + round256(pb.zb_cursor) + round256(pb.zb_bloom) +
+                    pb.zb_flags + round256(pb.zb_scan);
         // Bucket offsets go into the x words of the interleaved bucket array;
         // the scatter fills each non-empty bucket's y (its first key).
-        uint2* buckets = alloc<uint2>(nb + 1);
-        launched(scan_exclusive_u32_zeroed(ba.counts, reinterpret_cast<uint32_t*>(buckets), nb, scan_status,
-                                           ctx_->d_err, st_, 2));
-        HTView ht{};
-        ht.buckets = buckets;
+        pb.buckets = alloc<uint2>(size_t(pb.nb) + 1);
+        HTView& ht = pb.ht;
+        ht.buckets = pb.buckets;
         ht.keys = alloc<uint32_t>(nrep);
         ht.mult = alloc<uint64_t>(nrep);
         ht.pay = alloc<uint64_t>(size_t(nrep) * std::max<uint32_t>(width, 1));
@@ -1128,15 +1149,99 @@ class Executor {
         ht.shift = ba.shift;
         ht.nentries = nrep;
         ht.width = width;
-        launched(scatter_bloom(tb, ba.is_rep, ba.shift, buckets, cursor, ht, with_bloom ? bloom : nullptr, wlog2,
-                               ctx_->d_err, st_));
-        ht.bloom = with_bloom ? bloom : nullptr;
-        ht.bloom_log2 = wlog2;
-        hts_[pi].view = ht;
+        return pb;
+    }
+
+    // Points the build's zero-start buffers into z (zbytes, zeroed by the caller).
+    static void place_zero(PreparedBuild& pb, uint8_t* z) {
+        pb.ba.table = reinterpret_cast<uint32_t*>(z);
+        z += round256(pb.zb_table);
+        pb.ba.counts = reinterpret_cast<uint32_t*>(z);
+        z += round256(pb.zb_counts);
+        pb.cursor = reinterpret_cast<uint32_t*>(z);
+        z += round256(pb.zb_cursor);
+        pb.bloom = reinterpret_cast<uint32_t*>(z);
+        z += round256(pb.zb_bloom);
+        pb.dflags = reinterpret_cast<uint32_t*>(z);
+        z += pb.zb_flags;
+        pb.scan_status = pb.zb_scan ? z : nullptr;
+    }
+
+    void publish(size_t pi, PreparedBuild& pb) {
+        pb.ht.bloom = pb.with_bloom ? pb.bloom : nullptr;
+        pb.ht.bloom_log2 = pb.wlog2;
+        hts_[pi].view = pb.ht;
         hts_[pi].empty = false;
-        hts_[pi].dflags = dflags;
-        if (ctx_->tape_mode != 2) launched(ht_flags(ht, uint32_t(nb), dflags, ctx_->num_sms, st_));
+        hts_[pi].dflags = pb.dflags;
+    }
+
+    bool build(size_t pi, const Items& items, const SlotSources& src, const std::vector<HTView>& probes) {
+        PreparedBuild pb = prepare_build(pi, items, src, probes);
+        uint8_t* z = alloc<uint8_t>(pb.zbytes);
+        BJ_CK(cudaMemsetAsync(z, 0, pb.zbytes, st_));
+        place_zero(pb, z);
+        launched(emit_aggregate(pb.ba, st_));
+        launched(scan_exclusive_u32_zeroed(pb.ba.counts, reinterpret_cast<uint32_t*>(pb.buckets), pb.nb,
+                                           pb.scan_status, ctx_->d_err, st_, 2));
+        launched(scatter_bloom(pb.ba.tb, pb.ba.is_rep, pb.ba.shift, pb.buckets, pb.cursor, pb.ht,
+                               pb.with_bloom ? pb.bloom : nullptr, pb.wlog2, ctx_->d_err, st_));
+        publish(pi, pb);
+        if (ctx_->tape_mode != 2) launched(ht_flags(hts_[pi].view, pb.nb, pb.dflags, ctx_->num_sms, st_));
         return true;
+    }
+
+    // The builds of the pipelines in `leaves` (inputs that probe nothing),
+    // kMaxLeafBuilds at a time, each pass one launch over all of them on the
+    // current stream, with one memset for all their zero-start buffers.
+    void build_leaf_batch(const std::vector<size_t>& leaves) {
+        for (size_t i0 = 0; i0 < leaves.size(); i0 += kMaxLeafBuilds) {
+            const size_t i1 = std::min(leaves.size(), i0 + kMaxLeafBuilds);
+            std::vector<PreparedBuild> pbs;
+            size_t zbytes = 0;
+            for (size_t i = i0; i < i1; i++) {
+                const size_t pi = leaves[i];
+                pipes_++;
+                const PipelinePlan& pp = ex_.pipelines[pi];
+                Items items{};
+                items.count = uint32_t(ex_.inputs[pp.input].rows);
+                SlotSources src{};
+                src.n = int(pp.slots.size());
+                for (size_t j = 0; j < pp.slots.size(); j++) {
+                    src.s[j].kind = 0;  // a leaf's slots are its own columns
+                    src.s[j].col = col(pp.slots[j].attr);
+                }
+                pbs.push_back(prepare_build(pi, items, src, {}));
+                zbytes += pbs.back().zbytes;
+            }
+            uint8_t* z = alloc<uint8_t>(zbytes);
+            BJ_CK(cudaMemsetAsync(z, 0, zbytes, st_));
+            LeafBatch batch{};
+            batch.err = ctx_->d_err;
+            batch.flags = ctx_->tape_mode != 2 ? 1 : 0;
+            size_t zoff = 0;
+            for (size_t k = 0; k < pbs.size(); k++) {
+                PreparedBuild& pb = pbs[k];
+                place_zero(pb, z + zoff);
+                zoff += pb.zbytes;
+                LeafBuild& L = batch.l[batch.n];
+                L.a = pb.ba;
+                L.buckets = pb.buckets;
+                L.nb = pb.nb;
+                L.cursor = pb.cursor;
+                L.bloom = pb.with_bloom ? pb.bloom : nullptr;
+                L.log2w = pb.wlog2;
+                L.dflags = pb.dflags;
+                L.ht = pb.ht;
+                batch.tuple_start[batch.n + 1] = batch.tuple_start[batch.n] + pb.ba.tb.count;
+                batch.block_start[batch.n + 1] = batch.block_start[batch.n] + (pb.ba.tb.count + 255) / 256;
+                batch.tile_start[batch.n + 1] =
+                    batch.tile_start[batch.n] + (pb.nb + kLeafTileBuckets - 1) / kLeafTileBuckets;
+                batch.n++;
+            }
+            batch.tile_sums = alloc<uint32_t>(batch.tile_start[batch.n]);
+            launched(build_leaves(batch, st_));
+            for (size_t k = 0; k < pbs.size(); k++) publish(leaves[i0 + k], pbs[k]);
+        }
     }
 
     void output(const Items& items, const SlotSources& src, const std::vector<HTView>& probes, bj_result& res,
@@ -1178,6 +1283,7 @@ class Executor {
             uint64_t* start = nullptr;   // exclusive scan of row costs
             uint32_t* stats = nullptr;   // [0] max cost, [1] long string present
             uint32_t* block_off = nullptr;
+            uint64_t* resolved = nullptr;  // string handles of row-number values
             bool floor = false;
             uint64_t cp = 0;
         };
@@ -1207,6 +1313,9 @@ class Executor {
                 x.handles = fo.vals[j];
                 x.valid = fo.valid[j];
                 x.src = col(ex_.pipelines.back().slots[j].attr);
+                // Values of a VARCHAR column without NULLs are its row numbers
+                // (slot_value); the length pass turns them into string handles.
+                if (!(x.src.flags & kColNulls)) x.resolved = sp[c].resolved = alloc<uint64_t>(N);
                 x.lens = sp[c].lens = alloc<uint32_t>(N);
                 x.cost = alloc<uint64_t>(N);
                 x.stats = sp[c].stats = stats + 2 * (i - i0);
@@ -1312,6 +1421,7 @@ class Executor {
                     o.lens = sp[c].lens;
                     o.descs = descs[c];
                     o.src = col(ex_.pipelines.back().slots[j].attr);
+                    if (sp[c].resolved) o.vals = sp[c].resolved;
                 }
             }
             const uint64_t pages = res.page_base[c1 - 1] + res.npages[c1 - 1] - res.page_base[c0];
@@ -1635,8 +1745,12 @@ bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resid
         ctx->graph_output = true;
         BJ_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
         capturing = true;
+        // The graph clears the device error word first and copies it to the
+        // pinned read-back slot last, so a replay needs no other call.
+        BJ_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(uint32_t), ctx->stream));
         Executor exe(ctx, ex, tables);
         bool nonempty = exe.run(res, flags);
+        BJ_CK(cudaMemcpyAsync(&ctx->h_small[63], ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
         capturing = false;
         cudaGraph_t graph = nullptr;
         BJ_CK(cudaStreamEndCapture(ctx->stream, &graph));
@@ -1711,7 +1825,7 @@ int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& typ
     res->ctx = ctx;
     try {
         res->types = types;
-        BJ_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(uint32_t), ctx->stream));
+        ctx->h_small[63] = 0;  // the graph's last node writes the low half
         BJ_CK(cudaEventRecord(ctx->ev0, ctx->stream));
         BJ_CK(cudaGraphLaunch(g.exec, ctx->stream));
         res->rows = g.rows;
@@ -1728,8 +1842,9 @@ int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& typ
             res->stats.d2h_bytes = bytes;
         }
         BJ_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-        stash_err(ctx);
-        readback(ctx, 0);
+        BJ_CK(cudaStreamSynchronize(ctx->stream));
+        if (uint32_t code = uint32_t(ctx->h_small[63]))
+            throw Fail{BJ_ERR_INVALID, std::string("device check failed: ") + dev_error_text(code)};
         float ms = 0;
         BJ_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
         res->stats.device_ms = ms;
@@ -1904,6 +2019,7 @@ BJ_API int bj_context_create(int device, bj_context** out) {
     if (const char* zc = std::getenv("B200JOIN_ZERO_COPY")) ctx->zero_copy = std::atoi(zc) != 0;
     if (const char* gr = std::getenv("B200JOIN_GRAPHS")) ctx->graphs = std::atoi(gr) != 0;
     if (const char* ss = std::getenv("B200JOIN_STREAM_SCAN")) ctx->stream_scans = std::atoi(ss) != 0;
+    if (const char* lb = std::getenv("B200JOIN_LEAF_BATCH")) ctx->leaf_batch = std::atoi(lb) != 0;
     unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     ctx->pool = std::make_unique<ThreadPool>(std::min(hw, 16u) - 1);
     *out = ctx.release();

@@ -27,6 +27,7 @@
 #include "launch.h"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace bj {
 namespace {
@@ -48,10 +49,9 @@ __device__ __forceinline__ bool tuple_equal_cg(const TupleBuf& t, uint32_t a, ui
     return true;
 }
 
-__global__ void __launch_bounds__(256) k_emit_aggregate(BuildArgs a) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+// Emits tuple i of a build and folds it into the aggregation table.
+__device__ __forceinline__ void emit_tuple(const BuildArgs& a, uint32_t i) {
     const TupleBuf& t = a.tb;
-    if (i >= t.count) return;
     // Emit.
     const uint32_t row = item_row(a.in, i);
     uint64_t kv = 0;
@@ -97,11 +97,17 @@ __global__ void __launch_bounds__(256) k_emit_aggregate(BuildArgs a) {
     record_error(a.err, kErrCapacity);
 }
 
-__global__ void k_scatter_bloom(TupleBuf t, const uint32_t* __restrict__ is_rep, uint32_t shift,
-                                uint2* __restrict__ buckets, uint32_t* __restrict__ cursor, HTView ht,
-                                uint32_t* __restrict__ bloom, uint32_t log2w, uint32_t* __restrict__ err) {
+__global__ void __launch_bounds__(256) k_emit_aggregate(BuildArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= t.count || !is_rep[i]) return;
+    if (i < a.tb.count) emit_tuple(a, i);
+}
+
+// Places representative i in its bucket's range and sets its bloom bits.
+__device__ __forceinline__ void scatter_tuple(const TupleBuf& t, const uint32_t* __restrict__ is_rep, uint32_t shift,
+                                              uint2* __restrict__ buckets, uint32_t* __restrict__ cursor,
+                                              const HTView& ht, uint32_t* __restrict__ bloom, uint32_t log2w,
+                                              uint32_t* __restrict__ err, uint32_t i) {
+    if (!is_rep[i]) return;
     const uint32_t key = t.keys[i];
     const uint32_t b = uint32_t(key_hash(key) >> shift);
     const uint32_t first = buckets[b].x;
@@ -121,23 +127,152 @@ __global__ void k_scatter_bloom(TupleBuf t, const uint32_t* __restrict__ is_rep,
     for (uint32_t j = 0; j < t.width; j++) dst[j] = src[j];
 }
 
+__global__ void k_scatter_bloom(TupleBuf t, const uint32_t* __restrict__ is_rep, uint32_t shift,
+                                uint2* __restrict__ buckets, uint32_t* __restrict__ cursor, HTView ht,
+                                uint32_t* __restrict__ bloom, uint32_t log2w, uint32_t* __restrict__ err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < t.count) scatter_tuple(t, is_rep, shift, buckets, cursor, ht, bloom, log2w, err, i);
+}
+
+// Flags of entry e of a built table (see ht_flags).
+__device__ __forceinline__ void flag_entry(const HTView& ht, uint32_t e, uint32_t* __restrict__ flags) {
+    if (ht.mult[e] > 1) flags[1] = 1;
+    uint32_t key = ht.keys[e];
+    uint32_t b = uint32_t(key_hash(key) >> ht.shift);
+    uint32_t s = ht.buckets[b].x;
+    if (e - s > 256) {
+        flags[0] = 1;  // long bucket: assume repeats (only steers capacity choices)
+        return;
+    }
+    for (uint32_t j = s; j < e; j++)
+        if (ht.keys[j] == key) {
+            flags[0] = 1;
+            break;
+        }
+}
+
 __global__ void k_ht_flags(HTView ht, uint32_t nbuckets, uint32_t* __restrict__ flags) {
     const uint32_t n = ht.buckets[nbuckets].x;  // entries actually stored
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        if (ht.mult[e] > 1) flags[1] = 1;
-        uint32_t key = ht.keys[e];
-        uint32_t b = uint32_t(key_hash(key) >> ht.shift);
-        uint32_t s = ht.buckets[b].x;
-        if (e - s > 256) {
-            flags[0] = 1;  // long bucket: assume repeats (only steers capacity choices)
-            continue;
-        }
-        for (uint32_t j = s; j < e; j++)
-            if (ht.keys[j] == key) {
-                flags[0] = 1;
-                break;
-            }
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+        flag_entry(ht, e, flags);
+}
+
+// ---- leaf builds of a query, batched ----
+//
+// Builds whose input probes nothing (a query's leaves) run together: each of
+// the passes above is one launch over all builds' tuples or buckets at once
+// (blocks find their build from prefix sums of the builds' sizes), so the
+// leaves of a query cost four launches (five with the table flags) instead
+// of three or four per build, and the builds' small grids fill the GPU
+// together: 1. emit + aggregation + bucket counts; 2a. sums of bucket tiles
+// of 1024 counts; 2b. each tile's exclusive offsets (the sums of the earlier
+// tiles of its build plus a block scan) into the buckets' x words, and the
+// build's total into bucket nb; 3. scatter + bloom; 4. table flags.
+
+constexpr uint32_t kLeafTile = 1024;  // bucket counts per tile in pass 2
+
+__device__ __forceinline__ int leaf_of(const uint32_t* start, int n, uint32_t x) {
+    int b = 0;
+    while (b + 1 < n && x >= start[b + 1]) b++;
+    return b;
+}
+
+__device__ __forceinline__ uint32_t block_sum_u32(uint32_t v) {
+    __shared__ uint32_t ws[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    uint32_t t = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); w++) t += ws[w];
+    __syncthreads();
+    return t;
+}
+
+// Exclusive prefix of v over the block (256 threads), in thread order.
+__device__ __forceinline__ uint32_t block_excl_u32(uint32_t v) {
+    __shared__ uint32_t ws[8];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= uint32_t(o)) inc += u;
     }
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    uint32_t base = 0;
+    for (uint32_t w = 0; w < warp; w++) base += ws[w];
+    __syncthreads();
+    return base + inc - v;
+}
+
+// Blocks of 256 tuples, each within one build (block_start: prefix of the
+// builds' block counts), so a block's build and its arguments are uniform.
+__device__ __forceinline__ bool leaf_tuple(const LeafBatch& B, int& b, uint32_t& i) {
+    b = leaf_of(B.block_start, B.n, blockIdx.x);
+    i = (blockIdx.x - B.block_start[b]) * blockDim.x + threadIdx.x;
+    return i < B.tuple_start[b + 1] - B.tuple_start[b];
+}
+
+__global__ void __launch_bounds__(256) k_leaf_emit(LeafBatch B) {
+    int b;
+    uint32_t i;
+    if (leaf_tuple(B, b, i)) emit_tuple(B.l[b].a, i);
+}
+
+// One block per tile of 1024 bucket counts.
+__global__ void __launch_bounds__(256) k_leaf_tile_sums(LeafBatch B) {
+    const uint32_t tile = blockIdx.x;
+    const int b = leaf_of(B.tile_start, B.n, tile);
+    const LeafBuild& L = B.l[b];
+    const uint32_t i0 = (tile - B.tile_start[b]) * kLeafTile, i1 = min(i0 + kLeafTile, L.nb);
+    uint32_t v = 0;
+    for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) v += L.a.counts[i];
+    v = block_sum_u32(v);
+    if (threadIdx.x == 0) B.tile_sums[tile] = v;
+}
+
+// One block per tile; thread k takes counts 4k..4k+3 of the tile.
+__global__ void __launch_bounds__(256) k_leaf_offsets(LeafBatch B) {
+    const uint32_t tile = blockIdx.x;
+    const int b = leaf_of(B.tile_start, B.n, tile);
+    const LeafBuild& L = B.l[b];
+    const uint32_t first = B.tile_start[b];
+    uint32_t before = 0;
+    for (uint32_t k = first + threadIdx.x; k < tile; k += blockDim.x) before += B.tile_sums[k];
+    before = block_sum_u32(before);
+    const uint32_t i0 = (tile - first) * kLeafTile + 4 * threadIdx.x;
+    uint32_t c[4], own = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        c[j] = i0 + j < L.nb ? L.a.counts[i0 + j] : 0u;
+        own += c[j];
+    }
+    uint32_t run = before + block_excl_u32(own);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (i0 + j < L.nb) L.buckets[i0 + j].x = run;
+        run += c[j];
+    }
+    if (i0 < L.nb && i0 + 4 >= L.nb) L.buckets[L.nb].x = run;  // the build's total
+}
+
+__global__ void __launch_bounds__(256) k_leaf_scatter(LeafBatch B) {
+    int b;
+    uint32_t i;
+    if (!leaf_tuple(B, b, i)) return;
+    const LeafBuild& L = B.l[b];
+    scatter_tuple(L.a.tb, L.a.is_rep, L.a.shift, L.buckets, L.cursor, L.ht, L.bloom, L.log2w, B.err, i);
+}
+
+// Entries are numbered like tuples (a build stores at most its tuple count).
+__global__ void __launch_bounds__(256) k_leaf_flags(LeafBatch B) {
+    int b;
+    uint32_t e;
+    if (!leaf_tuple(B, b, e)) return;
+    const LeafBuild& L = B.l[b];
+    if (e < L.buckets[L.nb].x) flag_entry(L.ht, e, L.dflags);
 }
 
 // Hit counts of evenly spaced sample rows against every probe of a pipeline:
@@ -180,6 +315,19 @@ int ht_flags(HTView ht, uint32_t nbuckets, uint32_t* flags, int num_sms, cudaStr
     if (blocks > uint32_t(num_sms) * 8) blocks = uint32_t(num_sms) * 8;
     k_ht_flags<<<blocks, 256, 0, st>>>(ht, nbuckets, flags);
     return 1;
+}
+
+int build_leaves(const LeafBatch& batch, cudaStream_t st) {
+    const uint32_t tuples = batch.tuple_start[batch.n], tiles = batch.tile_start[batch.n];
+    if (batch.n <= 0 || tuples == 0) return 0;
+    const uint32_t blocks = batch.block_start[batch.n];
+    k_leaf_emit<<<blocks, 256, 0, st>>>(batch);
+    k_leaf_tile_sums<<<tiles, 256, 0, st>>>(batch);
+    k_leaf_offsets<<<tiles, 256, 0, st>>>(batch);
+    k_leaf_scatter<<<blocks, 256, 0, st>>>(batch);
+    if (!batch.flags) return 4;
+    k_leaf_flags<<<blocks, 256, 0, st>>>(batch);
+    return 5;
 }
 
 int sample_probes(const SampleSet& set, uint32_t nsample, uint32_t* hits, cudaStream_t st) {

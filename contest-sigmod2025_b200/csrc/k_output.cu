@@ -142,7 +142,16 @@ __global__ void k_string_len_cost(StrCols cols, uint64_t n, uint32_t* __restrict
     uint32_t len = 0;
     const bool v = sc.valid[i];
     if (v) {
-        const uint64_t h = sc.handles[i];
+        uint64_t h = sc.handles[i];
+        if (sc.resolved) {  // a row number of src: its string handle
+            uint64_t rh = 0;
+            if (h >= sc.src.nrows || !col_get(sc.src, uint32_t(h), rh)) {
+                record_error(err, kErrRowRange);
+                rh = make_str_handle(sc.src.npages, 0);  // out of range: reported below too
+            }
+            h = rh;
+            sc.resolved[i] = h;
+        }
         if (str_handle_page(h) >= sc.src.npages) {
             record_error(err, kErrRowRange);
         } else if (str_handle_dense(h) == 0xffff) {

@@ -173,7 +173,17 @@ __device__ __forceinline__ uint64_t item_mult(const Items& in, uint32_t i) { ret
 // Value of one slot for item i (row `row`): returns false for NULL.
 __device__ __forceinline__ bool slot_value(const SlotSource& s, const Items& in, uint32_t i, uint32_t row,
                                            const ProbeSet& ps, uint64_t& v) {
-    if (s.kind == 0) return col_get(s.col, row, v);
+    if (s.kind == 0) {
+        // A VARCHAR column without NULLs yields the row number, not a string
+        // handle: locating the row's page is left to the output, which does
+        // it for result rows only (StrCol::resolved), instead of every build
+        // tuple and item paying for it.
+        if (s.col.type == kVarchar && !(s.col.flags & kColNulls)) {
+            v = row;
+            return true;
+        }
+        return col_get(s.col, row, v);
+    }
     const uint32_t e = in.ents[s.probe][i];
     if (s.kind == 2) {
         v = ps.ht[s.probe].keys[e];
@@ -247,6 +257,36 @@ int emit_aggregate(const BuildArgs& a, cudaStream_t st);
 // null: no filter).
 int scatter_bloom(TupleBuf t, const uint32_t* is_rep, uint32_t shift, uint2* buckets, uint32_t* cursor,
                   HTView ht_mut, uint32_t* bloom, uint32_t log2w, uint32_t* err, cudaStream_t st);
+// The builds of inputs that probe nothing, up to kMaxLeafBuilds at a time,
+// each pass one launch over all of them (k_build.cu). Each build's zero
+// region (table, counts, cursor, bloom, flags) must be zero before;
+// tile_sums holds tile_start[n] words.
+constexpr int kMaxLeafBuilds = 6;
+struct LeafBuild {
+    BuildArgs a;        // emit / aggregation arguments (items: rows 0..n-1)
+    uint2* buckets;     // nb + 1: offsets written into x, first keys into y
+    uint32_t nb;
+    uint32_t* cursor;   // nb zero words
+    uint32_t* bloom;    // zero, 1 << log2w words; null: no filter
+    uint32_t log2w;
+    uint32_t* dflags;   // two zero words: table flags (pass 4)
+    HTView ht;          // the table's arrays to fill
+};
+struct LeafBatch {
+    LeafBuild l[kMaxLeafBuilds];
+    int n;
+    uint32_t tuple_start[kMaxLeafBuilds + 1];  // prefix of the builds' tuple counts
+    uint32_t block_start[kMaxLeafBuilds + 1];  // prefix of their blocks of 256 tuples
+    uint32_t tile_start[kMaxLeafBuilds + 1];   // prefix of their bucket tiles (1024 buckets each)
+    uint32_t* tile_sums;
+    uint32_t* err;
+    int flags;          // 1: compute the table flags
+};
+static_assert(sizeof(LeafBatch) <= 32000, "a LeafBatch is passed as one kernel parameter (limit 32,764 bytes)");
+// Returns the launches made.
+int build_leaves(const LeafBatch& batch, cudaStream_t st);
+constexpr uint32_t kLeafTileBuckets = 1024;
+
 // Flags of a built table: [0] = 1 if some key repeats, [1] = 1 if some mult > 1
 // (both words must be zero before). The entry count is read on the device
 // from buckets[nbuckets].x.
@@ -276,7 +316,8 @@ struct StrPageDesc {
 // in one launch; stats (2 words per column, zero before): [0] largest cost,
 // [1] 1 if some string is longer than PAGE_SIZE-7.
 struct StrCol {
-    const uint64_t* handles;  // string handles into src
+    const uint64_t* handles;  // string handles into src, or row numbers of src (see slot_value)
+    uint64_t* resolved;       // non-null: handles are row numbers; their string handles go here
     const uint8_t* valid;
     DevColumn src;            // the source column the handles point into
     uint32_t* lens;
