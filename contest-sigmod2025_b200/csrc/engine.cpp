@@ -677,7 +677,8 @@ class Executor {
         if (ctx_->leaf_batch) {
             std::vector<size_t> leaves;
             for (size_t p = 0; p + 1 < np; p++)
-                if (ex_.pipelines[p].probes.empty()) leaves.push_back(p);
+                if (ex_.pipelines[p].probes.empty() && ex_.pipelines[p].slots.size() <= size_t(kMaxLeafSlots))
+                    leaves.push_back(p);
             if (!leaves.empty()) {
                 build_leaf_batch(leaves);
                 trace("leaf builds enqueued");
@@ -1121,7 +1122,14 @@ class Executor {
         // most 128 KiB (shared-memory staging); none when that leaves fewer
         // than 8 bits per key (over 131,072 tuples), where it would pass
         // most keys and its build would be contended atomics for nothing.
-        ba.tlog2 = std::max<uint32_t>(1, bit_width(uint64_t(n) * 2));
+        // Items that are distinct rows of the input (a leaf: rows 0..n-1,
+        // multiplicity 1) carrying a row number as a payload (a VARCHAR column
+        // without NULLs, slot_value) make distinct tuples: nothing can be
+        // folded, so the aggregation table is left out.
+        for (int j = 0; j < src.n && items.rows == nullptr && items.mult == nullptr && items.nprobes == 0; j++)
+            if (src.s[j].kind == 0 && src.s[j].col.type == BJ_VARCHAR && !(src.s[j].col.flags & kColNulls))
+                ba.distinct = 1;
+        ba.tlog2 = ba.distinct ? 1u : std::max<uint32_t>(1, bit_width(uint64_t(n) * 2));
         const uint32_t nrep = n;
         const uint32_t blog2 = std::max<uint32_t>(bit_width(nrep), 4);
         ba.shift = 64 - blog2;
@@ -1224,7 +1232,16 @@ class Executor {
                 place_zero(pb, z + zoff);
                 zoff += pb.zbytes;
                 LeafBuild& L = batch.l[batch.n];
-                L.a = pb.ba;
+                L.key = pb.ba.key;
+                L.nslots = pb.ba.src.n;
+                for (int j = 0; j < pb.ba.src.n; j++) L.cols[j] = pb.ba.src.s[j].col;
+                L.tb = pb.ba.tb;
+                L.table = pb.ba.table;
+                L.tlog2 = pb.ba.tlog2;
+                L.is_rep = pb.ba.is_rep;
+                L.counts = pb.ba.counts;
+                L.shift = pb.ba.shift;
+                L.distinct = pb.ba.distinct;
                 L.buckets = pb.buckets;
                 L.nb = pb.nb;
                 L.cursor = pb.cursor;

@@ -49,21 +49,31 @@ __device__ __forceinline__ bool tuple_equal_cg(const TupleBuf& t, uint32_t a, ui
     return true;
 }
 
-// Emits tuple i of a build and folds it into the aggregation table.
-__device__ __forceinline__ void emit_tuple(const BuildArgs& a, uint32_t i) {
+// Where a build's tuples go (the parts of BuildArgs the emit writes).
+struct EmitTarget {
+    TupleBuf tb;
+    uint32_t* table;
+    uint32_t tlog2;
+    uint32_t* is_rep;
+    uint32_t* counts;
+    uint32_t shift;
+    uint32_t distinct;
+    uint32_t* err;
+};
+
+// Emits tuple i of a build (key kv, valid when key_ok; multiplicity m; the
+// slot values from slot(j, v), false for NULL) and folds it into the
+// aggregation table.
+template <typename Slot>
+__device__ __forceinline__ void emit_tuple_to(const EmitTarget& a, uint32_t i, uint64_t kv, uint64_t m, int nslots,
+                                              Slot&& slot) {
     const TupleBuf& t = a.tb;
-    // Emit.
-    const uint32_t row = item_row(a.in, i);
-    uint64_t kv = 0;
-    const bool key_ok = row < a.key.nrows && col_get(a.key, row, kv);
-    if (row >= a.key.nrows) record_error(a.err, kErrRowRange);
-    const uint64_t m = key_ok ? item_mult(a.in, i) : 0ull;
     t.keys[i] = uint32_t(kv);
     t.mult[i] = m;
     uint32_t nulls = 0;
-    for (int j = 0; j < a.src.n; j++) {
+    for (int j = 0; j < nslots; j++) {
         uint64_t v = 0;
-        if (!slot_value(a.src.s[j], a.in, i, row, a.ps, v)) {
+        if (!slot(j, v)) {
             nulls |= 1u << j;
             v = 0;
         }
@@ -72,6 +82,11 @@ __device__ __forceinline__ void emit_tuple(const BuildArgs& a, uint32_t i) {
     t.pnull[i] = nulls;
     if (m == 0) {
         a.is_rep[i] = 0;
+        return;
+    }
+    if (a.distinct) {
+        a.is_rep[i] = 1;
+        atomicAdd(&a.counts[uint32_t(key_hash(uint32_t(kv)) >> a.shift)], 1u);
         return;
     }
     // The tuple is visible device-wide before its index can be seen in the
@@ -95,6 +110,18 @@ __device__ __forceinline__ void emit_tuple(const BuildArgs& a, uint32_t i) {
     }
     a.is_rep[i] = 0;
     record_error(a.err, kErrCapacity);
+}
+
+// Emits tuple i of a build and folds it into the aggregation table.
+__device__ __forceinline__ void emit_tuple(const BuildArgs& a, uint32_t i) {
+    const uint32_t row = item_row(a.in, i);
+    uint64_t kv = 0;
+    const bool key_ok = row < a.key.nrows && col_get(a.key, row, kv);
+    if (row >= a.key.nrows) record_error(a.err, kErrRowRange);
+    const uint64_t m = key_ok ? item_mult(a.in, i) : 0ull;
+    const EmitTarget to{a.tb, a.table, a.tlog2, a.is_rep, a.counts, a.shift, a.distinct, a.err};
+    emit_tuple_to(to, i, kv, m, a.src.n,
+                  [&](int j, uint64_t& v) { return slot_value(a.src.s[j], a.in, i, row, a.ps, v); });
 }
 
 __global__ void __launch_bounds__(256) k_emit_aggregate(BuildArgs a) {
@@ -218,7 +245,14 @@ __device__ __forceinline__ bool leaf_tuple(const LeafBatch& B, int& b, uint32_t&
 __global__ void __launch_bounds__(256) k_leaf_emit(LeafBatch B) {
     int b;
     uint32_t i;
-    if (leaf_tuple(B, b, i)) emit_tuple(B.l[b].a, i);
+    if (!leaf_tuple(B, b, i)) return;
+    const LeafBuild& L = B.l[b];
+    // A leaf's item i is row i, multiplicity 1; its slots are its own columns.
+    uint64_t kv = 0;
+    const bool key_ok = col_get(L.key, i, kv);
+    const EmitTarget to{L.tb, L.table, L.tlog2, L.is_rep, L.counts, L.shift, L.distinct, B.err};
+    emit_tuple_to(to, i, kv, key_ok ? 1ull : 0ull, L.nslots,
+                  [&](int j, uint64_t& v) { return column_value(L.cols[j], i, v); });
 }
 
 // One block per tile of 1024 bucket counts.
@@ -228,7 +262,7 @@ __global__ void __launch_bounds__(256) k_leaf_tile_sums(LeafBatch B) {
     const LeafBuild& L = B.l[b];
     const uint32_t i0 = (tile - B.tile_start[b]) * kLeafTile, i1 = min(i0 + kLeafTile, L.nb);
     uint32_t v = 0;
-    for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) v += L.a.counts[i];
+    for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) v += L.counts[i];
     v = block_sum_u32(v);
     if (threadIdx.x == 0) B.tile_sums[tile] = v;
 }
@@ -246,7 +280,7 @@ __global__ void __launch_bounds__(256) k_leaf_offsets(LeafBatch B) {
     uint32_t c[4], own = 0;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-        c[j] = i0 + j < L.nb ? L.a.counts[i0 + j] : 0u;
+        c[j] = i0 + j < L.nb ? L.counts[i0 + j] : 0u;
         own += c[j];
     }
     uint32_t run = before + block_excl_u32(own);
@@ -263,7 +297,7 @@ __global__ void __launch_bounds__(256) k_leaf_scatter(LeafBatch B) {
     uint32_t i;
     if (!leaf_tuple(B, b, i)) return;
     const LeafBuild& L = B.l[b];
-    scatter_tuple(L.a.tb, L.a.is_rep, L.a.shift, L.buckets, L.cursor, L.ht, L.bloom, L.log2w, B.err, i);
+    scatter_tuple(L.tb, L.is_rep, L.shift, L.buckets, L.cursor, L.ht, L.bloom, L.log2w, B.err, i);
 }
 
 // Entries are numbered like tuples (a build stores at most its tuple count).

@@ -171,19 +171,21 @@ inline ProbeSet make_probe_set(const HTView* probes, int n) {
 __device__ __forceinline__ uint32_t item_row(const Items& in, uint32_t i) { return in.rows ? in.rows[i] : i; }
 __device__ __forceinline__ uint64_t item_mult(const Items& in, uint32_t i) { return in.mult ? in.mult[i] : 1ull; }
 // Value of one slot for item i (row `row`): returns false for NULL.
+// Value of `row` of column c as a slot carries it. A VARCHAR column without
+// NULLs yields the row number, not a string handle: locating the row's page
+// is left to the output, which does it for result rows only
+// (StrCol::resolved), instead of every build tuple and item paying for it.
+__device__ __forceinline__ bool column_value(const DevColumn& c, uint32_t row, uint64_t& v) {
+    if (c.type == kVarchar && !(c.flags & kColNulls)) {
+        v = row;
+        return true;
+    }
+    return col_get(c, row, v);
+}
+
 __device__ __forceinline__ bool slot_value(const SlotSource& s, const Items& in, uint32_t i, uint32_t row,
                                            const ProbeSet& ps, uint64_t& v) {
-    if (s.kind == 0) {
-        // A VARCHAR column without NULLs yields the row number, not a string
-        // handle: locating the row's page is left to the output, which does
-        // it for result rows only (StrCol::resolved), instead of every build
-        // tuple and item paying for it.
-        if (s.col.type == kVarchar && !(s.col.flags & kColNulls)) {
-            v = row;
-            return true;
-        }
-        return col_get(s.col, row, v);
-    }
+    if (s.kind == 0) return column_value(s.col, row, v);
     const uint32_t e = in.ents[s.probe][i];
     if (s.kind == 2) {
         v = ps.ht[s.probe].keys[e];
@@ -250,6 +252,7 @@ struct BuildArgs {
     uint32_t* counts;  // per bucket: representatives
     uint32_t shift;    // bucket = key_hash >> shift
     uint32_t* err;
+    uint32_t distinct; // 1: no two tuples can be equal (each is its own representative; no table)
 };
 int emit_aggregate(const BuildArgs& a, cudaStream_t st);
 // Scatters the representatives into their buckets' ranges (cursor: one zero
@@ -262,8 +265,18 @@ int scatter_bloom(TupleBuf t, const uint32_t* is_rep, uint32_t shift, uint2* buc
 // region (table, counts, cursor, bloom, flags) must be zero before;
 // tile_sums holds tile_start[n] words.
 constexpr int kMaxLeafBuilds = 6;
+constexpr int kMaxLeafSlots = 4;  // leaves with more payload columns build one by one
 struct LeafBuild {
-    BuildArgs a;        // emit / aggregation arguments (items: rows 0..n-1)
+    DevColumn key;                  // build key column
+    DevColumn cols[kMaxLeafSlots];  // payload columns (slot j)
+    int nslots;
+    TupleBuf tb;
+    uint32_t* table;    // aggregation table, 1 << tlog2 zero words (unused when distinct)
+    uint32_t tlog2;
+    uint32_t* is_rep;
+    uint32_t* counts;   // nb zero words
+    uint32_t shift;
+    uint32_t distinct;  // see BuildArgs::distinct
     uint2* buckets;     // nb + 1: offsets written into x, first keys into y
     uint32_t nb;
     uint32_t* cursor;   // nb zero words
@@ -282,7 +295,7 @@ struct LeafBatch {
     uint32_t* err;
     int flags;          // 1: compute the table flags
 };
-static_assert(sizeof(LeafBatch) <= 32000, "a LeafBatch is passed as one kernel parameter (limit 32,764 bytes)");
+static_assert(sizeof(LeafBatch) <= 4096, "a LeafBatch is one kernel parameter block; kept within 4 KiB");
 // Returns the launches made.
 int build_leaves(const LeafBatch& batch, cudaStream_t st);
 constexpr uint32_t kLeafTileBuckets = 1024;
