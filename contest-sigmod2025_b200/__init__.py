@@ -27,7 +27,7 @@ PAGE_SIZE = 8192
 INT32, INT64, FP64, VARCHAR = 0, 1, 2, 3
 TYPE_NAMES = {INT32: "INT32", INT64: "INT64", FP64: "FP64", VARCHAR: "VARCHAR"}
 NODE_JOIN, NODE_SCAN = 0, 1
-RESULT_HOST, RESULT_DEVICE = 0, 1
+RESULT_HOST, RESULT_DEVICE, RESULT_ASYNC = 0, 1, 2
 
 STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "OOM", 4: "UNSUPPORTED", 5: "INTERNAL", 6: "NO_DEVICE"}
 
@@ -107,6 +107,7 @@ ABI = {
     "bj_server_wait": (_INT, [_VP, _U64, ctypes.POINTER(_VP), ctypes.POINTER(ctypes.c_double)]),
     "bj_server_resident_free": (None, [_VP, _VP]),
     "bj_plan_explain": (_INT, [ctypes.POINTER(BjPlan), ctypes.c_char_p, _U64, ctypes.POINTER(_U64)]),
+    "bj_result_wait": (_INT, [_VP]),
 }
 
 WORKLOAD_ABI = {
@@ -430,6 +431,11 @@ class Result:
         self._ctx = ctx
         self.handle = handle
 
+    def _check(self, st: int, what: str):
+        if st != 0:
+            msg = lib().bj_last_error(self._ctx.handle).decode() if self._ctx else "see the server's worker context"
+            raise EngineError(st, f"{what}: {msg}")
+
     @property
     def num_rows(self) -> int:
         return lib().bj_result_num_rows(self.handle)
@@ -444,9 +450,13 @@ class Result:
     def column_pages(self, c: int) -> int:
         return lib().bj_result_column_num_pages(self.handle, c)
 
+    def wait(self) -> None:
+        """Completes a RESULT_ASYNC result; raises if its device checks failed."""
+        self._check(lib().bj_result_wait(self.handle), "bj_result_wait")
+
     def stats(self) -> BjStats:
         s = BjStats()
-        lib().bj_result_stats(self.handle, ctypes.byref(s))
+        self._check(lib().bj_result_stats(self.handle, ctypes.byref(s)), "bj_result_stats")
         return s
 
     def to_table(self) -> ColumnarTable:

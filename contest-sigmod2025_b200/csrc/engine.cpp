@@ -301,6 +301,11 @@ struct bj_context {
     bool leaf_batch = true;                // leaf builds batched (one launch per pass)
     std::vector<cudaEvent_t> pipe_events;  // one per pipeline, reused across calls
     std::vector<cudaEvent_t> window_events;  // a streamed scan's copy and release marks
+    // Asynchronous results: pinned error-word slots and completion events.
+    static constexpr uint32_t kAsyncSlots = 256;
+    uint32_t* async_err = nullptr;           // kAsyncSlots pinned words
+    std::vector<uint32_t> free_slots;
+    std::vector<cudaEvent_t> free_done;
 
     // `n` events without timing, created once and reused across calls.
     cudaEvent_t* events(std::vector<cudaEvent_t>& v, size_t n) {
@@ -379,6 +384,12 @@ struct bj_result {
     uint8_t* arena_pages = nullptr;  // capture only: where the graph leaves the result pages
     bool nonempty = false;
     bj_stats stats{};
+    // BJ_RESULT_ASYNC: the work is in flight until `done`; the error word
+    // lands in err_slot (one of the context's pinned slots).
+    bool pending = false;
+    cudaEvent_t done = nullptr;
+    uint32_t slot = 0;
+    int status = BJ_OK;
 };
 
 namespace bj {
@@ -1859,12 +1870,34 @@ int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& typ
             res->stats.d2h_bytes = bytes;
         }
         BJ_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-        BJ_CK(cudaStreamSynchronize(ctx->stream));
-        if (uint32_t code = uint32_t(ctx->h_small[63]))
-            throw Fail{BJ_ERR_INVALID, std::string("device check failed: ") + dev_error_text(code)};
-        float ms = 0;
-        BJ_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-        res->stats.device_ms = ms;
+        const bool async = (flags & BJ_RESULT_ASYNC) && ctx->async_err && !ctx->free_slots.empty() && g.prof.empty() &&
+                           g.phase.empty();
+        if (async) {
+            // The error word of this query goes to its own slot; the result
+            // completes in bj_result_wait (device_ms is not measured).
+            res->slot = ctx->free_slots.back();
+            ctx->free_slots.pop_back();
+            if (!ctx->free_done.empty()) {
+                res->done = ctx->free_done.back();
+                ctx->free_done.pop_back();
+            } else if (cudaEventCreateWithFlags(&res->done, cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                ctx->free_slots.push_back(res->slot);
+                throw Fail{BJ_ERR_CUDA, "event creation failed"};
+            }
+            ctx->async_err[res->slot] = 0;
+            res->pending = true;
+            BJ_CK(cudaMemcpyAsync(ctx->async_err + res->slot, ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+            BJ_CK(cudaEventRecord(res->done, ctx->stream));
+        } else {
+            BJ_CK(cudaStreamSynchronize(ctx->stream));
+            if (uint32_t code = uint32_t(ctx->h_small[63]))
+                throw Fail{BJ_ERR_INVALID, std::string("device check failed: ") + dev_error_text(code)};
+            float ms = 0;
+            BJ_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+            res->stats.device_ms = ms;
+        }
         for (size_t i = 0; i + 1 < g.prof.size(); i += 2) {
             float k = 0;
             BJ_CK(cudaEventElapsedTime(&k, g.prof[i], g.prof[i + 1]));
@@ -1880,11 +1913,17 @@ int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& typ
         res->stats.output_pages = g.total_pages;
         ctx->launches += g.stats.kernel_launches;
     } catch (const Fail& f) {
+        int st = fail_to_status(ctx, f);  // waits for the stream
+        if (res->pending) {
+            ctx->free_slots.push_back(res->slot);
+            ctx->free_done.push_back(res->done);
+            res->pending = false;
+        }
         if (res->dev) cudaFree(res->dev);
         res->dev = nullptr;
         ctx->give_pinned(res->host);
         res->host = PinnedBlock{};
-        return fail_to_status(ctx, f);
+        return st;
     }
     res->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     ctx->live_results++;
@@ -1895,7 +1934,7 @@ int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& typ
 
 int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int flags,
                            bj_result** out) {
-    std::vector<uint64_t> key = graph_key(*plan, tables, flags, ctx->profile);
+    std::vector<uint64_t> key = graph_key(*plan, tables, flags & ~BJ_RESULT_ASYNC, ctx->profile);
     GraphEntry* g = nullptr;
     for (auto& e : ctx->graph_cache)
         if (e->key == key) g = e.get();
@@ -2026,6 +2065,10 @@ BJ_API int bj_context_create(int device, bj_context** out) {
         return BJ_ERR_OOM;
     cudaMemset(ctx->d_err, 0, 256);
     cudaMemset(ctx->d_small, 0, sizeof(uint64_t) * 64);
+    if (cudaHostAlloc(reinterpret_cast<void**>(&ctx->async_err), sizeof(uint32_t) * bj_context::kAsyncSlots,
+                      cudaHostAllocDefault) != cudaSuccess)
+        return BJ_ERR_OOM;
+    for (uint32_t i = bj_context::kAsyncSlots; i > 0; i--) ctx->free_slots.push_back(i - 1);
     // Keep freed result buffers cached in the stream-ordered pool.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -2051,6 +2094,8 @@ BJ_API void bj_context_destroy(bj_context* ctx) {
     ctx->graph_cache.clear();
     for (cudaEvent_t e : ctx->pipe_events) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->window_events) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->free_done) cudaEventDestroy(e);
+    if (ctx->async_err) cudaFreeHost(ctx->async_err);
     for (cudaStream_t s : ctx->side)
         if (s) cudaStreamDestroy(s);
     if (ctx->copy) cudaStreamDestroy(ctx->copy);
@@ -2315,16 +2360,41 @@ BJ_API int32_t bj_result_column_type(const bj_result* r, uint64_t c) {
 BJ_API uint64_t bj_result_column_num_pages(const bj_result* r, uint64_t c) {
     return r && c < r->npages.size() ? r->npages[c] : 0;
 }
+BJ_API int bj_result_wait(bj_result* r) {
+    if (!r) return BJ_ERR_INVALID;
+    if (!r->pending) return r->status;
+    bj_context* ctx = r->ctx;
+    const cudaError_t e = cudaEventSynchronize(r->done);
+    const uint32_t code = *reinterpret_cast<volatile uint32_t*>(ctx->async_err + r->slot);
+    ctx->free_slots.push_back(r->slot);
+    ctx->free_done.push_back(r->done);
+    r->done = nullptr;
+    r->pending = false;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ctx->last_error = std::string("CUDA error: ") + cudaGetErrorString(e);
+        r->status = BJ_ERR_CUDA;
+    } else if (code) {
+        ctx->last_error = std::string("device check failed: ") + dev_error_text(code);
+        r->status = BJ_ERR_INVALID;
+    }
+    return r->status;
+}
+
+// The data accessors complete an asynchronous result first.
+static bool result_ready(const bj_result* r) { return r && bj_result_wait(const_cast<bj_result*>(r)) == BJ_OK; }
+
 BJ_API const void* bj_result_page(const bj_result* r, uint64_t c, uint64_t p) {
-    if (!r || !r->host.p || c >= r->npages.size() || p >= r->npages[c]) return nullptr;
+    if (!result_ready(r) || !r->host.p || c >= r->npages.size() || p >= r->npages[c]) return nullptr;
     return r->host.p + (r->page_base[c] + p) * kPageSize;
 }
 BJ_API const void* bj_result_device_page(const bj_result* r, uint64_t c, uint64_t p) {
-    if (!r || !r->dev || c >= r->npages.size() || p >= r->npages[c]) return nullptr;
+    if (!result_ready(r) || !r->dev || c >= r->npages.size() || p >= r->npages[c]) return nullptr;
     return r->dev + (r->page_base[c] + p) * kPageSize;
 }
 BJ_API int bj_result_copy_pages(const bj_result* r, uint64_t c, void* const* dst) {
     if (!r || c >= r->npages.size() || (r->npages[c] && !dst)) return BJ_ERR_INVALID;
+    if (const int st = bj_result_wait(const_cast<bj_result*>(r))) return st;
     for (uint64_t p = 0; p < r->npages[c]; p++) {
         if (!dst[p]) return BJ_ERR_INVALID;
         if (r->host.p) {
@@ -2341,11 +2411,13 @@ BJ_API int bj_result_copy_pages(const bj_result* r, uint64_t c, void* const* dst
 }
 BJ_API int bj_result_stats(const bj_result* r, bj_stats* out) {
     if (!r || !out) return BJ_ERR_INVALID;
+    if (const int st = bj_result_wait(const_cast<bj_result*>(r))) return st;
     *out = r->stats;
     return BJ_OK;
 }
 BJ_API void bj_result_free(bj_result* r) {
     if (!r) return;
+    bj_result_wait(r);
     if (r->ctx) {
         if (r->dev) {
             cudaFreeAsync(r->dev, r->ctx->stream);

@@ -56,7 +56,7 @@ struct ScanArgs {
     HTView ht;
     uint32_t mode;             // 0 count per unit, 1 emit at unit offsets, 2 emit with atomics (unique keys)
     uint32_t use_bloom;        // stage ht.bloom in shared memory and test it
-    uint32_t prefetch;         // work units ahead of its current one a warp prefetches into L2 (0-2)
+    uint32_t prefetch;         // 1-2: a warp prefetches the unit that many units ahead into L2; 3: the next into L1
     // Multipliers for the bloom test, given at run time so that the shifts
     // they stand for (hh >> (32 - log2w), hh >> 5) run on the multiply pipe
     // as __umulhi instead of competing with the shifts on the integer pipe.
@@ -76,6 +76,9 @@ struct ScanArgs {
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 
 // Brings the line holding p into L2; nothing waits for it.
+__device__ __forceinline__ void prefetch_line_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 __device__ __forceinline__ void prefetch_line_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
@@ -395,9 +398,16 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
     uint32_t hdr_l = 0, row0_l = 0;
 
     if (use_bloom) {
+        // Asynchronous 16-byte copies (no registers, all in flight at once):
+        // a load-then-store loop pays an L2 round trip per iteration, about
+        // a fifth of the kernel's time for a 128 KiB filter.
         const uint4* src = reinterpret_cast<const uint4*>(a.ht.bloom);
         const uint32_t n4 = (1u << a.ht.bloom_log2) / 4;
-        for (uint32_t i = threadIdx.x; i < n4; i += kCtaThreads) bloom4[i] = src[i];
+        for (uint32_t i = threadIdx.x; i < n4; i += kCtaThreads) {
+            const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(bloom4 + i));
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src + i) : "memory");
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
     }
     __syncthreads();
 
@@ -406,11 +416,18 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
         const uint32_t p = u / kUnitsPerPage, part = u % kUnitsPerPage;
         load_unit(u, q, hdr_l, row0_l);
         if (a.prefetch) {
-            // One 128-byte line per lane of the unit a.prefetch units ahead.
-            const uint64_t un = uint64_t(u) + uint64_t(a.prefetch) * total_warps;
-            if (un < nunits)
-                prefetch_line_l2(a.key.pages + size_t(un / kUnitsPerPage) * kPageSize +
-                                 (un % kUnitsPerPage) * (16 * kWordsPerStep) + (lane * 128) % (16 * kWordsPerStep));
+            // One 128-byte line per lane of the unit a.prefetch units ahead
+            // (mode 3: the next unit, into L1).
+            const uint32_t ahead = a.prefetch == 3 ? 1u : a.prefetch;
+            const uint64_t un = uint64_t(u) + uint64_t(ahead) * total_warps;
+            if (un < nunits) {
+                const uint8_t* line = a.key.pages + size_t(un / kUnitsPerPage) * kPageSize +
+                                      (un % kUnitsPerPage) * (16 * kWordsPerStep) + (lane * 128) % (16 * kWordsPerStep);
+                if (a.prefetch == 3)
+                    prefetch_line_l1(line);
+                else
+                    prefetch_line_l2(line);
+            }
         }
         const uint32_t hdr = __shfl_sync(0xffffffffu, hdr_l, 0);
         const uint32_t row0 = __shfl_sync(0xffffffffu, row0_l, 0);
@@ -448,12 +465,12 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
     if (!key.npages) return 0;
     size_t bloom_bytes = bloom_smem && ht.bloom ? (sizeof(uint32_t) << ht.bloom_log2) : 0;
     if (bloom_bytes > kBloomSmemMax) bloom_bytes = 0;
-    // L2 prefetch of the work unit this many units ahead of each warp's
-    // current one (tuning knob B200JOIN_SCAN_PREFETCH = 0-2; device-memory
-    // pages only).
+    // Prefetch of the work unit this many units ahead of each warp's current
+    // one into L2, or (3) of the next one into L1 (tuning knob
+    // B200JOIN_SCAN_PREFETCH = 0-3; device-memory pages only).
     static const uint32_t ahead = [] {
         const char* e = std::getenv("B200JOIN_SCAN_PREFETCH");
-        return e ? uint32_t(std::min(2, std::max(0, std::atoi(e)))) : 0u;
+        return e ? uint32_t(std::min(3, std::max(0, std::atoi(e)))) : 0u;
     }();
     const uint32_t prefetch = (key.flags & kColHostPages) ? 0u : ahead;
     ScanArgs a{key,      ht,       uint32_t(mode), bloom_bytes ? 1u : 0u, prefetch,

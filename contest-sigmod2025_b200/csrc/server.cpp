@@ -78,7 +78,8 @@ struct bj_server {
             const int flags = r.flags;
             g.unlock();
             bj_result* res = nullptr;
-            const int st = bj_execute_resident(ctx[w], plan, tables.data(), flags, &res);
+            // A worker's query completes before it is handed back.
+            const int st = bj_execute_resident(ctx[w], plan, tables.data(), flags & ~BJ_RESULT_ASYNC, &res);
             const auto now = std::chrono::steady_clock::now();
             g.lock();
             admitted -= est;

@@ -181,11 +181,22 @@ BJ_API int bj_resident_load(bj_context* ctx, const char* path, bj_resident** out
 /* Flags of bj_execute_resident. */
 #define BJ_RESULT_HOST 0   /* copy result pages to host memory */
 #define BJ_RESULT_DEVICE 1 /* leave result pages in device memory */
+/* A call that replays a captured graph (a repeated resident query) returns
+ * once its work is enqueued, so the caller can enqueue the next query while
+ * this one runs; bj_result_wait completes it and reports its device checks
+ * (the page accessors, bj_result_copy_pages and bj_result_stats wait too).
+ * Row count, columns and page counts are known at once. Other calls ignore
+ * the flag. */
+#define BJ_RESULT_ASYNC 2
 
 /* Like bj_execute, but input i of the plan is the resident table tables[i]
  * (plan->inputs is ignored and may be NULL). */
 BJ_API int bj_execute_resident(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables,
                         int flags, bj_result** out);
+
+/* Waits for a BJ_RESULT_ASYNC result's work; returns BJ_OK or the status its
+ * device checks report (BJ_OK at once for any other result). */
+BJ_API int bj_result_wait(bj_result* r);
 
 /* Result accessors. */
 BJ_API uint64_t bj_result_num_rows(const bj_result* r);

@@ -267,6 +267,36 @@ def _uniform_int32_pages(keys, rows_per_page=1984, ragged=False):
     return buf
 
 
+@pytest.mark.parametrize("name,seed,scale", [("snowflake", 11, 0.05), ("join2", 12, 0.1)])
+def test_async_resident_results(pkg, ctx, oracle, name, seed, scale):
+    """RESULT_ASYNC: replays of a captured query are enqueued back to back
+    (five in flight at once) and completed afterwards, in a different order
+    than issued; each one's rows equal the oracle's, its stats are readable
+    after the wait, and a synchronous call after them still works."""
+    w = pkg.Workload(name, seed, scale)
+    plan = w.plan_ptr().contents
+    res = [ctx.upload(plan.inputs[i]) for i in range(plan.num_inputs)]
+    want = oracle.execute(w.plan_ptr())
+    try:
+        for _ in range(2):  # record, then capture
+            ctx.execute_resident(w.plan_ptr(), res).free()
+        pending = [ctx.execute_resident(w.plan_ptr(), res, flags=pkg.RESULT_HOST | pkg.RESULT_ASYNC)
+                   for _ in range(5)]
+        for k in (3, 0, 4, 1, 2):
+            r = pending[k]
+            r.wait()
+            got, keep = r.table_struct()
+            oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), f"{name} async #{k}")
+            assert r.stats().kernel_launches > 0
+            r.free()
+        with ctx.execute_resident(w.plan_ptr(), res) as r:
+            got, keep = r.table_struct()
+            oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), f"{name} sync after async")
+    finally:
+        for x in res:
+            x.free()
+
+
 @pytest.mark.parametrize("layout", ["uniform", "null_page", "ragged"])
 def test_pinned_uniform_column_speculation(pkg, ctx, oracle, layout):
     """A large pinned INT32 column whose first and last pages look uniform
