@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--serve-queries", type=int, default=2000,
                     help="queries per serving measurement (0 skips serving)")
     ap.add_argument("--serve-workers", type=int, default=8)
+    ap.add_argument("--serve-large", type=int, default=200,
+                    help="large queries in the serving bench's large-only closed loop")
     ap.add_argument("--mode", default="all", choices=["all", "value", "e2e", "serve"],
                     help="value / e2e run one measurement only (for profiling); all prints the bench line")
     return ap.parse_args()
@@ -186,7 +188,7 @@ def serve_bench(pkg, args, large):
     through a server of 1 worker (the plain path: one query at a time) and of
     `--serve-workers` workers (queries overlap on the device). Closed loop:
     every query submitted at once, queries/s = queries / time to the last
-    completion. Open loop: Poisson arrivals at 50% of the plain path's
+    completion; the same for `--serve-large` large queries alone. Open loop: Poisson arrivals at 50% of the plain path's
     closed-loop rate, p50/p99 of submit-to-completion latency."""
     import random
     import threading
@@ -220,6 +222,12 @@ def serve_bench(pkg, args, large):
                     srv.wait(t)[0].free()
                 qps = len(mix) / (time.perf_counter() - t0)
                 plain_qps = plain_qps or qps
+                # Closed loop of large queries only (the bench's own query).
+                t0 = time.perf_counter()
+                tickets = [submit(("large", None)) for _ in range(args.serve_large)]
+                for t in tickets:
+                    srv.wait(t)[0].free()
+                large_qps = args.serve_large / (time.perf_counter() - t0)
                 # Open loop: Poisson arrivals; a waiter thread collects results.
                 rate = 0.5 * plain_qps
                 lat, issued = [], []
@@ -251,7 +259,8 @@ def serve_bench(pkg, args, large):
                         issued.append(t)
                 th.join()
                 lat.sort()
-                out[label] = {"workers": workers, "queries_per_s": qps, "arrival_rate_qps": rate,
+                out[label] = {"workers": workers, "queries_per_s": qps, "large_only_queries_per_s": large_qps,
+                              "arrival_rate_qps": rate,
                               "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]}
             finally:
                 for xs in tabs.values():
