@@ -1303,7 +1303,9 @@ class Executor {
             fo.valid[j] = alloc<uint8_t>(N);
             any_flat = true;
         }
-        if (any_flat) launched(emit_output(items, off, src, probes.data(), fo, ctx_->d_err, st_));
+        // With every item one result row the only flat slots are VARCHAR
+        // ones, and the length pass computes them from the items itself.
+        if (any_flat && !direct) launched(emit_output(items, off, src, probes.data(), fo, ctx_->d_err, st_));
         // Page counts per result column.
         res.npages.assign(ncol, 0);
         struct StrPlan {
@@ -1333,6 +1335,8 @@ class Executor {
             uint32_t* stats = alloc<uint32_t>(2 * (i1 - i0));
             BJ_CK(cudaMemsetAsync(stats, 0, sizeof(uint32_t) * 2 * (i1 - i0), st_));
             StrCols sc{};
+            sc.items = items;
+            sc.ps = make_probe_set(probes.data(), items.nprobes);
             ScanBatch64 sb{};
             for (size_t i = i0; i < i1; i++) {
                 const size_t c = strcols[i];
@@ -1340,6 +1344,12 @@ class Executor {
                 StrCol& x = sc.c[sc.n++];
                 x.handles = fo.vals[j];
                 x.valid = fo.valid[j];
+                if (direct) {
+                    x.from_items = 1;
+                    x.slot = src.s[j];
+                    x.vals_out = fo.vals[j];
+                    x.valid_out = fo.valid[j];
+                }
                 x.src = col(ex_.pipelines.back().slots[j].attr);
                 // Values of a VARCHAR column without NULLs are its row numbers
                 // (slot_value); the length pass turns them into string handles.

@@ -140,9 +140,17 @@ __global__ void k_string_len_cost(StrCols cols, uint64_t n, uint32_t* __restrict
     const StrCol& sc = cols.c[blockIdx.y];
     if (i >= n) return;
     uint32_t len = 0;
-    const bool v = sc.valid[i];
+    bool v;
+    uint64_t h = 0;
+    if (sc.from_items) {
+        v = slot_value(sc.slot, cols.items, uint32_t(i), item_row(cols.items, uint32_t(i)), cols.ps, h);
+        sc.valid_out[i] = v;
+        if (!sc.resolved) sc.vals_out[i] = v ? h : 0;
+    } else {
+        v = sc.valid[i];
+        if (v) h = sc.handles[i];
+    }
     if (v) {
-        uint64_t h = sc.handles[i];
         if (sc.resolved) {  // a row number of src: its string handle
             uint64_t rh = 0;
             if (h >= sc.src.nrows || !col_get(sc.src, uint32_t(h), rh)) {
@@ -161,6 +169,7 @@ __global__ void k_string_len_cost(StrCols cols, uint64_t n, uint32_t* __restrict
             short_string(sc.src, h, b, len);
         }
     }
+    if (sc.resolved && !v) sc.resolved[i] = 0;
     sc.lens[i] = len;
     const uint32_t c = v ? 8 * (2 + min(len, kPageSize)) + 1 : 1;
     sc.cost[i] = c;

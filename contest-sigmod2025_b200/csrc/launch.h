@@ -332,6 +332,13 @@ struct StrCol {
     const uint64_t* handles;  // string handles into src, or row numbers of src (see slot_value)
     uint64_t* resolved;       // non-null: handles are row numbers; their string handles go here
     const uint8_t* valid;
+    // from_items: row i's value is computed here from item i (every item one
+    // result row) instead of read from handles/valid, and stored to
+    // vals_out (when not resolved) and valid_out.
+    int from_items;
+    SlotSource slot;
+    uint64_t* vals_out;
+    uint8_t* valid_out;
     DevColumn src;            // the source column the handles point into
     uint32_t* lens;
     uint64_t* cost;
@@ -340,6 +347,8 @@ struct StrCol {
 struct StrCols {
     StrCol c[kMaxOut];
     int n;
+    Items items;  // from_items columns
+    ProbeSet ps;
 };
 int string_len_cost(const StrCols& cols, uint64_t n, uint32_t* err, cudaStream_t st);
 // Greedy page packing per block of kStrBlock rows: pass 0 counts pages per
