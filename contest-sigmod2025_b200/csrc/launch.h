@@ -170,7 +170,6 @@ inline ProbeSet make_probe_set(const HTView* probes, int n) {
 #if defined(__CUDACC__)
 __device__ __forceinline__ uint32_t item_row(const Items& in, uint32_t i) { return in.rows ? in.rows[i] : i; }
 __device__ __forceinline__ uint64_t item_mult(const Items& in, uint32_t i) { return in.mult ? in.mult[i] : 1ull; }
-// Value of one slot for item i (row `row`): returns false for NULL.
 // Value of `row` of column c as a slot carries it. A VARCHAR column without
 // NULLs yields the row number, not a string handle: locating the row's page
 // is left to the output, which does it for result rows only
@@ -183,6 +182,7 @@ __device__ __forceinline__ bool column_value(const DevColumn& c, uint32_t row, u
     return col_get(c, row, v);
 }
 
+// Value of one slot for item i (row `row`): returns false for NULL.
 __device__ __forceinline__ bool slot_value(const SlotSource& s, const Items& in, uint32_t i, uint32_t row,
                                            const ProbeSet& ps, uint64_t& v) {
     if (s.kind == 0) return column_value(s.col, row, v);
