@@ -242,6 +242,32 @@ __device__ __forceinline__ bool leaf_tuple(const LeafBatch& B, int& b, uint32_t&
     return i < B.tuple_start[b + 1] - B.tuple_start[b];
 }
 
+// Every leaf of the batch has distinct tuples: emit and count only (no
+// aggregation code in the kernel).
+__global__ void __launch_bounds__(256) k_leaf_emit_distinct(LeafBatch B) {
+    int b;
+    uint32_t i;
+    if (!leaf_tuple(B, b, i)) return;
+    const LeafBuild& L = B.l[b];
+    uint64_t kv = 0;
+    const bool key_ok = col_get(L.key, i, kv);
+    const TupleBuf& t = L.tb;
+    t.keys[i] = uint32_t(kv);
+    t.mult[i] = key_ok ? 1ull : 0ull;
+    uint32_t nulls = 0;
+    for (int j = 0; j < L.nslots; j++) {
+        uint64_t v = 0;
+        if (!column_value(L.cols[j], i, v)) {
+            nulls |= 1u << j;
+            v = 0;
+        }
+        t.pay[size_t(i) * t.width + j] = v;
+    }
+    t.pnull[i] = nulls;
+    L.is_rep[i] = key_ok ? 1u : 0u;
+    if (key_ok) atomicAdd(&L.counts[uint32_t(key_hash(uint32_t(kv)) >> L.shift)], 1u);
+}
+
 __global__ void __launch_bounds__(256) k_leaf_emit(LeafBatch B) {
     int b;
     uint32_t i;
@@ -355,7 +381,12 @@ int build_leaves(const LeafBatch& batch, cudaStream_t st) {
     const uint32_t tuples = batch.tuple_start[batch.n], tiles = batch.tile_start[batch.n];
     if (batch.n <= 0 || tuples == 0) return 0;
     const uint32_t blocks = batch.block_start[batch.n];
-    k_leaf_emit<<<blocks, 256, 0, st>>>(batch);
+    bool all_distinct = true;
+    for (int b = 0; b < batch.n; b++) all_distinct = all_distinct && batch.l[b].distinct;
+    if (all_distinct)
+        k_leaf_emit_distinct<<<blocks, 256, 0, st>>>(batch);
+    else
+        k_leaf_emit<<<blocks, 256, 0, st>>>(batch);
     k_leaf_tile_sums<<<tiles, 256, 0, st>>>(batch);
     k_leaf_offsets<<<tiles, 256, 0, st>>>(batch);
     k_leaf_scatter<<<blocks, 256, 0, st>>>(batch);
