@@ -1133,20 +1133,14 @@ class Executor {
         // most 128 KiB (shared-memory staging); none when that leaves fewer
         // than 8 bits per key (over 131,072 tuples), where it would pass
         // most keys and its build would be contended atomics for nothing.
-        // Items that are distinct rows of the input (a leaf: rows 0..n-1,
-        // multiplicity 1) carrying a row number as a payload (a VARCHAR column
-        // without NULLs, slot_value) make distinct tuples: nothing can be
-        // folded, so the aggregation table is left out. A leaf without payload
-        // skips it too: its only duplicates are repeated keys, which stay
-        // separate entries of multiplicity 1 (the same result rows; the
-        // table's flags then report the repeats and probes take the path for
-        // repeated keys). Join keys of a leaf are mostly a primary key, where
-        // folding finds nothing.
-        const bool leaf = items.rows == nullptr && items.mult == nullptr && items.nprobes == 0;
-        if (leaf && src.n == 0) ba.distinct = 1;
-        for (int j = 0; j < src.n && leaf; j++)
-            if (src.s[j].kind == 0 && src.s[j].col.type == BJ_VARCHAR && !(src.s[j].col.flags & kColNulls))
-                ba.distinct = 1;
+        // A leaf (items are the input's rows 0..n-1, multiplicity 1) is built
+        // without eager aggregation: its tuples can only repeat where whole
+        // rows repeat (or, without payload, where keys repeat), and such
+        // copies may stay separate entries of multiplicity 1 (the same result
+        // rows; the table's flags then report repeated keys and probes take
+        // the path for them). Folding pays off in builds fed by probes, where
+        // one row comes back once per match.
+        ba.distinct = items.rows == nullptr && items.mult == nullptr && items.nprobes == 0 ? 1u : 0u;
         ba.tlog2 = ba.distinct ? 1u : std::max<uint32_t>(1, bit_width(uint64_t(n) * 2));
         const uint32_t nrep = n;
         const uint32_t blog2 = std::max<uint32_t>(bit_width(nrep), 4);

@@ -8,14 +8,16 @@
 // 208-263). Sizing: 2^max(bit_width(n), 4) buckets (Hashtable.cpp:94-104).
 //
 // On the GPU the build is three passes:
-//  1. emit, eager aggregation and bucket counts (K6) in one kernel: each
-//     thread writes its tuple (key, NULL mask, payload, multiplicity), makes
-//     it visible device-wide, and inserts its index into an open-addressing
-//     table keyed by the whole tuple. The first copy of each distinct tuple
-//     claims a slot with atomicCAS and becomes its representative (and counts
-//     itself into its bucket); every other copy adds its multiplicity to the
+//  1. emit (each thread writes its tuple: key, NULL mask, payload,
+//     multiplicity), then eager aggregation and bucket counts (K6) in the next
+//     launch: each tuple's index goes into an open-addressing table keyed by
+//     the whole tuple. The first copy of each distinct tuple claims a slot
+//     with atomicCAS and becomes its representative (and counts itself into
+//     its bucket); every other copy adds its multiplicity to the
 //     representative with atomicAdd. Unlike the reference, which only merges
-//     with the current bucket head, this folds every duplicate.
+//     with the current bucket head, this folds every duplicate. Builds whose
+//     tuples cannot repeat (BuildArgs::distinct) count in the emit and skip
+//     the aggregation launch.
 //  2. an exclusive scan of the bucket counts (CSR offsets), then a scatter of
 //     the representatives into their bucket's contiguous range that also sets
 //     their bits in a blocked bloom filter (K3/K4). The same bucket index as
@@ -61,9 +63,11 @@ struct EmitTarget {
     uint32_t* err;
 };
 
-// Emits tuple i of a build (key kv, valid when key_ok; multiplicity m; the
-// slot values from slot(j, v), false for NULL) and folds it into the
-// aggregation table.
+// Writes tuple i of a build (key kv; multiplicity m, 0 for a NULL key; the
+// slot values from slot(j, v), false for NULL). A zero-multiplicity tuple
+// represents nothing; a tuple of a distinct build represents itself and is
+// counted into its bucket here. The others are folded by aggregate_tuple in
+// a later launch, which sees every tuple written (no fence needed here).
 template <typename Slot>
 __device__ __forceinline__ void emit_tuple_to(const EmitTarget& a, uint32_t i, uint64_t kv, uint64_t m, int nslots,
                                               Slot&& slot) {
@@ -87,18 +91,24 @@ __device__ __forceinline__ void emit_tuple_to(const EmitTarget& a, uint32_t i, u
     if (a.distinct) {
         a.is_rep[i] = 1;
         atomicAdd(&a.counts[uint32_t(key_hash(uint32_t(kv)) >> a.shift)], 1u);
-        return;
     }
-    // The tuple is visible device-wide before its index can be seen in the
-    // table; other threads read it with L2 (.cg) loads.
-    __threadfence();
+}
+
+// Eager aggregation of tuple i (every tuple written by an earlier launch):
+// the first copy of a distinct tuple to claim a slot of the open-addressing
+// table keyed by the whole tuple represents it and is counted into its
+// bucket; every other copy adds its multiplicity to the representative.
+__device__ __forceinline__ void aggregate_tuple(const EmitTarget& a, uint32_t i) {
+    const TupleBuf& t = a.tb;
+    const uint64_t m = t.mult[i];  // only a representative's grows, after it claimed its slot
+    if (m == 0) return;
     const uint32_t mask = (1u << a.tlog2) - 1;
     uint32_t pos = uint32_t(tuple_hash(t, i) >> (64 - a.tlog2)) & mask;
     for (uint32_t step = 0; step <= mask; step++) {
         const uint32_t cur = atomicCAS(&a.table[pos], 0u, i + 1);
         if (cur == 0) {
             a.is_rep[i] = 1;
-            atomicAdd(&a.counts[uint32_t(key_hash(uint32_t(kv)) >> a.shift)], 1u);
+            atomicAdd(&a.counts[uint32_t(key_hash(t.keys[i]) >> a.shift)], 1u);
             return;
         }
         if (tuple_equal_cg(t, cur - 1, i)) {
@@ -112,21 +122,29 @@ __device__ __forceinline__ void emit_tuple_to(const EmitTarget& a, uint32_t i, u
     record_error(a.err, kErrCapacity);
 }
 
-// Emits tuple i of a build and folds it into the aggregation table.
+__device__ __forceinline__ EmitTarget emit_target(const BuildArgs& a) {
+    return EmitTarget{a.tb, a.table, a.tlog2, a.is_rep, a.counts, a.shift, a.distinct, a.err};
+}
+
+// Writes tuple i of a build.
 __device__ __forceinline__ void emit_tuple(const BuildArgs& a, uint32_t i) {
     const uint32_t row = item_row(a.in, i);
     uint64_t kv = 0;
     const bool key_ok = row < a.key.nrows && col_get(a.key, row, kv);
     if (row >= a.key.nrows) record_error(a.err, kErrRowRange);
     const uint64_t m = key_ok ? item_mult(a.in, i) : 0ull;
-    const EmitTarget to{a.tb, a.table, a.tlog2, a.is_rep, a.counts, a.shift, a.distinct, a.err};
-    emit_tuple_to(to, i, kv, m, a.src.n,
+    emit_tuple_to(emit_target(a), i, kv, m, a.src.n,
                   [&](int j, uint64_t& v) { return slot_value(a.src.s[j], a.in, i, row, a.ps, v); });
 }
 
-__global__ void __launch_bounds__(256) k_emit_aggregate(BuildArgs a) {
+__global__ void __launch_bounds__(256) k_emit(BuildArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < a.tb.count) emit_tuple(a, i);
+}
+
+__global__ void __launch_bounds__(256) k_aggregate(BuildArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.tb.count) aggregate_tuple(emit_target(a), i);
 }
 
 // Places representative i in its bucket's range and sets its bloom bits.
@@ -242,30 +260,8 @@ __device__ __forceinline__ bool leaf_tuple(const LeafBatch& B, int& b, uint32_t&
     return i < B.tuple_start[b + 1] - B.tuple_start[b];
 }
 
-// Every leaf of the batch has distinct tuples: emit and count only (no
-// aggregation code in the kernel).
-__global__ void __launch_bounds__(256) k_leaf_emit_distinct(LeafBatch B) {
-    int b;
-    uint32_t i;
-    if (!leaf_tuple(B, b, i)) return;
-    const LeafBuild& L = B.l[b];
-    uint64_t kv = 0;
-    const bool key_ok = col_get(L.key, i, kv);
-    const TupleBuf& t = L.tb;
-    t.keys[i] = uint32_t(kv);
-    t.mult[i] = key_ok ? 1ull : 0ull;
-    uint32_t nulls = 0;
-    for (int j = 0; j < L.nslots; j++) {
-        uint64_t v = 0;
-        if (!column_value(L.cols[j], i, v)) {
-            nulls |= 1u << j;
-            v = 0;
-        }
-        t.pay[size_t(i) * t.width + j] = v;
-    }
-    t.pnull[i] = nulls;
-    L.is_rep[i] = key_ok ? 1u : 0u;
-    if (key_ok) atomicAdd(&L.counts[uint32_t(key_hash(uint32_t(kv)) >> L.shift)], 1u);
+__device__ __forceinline__ EmitTarget leaf_target(const LeafBatch& B, const LeafBuild& L) {
+    return EmitTarget{L.tb, L.table, L.tlog2, L.is_rep, L.counts, L.shift, L.distinct, B.err};
 }
 
 __global__ void __launch_bounds__(256) k_leaf_emit(LeafBatch B) {
@@ -276,9 +272,18 @@ __global__ void __launch_bounds__(256) k_leaf_emit(LeafBatch B) {
     // A leaf's item i is row i, multiplicity 1; its slots are its own columns.
     uint64_t kv = 0;
     const bool key_ok = col_get(L.key, i, kv);
-    const EmitTarget to{L.tb, L.table, L.tlog2, L.is_rep, L.counts, L.shift, L.distinct, B.err};
-    emit_tuple_to(to, i, kv, key_ok ? 1ull : 0ull, L.nslots,
+    emit_tuple_to(leaf_target(B, L), i, kv, key_ok ? 1ull : 0ull, L.nslots,
                   [&](int j, uint64_t& v) { return column_value(L.cols[j], i, v); });
+}
+
+// Aggregation pass of the leaves that are not distinct (launched only when
+// some leaf of the batch is not).
+__global__ void __launch_bounds__(256) k_leaf_aggregate(LeafBatch B) {
+    int b;
+    uint32_t i;
+    if (!leaf_tuple(B, b, i)) return;
+    const LeafBuild& L = B.l[b];
+    if (!L.distinct) aggregate_tuple(leaf_target(B, L), i);
 }
 
 // One block per tile of 1024 bucket counts.
@@ -357,8 +362,11 @@ __global__ void k_sample_probes(SampleSet set, uint32_t nsample, uint32_t* hits)
 
 int emit_aggregate(const BuildArgs& a, cudaStream_t st) {
     if (!a.tb.count) return 0;
-    k_emit_aggregate<<<(a.tb.count + 255) / 256, 256, 0, st>>>(a);
-    return 1;
+    const uint32_t blocks = (a.tb.count + 255) / 256;
+    k_emit<<<blocks, 256, 0, st>>>(a);
+    if (a.distinct) return 1;
+    k_aggregate<<<blocks, 256, 0, st>>>(a);
+    return 2;
 }
 
 int scatter_bloom(TupleBuf t, const uint32_t* is_rep, uint32_t shift, uint2* buckets, uint32_t* cursor,
@@ -383,16 +391,15 @@ int build_leaves(const LeafBatch& batch, cudaStream_t st) {
     const uint32_t blocks = batch.block_start[batch.n];
     bool all_distinct = true;
     for (int b = 0; b < batch.n; b++) all_distinct = all_distinct && batch.l[b].distinct;
-    if (all_distinct)
-        k_leaf_emit_distinct<<<blocks, 256, 0, st>>>(batch);
-    else
-        k_leaf_emit<<<blocks, 256, 0, st>>>(batch);
+    k_leaf_emit<<<blocks, 256, 0, st>>>(batch);
+    if (!all_distinct) k_leaf_aggregate<<<blocks, 256, 0, st>>>(batch);
     k_leaf_tile_sums<<<tiles, 256, 0, st>>>(batch);
     k_leaf_offsets<<<tiles, 256, 0, st>>>(batch);
     k_leaf_scatter<<<blocks, 256, 0, st>>>(batch);
-    if (!batch.flags) return 4;
+    const int launches = all_distinct ? 4 : 5;
+    if (!batch.flags) return launches;
     k_leaf_flags<<<blocks, 256, 0, st>>>(batch);
-    return 5;
+    return launches + 1;
 }
 
 int sample_probes(const SampleSet& set, uint32_t nsample, uint32_t* hits, cudaStream_t st) {

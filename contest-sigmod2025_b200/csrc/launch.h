@@ -238,8 +238,9 @@ struct TupleBuf {
     uint32_t count;
     uint32_t width;
 };
-// Emit, eager aggregation and bucket counts of a hash build in one pass.
-// table (1 << tlog2 words) and counts (one per bucket) must be zero.
+// Emit, eager aggregation and bucket counts of a hash build (emit_aggregate:
+// two launches, one when the build is distinct). table (1 << tlog2 words)
+// and counts (one per bucket) must be zero.
 struct BuildArgs {
     Items in;
     DevColumn key;
