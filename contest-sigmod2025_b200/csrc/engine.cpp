@@ -301,6 +301,14 @@ struct bj_context {
     bool leaf_batch = true;                // leaf builds batched (one launch per pass)
     std::vector<cudaEvent_t> pipe_events;  // one per pipeline, reused across calls
     std::vector<cudaEvent_t> window_events;  // a streamed scan's copy and release marks
+    // Windows of a streamed scan whose copies began before the scan's column
+    // was chosen (the drop-in path's guess; Executor::streamed_scan takes
+    // them over when the guess holds).
+    struct WindowPrefetch {
+        const uint8_t* src = nullptr;  // mapped pages of the guessed column
+        uint8_t* win[3] = {};
+        uint32_t enqueued = 0;         // windows copying (their copy events recorded)
+    } prefetch;
     // Asynchronous results: pinned error-word slots and completion events.
     static constexpr uint32_t kAsyncSlots = 256;
     uint32_t* async_err = nullptr;           // kAsyncSlots pinned words
@@ -663,6 +671,91 @@ struct BuiltHT {
     bool unit_mult = false;
 };
 
+// Streamed scans (Executor::streamed_scan): windows of 16 MiB, three in flight.
+constexpr uint32_t kWindowPages = 2048;
+constexpr uint32_t kWindowRing = 3;
+
+// Begins the copies of the first windows of a host-mapped column (pages,
+// npages) on the copy stream, after the work enqueued on `after` so far (the
+// small inputs' copies keep the host link first), before the executor has
+// chosen what to scan; streamed_scan takes them over if it scans this column.
+void start_window_prefetch(bj_context* ctx, const uint8_t* pages, uint32_t npages, cudaStream_t after) {
+    const uint32_t nwin = (npages + kWindowPages - 1) / kWindowPages;
+    const uint32_t n = std::min(kWindowRing, nwin);
+    cudaEvent_t* ev = ctx->events(ctx->window_events, 2 * kWindowRing + 2);
+    if (!ev || n == 0) return;
+    BJ_CK(cudaEventRecord(ev[2 * kWindowRing], after));
+    BJ_CK(cudaStreamWaitEvent(ctx->copy, ev[2 * kWindowRing], 0));
+    bj_context::WindowPrefetch& pf = ctx->prefetch;
+    pf.src = pages;
+    pf.enqueued = 0;
+    for (uint32_t r = 0; r < n; r++) {
+        pf.win[r] = static_cast<uint8_t*>(ctx->arena.alloc(size_t(kWindowPages) * kPageSize));
+        const uint32_t np = std::min(kWindowPages, npages - r * kWindowPages);
+        BJ_CK(cudaMemcpyAsync(pf.win[r], pages + size_t(r) * kWindowPages * kPageSize, size_t(np) * kPageSize,
+                              cudaMemcpyDefault, ctx->copy));
+        BJ_CK(cudaEventRecord(ev[r], ctx->copy));
+        pf.enqueued++;
+    }
+}
+
+// Makes `st` wait for every prefetched window copy (used or not) and clears
+// the prefetch, so the call's arena outlives the copies into it.
+void end_window_prefetch(bj_context* ctx, cudaStream_t st) {
+    if (!ctx->prefetch.src) return;
+    cudaEvent_t* ev = ctx->events(ctx->window_events, 2 * kWindowRing + 2);
+    if (ev) {
+        BJ_CK(cudaEventRecord(ev[2 * kWindowRing + 1], ctx->copy));
+        BJ_CK(cudaStreamWaitEvent(st, ev[2 * kWindowRing + 1], 0));
+    } else {
+        BJ_CK(cudaStreamSynchronize(ctx->copy));
+    }
+    ctx->prefetch = bj_context::WindowPrefetch{};
+}
+
+// The probe of the output pipeline the device's sampling will most likely
+// rank first (the most selective): the one whose build input's key column is
+// the sparsest over its key range (values / (max - min + 1)), read from the
+// host pages of INT32 key columns of at most 2^20 rows. -1: no guess.
+int guess_first_probe(const ExecPlan& ex, const bj_plan& plan) {
+    if (ex.pipelines.empty()) return -1;
+    const PipelinePlan& root = ex.pipelines.back();
+    int best = -1;
+    double best_density = 2.0;
+    for (size_t k = 0; k < root.probes.size(); k++) {
+        const PipelinePlan& child = ex.pipelines[root.probes[k].child];
+        if (child.build_key < 0) continue;
+        const PlanAttr& a = ex.attrs[size_t(child.build_key)];
+        const uint32_t table = ex.inputs[a.input].table;
+        if (table >= plan.num_inputs || a.column >= plan.inputs[table].num_columns) continue;
+        const bj_column& hc = plan.inputs[table].columns[a.column];
+        if (hc.type != BJ_INT32 || plan.inputs[table].num_rows > (1u << 20) || !hc.pages) continue;
+        int64_t lo = INT64_MAX, hi = INT64_MIN;
+        uint64_t values = 0;
+        for (uint64_t p = 0; p < hc.num_pages; p++) {
+            const uint8_t* pg = static_cast<const uint8_t*>(hc.pages[p]);
+            if (!pg) return -1;
+            uint16_t nn;
+            std::memcpy(&nn, pg + 2, 2);
+            if (4 + 4 * uint64_t(nn) > kPageSize) return -1;
+            for (uint32_t v = 0; v < nn; v++) {
+                int32_t x;
+                std::memcpy(&x, pg + 4 + 4 * v, 4);
+                lo = std::min<int64_t>(lo, x);
+                hi = std::max<int64_t>(hi, x);
+            }
+            values += nn;
+        }
+        if (!values) continue;
+        const double density = double(values) / double(hi - lo + 1);
+        if (density < best_density) {
+            best_density = density;
+            best = int(k);
+        }
+    }
+    return best;
+}
+
 class Executor {
     public:
     Executor(bj_context* ctx, const ExecPlan& ex, std::vector<const DevTable*> tables)
@@ -818,14 +911,16 @@ class Executor {
     // the cursor), on the main stream while the next copies are in flight.
     void streamed_scan(const DevColumn& key, const HTView& ht, bool bloom, uint32_t* cursor, const ItemsOut& out,
                        uint32_t cap, ChainRun* chain, const Items& scanned) {
-        constexpr uint32_t kWindowPages = 2048;  // 16 MiB
-        constexpr uint32_t kRing = 3;
+        constexpr uint32_t kRing = kWindowRing;
         const uint32_t nwin = (key.npages + kWindowPages - 1) / kWindowPages;
         const uint32_t ring = std::min(kRing, nwin);
+        // Windows whose copies the call began before this column was chosen.
+        const bool pre = ctx_->prefetch.src == key.pages && ctx_->prefetch.enqueued > 0;
         uint8_t* win[kRing] = {};
-        for (uint32_t r = 0; r < ring; r++) win[r] = alloc<uint8_t>(size_t(kWindowPages) * kPageSize);
-        // [0, kRing): window copied; [kRing, 2 kRing): window scanned; last: start.
-        cudaEvent_t* ev = ctx_->events(ctx_->window_events, 2 * kRing + 1);
+        for (uint32_t r = 0; r < ring; r++)
+            win[r] = pre ? ctx_->prefetch.win[r] : alloc<uint8_t>(size_t(kWindowPages) * kPageSize);
+        // [0, kRing): window copied; [kRing, 2 kRing): window scanned; then: start, prefetch done.
+        cudaEvent_t* ev = ctx_->events(ctx_->window_events, 2 * kRing + 2);
         if (!ev) throw Fail{BJ_ERR_CUDA, "event creation failed"};
         cudaStream_t cp = ctx_->copy;
         uint32_t* marks = nullptr;  // marks[i]: items appended before window i
@@ -837,11 +932,13 @@ class Executor {
         BJ_CK(cudaStreamWaitEvent(cp, ev[2 * kRing], 0));
         for (uint32_t i = 0; i < nwin; i++) {
             const uint32_t p0 = i * kWindowPages, np = std::min(kWindowPages, key.npages - p0), r = i % kRing;
-            if (i >= kRing) BJ_CK(cudaStreamWaitEvent(cp, ev[kRing + r], 0));
-            // key.pages is the mapped (unified) address of the pinned pages.
-            BJ_CK(cudaMemcpyAsync(win[r], key.pages + size_t(p0) * kPageSize, size_t(np) * kPageSize,
-                                  cudaMemcpyDefault, cp));
-            BJ_CK(cudaEventRecord(ev[r], cp));
+            if (!(pre && i < ctx_->prefetch.enqueued)) {
+                if (i >= kRing) BJ_CK(cudaStreamWaitEvent(cp, ev[kRing + r], 0));
+                // key.pages is the mapped (unified) address of the pinned pages.
+                BJ_CK(cudaMemcpyAsync(win[r], key.pages + size_t(p0) * kPageSize, size_t(np) * kPageSize,
+                                      cudaMemcpyDefault, cp));
+                BJ_CK(cudaEventRecord(ev[r], cp));
+            }
             BJ_CK(cudaStreamWaitEvent(st_, ev[r], 0));
             DevColumn w = key;
             w.pages = win[r];
@@ -1501,6 +1598,7 @@ int fail_to_status(bj_context* ctx, const Fail& f) {
     ctx->prof_bytes = 0;
     // Leave every stream idle and the arena reusable after a failure.
     ctx->sync_all();
+    ctx->prefetch = bj_context::WindowPrefetch{};
     cudaGetLastError();
     uint32_t zero = 0;
     cudaMemcpy(ctx->d_err, &zero, sizeof(zero), cudaMemcpyHostToDevice);
@@ -1567,6 +1665,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
     auto t0 = std::chrono::steady_clock::now();
     if (!ctx || !plan || !out) return BJ_ERR_INVALID;
     trace_begin(ctx->stream);
+    ctx->prefetch = bj_context::WindowPrefetch{};  // a prefetch never outlives its call
     *out = nullptr;
     std::unique_ptr<bj_result> res(new bj_result);
     res->ctx = ctx;
@@ -1633,6 +1732,33 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
             if (!ex.empty) {
                 res->stats.h2d_bytes += upload_pages(ctx, jobs);
                 trace("pages staged");
+            }
+            if (!ex.empty && ctx->stream_scans && ctx->zero_copy) {
+                // Begin streaming the key column the output pipeline will most
+                // likely scan once the small inputs are across the host link,
+                // while they are indexed and built; the executor takes the
+                // windows over if it agrees.
+                const int k = guess_first_probe(ex, *plan);
+                if (k >= 0) {
+                    const PipelinePlan& root = ex.pipelines.back();
+                    const PlanAttr& pa = ex.attrs[root.probes[size_t(k)].probe_attr];
+                    const uint32_t table = ex.inputs[pa.input].table;
+                    const DevColumn& dc = owned[table].cols[pa.column];
+                    const uint8_t* pages = dc.pages;
+                    uint32_t npages = dc.npages;
+                    if (!pages)  // a mapped column indexed below: its job has the address
+                        for (const ColumnJob& j : jobs)
+                            if (j.out == &dc && j.in_place) {
+                                pages = j.dpages;
+                                npages = uint32_t(j.src->num_pages);
+                            }
+                    if (pages && npages >= kWindowPages && (dc.flags & kColHostPages || !dc.pages)) {
+                        start_window_prefetch(ctx, pages, npages, ctx->stream);
+                        trace("scan windows prefetching");
+                    }
+                }
+            }
+            if (!ex.empty) {
                 index_columns(ctx, jobs, ctx->arena);
                 trace("pages indexed");
                 spec.start(ctx->pool.get());
@@ -1656,6 +1782,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
             nonempty = exe.run(*res, flags);
             pipes = exe.pipelines_run();
         }
+        end_window_prefetch(ctx, ctx->stream);
         if (!nonempty) {
             if (res->dev) cudaFreeAsync(res->dev, ctx->stream);
             res->dev = nullptr;

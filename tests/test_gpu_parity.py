@@ -341,6 +341,47 @@ def test_pinned_uniform_column_speculation(pkg, ctx, oracle, layout):
         torch._C._cudart.cudaHostUnregister(base)
 
 
+def test_pinned_scan_window_guess_mismatch(pkg, ctx, oracle):
+    """Two pinned fact key columns; the host's guess of the probe to scan
+    first (the build key column sparsest over its range) is wrong here, so the
+    windows it began copying go unused and the scan streams the other column:
+    the rows are still the oracle's."""
+    import numpy as np
+    import torch
+
+    rows = 2100 * 1984
+    rng = np.random.default_rng(5)
+    fk_a = rng.integers(0, 1000, rows)    # hits A's keys 0..99: 10%
+    fk_b = rng.integers(0, 10000, rows)   # hits B's keys 0..9: 0.1%, the most selective
+    cols = [pkg.Column(pkg.INT32, _uniform_int32_pages(fk_a).tobytes()),
+            pkg.Column(pkg.INT32, _uniform_int32_pages(fk_b).tobytes())]
+    plan = pkg.Plan()
+    plan.new_input(pkg.ColumnarTable(rows, cols))
+    plan.new_input(pkg.table_from_rows([[k] for k in list(range(100)) + [100000]], [pkg.INT32]))  # sparse range
+    plan.new_input(pkg.table_from_rows([[k] for k in range(10)], [pkg.INT32]))  # dense range
+    f = plan.new_scan_node(0, [(0, pkg.INT32), (1, pkg.INT32)])
+    a = plan.new_scan_node(1, [(0, pkg.INT32)])
+    b = plan.new_scan_node(2, [(0, pkg.INT32)])
+    j1 = plan.new_join_node(False, f, a, 0, 0, [(0, pkg.INT32), (1, pkg.INT32)])
+    plan.root = plan.new_join_node(False, j1, b, 1, 0, [(0, pkg.INT32), (1, pkg.INT32)])
+    cp = pkg.CPlan(plan)
+    regs = []
+    try:
+        for c in range(2):
+            col = cp.struct.inputs[0].columns[c]
+            assert torch._C._cudart.cudaHostRegister(col.pages[0], col.num_pages * pkg.PAGE_SIZE, 3) == 0
+            regs.append(col.pages[0])
+        want = oracle.execute(cp.ref())
+        for _ in range(2):
+            with ctx.execute_raw(cp) as r:
+                assert r.stats().mapped_input_bytes > 0
+                got, keep = r.table_struct()
+                assert oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), "guess mismatch") > 0
+    finally:
+        for p_ in regs:
+            torch._C._cudart.cudaHostUnregister(p_)
+
+
 def test_resident_snapshot_round_trip(pkg, ctx, oracle, tmp_path):
     """Resident tables saved to snapshot files and loaded back (no page index
     pass) answer the query exactly; truncated or foreign files are rejected."""
