@@ -285,7 +285,7 @@ struct bj_context {
     uint64_t* d_small = nullptr;       // device readback slots
     GatherList gather{};               // values queued for the next read-back
     uint64_t launches = 0;
-    uint64_t live_results = 0;
+    std::atomic<uint64_t> live_results{0};
     int num_sms = 148;
     bool profile = false;
     int tape_mode = 0;               // 0 off, 1 record read-backs, 2 replay them (graph capture)
@@ -349,13 +349,46 @@ struct bj_context {
     std::vector<cudaEvent_t> phase_events; // phase marks of the call (kPhaseMarks when complete)
     uint64_t prof_bytes = 0;
 
-    PinnedBlock take_pinned(size_t bytes) {
-        for (size_t i = 0; i < pinned_free.size(); i++)
-            if (pinned_free[i].size >= bytes) {
-                PinnedBlock b = pinned_free[i];
-                pinned_free.erase(pinned_free.begin() + i);
-                return b;
+    // Memory that results give back, possibly on other threads than the one
+    // running this context (a server hands results to its callers): kept
+    // here under release_m and freed by the context's own next call, never
+    // while one of its streams may be capturing a graph (a free enqueued on
+    // a capturing stream would land in the graph).
+    std::mutex release_m;
+    std::vector<uint8_t*> release_dev;
+    void release_device(uint8_t* p) {
+        std::lock_guard<std::mutex> g(release_m);
+        release_dev.push_back(p);
+    }
+    // On the context's own thread, outside stream capture.
+    void drain_releases() {
+        std::vector<uint8_t*> dev;
+        std::vector<PinnedBlock> excess;
+        {
+            std::lock_guard<std::mutex> g(release_m);
+            dev.swap(release_dev);
+            while (pinned_free.size() > 4) {
+                excess.push_back(pinned_free.front());
+                pinned_free.erase(pinned_free.begin());
             }
+        }
+        for (uint8_t* p : dev) cudaFreeAsync(p, stream);
+        if (!excess.empty()) {
+            cudaStreamSynchronize(stream);
+            for (const PinnedBlock& b : excess) cudaFreeHost(b.p);
+        }
+    }
+
+    PinnedBlock take_pinned(size_t bytes) {
+        {
+            std::lock_guard<std::mutex> g(release_m);
+            for (size_t i = 0; i < pinned_free.size(); i++)
+                if (pinned_free[i].size >= bytes) {
+                    PinnedBlock b = pinned_free[i];
+                    pinned_free.erase(pinned_free.begin() + i);
+                    return b;
+                }
+        }
         PinnedBlock b;
         b.size = std::max<size_t>(bytes, 1 << 20);
         cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&b.p), b.size, cudaHostAllocDefault);
@@ -367,11 +400,8 @@ struct bj_context {
     }
     void give_pinned(PinnedBlock b) {
         if (!b.p) return;
-        pinned_free.push_back(b);
-        while (pinned_free.size() > 4) {
-            cudaFreeHost(pinned_free.front().p);
-            pinned_free.erase(pinned_free.begin());
-        }
+        std::lock_guard<std::mutex> g(release_m);
+        pinned_free.push_back(b);  // beyond four blocks, drain_releases frees the oldest
     }
 };
 
@@ -1666,6 +1696,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
     if (!ctx || !plan || !out) return BJ_ERR_INVALID;
     trace_begin(ctx->stream);
     ctx->prefetch = bj_context::WindowPrefetch{};  // a prefetch never outlives its call
+    ctx->drain_releases();
     *out = nullptr;
     std::unique_ptr<bj_result> res(new bj_result);
     res->ctx = ctx;
@@ -2008,21 +2039,30 @@ int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& typ
             res->stats.d2h_bytes = bytes;
         }
         BJ_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-        const bool async = (flags & BJ_RESULT_ASYNC) && ctx->async_err && !ctx->free_slots.empty() && g.prof.empty() &&
-                           g.phase.empty();
+        bool async = (flags & BJ_RESULT_ASYNC) && ctx->async_err && g.prof.empty() && g.phase.empty();
         if (async) {
             // The error word of this query goes to its own slot; the result
             // completes in bj_result_wait (device_ms is not measured).
-            res->slot = ctx->free_slots.back();
-            ctx->free_slots.pop_back();
-            if (!ctx->free_done.empty()) {
-                res->done = ctx->free_done.back();
-                ctx->free_done.pop_back();
-            } else if (cudaEventCreateWithFlags(&res->done, cudaEventDisableTiming) != cudaSuccess) {
+            {
+                std::lock_guard<std::mutex> lk(ctx->release_m);
+                async = !ctx->free_slots.empty();
+                if (async) {
+                    res->slot = ctx->free_slots.back();
+                    ctx->free_slots.pop_back();
+                    if (!ctx->free_done.empty()) {
+                        res->done = ctx->free_done.back();
+                        ctx->free_done.pop_back();
+                    }
+                }
+            }
+            if (async && !res->done && cudaEventCreateWithFlags(&res->done, cudaEventDisableTiming) != cudaSuccess) {
                 cudaGetLastError();
+                std::lock_guard<std::mutex> lk(ctx->release_m);
                 ctx->free_slots.push_back(res->slot);
                 throw Fail{BJ_ERR_CUDA, "event creation failed"};
             }
+        }
+        if (async) {
             ctx->async_err[res->slot] = 0;
             res->pending = true;
             BJ_CK(cudaMemcpyAsync(ctx->async_err + res->slot, ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -2053,6 +2093,7 @@ int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& typ
     } catch (const Fail& f) {
         int st = fail_to_status(ctx, f);  // waits for the stream
         if (res->pending) {
+            std::lock_guard<std::mutex> lk(ctx->release_m);
             ctx->free_slots.push_back(res->slot);
             ctx->free_done.push_back(res->done);
             res->pending = false;
@@ -2072,6 +2113,7 @@ int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& typ
 
 int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int flags,
                            bj_result** out) {
+    ctx->drain_releases();
     std::vector<uint64_t> key = graph_key(*plan, tables, flags & ~BJ_RESULT_ASYNC, ctx->profile);
     GraphEntry* g = nullptr;
     for (auto& e : ctx->graph_cache)
@@ -2234,6 +2276,7 @@ BJ_API void bj_context_destroy(bj_context* ctx) {
     for (cudaEvent_t e : ctx->window_events) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->free_done) cudaEventDestroy(e);
     if (ctx->async_err) cudaFreeHost(ctx->async_err);
+    for (uint8_t* p : ctx->release_dev) cudaFree(p);
     for (cudaStream_t s : ctx->side)
         if (s) cudaStreamDestroy(s);
     if (ctx->copy) cudaStreamDestroy(ctx->copy);
@@ -2504,8 +2547,11 @@ BJ_API int bj_result_wait(bj_result* r) {
     bj_context* ctx = r->ctx;
     const cudaError_t e = cudaEventSynchronize(r->done);
     const uint32_t code = *reinterpret_cast<volatile uint32_t*>(ctx->async_err + r->slot);
-    ctx->free_slots.push_back(r->slot);
-    ctx->free_done.push_back(r->done);
+    {
+        std::lock_guard<std::mutex> lk(ctx->release_m);
+        ctx->free_slots.push_back(r->slot);
+        ctx->free_done.push_back(r->done);
+    }
     r->done = nullptr;
     r->pending = false;
     if (e != cudaSuccess) {
@@ -2558,7 +2604,7 @@ BJ_API void bj_result_free(bj_result* r) {
     bj_result_wait(r);
     if (r->ctx) {
         if (r->dev) {
-            cudaFreeAsync(r->dev, r->ctx->stream);
+            r->ctx->release_device(r->dev);
             r->dev = nullptr;
         }
         if (r->host.p) r->ctx->give_pinned(r->host);
