@@ -2208,6 +2208,15 @@ BJ_API int bj_plan_explain(const bj_plan* plan, char* buf, uint64_t cap, uint64_
                 }
                 out += "\n";
             }
+            // The drop-in path's guess of the probe scanned first (it starts
+            // copying that column's pages before the device sampling decides).
+            const int g = guess_first_probe(ex, *plan);
+            if (g >= 0) {
+                const PipelinePlan& root = ex.pipelines.back();
+                std::snprintf(line, sizeof line, "scan guess: pipeline %u on attr %u\n", root.probes[size_t(g)].child,
+                              root.probes[size_t(g)].probe_attr);
+                out += line;
+            }
         }
         *len = out.size();
         if (cap) {
