@@ -1028,7 +1028,11 @@ class Executor {
         std::iota(order.begin(), order.end(), 0u);
         std::vector<double> rate(np, 1.0);
         if (np) {
-            uint32_t nsample = uint32_t(std::min<uint64_t>(in.rows, 4096));
+            // Sample rows read from pinned host memory cross the host link one
+            // by one, beside the scan windows' copies: fewer of them there.
+            bool host_keys = false;
+            for (size_t k = 0; k < np; k++) host_keys = host_keys || (col(pp.probes[k].probe_attr).flags & kColHostPages);
+            uint32_t nsample = uint32_t(std::min<uint64_t>(in.rows, host_keys ? 1024 : 4096));
             uint32_t* hits = alloc<uint32_t>(np);
             SampleSet set{};
             set.n = int(np);
