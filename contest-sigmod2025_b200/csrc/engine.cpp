@@ -792,9 +792,10 @@ class Executor {
         : ctx_(ctx), ex_(ex), tables_(std::move(tables)), st_(ctx->stream), A_(ctx->arena) {}
 
     // Runs every pipeline; returns false if the result is empty. Pipelines
-    // without probes (leaf builds) need no host round trip, so they run on
-    // side streams and overlap; a pipeline that probes waits for its
-    // children's events and runs on the main stream.
+    // without probes (leaf builds) need no host round trip: they run first,
+    // batched (each pass one launch over all of them), or one per side stream;
+    // a pipeline that probes waits for its children's events and runs on the
+    // main stream.
     bool run(bj_result& res, int flags) {
         const size_t np = ex_.pipelines.size();
         hts_.resize(np);
