@@ -2194,6 +2194,10 @@ BJ_API int bj_plan_explain(const bj_plan* plan, char* buf, uint64_t cap, uint64_
                               ex.est_cost);
                 out += line;
             }
+            if (ex.ref_cost >= 0) {
+                std::snprintf(line, sizeof line, "; the reference's plan space at best %.4g", ex.ref_cost);
+                out += line;
+            }
             out += "\n";
             for (size_t p = 0; p < ex.pipelines.size(); p++) {
                 const PipelinePlan& pp = ex.pipelines[p];

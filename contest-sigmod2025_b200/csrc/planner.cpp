@@ -176,6 +176,75 @@ uint32_t choose_driver(const std::vector<double>& card, const std::vector<Edge>&
     return driver;
 }
 
+// The reference's own dynamic program over its plan space, for comparison
+// (engine/query/QueryGraph.cpp:107-216 with DPccp, DPccp.hpp:16-56): a plan for
+// a connected set of inputs and a count of probes in its top pipeline (0-2,
+// maxPipelineLength = 3, QueryGraph.hpp:39); joining `left` as a hash table into
+// the pipeline of `right` adds card(left + right) + 10 card(left) and one probe
+// (consider, QueryGraph.cpp:90-108). Its pipelines may probe with an earlier
+// probe's payload, which the executor does not run, and probe at most twice,
+// which the executor does not need. On a tree of join edges, the pairs DPccp
+// enumerates are the two sides of each edge of a connected set. Returns the
+// cheapest full plan's cost, or -1 above kMaxDpInputs inputs.
+double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge>& edges) {
+    const uint32_t n = uint32_t(card.size());
+    if (n == 0 || n > kMaxDpInputs) return -1;
+    if (n == 1) return card[0];
+    std::vector<uint32_t> nbr(n, 0);
+    for (const Edge& e : edges) {
+        nbr[e.a] |= 1u << e.b;
+        nbr[e.b] |= 1u << e.a;
+    }
+    auto reach = [&](uint32_t v, uint32_t set) {
+        uint32_t seen = 1u << v, frontier = seen;
+        while (frontier) {
+            uint32_t next = 0;
+            for (uint32_t f = frontier; f; f &= f - 1) next |= nbr[__builtin_ctz(f)];
+            next &= set & ~seen;
+            seen |= next;
+            frontier = next;
+        }
+        return seen;
+    };
+    constexpr int kPipes = 3;
+    const uint32_t full = (1u << n) - 1;
+    const double inf = std::numeric_limits<double>::infinity();
+    std::vector<double> best(size_t(full + 1) * kPipes, inf), setcard(full + 1, 0.0);
+    for (uint32_t S = 1; S <= full; S++) {
+        const uint32_t low = __builtin_ctz(S);
+        setcard[S] = std::max(setcard[S & (S - 1)], card[low]);
+        if (S == (1u << low)) {
+            best[size_t(S) * kPipes] = card[low];  // a base relation costs its cardinality
+            continue;
+        }
+        if (reach(low, S) != S) continue;
+        // Each edge of S splits it into two connected sides; either side can
+        // be the hash table joined into the other's pipeline.
+        for (uint32_t us = S; us; us &= us - 1) {
+            const uint32_t u = __builtin_ctz(us);
+            for (uint32_t vs = nbr[u] & S; vs; vs &= vs - 1) {
+                const uint32_t v = __builtin_ctz(vs);
+                if (v < u) continue;  // each edge once
+                const uint32_t A = reach(v, S & ~(1u << u)), B = S & ~A;
+                for (int side = 0; side < 2; side++) {
+                    const uint32_t left = side ? B : A, right = side ? A : B;
+                    const double base = setcard[S] + 10.0 * setcard[left];
+                    double lbest = inf;
+                    for (int lp = 0; lp < kPipes; lp++) lbest = std::min(lbest, best[size_t(left) * kPipes + lp]);
+                    for (int rp = 0; rp + 1 < kPipes; rp++) {
+                        const double c = lbest + best[size_t(right) * kPipes + rp] + base;
+                        double& t = best[size_t(S) * kPipes + rp + 1];
+                        t = std::min(t, c);
+                    }
+                }
+            }
+        }
+    }
+    double r = inf;
+    for (int p = 0; p < kPipes; p++) r = std::min(r, best[size_t(full) * kPipes + p]);
+    return r;
+}
+
 } // namespace
 
 int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err) {
@@ -209,6 +278,7 @@ int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err) {
     for (uint32_t i = 0; i < ni; i++) card[i] = double(ex.inputs[i].rows);
     const uint32_t driver = choose_driver(card, im.edges, ex.est_cost);
     ex.driver = driver;
+    ex.ref_cost = reference_dp_cost(card, im.edges);
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> adj(ni);  // (neighbour, edge)
     for (uint32_t e = 0; e < im.edges.size(); e++) {
         adj[im.edges[e].a].push_back({im.edges[e].b, e});

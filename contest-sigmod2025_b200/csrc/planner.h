@@ -67,6 +67,7 @@ struct ExecPlan {
     bool empty = false;                   // some input has no rows
     uint32_t driver = 0;                  // input scanned by the output pipeline
     double est_cost = -1;                 // cost of the chosen plan (-1: not costed)
+    double ref_cost = -1;                 // the cheapest plan of the reference's plan space, same cost model
 };
 
 // Builds the execution plan; returns BJ_OK or a status with `err` set.

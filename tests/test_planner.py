@@ -159,3 +159,41 @@ def test_scan_guess_follows_the_key_range_not_the_hit_rate(pkg):
     j1 = plan.new_join_node(False, f, a, 0, 0, [(0, pkg.INT32), (1, pkg.INT32)])
     plan.root = plan.new_join_node(False, j1, b, 1, 0, [(0, pkg.INT32), (1, pkg.INT32)])
     assert _scan_guess(pkg.explain(plan))[1] == 1
+
+
+def _costs(pkg, plan):
+    first = pkg.explain(plan).splitlines()[0]
+    m = re.search(r"estimated cost ([0-9.e+]+).*plan space at best ([0-9.e+]+)", first)
+    assert m, first
+    return float(m.group(1)), float(m.group(2))
+
+
+def test_reference_space_equal_for_two_probes(pkg):
+    """A fact with two dimensions: the reference's dynamic program (at most two
+    probes per pipeline) finds the executor's plan: fact scanned, both hashed,
+    100 + 10 + 10 + (100 + 100) x 2 = 520."""
+    plan = _tree_plan(pkg, [100, 10, 10], [(0, 1), (0, 2)])
+    est, ref = _costs(pkg, plan)
+    assert est == pytest.approx(520) and ref == pytest.approx(520)
+
+
+def test_reference_space_dearer_for_a_wide_star(pkg):
+    """Three dimensions: the executor probes all three from the fact's pipeline
+    (730); the reference's pipelines stop at two probes, so a partial join must
+    be hashed (1,630)."""
+    plan = _tree_plan(pkg, [100, 10, 10, 10], [(0, 1), (0, 2), (0, 3)])
+    est, ref = _costs(pkg, plan)
+    assert est == pytest.approx(730) and ref == pytest.approx(1630)
+
+
+def test_reference_space_cheaper_with_payload_keys(pkg):
+    """A chain fact(500) - D(10) - E(200): the reference's plans may key a hash
+    table on an earlier probe's payload. Its best: E's pipeline probes D's table
+    (10 + 200 + (200 + 100) = 510), the result is hashed on D's key to the fact,
+    carried as D's payload, and probed by the fact (510 + 500 + (500 + 2,000) =
+    3,510). The executor's rooted plans key every table on the scanned input's
+    own column: D's pipeline probes E's table (2,410) and the fact probes that
+    (5,410)."""
+    plan = _tree_plan(pkg, [500, 10, 200], [(0, 1), (1, 2)])
+    est, ref = _costs(pkg, plan)
+    assert est == pytest.approx(5410) and ref == pytest.approx(3510)
