@@ -2175,7 +2175,7 @@ BJ_API int bj_plan_explain(const bj_plan* plan, char* buf, uint64_t cap, uint64_
     try {
         ExecPlan ex;
         std::string err;
-        int st = make_exec_plan(*plan, ex, err);
+        int st = make_exec_plan(*plan, ex, err, true);
         if (st != BJ_OK) return st;
         std::string out;
         char line[256];

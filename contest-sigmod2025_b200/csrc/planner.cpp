@@ -247,7 +247,7 @@ double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge
 
 } // namespace
 
-int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err) {
+int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err, bool reference_cost) {
     ex = ExecPlan{};
     if (plan.num_nodes == 0 || !plan.nodes) {
         err = "empty plan";
@@ -278,7 +278,7 @@ int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err) {
     for (uint32_t i = 0; i < ni; i++) card[i] = double(ex.inputs[i].rows);
     const uint32_t driver = choose_driver(card, im.edges, ex.est_cost);
     ex.driver = driver;
-    ex.ref_cost = reference_dp_cost(card, im.edges);
+    if (reference_cost) ex.ref_cost = reference_dp_cost(card, im.edges);
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> adj(ni);  // (neighbour, edge)
     for (uint32_t e = 0; e < im.edges.size(); e++) {
         adj[im.edges[e].a].push_back({im.edges[e].b, e});

@@ -71,6 +71,8 @@ struct ExecPlan {
 };
 
 // Builds the execution plan; returns BJ_OK or a status with `err` set.
-int make_exec_plan(const bj_plan& plan, ExecPlan& out, std::string& err);
+// reference_cost: also cost the reference's plan space (ExecPlan::ref_cost;
+// for bj_plan_explain, not needed to run the plan).
+int make_exec_plan(const bj_plan& plan, ExecPlan& out, std::string& err, bool reference_cost = false);
 
 } // namespace bj
