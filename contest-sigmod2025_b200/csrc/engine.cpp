@@ -2217,6 +2217,7 @@ BJ_API int bj_plan_explain(const bj_plan* plan, char* buf, uint64_t cap, uint64_
                 }
                 out += "\n";
             }
+            if (!ex.ref_plan.empty()) out += "reference plan space, cheapest: " + ex.ref_plan + "\n";
             // The drop-in path's guess of the probe scanned first (it starts
             // copying that column's pages before the device sampling decides).
             const int g = guess_first_probe(ex, *plan);

@@ -186,10 +186,17 @@ uint32_t choose_driver(const std::vector<double>& card, const std::vector<Edge>&
 // which the executor does not need. On a tree of join edges, the pairs DPccp
 // enumerates are the two sides of each edge of a connected set. Returns the
 // cheapest full plan's cost, or -1 above kMaxDpInputs inputs.
-double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge>& edges) {
+// `plan_text` (optional) receives the cheapest plan in the notation
+// probe(R, hash(L)): input R's pipeline (or the pipeline of plan R) probes the
+// hash table built from plan L.
+double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge>& edges,
+                         std::string* plan_text = nullptr) {
     const uint32_t n = uint32_t(card.size());
     if (n == 0 || n > kMaxDpInputs) return -1;
-    if (n == 1) return card[0];
+    if (n == 1) {
+        if (plan_text) *plan_text = "input 0";
+        return card[0];
+    }
     std::vector<uint32_t> nbr(n, 0);
     for (const Edge& e : edges) {
         nbr[e.a] |= 1u << e.b;
@@ -210,6 +217,11 @@ double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge
     const uint32_t full = (1u << n) - 1;
     const double inf = std::numeric_limits<double>::infinity();
     std::vector<double> best(size_t(full + 1) * kPipes, inf), setcard(full + 1, 0.0);
+    struct Choice {
+        uint32_t left = 0, right = 0;
+        int lpipes = 0, rpipes = 0;
+    };
+    std::vector<Choice> how(plan_text ? size_t(full + 1) * kPipes : 0);
     for (uint32_t S = 1; S <= full; S++) {
         const uint32_t low = __builtin_ctz(S);
         setcard[S] = std::max(setcard[S & (S - 1)], card[low]);
@@ -230,18 +242,39 @@ double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge
                     const uint32_t left = side ? B : A, right = side ? A : B;
                     const double base = setcard[S] + 10.0 * setcard[left];
                     double lbest = inf;
-                    for (int lp = 0; lp < kPipes; lp++) lbest = std::min(lbest, best[size_t(left) * kPipes + lp]);
+                    int lpick = 0;
+                    for (int lp = 0; lp < kPipes; lp++)
+                        if (best[size_t(left) * kPipes + lp] < lbest) {
+                            lbest = best[size_t(left) * kPipes + lp];
+                            lpick = lp;
+                        }
                     for (int rp = 0; rp + 1 < kPipes; rp++) {
                         const double c = lbest + best[size_t(right) * kPipes + rp] + base;
                         double& t = best[size_t(S) * kPipes + rp + 1];
-                        t = std::min(t, c);
+                        if (c < t) {
+                            t = c;
+                            if (plan_text) how[size_t(S) * kPipes + rp + 1] = Choice{left, right, lpick, rp};
+                        }
                     }
                 }
             }
         }
     }
     double r = inf;
-    for (int p = 0; p < kPipes; p++) r = std::min(r, best[size_t(full) * kPipes + p]);
+    int rp = 0;
+    for (int p = 0; p < kPipes; p++)
+        if (best[size_t(full) * kPipes + p] < r) {
+            r = best[size_t(full) * kPipes + p];
+            rp = p;
+        }
+    if (plan_text && r < inf) {
+        std::function<std::string(uint32_t, int)> show = [&](uint32_t S, int p) -> std::string {
+            if (p == 0) return "input " + std::to_string(__builtin_ctz(S));
+            const Choice& c = how[size_t(S) * kPipes + p];
+            return "probe(" + show(c.right, c.rpipes) + ", hash(" + show(c.left, c.lpipes) + "))";
+        };
+        *plan_text = show(full, rp);
+    }
     return r;
 }
 
@@ -278,7 +311,7 @@ int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err, bool ref
     for (uint32_t i = 0; i < ni; i++) card[i] = double(ex.inputs[i].rows);
     const uint32_t driver = choose_driver(card, im.edges, ex.est_cost);
     ex.driver = driver;
-    if (reference_cost) ex.ref_cost = reference_dp_cost(card, im.edges);
+    if (reference_cost) ex.ref_cost = reference_dp_cost(card, im.edges, &ex.ref_plan);
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> adj(ni);  // (neighbour, edge)
     for (uint32_t e = 0; e < im.edges.size(); e++) {
         adj[im.edges[e].a].push_back({im.edges[e].b, e});

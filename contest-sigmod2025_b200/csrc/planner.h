@@ -68,6 +68,7 @@ struct ExecPlan {
     uint32_t driver = 0;                  // input scanned by the output pipeline
     double est_cost = -1;                 // cost of the chosen plan (-1: not costed)
     double ref_cost = -1;                 // the cheapest plan of the reference's plan space, same cost model
+    std::string ref_plan;                 // that plan, as probe(R, hash(L)) over input indices
 };
 
 // Builds the execution plan; returns BJ_OK or a status with `err` set.

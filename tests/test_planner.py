@@ -197,3 +197,5 @@ def test_reference_space_cheaper_with_payload_keys(pkg):
     plan = _tree_plan(pkg, [500, 10, 200], [(0, 1), (1, 2)])
     est, ref = _costs(pkg, plan)
     assert est == pytest.approx(5410) and ref == pytest.approx(3510)
+    text = pkg.explain(plan)
+    assert "reference plan space, cheapest: probe(input 0, hash(probe(input 2, hash(input 1))))" in text, text
