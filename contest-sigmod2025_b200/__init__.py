@@ -116,6 +116,8 @@ WORKLOAD_ABI = {
     "bjw_workload_plan": (ctypes.POINTER(BjPlan), [_VP]),
     "bjw_workload_scan_bytes": (_U64, [_VP]),
     "bjw_workload_variant": (ctypes.POINTER(BjPlan), [_VP, _INT]),
+    "bjw_workload_num_queries": (_U64, [_VP]),
+    "bjw_workload_query": (ctypes.POINTER(BjPlan), [_VP, _U64]),
     "bjw_workload_free": (None, [_VP]),
     "bjw_save_plan": (_INT, [ctypes.c_char_p, ctypes.POINTER(BjPlan)]),
     "bjw_save_table": (_INT, [ctypes.c_char_p, ctypes.POINTER(BjTable)]),
@@ -399,6 +401,17 @@ class Workload:
 
     def scan_bytes(self) -> int:
         return wlib().bjw_workload_scan_bytes(self.handle)
+
+    def num_queries(self) -> int:
+        return wlib().bjw_workload_num_queries(self.handle)
+
+    def query_ptr(self, k: int):
+        """Query k of a batched workload ("schema20": 256 queries over shared
+        tables; query 0 is plan_ptr())."""
+        p = wlib().bjw_workload_query(self.handle, k)
+        if not p:
+            raise EngineError(1, f"{self.name} has no query {k}")
+        return p
 
     def variant_ptr(self, dims: int):
         """Snowflake: the fact joined with its first `dims` dimensions (its

@@ -341,6 +341,235 @@ void make_snowflake(plan_io::OwnedPlan& p, uint64_t seed, double scale) {
     p.root = 8;
 }
 
+// "schema20": 20 tables in a random PK-FK tree and a batch of random acyclic
+// join queries over them (the batched-workload shape: 2-12 tables per query,
+// tables of 10K-40M rows before their filter, per-table filter selectivity
+// log-uniform in [0.1%, 100%], PK-FK edges uniform or Zipf(0.8-1.5)).
+// Table t: c0 INT32 primary key (a permutation of the unfiltered rows), c1
+// INT32 foreign key to its parent's c0 (table 0: uniform values), c2 INT32
+// uniform in [0, 1e6), c3 FP64 uniform in [0, 1), c4 VARCHAR of 1-32
+// printable characters. The filter keeps a row when a seeded draw falls under
+// the table's selectivity (applied at load time, as the contest does).
+struct QuerySpec {
+    std::vector<uint32_t> tables;  // in join order: each after a neighbour
+    std::vector<uint32_t> via;     // via[i]: the earlier table tables[i] joins (i >= 1)
+    std::vector<uint32_t> payload; // per table: the payload column its scan outputs (2, 3 or 4)
+    std::vector<std::pair<uint32_t, uint32_t>> out;  // (position in tables, 0 key / 1 payload)
+};
+
+constexpr uint32_t kSchemaTables = 20;
+
+constexpr uint32_t kNoRow = 0xffffffffu;
+
+// The exact result size of a query: a count over the join tree, children
+// before parents (a table joins one added before it, so reverse order works).
+// prow[t][r]: the parent row that row r of table t references (kNoRow: none).
+double schema20_count(const QuerySpec& q, const std::vector<uint32_t>& parent,
+                      const std::vector<std::vector<uint32_t>>& prow) {
+    const size_t m = q.tables.size();
+    std::vector<std::vector<double>> w(m);
+    for (size_t i = 0; i < m; i++) w[i].assign(prow[q.tables[i]].size(), 1.0);
+    for (size_t i = m; i-- > 1;) {
+        const uint32_t t = q.tables[i], v = q.via[i];
+        size_t j = 0;
+        while (q.tables[j] != v) j++;
+        if (parent[t] == v && t != v) {  // t is v's child: sum t's weights into the rows they reference
+            std::vector<double> agg(w[j].size(), 0.0);
+            for (size_t r = 0; r < w[i].size(); r++)
+                if (prow[t][r] != kNoRow) agg[prow[t][r]] += w[i][r];
+            for (size_t r = 0; r < w[j].size(); r++) w[j][r] *= agg[r];
+        } else {                         // t is v's parent: each row of v takes the weight of its row of t
+            for (size_t r = 0; r < w[j].size(); r++)
+                w[j][r] *= prow[v][r] == kNoRow ? 0.0 : w[i][prow[v][r]];
+        }
+    }
+    double total = 0;
+    for (double x : w[0]) total += x;
+    return total;
+}
+
+void make_schema20(plan_io::OwnedPlan& p, uint64_t seed, double scale, uint32_t nqueries,
+                   std::vector<uint32_t>& parent, std::vector<QuerySpec>& queries) {
+    std::vector<std::vector<uint32_t>> prow;
+    Rng g(stream_seed(seed, 200, 0, 0));
+    std::vector<uint64_t> rows(kSchemaTables);
+    std::vector<double> sel(kSchemaTables), skew(kSchemaTables);
+    parent.assign(kSchemaTables, 0);
+    for (uint32_t t = 0; t < kSchemaTables; t++) {
+        rows[t] = scaled(std::exp(std::log(1e4) + g.unit() * (std::log(4e7) - std::log(1e4))), scale);
+        sel[t] = std::exp(std::log(1e-3) + g.unit() * (0.0 - std::log(1e-3)));
+        skew[t] = g.unit() < 0.5 ? 0.0 : 0.8 + 0.7 * g.unit();  // 0: uniform FK
+        parent[t] = t ? uint32_t(g.below(t)) : 0u;
+    }
+    // Tables in order (a parent precedes its children): a foreign key draws a
+    // rank over the parent's rows that passed its filter (uniform or Zipf),
+    // mapped to a row by a seeded permutation, so every edge joins.
+    std::vector<std::vector<uint32_t>> ranked(kSchemaTables);  // per table: its rows in rank order
+    std::vector<std::vector<int32_t>> key(kSchemaTables);      // per table: c0 of its rows
+    prow.assign(kSchemaTables, {});
+    p.tables.resize(kSchemaTables);
+    for (uint32_t t = 0; t < kSchemaTables; t++) {
+        const uint64_t n = rows[t];
+        const auto keys = permutation(n, stream_seed(seed, 202, t, 0));
+        Rng r(stream_seed(seed, 203, t, 0));
+        const std::vector<uint32_t>& pr = ranked[parent[t]];
+        std::unique_ptr<Zipf> z;
+        if (t && skew[t] > 0 && !pr.empty()) z = std::make_unique<Zipf>(pr.size(), skew[t]);
+        std::vector<int32_t>& c0 = key[t];
+        std::vector<int32_t> c1, c2;
+        std::vector<double> c3;
+        std::vector<uint64_t> off{0};
+        std::string bytes;
+        for (uint64_t i = 0; i < n; i++) {
+            int32_t fk;
+            uint32_t to = kNoRow;
+            if (!t || pr.empty()) {
+                fk = int32_t(r.below(1000000));
+            } else {
+                to = z ? pr[z->sample(r) - 1] : pr[r.below(pr.size())];
+                fk = key[parent[t]][to];
+            }
+            const int32_t a = int32_t(r.below(1000000));
+            const double d = r.unit();
+            const uint32_t len = 1 + uint32_t(r.below(32));
+            const bool keep = r.unit() < sel[t];
+            if (!keep) {
+                for (uint32_t c = 0; c < len; c++) r.next();
+                continue;
+            }
+            c0.push_back(keys[i]);
+            c1.push_back(fk);
+            prow[t].push_back(to);
+            c2.push_back(a);
+            c3.push_back(d);
+            for (uint32_t c = 0; c < len; c++) bytes.push_back(char(32 + r.below(95)));
+            off.push_back(bytes.size());
+        }
+        // The kept rows in a seeded order (the rank -> row map of the FKs).
+        ranked[t].resize(c0.size());
+        for (uint32_t i = 0; i < c0.size(); i++) ranked[t][i] = i;
+        Rng sh(stream_seed(seed, 201, t, 0));
+        for (uint64_t i = ranked[t].size(); i > 1; i--) std::swap(ranked[t][i - 1], ranked[t][sh.below(i)]);
+        auto& tab = p.tables[t];
+        tab.num_rows = c0.size();
+        tab.columns.resize(5);
+        encode_any(tab.columns[0], BJ_INT32, c0.size(), c0.data(), nullptr, nullptr, nullptr);
+        encode_any(tab.columns[1], BJ_INT32, c1.size(), c1.data(), nullptr, nullptr, nullptr);
+        encode_any(tab.columns[2], BJ_INT32, c2.size(), c2.data(), nullptr, nullptr, nullptr);
+        encode_any(tab.columns[3], BJ_FP64, c3.size(), c3.data(), nullptr, nullptr, nullptr);
+        encode_any(tab.columns[4], BJ_VARCHAR, c0.size(), nullptr, nullptr, off.data(), bytes.data());
+    }
+    // Queries: a random connected set of 2-12 tables grown from a random table.
+    std::vector<std::vector<uint32_t>> nbr(kSchemaTables);
+    for (uint32_t t = 1; t < kSchemaTables; t++) {
+        nbr[t].push_back(parent[t]);
+        nbr[parent[t]].push_back(t);
+    }
+    queries.clear();
+    for (uint32_t k = 0; k < nqueries; k++) {
+        Rng q(stream_seed(seed, 204, k, 0));
+        const uint32_t want = 2 + uint32_t(q.below(11));
+        QuerySpec spec;
+        std::vector<uint8_t> in(kSchemaTables, 0);
+        const uint32_t start = uint32_t(q.below(kSchemaTables));
+        spec.tables.push_back(start);
+        spec.via.push_back(start);
+        in[start] = 1;
+        // A table joins only when the result of the tables so far stays within
+        // the largest of them (no many-to-many blow-up through a shared parent
+        // under skew); the plan joins in this order, so every intermediate
+        // result is bounded the same way.
+        uint64_t largest = p.tables[start].num_rows;
+        while (spec.tables.size() < want) {
+            std::vector<std::pair<uint32_t, uint32_t>> frontier;  // (new table, its neighbour in the set)
+            for (uint32_t x : spec.tables)
+                for (uint32_t y : nbr[x])
+                    if (!in[y]) frontier.push_back({y, x});
+            bool added = false;
+            while (!frontier.empty() && !added) {
+                const size_t at = q.below(frontier.size());
+                const auto pick = frontier[at];
+                spec.tables.push_back(pick.first);
+                spec.via.push_back(pick.second);
+                const uint64_t cap = std::max<uint64_t>(largest, p.tables[pick.first].num_rows);
+                if (spec.tables.size() == 2 || schema20_count(spec, parent, prow) <= double(cap)) {
+                    in[pick.first] = 1;
+                    largest = cap;
+                    added = true;
+                } else {
+                    spec.tables.pop_back();
+                    spec.via.pop_back();
+                    frontier.erase(frontier.begin() + at);
+                }
+            }
+            if (!added) break;
+        }
+        for (size_t i = 0; i < spec.tables.size(); i++) spec.payload.push_back(2 + uint32_t(q.below(3)));
+        const uint32_t nout = 1 + uint32_t(q.below(4));
+        for (uint32_t o = 0; o < nout; o++)
+            spec.out.push_back({uint32_t(q.below(spec.tables.size())), q.below(4) == 0 ? 0u : 1u});
+        queries.push_back(std::move(spec));
+    }
+}
+
+// The plan of one schema20 query: scans output (c0, c1, payload) per table;
+// each join appends a table joined on its edge to an earlier one (child's c1
+// = parent's c0) and keeps every attribute; the root projects the query's
+// outputs.
+void schema20_plan(const QuerySpec& q, const std::vector<uint32_t>& parent, std::vector<bj_node>& nodes,
+                   std::vector<std::vector<bj_attr>>& attrs, uint64_t& root) {
+    nodes.clear();
+    attrs.clear();
+    auto type_of = [](uint32_t c) { return c == 3 ? BJ_FP64 : c == 4 ? BJ_VARCHAR : BJ_INT32; };
+    std::vector<uint32_t> base;  // attribute index of each table's c0 in the growing join output
+    std::vector<bj_attr> acc;    // the growing join output
+    uint64_t left = 0;
+    for (size_t i = 0; i < q.tables.size(); i++) {
+        const uint32_t t = q.tables[i];
+        nodes.push_back(scan_node(t));
+        attrs.push_back({{0, BJ_INT32, 0}, {1, BJ_INT32, 0}, {q.payload[i], type_of(q.payload[i]), 0}});
+        const uint64_t scan = nodes.size() - 1;
+        if (i == 0) {
+            left = scan;
+            base.push_back(0);
+            acc = attrs.back();
+            for (uint32_t a = 0; a < 3; a++) acc[a].index = a;
+            continue;
+        }
+        // Join the new table with its neighbour v (position j): child.c1 = parent.c0.
+        const uint32_t v = q.via[i];
+        size_t j = 0;
+        while (q.tables[j] != v) j++;
+        uint64_t la, ra;
+        if (parent[t] == v && t != v) {  // t is v's child
+            la = base[j] + 0;            // v.c0
+            ra = 1;                      // t.c1
+        } else {                         // t is v's parent
+            la = base[j] + 1;            // v.c1
+            ra = 0;                      // t.c0
+        }
+        std::vector<bj_attr> out;
+        const uint32_t width = uint32_t(acc.size());
+        for (uint32_t a = 0; a < width + 3; a++) {
+            const int32_t ty = a < width ? acc[a].type : attrs[scan][a - width].type;
+            out.push_back({a, ty, 0});
+        }
+        nodes.push_back(join_node(left, scan, la, ra, true));
+        attrs.push_back(out);
+        base.push_back(width);
+        acc = out;
+        left = nodes.size() - 1;
+    }
+    // Root: the outputs (a table's key, or its payload).
+    std::vector<bj_attr> out;
+    for (const auto& [pos, what] : q.out) {
+        const uint32_t a = base[pos] + (what == 0 ? 0u : 2u);
+        out.push_back({a, acc[a].type, 0});
+    }
+    attrs[left] = out;  // the last join (queries have two tables or more) projects the outputs
+    root = left;
+}
+
 } // namespace
 
 // A plan over a prefix of a workload's tables (page arrays shared, not copied).
@@ -356,6 +585,7 @@ struct bjw_workload {
     bj_plan view{};
     std::string name;
     std::vector<std::unique_ptr<VariantPlan>> variants;  // by dimension count
+    std::vector<std::unique_ptr<VariantPlan>> queries;   // schema20: every query over the shared tables
 };
 
 struct bjw_pages {
@@ -369,12 +599,35 @@ int bjw_workload_create(const char* name, uint64_t seed, double scale, bjw_workl
         auto w = std::make_unique<bjw_workload>();
         std::string n(name ? name : "");
         w->name = n;
-        if (n == "join2")
+        if (n == "join2") {
             make_join2(w->plan, seed, scale);
-        else if (n == "snowflake")
+        } else if (n == "snowflake") {
             make_snowflake(w->plan, seed, scale);
-        else
+        } else if (n == "schema20") {
+            std::vector<uint32_t> parent;
+            std::vector<QuerySpec> specs;
+            make_schema20(w->plan, seed, scale, 256, parent, specs);
+            // Query 0 is the workload's own plan; every query is also a plan
+            // over the shared tables.
+            schema20_plan(specs[0], parent, w->plan.nodes, w->plan.attrs, w->plan.root);
+            w->view = w->plan.view();
+            for (const QuerySpec& q : specs) {
+                auto v = std::make_unique<VariantPlan>();
+                v->tables.assign(w->view.inputs, w->view.inputs + w->view.num_inputs);
+                uint64_t root = 0;
+                schema20_plan(q, parent, v->nodes, v->attrs, root);
+                for (size_t i = 0; i < v->nodes.size(); i++) {
+                    v->nodes[i].num_output_attrs = v->attrs[i].size();
+                    v->nodes[i].output_attrs = v->attrs[i].data();
+                }
+                v->view = bj_plan{v->nodes.size(), v->nodes.data(), v->tables.size(), v->tables.data(), root};
+                w->queries.push_back(std::move(v));
+            }
+            *out = w.release();
+            return BJ_OK;
+        } else {
             return BJ_ERR_INVALID;
+        }
         w->view = w->plan.view();
         *out = w.release();
         return BJ_OK;
@@ -429,6 +682,14 @@ const bj_plan* bjw_workload_variant(bjw_workload* w, int dims) {
         v->view = bj_plan{v->nodes.size(), v->nodes.data(), v->tables.size(), v->tables.data(), left};
     }
     return &v->view;
+}
+
+uint64_t bjw_workload_num_queries(bjw_workload* w) { return w ? (w->queries.empty() ? 1 : w->queries.size()) : 0; }
+
+const bj_plan* bjw_workload_query(bjw_workload* w, uint64_t k) {
+    if (!w) return nullptr;
+    if (w->queries.empty()) return k == 0 ? &w->view : nullptr;
+    return k < w->queries.size() ? &w->queries[k]->view : nullptr;
 }
 
 uint64_t bjw_workload_scan_bytes(bjw_workload* w) {

@@ -19,6 +19,13 @@
  *               contest applies SQL filters at load time. Output: two
  *               dimension strings and two fact keys.
  *
+ *   "schema20"  20 tables in a random PK-FK tree (10K-40M rows before a
+ *               per-table filter of selectivity log-uniform in [0.1%, 100%];
+ *               FKs uniform or Zipf(0.8-1.5) over the parent's keys; columns:
+ *               INT32 key, INT32 FK, INT32 / FP64 / VARCHAR payloads) and 256
+ *               random acyclic queries of 2-12 tables over them
+ *               (bjw_workload_query); the workload's plan is query 0.
+ *
  * `scale` multiplies every row count (1.0 = the sizes above).
  */
 #ifndef B200JOIN_WORKLOADS_H
@@ -44,6 +51,10 @@ BJ_API const bj_plan* bjw_workload_plan(bjw_workload* w);
  * four fact keys and the joined dimensions' names. NULL for other workloads.
  * Valid until bjw_workload_free. */
 BJ_API const bj_plan* bjw_workload_variant(bjw_workload* w, int dims);
+/* Queries of the workload (1 except for "schema20") and query k (valid until
+ * bjw_workload_free; NULL when k is out of range). */
+BJ_API uint64_t bjw_workload_num_queries(bjw_workload* w);
+BJ_API const bj_plan* bjw_workload_query(bjw_workload* w, uint64_t k);
 /* Total bytes of input pages the plan's scans read. */
 BJ_API uint64_t bjw_workload_scan_bytes(bjw_workload* w);
 BJ_API void bjw_workload_free(bjw_workload* w);
