@@ -14,6 +14,9 @@
 //       one JSON line.
 //   ref_runner benchfile <plan.bjplan> <warmup> <steps>
 //       same timing on a plan file.
+//   ref_runner batch <workload> <seed> <scale> <passes>
+//       every query of a batched workload ("schema20") once per pass, one
+//       context for all; print queries/s and per-query latency as JSON.
 #include <plan.h>
 
 #include "../contest-sigmod2025_b200/csrc/workloads.h"
@@ -25,6 +28,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -110,6 +114,34 @@ int bench(const bj_plan& p, int warmup, int steps, const char* out_path, const c
     return 0;
 }
 
+int batch(bjw_workload* w, int passes, const char* label) {
+    const uint64_t n = bjw_workload_num_queries(w);
+    std::vector<std::unique_ptr<BorrowedPlan>> plans;
+    for (uint64_t k = 0; k < n; k++) plans.push_back(std::make_unique<BorrowedPlan>(*bjw_workload_query(w, k)));
+    void* ctx = Contest::build_context();
+    std::vector<double> ms;
+    uint64_t rows = 0;
+    const auto start = std::chrono::steady_clock::now();
+    for (int pass = 0; pass < passes; pass++)
+        for (auto& bp : plans) {
+            auto t0 = std::chrono::steady_clock::now();
+            ColumnarTable r = Contest::execute(bp->plan, ctx);
+            auto t1 = std::chrono::steady_clock::now();
+            rows += r.num_rows;
+            ms.push_back(std::chrono::duration<double, std::milli>(t1 - t0).count());
+        }
+    const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+    Contest::destroy_context(ctx);
+    std::vector<double> sorted = ms;
+    std::sort(sorted.begin(), sorted.end());
+    auto at = [&](double q) { return sorted.empty() ? 0.0 : sorted[std::min(sorted.size() - 1, size_t(q * sorted.size()))]; };
+    std::printf("{\"workload\": \"%s\", \"threads\": %d, \"queries\": %zu, \"rows\": %llu, \"seconds\": %.4f, "
+                "\"queries_per_s\": %.2f, \"p50_ms\": %.4f, \"p99_ms\": %.4f}\n",
+                label, cores(), ms.size(), (unsigned long long)rows, total, total > 0 ? ms.size() / total : 0.0,
+                at(0.5), at(0.99));
+    return 0;
+}
+
 } // namespace
 
 int main(int argc, char** argv) {
@@ -138,6 +170,16 @@ int main(int argc, char** argv) {
             bjw_workload_free(w);
             return rc;
         }
+        if (argc >= 6 && std::string(argv[1]) == "batch") {
+            bjw_workload* w = nullptr;
+            if (bjw_workload_create(argv[2], std::stoull(argv[3]), std::stod(argv[4]), &w) != 0) {
+                std::fprintf(stderr, "cannot build workload %s\n", argv[2]);
+                return 2;
+            }
+            int rc = batch(w, std::stoi(argv[5]), argv[2]);
+            bjw_workload_free(w);
+            return rc;
+        }
         if (argc >= 5 && std::string(argv[1]) == "benchfile") {
             plan_io::OwnedPlan op;
             plan_io::Reader rd(argv[2]);
@@ -149,6 +191,6 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "ref_runner: %s\n", e.what());
         return 3;
     }
-    std::fprintf(stderr, "usage: ref_runner run <plan> <out> | bench <workload> <seed> <scale> <warmup> <steps> [out] | benchfile <plan> <warmup> <steps>\n");
+    std::fprintf(stderr, "usage: ref_runner run <plan> <out> | bench <workload> <seed> <scale> <warmup> <steps> [out] | benchfile <plan> <warmup> <steps> | batch <workload> <seed> <scale> <passes>\n");
     return 1;
 }
