@@ -256,6 +256,7 @@ void phase_stats(const std::vector<cudaEvent_t>& marks, bj_stats& st) {
 // A repeated resident query captured into a CUDA graph.
 struct GraphEntry {
     std::vector<uint64_t> key;               // plan, resident handles, flags
+    uint64_t hash = 0;                       // of key
     std::vector<bj_resident*> tables;
     ReadbackTape tape;
     cudaGraphExec_t exec = nullptr;
@@ -292,7 +293,8 @@ struct bj_context {
     ReadbackTape* tape = nullptr;
     bool graph_output = false;       // result pages stay in the arena (graph capture)
     bool graphs = true;              // replay repeated resident queries as CUDA graphs
-    std::vector<std::unique_ptr<GraphEntry>> graph_cache;
+    std::vector<std::unique_ptr<GraphEntry>> graph_cache;  // least recently used first
+    static constexpr size_t kGraphCache = 1024;  // graphs kept: a batch of 256 distinct queries replays whole
     bool zero_copy = true;  // read pinned, contiguous input columns in place
     static constexpr int kSideStreams = 4;
     cudaStream_t side[kSideStreams] = {};  // independent build pipelines run here
@@ -2120,12 +2122,21 @@ int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* co
                            bj_result** out) {
     ctx->drain_releases();
     std::vector<uint64_t> key = graph_key(*plan, tables, flags & ~BJ_RESULT_ASYNC, ctx->profile);
+    uint64_t hash = 0x9e3779b97f4a7c15ull;
+    for (uint64_t v : key) hash = (hash ^ v) * 0x100000001b3ull + (hash >> 29);
     GraphEntry* g = nullptr;
-    for (auto& e : ctx->graph_cache)
-        if (e->key == key) g = e.get();
+    auto& gc = ctx->graph_cache;
+    for (size_t i = gc.size(); i-- > 0;)
+        if (gc[i]->hash == hash && gc[i]->key == key) {
+            // Most recently used goes last.
+            std::rotate(gc.begin() + i, gc.begin() + i + 1, gc.end());
+            g = gc.back().get();
+            break;
+        }
     if (!g) {
         auto e = std::make_unique<GraphEntry>();
         e->key = std::move(key);
+        e->hash = hash;
         e->tables.assign(tables, tables + plan->num_inputs);
         ctx->tape = &e->tape;
         ctx->tape_mode = 1;
@@ -2133,11 +2144,11 @@ int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* co
         ctx->tape_mode = 0;
         ctx->tape = nullptr;
         if (st == BJ_OK) {
-            if (ctx->graph_cache.size() >= 64) {
-                destroy_graph(*ctx->graph_cache.front());
-                ctx->graph_cache.erase(ctx->graph_cache.begin());
+            if (gc.size() >= bj_context::kGraphCache) {
+                destroy_graph(*gc.front());
+                gc.erase(gc.begin());
             }
-            ctx->graph_cache.push_back(std::move(e));
+            gc.push_back(std::move(e));
         }
         return st;
     }

@@ -25,18 +25,23 @@ def test_schema20_queries_from_host_pages(pkg, ctx, oracle, schema20):
 
 
 def test_schema20_batch_resident(pkg, ctx, oracle, schema20):
+    """The batch three times over resident tables: each query's first run
+    records, its second is captured into a CUDA graph, its third replays it
+    (the engine keeps the graphs of all 256 queries)."""
     plan = schema20.plan_ptr().contents
     res = [ctx.upload(plan.inputs[i]) for i in range(plan.num_inputs)]
+    wants = [oracle.execute(schema20.query_ptr(k)) for k in range(256)]
     try:
-        nonempty = 0
-        for k in range(256):
-            q = schema20.query_ptr(k)
-            want = oracle.execute(q)
-            with ctx.execute_resident(q, res) as r:
-                got, keep = r.table_struct()
-                nonempty += oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(),
-                                                        f"schema20 resident query {k}") > 0
-        assert nonempty > 200
+        for run in ("record", "capture", "replay"):
+            nonempty = 0
+            for k in range(256):
+                q = schema20.query_ptr(k)
+                with ctx.execute_resident(q, res, flags=pkg.RESULT_HOST | pkg.RESULT_ASYNC) as r:
+                    r.wait()
+                    got, keep = r.table_struct()
+                    nonempty += oracle_lib.assert_same_rows(oracle, ctypes.byref(got), wants[k].view(),
+                                                            f"schema20 resident query {k} ({run})") > 0
+            assert nonempty > 200
     finally:
         for x in res:
             x.free()
