@@ -85,3 +85,20 @@ def test_schema20_oracle_matches_reference_engine(pkg, oracle, schema20, k):
     ref_struct, keep = table_struct(pkg, ref)
     ora = oracle.execute(q)
     oracle_lib.assert_same_rows(oracle, ctypes.byref(ref_struct), ora.view(), f"schema20 query {k}")
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", [4, 5])
+def test_schema20_widest_queries_match_reference_engine(pkg, oracle, seed):
+    # Other schemas: the four queries with the most tables, compared with the
+    # reference engine.
+    w = pkg.Workload("schema20", seed, SCALE)
+    widest = sorted(range(256), key=lambda k: (-_tables(w.query_ptr(k)), k))[:4]
+    assert _tables(w.query_ptr(widest[-1])) >= 6
+    for k in widest:
+        q = w.query_ptr(k)
+        with tempfile.TemporaryDirectory() as tmp:
+            ref = run_reference(pkg, q, tmp)
+        ref_struct, keep = table_struct(pkg, ref)
+        ora = oracle.execute(q)
+        oracle_lib.assert_same_rows(oracle, ctypes.byref(ref_struct), ora.view(), f"schema20 seed {seed} query {k}")
