@@ -408,7 +408,7 @@ void make_schema20(plan_io::OwnedPlan& p, uint64_t seed, double scale, uint32_t 
     std::vector<std::vector<int32_t>> key(kSchemaTables);      // per table: c0 of its rows
     prow.assign(kSchemaTables, {});
     p.tables.resize(kSchemaTables);
-    for (uint32_t t = 0; t < kSchemaTables; t++) {
+    auto make_table = [&](uint32_t t) {
         const uint64_t n = rows[t];
         const auto keys = permutation(n, stream_seed(seed, 202, t, 0));
         Rng r(stream_seed(seed, 203, t, 0));
@@ -458,6 +458,17 @@ void make_schema20(plan_io::OwnedPlan& p, uint64_t seed, double scale, uint32_t 
         encode_any(tab.columns[2], BJ_INT32, c2.size(), c2.data(), nullptr, nullptr, nullptr);
         encode_any(tab.columns[3], BJ_FP64, c3.size(), c3.data(), nullptr, nullptr, nullptr);
         encode_any(tab.columns[4], BJ_VARCHAR, c0.size(), nullptr, nullptr, off.data(), bytes.data());
+    };
+    // A table needs its parent's rows: tables are made level by level of the
+    // tree, the tables of one level in parallel (each from its own streams).
+    std::vector<uint8_t> made(kSchemaTables, 0);
+    for (size_t left = kSchemaTables; left;) {
+        std::vector<uint32_t> level;
+        for (uint32_t t = 0; t < kSchemaTables; t++)
+            if (!made[t] && (t == 0 || made[parent[t]])) level.push_back(t);
+        parallel_for(level.size(), [&](size_t i) { make_table(level[i]); });
+        for (uint32_t t : level) made[t] = 1;
+        left -= level.size();
     }
     // Queries: a random connected set of 2-12 tables grown from a random table.
     std::vector<std::vector<uint32_t>> nbr(kSchemaTables);
@@ -465,8 +476,8 @@ void make_schema20(plan_io::OwnedPlan& p, uint64_t seed, double scale, uint32_t 
         nbr[t].push_back(parent[t]);
         nbr[parent[t]].push_back(t);
     }
-    queries.clear();
-    for (uint32_t k = 0; k < nqueries; k++) {
+    queries.assign(nqueries, QuerySpec{});
+    parallel_for(nqueries, [&](size_t k) {
         Rng q(stream_seed(seed, 204, k, 0));
         const uint32_t want = 2 + uint32_t(q.below(11));
         QuerySpec spec;
@@ -508,8 +519,8 @@ void make_schema20(plan_io::OwnedPlan& p, uint64_t seed, double scale, uint32_t 
         const uint32_t nout = 1 + uint32_t(q.below(4));
         for (uint32_t o = 0; o < nout; o++)
             spec.out.push_back({uint32_t(q.below(spec.tables.size())), q.below(4) == 0 ? 0u : 1u});
-        queries.push_back(std::move(spec));
-    }
+        queries[k] = std::move(spec);
+    });
 }
 
 // The plan of one schema20 query: scans output (c0, c1, payload) per table;
