@@ -65,3 +65,29 @@ def test_one_rank_needs_no_process_group():
     rep = _bench().Replicas(None, "cpu")
     rate, ms = rep.job_rate(10, 5.0)
     assert rep.world == 1 and ms == 5.0 and rate == pytest.approx(2000.0)
+
+
+REF_RUNNER = ROOT / "oracle" / "_ref" / "ref_runner"
+
+
+@pytest.mark.skipif(not REF_RUNNER.exists(), reason="reference engine not built (oracle/Makefile ref)")
+def test_reference_arm_prints_the_bench_line():
+    # `bench.py --impl reference` runs on host cores only: one JSON line with
+    # the bench's keys, its own e2e and cpu_baseline.
+    import json
+    import subprocess
+    import sys
+
+    p = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--scale", "0.02",
+                        "--steps", "3", "--warmup", "1"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["steps"] == 3 and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["rows"] > 0
