@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--e2e-steps", type=int, default=None)
-    ap.add_argument("--cpu-steps", type=int, default=3, help="0 skips the CPU baseline")
+    ap.add_argument("--cpu-steps", type=int, default=20, help="0 skips the CPU baseline")
     ap.add_argument("--serve-queries", type=int, default=2000,
                     help="queries per serving measurement (0 skips serving)")
     ap.add_argument("--serve-workers", type=int, default=8)
@@ -662,12 +662,12 @@ def main():
         "clocks": clk,
     }
     if world == 1 and args.cpu_steps > 0:
-        res, err = run_reference(args, args.cpu_steps, 1)
+        res, err = run_reference(args, args.cpu_steps, 5)
         if res:
             mean = statistics.fmean(res["times_ms"])
             out["cpu_baseline"] = {"value": 1000.0 / mean, "unit": "queries/s", "cores": res["threads"],
                                    "kind": "reference",
-                                   "sample": f"{args.cpu_steps} executions (+1 warm-up) of the full query by the "
+                                   "sample": f"{args.cpu_steps} executions (+5 warm-up) of the full query by the "
                                              f"reference engine, wall clock"}
         else:
             out["cpu_baseline"] = {"value": None, "unit": "queries/s", "cores": None, "kind": "reference",

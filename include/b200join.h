@@ -253,19 +253,25 @@ BJ_API const char* bj_version(void);
  * allocating any memory. No counterpart in the reference: it exists for
  * callers that cannot call cudaMalloc (their device memory belongs to another
  * allocator, or cudaMalloc's implicit device synchronisation is not allowed
- * where they run). The result equals bj_result_num_rows of bj_execute on
- * Scan(A) JOIN Scan(B) over these columns; NULL keys never match.
+ * where they run). On well-formed pages the result equals
+ * bj_result_num_rows of bj_execute on Scan(A) JOIN Scan(B) over these
+ * columns; NULL keys never match.
  *
  * build_pages / probe_pages: device addresses of the columns' 8 KiB pages,
  * back to back. build_rows: rows the build pages hold, at most 262144 (the
  * fixed scratch's capacity; larger counts return BJ_ERR_INVALID).
  * out_count: a device u64 that receives the count; stream: a cudaStream_t
- * (NULL = default stream). The call only enqueues work on `stream`.
+ * (NULL = default stream). The call only enqueues work on `stream`, so errors
+ * the kernels find cannot reach the return status: when a page header is not
+ * that of an INT32 page, or the build pages hold more non-null values than
+ * build_rows, *out_count receives ~0ull (UINT64_MAX) instead of a count.
  *
  * Scratch: a 4 MiB array compiled into the library, held by every GPU that
  * loads it until the process exits. The first call on a device looks up its
- * device address; make that first call before any stream capture. All calls
- * share the array: calls that overlap on the GPU race and give wrong counts. */
+ * device address; make that first call before any stream capture, and do not
+ * call it across a cudaDeviceReset (the cached address may go stale). All
+ * calls share the array: calls that overlap on the GPU race and give wrong
+ * counts. */
 BJ_API int bj_join_count_static(const void* build_pages, uint64_t build_num_pages, uint64_t build_rows,
                                 const void* probe_pages, uint64_t probe_num_pages,
                                 unsigned long long* out_count, void* stream);

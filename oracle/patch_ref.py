@@ -9,15 +9,17 @@ The reference engine targets Clang 18.  Two spots do not compile with g++ 13:
   `ext_vector_type(bool)`.  The copy computes the same mask with a scalar loop
   over the GCC vector lanes.
 
-Nothing is written outside oracle/_ref/, and /root/reference is only read.
+Nothing is written outside oracle/_ref/, and the reference sources are only read.
 This is test infrastructure for the oracle, not part of the product.
 """
 import pathlib
 import re
 import sys
 
-REF = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
-OUT = pathlib.Path(sys.argv[2] if len(sys.argv) > 2 else pathlib.Path(__file__).parent / "_ref" / "patched")
+if len(sys.argv) != 3:
+    sys.exit("usage: patch_ref.py <reference source root> <output dir>  (oracle/Makefile passes both)")
+REF = pathlib.Path(sys.argv[1])
+OUT = pathlib.Path(sys.argv[2])
 
 
 def patch_scheduler(text: str) -> str:
