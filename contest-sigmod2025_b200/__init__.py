@@ -108,10 +108,33 @@ ABI = {
     "bj_server_resident_free": (None, [_VP, _VP]),
     "bj_plan_explain": (_INT, [ctypes.POINTER(BjPlan), ctypes.c_char_p, _U64, ctypes.POINTER(_U64)]),
     "bj_result_wait": (_INT, [_VP]),
+    "bj_context_set_ordering": (_INT, [_VP, _INT, _VP]),
+    "bj_resident_set_base_rows": (_INT, [_VP, _U64]),
+    "bj_subplans": (_INT, [ctypes.POINTER(BjPlan), ctypes.c_uint32, _U64, _VP, ctypes.POINTER(_U64)]),
+    "bj_subplan_cards": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), _VP, _U64, _VP]),
+    "bj_subplan_sample_cards": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), _VP, _U64, _VP]),
+    "bj_subplan_features": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), _VP, _U64, _VP]),
+    "bj_join_order": (_INT, [ctypes.POINTER(BjPlan), _VP, _INT, ctypes.POINTER(ctypes.c_uint32),
+                             ctypes.POINTER(ctypes.c_double)]),
+    "bj_estimator_create": (_INT, [_INT, _U64, ctypes.POINTER(_VP)]),
+    "bj_estimator_destroy": (None, [_VP]),
+    "bj_estimator_num_params": (_U64, []),
+    "bj_estimator_get_params": (_INT, [_VP, _VP]),
+    "bj_estimator_set_params": (_INT, [_VP, _VP]),
+    "bj_estimator_train": (_INT, [_VP, _VP, _VP, _U64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _U64, _VP]),
+    "bj_estimator_predict": (_INT, [_VP, _VP, _U64, _VP]),
+    "bj_estimator_gradients": (_INT, [_VP, _VP, _VP, _U64, _VP, _VP]),
+    "bj_estimator_save": (_INT, [_VP, ctypes.c_char_p]),
+    "bj_estimator_load": (_INT, [_INT, ctypes.c_char_p, ctypes.POINTER(_VP)]),
 }
+
+ORDER_ROWS, ORDER_SAMPLING, ORDER_LEARNED = 0, 1, 2
+EST_FEATURES, EST_HIDDEN, EST_MAX_TABLES = 1792, 256, 12
 
 WORKLOAD_ABI = {
     "bjw_workload_create": (_INT, [ctypes.c_char_p, _U64, ctypes.c_double, ctypes.POINTER(_VP)]),
+    "bjw_workload_create_queries": (_INT, [ctypes.c_char_p, _U64, ctypes.c_double, _U64, ctypes.POINTER(_VP)]),
+    "bjw_workload_base_rows": (_U64, [_VP, _U64]),
     "bjw_workload_load": (_INT, [ctypes.c_char_p, ctypes.POINTER(_VP)]),
     "bjw_workload_plan": (ctypes.POINTER(BjPlan), [_VP]),
     "bjw_workload_scan_bytes": (_U64, [_VP]),
@@ -385,10 +408,13 @@ def read_table_file(path: str) -> ColumnarTable:
 class Workload:
     """A seeded synthetic workload built by libb200join_workloads.so."""
 
-    def __init__(self, name: str, seed: int, scale: float = 1.0, path: Optional[str] = None):
+    def __init__(self, name: str, seed: int, scale: float = 1.0, path: Optional[str] = None,
+                 queries: Optional[int] = None):
         h = ctypes.c_void_p()
         if path:
             st = wlib().bjw_workload_load(path.encode(), ctypes.byref(h))
+        elif queries is not None:
+            st = wlib().bjw_workload_create_queries(name.encode(), seed, scale, queries, ctypes.byref(h))
         else:
             st = wlib().bjw_workload_create(name.encode(), seed, scale, ctypes.byref(h))
         if st != 0:
@@ -401,6 +427,10 @@ class Workload:
 
     def scan_bytes(self) -> int:
         return wlib().bjw_workload_scan_bytes(self.handle)
+
+    def base_rows(self, table: int) -> int:
+        """Rows of input `table` before its load-time filter (schema20)."""
+        return wlib().bjw_workload_base_rows(self.handle, table)
 
     def num_queries(self) -> int:
         return wlib().bjw_workload_num_queries(self.handle)
@@ -514,6 +544,10 @@ class Resident:
     def __init__(self, ctx: "Context", handle):
         self._ctx, self.handle = ctx, handle
 
+    def set_base_rows(self, base_rows: int) -> None:
+        """Rows before the load-time filter (the estimator's selectivity feature)."""
+        lib().bj_resident_set_base_rows(self.handle, base_rows)
+
     def free(self):
         if self.handle:
             lib().bj_resident_free(self._ctx.handle, self.handle)
@@ -570,6 +604,36 @@ class Context:
     def stream(self) -> int:
         return lib().bj_context_stream(self.handle) or 0
 
+    def set_ordering(self, mode: int, estimator: Optional["Estimator"] = None) -> None:
+        """Join ordering of resident queries: ORDER_ROWS, ORDER_SAMPLING or
+        ORDER_LEARNED (with an estimator; sampling is its fallback)."""
+        self._check(lib().bj_context_set_ordering(self.handle, mode, estimator.handle if estimator else None),
+                    "bj_context_set_ordering")
+
+    def _subplan_call(self, fn, plan, residents, masks, out, what):
+        import numpy as np
+        m = np.ascontiguousarray(masks, dtype=np.uint32)
+        arr = (ctypes.c_void_p * max(len(residents), 1))(*[x.handle for x in residents])
+        p = plan.ref() if isinstance(plan, CPlan) else plan
+        self._check(fn(self.handle, p, arr, m.ctypes.data, len(m), out.ctypes.data), what)
+        return out
+
+    def subplan_cards(self, plan, residents, masks):
+        """Exact cardinality of each sub-plan (device counts)."""
+        import numpy as np
+        return self._subplan_call(lib().bj_subplan_cards, plan, residents, masks,
+                                  np.zeros(len(masks), dtype=np.float64), "bj_subplan_cards")
+
+    def subplan_sample_cards(self, plan, residents, masks):
+        import numpy as np
+        return self._subplan_call(lib().bj_subplan_sample_cards, plan, residents, masks,
+                                  np.zeros(len(masks), dtype=np.float64), "bj_subplan_sample_cards")
+
+    def subplan_features(self, plan, residents, masks):
+        import numpy as np
+        return self._subplan_call(lib().bj_subplan_features, plan, residents, masks,
+                                  np.zeros((len(masks), EST_FEATURES), dtype=np.float32), "bj_subplan_features")
+
     def profile(self, on: bool) -> None:
         lib().bj_context_profile(self.handle, 1 if on else 0)
 
@@ -583,6 +647,158 @@ class Context:
 
     def __exit__(self, *a):
         self.close()
+
+
+def subplans(plan, max_tables: int = EST_MAX_TABLES):
+    """Connected input sets of a plan (bit masks over its scans in depth-first
+    order, left child first), ascending."""
+    import numpy as np
+    p = plan.ref() if isinstance(plan, CPlan) else plan
+    n = ctypes.c_uint64()
+    st = lib().bj_subplans(p, max_tables, 0, None, ctypes.byref(n))
+    if st != 0:
+        raise EngineError(st, "bj_subplans")
+    out = np.zeros(max(n.value, 1), dtype=np.uint32)
+    st = lib().bj_subplans(p, max_tables, n.value, out.ctypes.data, ctypes.byref(n))
+    if st != 0:
+        raise EngineError(st, "bj_subplans")
+    return out[:n.value]
+
+
+def join_order(plan, cards=None, driver: int = -1):
+    """(driver, cost) of the executor's cheapest plan under set cardinalities
+    cards[mask] (None: the row-count model); driver >= 0 costs that driver."""
+    import numpy as np
+    p = plan.ref() if isinstance(plan, CPlan) else plan
+    c = None if cards is None else np.ascontiguousarray(cards, dtype=np.float64)
+    d, cost = ctypes.c_uint32(), ctypes.c_double()
+    st = lib().bj_join_order(p, None if c is None else c.ctypes.data, driver, ctypes.byref(d), ctypes.byref(cost))
+    if st != 0:
+        raise EngineError(st, "bj_join_order")
+    return d.value, cost.value
+
+
+class Estimator:
+    """The learned cardinality estimator (bj_estimator_*): a BF16 MLP trained
+    and run on the device by the library's own kernels."""
+
+    def __init__(self, device: int = 0, seed: int = 0, path: Optional[str] = None):
+        h = ctypes.c_void_p()
+        if path:
+            st = lib().bj_estimator_load(device, path.encode(), ctypes.byref(h))
+        else:
+            st = lib().bj_estimator_create(device, seed, ctypes.byref(h))
+        if st != 0:
+            raise EngineError(st, "cannot create the estimator")
+        self.handle = h
+
+    @staticmethod
+    def num_params() -> int:
+        return lib().bj_estimator_num_params()
+
+    def params(self):
+        import numpy as np
+        out = np.zeros(self.num_params(), dtype=np.float32)
+        st = lib().bj_estimator_get_params(self.handle, out.ctypes.data)
+        if st != 0:
+            raise EngineError(st, "bj_estimator_get_params")
+        return out
+
+    def set_params(self, p) -> None:
+        import numpy as np
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        assert a.size == self.num_params()
+        st = lib().bj_estimator_set_params(self.handle, a.ctypes.data)
+        if st != 0:
+            raise EngineError(st, "bj_estimator_set_params")
+
+    def train(self, features, targets, epochs: int = 30, batch: int = 256, lr: float = 1e-3, seed: int = 0):
+        import numpy as np
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        losses = np.zeros(epochs, dtype=np.float32)
+        st = lib().bj_estimator_train(self.handle, f.ctypes.data, t.ctypes.data, len(t), epochs, batch, lr, seed,
+                                      losses.ctypes.data)
+        if st != 0:
+            raise EngineError(st, "bj_estimator_train")
+        return losses
+
+    def predict(self, features):
+        import numpy as np
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        out = np.zeros(len(f), dtype=np.float32)
+        st = lib().bj_estimator_predict(self.handle, f.ctypes.data, len(f), out.ctypes.data)
+        if st != 0:
+            raise EngineError(st, "bj_estimator_predict")
+        return out
+
+    def gradients(self, features, targets):
+        import numpy as np
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        g = np.zeros(self.num_params(), dtype=np.float32)
+        st = lib().bj_estimator_gradients(self.handle, f.ctypes.data, t.ctypes.data, len(t), loss.ctypes.data,
+                                          g.ctypes.data)
+        if st != 0:
+            raise EngineError(st, "bj_estimator_gradients")
+        return float(loss[0]), g
+
+    def save(self, path: str) -> None:
+        st = lib().bj_estimator_save(self.handle, path.encode())
+        if st != 0:
+            raise EngineError(st, "bj_estimator_save")
+
+    def close(self):
+        if self.handle:
+            lib().bj_estimator_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def q_error(est, true):
+    """max(est / true, true / est) with both floored at 1 (the usual q-error)."""
+    import numpy as np
+    e = np.maximum(np.asarray(est, dtype=np.float64), 1.0)
+    t = np.maximum(np.asarray(true, dtype=np.float64), 1.0)
+    return np.maximum(e / t, t / e)
+
+
+def subplan_corpus(ctx: "Context", workload: "Workload", residents, queries, max_per_query: int = 256, seed: int = 0,
+                   with_features: bool = True):
+    """Sub-plans of the given queries of a batched workload over its resident
+    tables, labelled with their exact cardinalities (device counts): returns a
+    dict of arrays `features` (n x EST_FEATURES; absent without
+    with_features), `card` (exact), `sample` (sampling estimates), `query`,
+    `mask`. A query with more than max_per_query sub-plans of two or more
+    inputs contributes a seeded random choice of them."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    feats, cards, samples, qids, masks = [], [], [], [], []
+    for k in queries:
+        plan = workload.query_ptr(k)
+        m = subplans(plan, EST_MAX_TABLES)
+        m = m[[bin(int(x)).count("1") >= 2 for x in m]]
+        if len(m) > max_per_query:
+            m = np.sort(rng.choice(m, max_per_query, replace=False))
+        if len(m) == 0:
+            continue
+        cards.append(ctx.subplan_cards(plan, residents, m))
+        samples.append(ctx.subplan_sample_cards(plan, residents, m))
+        if with_features:
+            feats.append(ctx.subplan_features(plan, residents, m))
+        qids.append(np.full(len(m), k, dtype=np.int64))
+        masks.append(m)
+    out = {"card": np.concatenate(cards), "sample": np.concatenate(samples), "query": np.concatenate(qids),
+           "mask": np.concatenate(masks)}
+    if with_features:
+        out["features"] = np.concatenate(feats)
+    return out
 
 
 class ServerResident:

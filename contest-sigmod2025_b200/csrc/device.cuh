@@ -168,6 +168,15 @@ BJ_HD uint64_t mix64(uint64_t x) {
     return x;
 }
 
+// Hash of a join-key slot of either width. An INT32 key (zero-extended in
+// its slot) hashes as the reference's does; an INT64 key, which has no
+// reference counterpart (the reference reads every join key as 32 bits,
+// engine/op/TableScan.cpp:328), is mixed with the murmur3 finaliser first and
+// then multiplied like a 32-bit key, so its high bits reach the bucket bits.
+BJ_HD uint64_t key_hash_any(uint64_t key, int32_t type) {
+    return type == kInt32 ? key_hash(uint32_t(key)) : mix64(key) * 0x9E3779B97F4A7C15ull;
+}
+
 // Blocked bloom filter: one 32-bit word per key with up to four bits set.
 // The word is the top log2w bits (at most 15, so a filter is at most 128 KiB
 // and fits in shared memory) of the high half hh of the key hash. The bits

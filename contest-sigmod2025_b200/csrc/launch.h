@@ -318,6 +318,118 @@ struct SampleSet {
 };
 int sample_probes(const SampleSet& set, uint32_t nsample, uint32_t* hits, cudaStream_t st);
 
+// ---- join-ordering statistics (k_stats.cu) ----
+// Open-addressing map from a key slot (u64) to a u64 value: keys[i] = ~0ull
+// marks an empty slot; the key ~0ull itself keeps its value in vals[cap].
+// cap = 1 << log2cap; keys has cap words, vals cap + 1.
+struct KeyMap {
+    unsigned long long* keys;
+    unsigned long long* vals;
+    uint32_t log2cap;
+};
+constexpr int kHistBins = 64;
+int map_clear(const KeyMap& m, cudaStream_t st);
+// Statistics of a join-key column (INT32 or INT64): hist[64] (zero before)
+// counts non-null values by the top six bits of their key hash; m (cleared)
+// receives key -> count; totals[0] += non-null values, totals[1] += distinct
+// keys (both zero before).
+int column_stats(const DevColumn& c, const KeyMap& m, uint32_t* hist, unsigned int* totals, uint32_t* err,
+                 int num_sms, cudaStream_t st);
+// One table of a sub-plan's exact count. For every row r: w = product over
+// the children j of ch[j].map[value of ch[j].key at r] (0 when the value is
+// NULL or absent); then, with has_out, out[value of pkey at r] += w (rows
+// with a NULL pkey skipped), else *total += w. flags[0] |= 1 when a weight
+// or the total passes 2^64 - 1.
+constexpr int kMaxCountChildren = 12;
+struct CountChild {
+    DevColumn key;  // this table's column on the edge to the child
+    KeyMap map;     // child's key -> weight
+};
+struct CountNode {
+    CountChild ch[kMaxCountChildren];
+    int nch;
+    int has_out;
+    DevColumn pkey;  // this table's column on the edge to its parent
+    KeyMap out;
+    uint32_t nrows;
+    unsigned long long* total;
+    unsigned int* flags;
+};
+int count_node(const CountNode& n, uint32_t* err, int num_sms, cudaStream_t st);
+// Join samples: for directed edge d, hits[d] (zero before) = how many of
+// nsample seeded rows of e[d].key have a non-null value present in e[d].map.
+constexpr int kMaxSampleEdges = 24;
+struct SampleEdge {
+    DevColumn key;
+    KeyMap map;
+    uint32_t seed;
+};
+struct SampleEdges {
+    SampleEdge e[kMaxSampleEdges];
+    int n;
+};
+int sample_edges(const SampleEdges& e, uint32_t nsample, uint32_t* hits, cudaStream_t st);
+
+// ---- learned cardinality estimator (k_mlp.cu) ----
+// BF16 matrices are passed as raw 16-bit words. C (M x N) = A (M x K) B (K x N)
+// on the tensor cores, FP32 accumulation; A(m, k) = A[m * a_rs + k * a_cs],
+// B(k, n) = B[k * b_rs + n * b_cs], one stride of each being 1 and the other
+// a multiple of 8. K must be a multiple of 32 and N of 64; an operand whose
+// contiguous dimension is its rows (m for A, n for B) needs those rows a
+// multiple of 8.
+constexpr int kMlpHidden = 256;
+enum GemmEpi : int {
+    kEpiBiasRelu = 0,  // Cb = bf16(relu(acc + bias[n]))
+    kEpiReluMask = 1,  // Cb = bf16(mask[m, n] > 0 ? acc : 0), mask laid out like C
+    kEpiStoreF32 = 2,  // Cf = acc
+};
+struct GemmArgs {
+    const uint16_t* A;
+    long a_rs, a_cs;
+    const uint16_t* B;
+    long b_rs, b_cs;
+    int M, N, K;
+    int epi;
+    const uint16_t* bias;
+    const uint16_t* mask;
+    uint16_t* Cb;
+    float* Cf;
+    long ldc;
+};
+int gemm_bf16(const GemmArgs& g, cudaStream_t st);
+// Output layer (one CTA per row): y = H2 . w3 + b3; with targets t, loss +=
+// (y - t)^2 and, for rows below n_real, dy = 2 (y - t) / n_real and dH2 =
+// bf16(dy * w3 * [H2 > 0]) (zero for the other rows). Optional outputs may
+// be null.
+struct MlpHeadArgs {
+    const uint16_t* H2;
+    const uint16_t* w3;
+    const uint16_t* b3;
+    const float* t;
+    float* y;
+    float* loss;
+    float* dy;
+    uint16_t* dH2;
+    int n_real;
+};
+int mlp_head(const MlpHeadArgs& a, int rows, cudaStream_t st);
+// out[n] += sum over rows of X[m][n] (times dy[m] when dy is given).
+int colsum(const uint16_t* X, const float* dy, int rows, int cols, float* out, cudaStream_t st);
+int sum_f32(const float* v, int n, float* out, cudaStream_t st);
+struct AdamArgs {
+    float* w;
+    uint16_t* wb;
+    const float* grad;
+    float* m;
+    float* v;
+    long n;
+    float lr, beta1, beta2, eps, bc1, bc2;  // bc: 1 - beta^t
+};
+int adam_step(const AdamArgs& a, cudaStream_t st);
+int f32_to_bf16(const float* in, uint16_t* out, long n, cudaStream_t st);
+int gather_rows(const uint16_t* src, const float* tsrc, const uint32_t* idx, int n, int n_pad, int cols, uint16_t* dst,
+                float* tdst, cudaStream_t st);
+
 // ---- output pages (k_output.cu) ----
 // Page descriptors of a VARCHAR column.
 constexpr uint32_t kStrBlock = 4096;

@@ -117,13 +117,14 @@ struct Importer {
 // kMaxDpInputs inputs take the largest input.
 constexpr uint32_t kMaxDpInputs = 14;
 
-uint32_t choose_driver(const std::vector<double>& card, const std::vector<Edge>& edges, double& cost) {
+uint32_t choose_driver(const std::vector<double>& card, const std::vector<Edge>& edges, double& cost,
+                       const std::vector<double>* set_card = nullptr, int forced_driver = -1) {
     const uint32_t n = uint32_t(card.size());
     uint32_t largest = 0;
     for (uint32_t i = 1; i < n; i++)
         if (card[i] > card[largest]) largest = i;
     cost = -1;
-    if (n == 1 || n > kMaxDpInputs) return largest;
+    if (n == 1 || n > kMaxDpInputs) return forced_driver >= 0 ? uint32_t(forced_driver) : largest;
     std::vector<uint32_t> nbr(n, 0);
     for (const Edge& e : edges) {
         nbr[e.a] |= 1u << e.b;
@@ -149,10 +150,12 @@ uint32_t choose_driver(const std::vector<double>& card, const std::vector<Edge>&
         const uint32_t low = __builtin_ctz(S);
         setcard[S] = std::max(setcard[S & (S - 1)], card[low]);
         if (S == (1u << low)) {
-            best[size_t(S) * n + low] = card[low];
+            best[size_t(S) * n + low] = set_card ? (*set_card)[S] : card[low];
+            if (set_card) setcard[S] = (*set_card)[S];
             continue;
         }
         if (reach(low, S) != S) continue;  // not connected
+        if (set_card) setcard[S] = (*set_card)[S];
         for (uint32_t ds = S; ds; ds &= ds - 1) {
             const uint32_t d = __builtin_ctz(ds);
             double c = inf;
@@ -172,6 +175,7 @@ uint32_t choose_driver(const std::vector<double>& card, const std::vector<Edge>&
         const double c = best[size_t(full) * n + d], cb = best[size_t(full) * n + driver];
         if (c < cb || (c == cb && (card[d] > card[driver] || (card[d] == card[driver] && d < driver)))) driver = d;
     }
+    if (forced_driver >= 0 && uint32_t(forced_driver) < n) driver = uint32_t(forced_driver);
     cost = best[size_t(full) * n + driver];
     return driver;
 }
@@ -280,7 +284,51 @@ double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge
 
 } // namespace
 
-int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err, bool reference_cost) {
+int plan_graph(const bj_plan& plan, PlanGraph& g, std::string& err) {
+    g = PlanGraph{};
+    ExecPlan ex;
+    if (plan.num_nodes == 0 || !plan.nodes || (plan.num_inputs && !plan.inputs)) {
+        err = "empty plan or missing inputs";
+        return BJ_ERR_INVALID;
+    }
+    Importer im{plan, ex, {}, {}, {}, BJ_OK};
+    std::vector<uint32_t> root_attrs;
+    if (!im.rec(plan.root, root_attrs, 0)) {
+        err = im.err;
+        return im.status;
+    }
+    for (const PlanInput& in : ex.inputs) g.inputs.push_back({in.table, in.rows});
+    for (const Edge& e : im.edges)
+        g.edges.push_back({e.a, e.b, ex.attrs[e.attr_a].column, ex.attrs[e.attr_b].column, ex.attrs[e.attr_a].type});
+    return BJ_OK;
+}
+
+int join_order(const bj_plan& plan, const std::vector<double>* set_card, int forced_driver, uint32_t& driver,
+               double& cost, std::string& err) {
+    ExecPlan ex;
+    if (plan.num_nodes == 0 || !plan.nodes || (plan.num_inputs && !plan.inputs)) {
+        err = "empty plan or missing inputs";
+        return BJ_ERR_INVALID;
+    }
+    Importer im{plan, ex, {}, {}, {}, BJ_OK};
+    std::vector<uint32_t> root_attrs;
+    if (!im.rec(plan.root, root_attrs, 0)) {
+        err = im.err;
+        return im.status;
+    }
+    const uint32_t ni = uint32_t(ex.inputs.size());
+    if (set_card && set_card->size() < (size_t(1) << std::min<uint32_t>(ni, 31))) {
+        err = "set cardinalities: fewer than 2^inputs entries";
+        return BJ_ERR_INVALID;
+    }
+    std::vector<double> card(ni);
+    for (uint32_t i = 0; i < ni; i++) card[i] = double(ex.inputs[i].rows);
+    driver = choose_driver(card, im.edges, cost, set_card, forced_driver);
+    return BJ_OK;
+}
+
+int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err, bool reference_cost,
+                   const std::vector<double>* set_card) {
     ex = ExecPlan{};
     if (plan.num_nodes == 0 || !plan.nodes) {
         err = "empty plan";
@@ -309,7 +357,8 @@ int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err, bool ref
     // an input: its row count).
     std::vector<double> card(ni);
     for (uint32_t i = 0; i < ni; i++) card[i] = double(ex.inputs[i].rows);
-    const uint32_t driver = choose_driver(card, im.edges, ex.est_cost);
+    if (set_card && set_card->size() < (size_t(1) << std::min<uint32_t>(ni, 31))) set_card = nullptr;
+    const uint32_t driver = choose_driver(card, im.edges, ex.est_cost, set_card);
     ex.driver = driver;
     if (reference_cost) ex.ref_cost = reference_dp_cost(card, im.edges, &ex.ref_plan);
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> adj(ni);  // (neighbour, edge)

@@ -74,6 +74,38 @@ struct ExecPlan {
 // Builds the execution plan; returns BJ_OK or a status with `err` set.
 // reference_cost: also cost the reference's plan space (ExecPlan::ref_cost;
 // for bj_plan_explain, not needed to run the plan).
-int make_exec_plan(const bj_plan& plan, ExecPlan& out, std::string& err, bool reference_cost = false);
+// set_card (optional): estimated cardinality of every set of inputs, indexed
+// by the bit mask of its inputs (inputs numbered in scan order, see
+// PlanGraph), 2^n entries; entries of sets that are not connected are never
+// read. Without it, a set's cardinality is its largest input's row count
+// (the reference's model, engine/query/QueryGraph.cpp:53-68).
+int make_exec_plan(const bj_plan& plan, ExecPlan& out, std::string& err, bool reference_cost = false,
+                   const std::vector<double>* set_card = nullptr);
+
+// The join graph of a plan: its scans (inputs, numbered in the order a
+// depth-first walk from the root reaches them, left child first) and one
+// edge per join node. A plan's joins always form a tree over its scans.
+struct PlanGraph {
+    struct Input {
+        uint32_t table;  // base table id
+        uint64_t rows;
+    };
+    struct Edge {
+        uint32_t a, b;          // inputs
+        uint32_t col_a, col_b;  // base columns of a and b joined
+        int32_t type;           // key type (both sides)
+    };
+    std::vector<Input> inputs;
+    std::vector<Edge> edges;
+};
+int plan_graph(const bj_plan& plan, PlanGraph& g, std::string& err);
+
+// Join order under the given set cardinalities (as make_exec_plan's
+// set_card; null: the reference's row-count model): the executor's cheapest
+// driver and its cost. With `forced_driver` >= 0, the cost of the cheapest
+// plan that driver roots instead. Plans of more than 14 inputs are not
+// costed (cost -1, the largest input drives).
+int join_order(const bj_plan& plan, const std::vector<double>* set_card, int forced_driver, uint32_t& driver,
+               double& cost, std::string& err);
 
 } // namespace bj

@@ -389,10 +389,10 @@ double schema20_count(const QuerySpec& q, const std::vector<uint32_t>& parent,
 }
 
 void make_schema20(plan_io::OwnedPlan& p, uint64_t seed, double scale, uint32_t nqueries,
-                   std::vector<uint32_t>& parent, std::vector<QuerySpec>& queries) {
+                   std::vector<uint32_t>& parent, std::vector<QuerySpec>& queries, std::vector<uint64_t>& rows) {
     std::vector<std::vector<uint32_t>> prow;
     Rng g(stream_seed(seed, 200, 0, 0));
-    std::vector<uint64_t> rows(kSchemaTables);
+    rows.assign(kSchemaTables, 0);
     std::vector<double> sel(kSchemaTables), skew(kSchemaTables);
     parent.assign(kSchemaTables, 0);
     for (uint32_t t = 0; t < kSchemaTables; t++) {
@@ -595,6 +595,7 @@ struct bjw_workload {
     plan_io::OwnedPlan plan;
     bj_plan view{};
     std::string name;
+    std::vector<uint64_t> base_rows;  // schema20: rows of each table before its filter
     std::vector<std::unique_ptr<VariantPlan>> variants;  // by dimension count
     std::vector<std::unique_ptr<VariantPlan>> queries;   // schema20: every query over the shared tables
 };
@@ -606,6 +607,11 @@ struct bjw_pages {
 extern "C" {
 
 int bjw_workload_create(const char* name, uint64_t seed, double scale, bjw_workload** out) {
+    return bjw_workload_create_queries(name, seed, scale, 256, out);
+}
+
+int bjw_workload_create_queries(const char* name, uint64_t seed, double scale, uint64_t nqueries,
+                                bjw_workload** out) {
     try {
         auto w = std::make_unique<bjw_workload>();
         std::string n(name ? name : "");
@@ -617,7 +623,8 @@ int bjw_workload_create(const char* name, uint64_t seed, double scale, bjw_workl
         } else if (n == "schema20") {
             std::vector<uint32_t> parent;
             std::vector<QuerySpec> specs;
-            make_schema20(w->plan, seed, scale, 256, parent, specs);
+            if (nqueries < 1 || nqueries > (1u << 20)) return BJ_ERR_INVALID;
+            make_schema20(w->plan, seed, scale, uint32_t(nqueries), parent, specs, w->base_rows);
             // Query 0 is the workload's own plan; every query is also a plan
             // over the shared tables.
             schema20_plan(specs[0], parent, w->plan.nodes, w->plan.attrs, w->plan.root);
@@ -693,6 +700,11 @@ const bj_plan* bjw_workload_variant(bjw_workload* w, int dims) {
         v->view = bj_plan{v->nodes.size(), v->nodes.data(), v->tables.size(), v->tables.data(), left};
     }
     return &v->view;
+}
+
+uint64_t bjw_workload_base_rows(bjw_workload* w, uint64_t table) {
+    if (!w || table >= w->view.num_inputs) return 0;
+    return table < w->base_rows.size() ? w->base_rows[table] : w->view.inputs[table].num_rows;
 }
 
 uint64_t bjw_workload_num_queries(bjw_workload* w) { return w ? (w->queries.empty() ? 1 : w->queries.size()) : 0; }

@@ -42,6 +42,14 @@ typedef struct bjw_pages bjw_pages;
 
 /* Builds a named workload; returns 0 on success. */
 BJ_API int bjw_workload_create(const char* name, uint64_t seed, double scale, bjw_workload** out);
+/* The same with `nqueries` queries for "schema20" (query k depends only on
+ * the seed, the scale and k, so the first 256 equal the default workload's);
+ * other names ignore nqueries. */
+BJ_API int bjw_workload_create_queries(const char* name, uint64_t seed, double scale, uint64_t nqueries,
+                                       bjw_workload** out);
+/* Rows of input `table` before the filter applied at load time (schema20),
+ * else its row count. */
+BJ_API uint64_t bjw_workload_base_rows(bjw_workload* w, uint64_t table);
 /* Loads a plan written by bjw_save_plan. */
 BJ_API int bjw_workload_load(const char* path, bjw_workload** out);
 /* The plan view (valid until bjw_workload_free). */

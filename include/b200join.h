@@ -239,6 +239,100 @@ BJ_API int bj_server_submit(bj_server* s, const bj_plan* plan, bj_resident* cons
 BJ_API int bj_server_wait(bj_server* s, uint64_t ticket, bj_result** out, double* latency_ms);
 BJ_API void bj_server_resident_free(bj_server* s, bj_resident* table);
 
+/* ---- Join ordering: sub-plan cardinalities and the learned estimator ----
+ *
+ * The reference orders joins with a dynamic program over connected input
+ * sets (engine/query/QueryGraph.cpp:107-216) whose cardinalities come from
+ * 64 sampled rows per input (engine/query/QueryPlan.cpp:719-746); its set
+ * cardinality is the largest input's (QueryGraph.cpp:53-68). Here the same
+ * program (over the executor's plans) takes the cardinality of every
+ * connected input set from one of three sources, chosen per context:
+ *   BJ_ORDER_ROWS      the reference's model: the largest input's row count;
+ *   BJ_ORDER_SAMPLING  join samples: an input's rows times, per neighbour in
+ *                      the set, the share of 64 sampled rows whose key the
+ *                      neighbour's key column holds (0 hits: 1/128, the
+ *                      reference's rule); a set takes its largest member;
+ *   BJ_ORDER_LEARNED   the MLP estimator below, with sampling as its fallback
+ *                      (plans of more than BJ_EST_MAX_TABLES inputs, or an
+ *                      estimate that is not finite).
+ * Only the join order changes; results are the same rows in every mode.
+ * Applies to bj_execute_resident (statistics are kept with resident tables).
+ *
+ * Sub-plans are named by bit masks over a plan's scans, numbered in the
+ * order a depth-first walk from the root reaches them, left child first. */
+#define BJ_ORDER_ROWS 0
+#define BJ_ORDER_SAMPLING 1
+#define BJ_ORDER_LEARNED 2
+#define BJ_EST_MAX_TABLES 12
+#define BJ_EST_FEATURES 1792
+#define BJ_EST_HIDDEN 256
+
+typedef struct bj_estimator bj_estimator;
+
+/* Ordering mode of a context (estimator: required for BJ_ORDER_LEARNED, must
+ * outlive its use by the context). */
+BJ_API int bj_context_set_ordering(bj_context* ctx, int mode, bj_estimator* estimator);
+
+/* Rows of a resident table before its load-time filter (for the estimator's
+ * filter-selectivity feature; default: its row count). */
+BJ_API int bj_resident_set_base_rows(bj_resident* table, uint64_t base_rows);
+
+/* Connected input sets of a plan with at most max_tables inputs, ascending
+ * masks: writes min(cap, total) masks and the total to *n. Plans of more than
+ * 20 scans return BJ_ERR_UNSUPPORTED. */
+BJ_API int bj_subplans(const bj_plan* plan, uint32_t max_tables, uint64_t cap, uint32_t* masks, uint64_t* n);
+
+/* Exact cardinality of each sub-plan (the row count bj_execute_resident
+ * returns for the join of those inputs), computed on the device by weights
+ * (a row's weight is the number of join rows it takes part in below it), so
+ * no join result is materialised. out[i] = +inf when a count passes 2^64-1. */
+BJ_API int bj_subplan_cards(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, const uint32_t* masks,
+                            uint64_t n, double* out);
+/* Sampling estimate of each sub-plan (BJ_ORDER_SAMPLING's cardinality). */
+BJ_API int bj_subplan_sample_cards(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables,
+                                   const uint32_t* masks, uint64_t n, double* out);
+/* Estimator features of each sub-plan: n rows of BJ_EST_FEATURES floats.
+ * Up to BJ_EST_MAX_TABLES inputs in a canonical order (the largest first,
+ * then depth first, larger neighbours first); per input: presence, log2
+ * rows, filter selectivity (rows / base rows), log2 distinct keys of its
+ * column on the edge to its parent and of the parent's, the parent's slot
+ * (one-hot: the edge list), and 64-bin log-frequency histograms of both of
+ * those key columns. */
+BJ_API int bj_subplan_features(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, const uint32_t* masks,
+                               uint64_t n, float* out);
+
+/* Join order under given set cardinalities (card[mask], 2^scans entries;
+ * NULL: the row-count model): the input the output pipeline scans and the
+ * plan's cost. driver_in >= 0 costs the cheapest plan that input drives
+ * instead (to cost a choice under other cardinalities). Up to 14 scans. */
+BJ_API int bj_join_order(const bj_plan* plan, const double* card, int driver_in, uint32_t* driver, double* cost);
+
+/* The learned estimator: features -> 256 -> 256 -> log2(cardinality + 1),
+ * ReLU, BF16 weights with FP32 accumulation on the tensor cores, trained on
+ * the device with the library's own forward and backward kernels and Adam.
+ * Parameters, in bj_estimator_get_params order: W1 (features x 256, row
+ * major), b1 (256), W2 (256 x 256), b2, w3 (256), b3 (1), padding. */
+BJ_API int bj_estimator_create(int device, uint64_t seed, bj_estimator** out);
+BJ_API void bj_estimator_destroy(bj_estimator* e);
+BJ_API uint64_t bj_estimator_num_params(void);
+BJ_API int bj_estimator_get_params(bj_estimator* e, float* out);
+BJ_API int bj_estimator_set_params(bj_estimator* e, const float* in);
+/* Trains on n rows (features as bj_subplan_features writes them, rounded to
+ * BF16; targets log2(cardinality + 1)) for `epochs` passes in shuffled
+ * batches of `batch` rows, learning rate `lr` (cosine decay to a tenth).
+ * epoch_loss (optional, `epochs` entries) receives each pass's mean squared
+ * error. */
+BJ_API int bj_estimator_train(bj_estimator* e, const float* features, const float* targets, uint64_t n,
+                              uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float* epoch_loss);
+/* log2(cardinality + 1) of n feature rows. */
+BJ_API int bj_estimator_predict(bj_estimator* e, const float* features, uint64_t n, float* out);
+/* One forward and backward pass over n rows (n <= 4096) without an update:
+ * the mean squared error and its gradient for every parameter. */
+BJ_API int bj_estimator_gradients(bj_estimator* e, const float* features, const float* targets, uint64_t n,
+                                  float* loss, float* grads);
+BJ_API int bj_estimator_save(bj_estimator* e, const char* path);
+BJ_API int bj_estimator_load(int device, const char* path, bj_estimator** out);
+
 /* Turns per-kernel event timing of the scan-side probe stage on (1) or off (0).
  * Adds two event records per timed launch; off by default. */
 BJ_API void bj_context_profile(bj_context* ctx, int on);
