@@ -222,14 +222,32 @@ struct HTView {
     const uint64_t* mult;        // nentries
     const uint64_t* pay;         // nentries * width
     const uint32_t* pnull;       // nentries (bit j: slot j is NULL)
-    const uint32_t* bloom;       // 1 << bloom_log2 words, or null
+    const uint32_t* bloom;       // 1 << bloom_log2 words, or null (always null for INT64 keys)
+    const uint32_t* keys_hi;     // INT64 keys: high halves (keys holds the low ones); null for INT32
     uint32_t shift;              // bucket = key_hash >> shift
     uint32_t bloom_log2;
     uint32_t nentries;
     uint32_t width;
 };
 
+// Bucket of key slot k in a table keyed on 64-bit (wide) or 32-bit keys.
+BJ_HD uint32_t bucket_of(uint64_t k, bool wide, uint32_t shift) {
+    return uint32_t((wide ? key_hash_any(k, kInt64) : key_hash(uint32_t(k))) >> shift);
+}
+
 #if defined(__CUDACC__)
+__device__ __forceinline__ uint32_t ht_bucket(const HTView& ht, uint64_t k) {
+    return bucket_of(k, ht.keys_hi != nullptr, ht.shift);
+}
+// Entry e's key equals key slot k.
+__device__ __forceinline__ bool ht_key_eq(const HTView& ht, uint32_t e, uint64_t k) {
+    return ht.keys[e] == uint32_t(k) && (!ht.keys_hi || ht.keys_hi[e] == uint32_t(k >> 32));
+}
+// Entry e's key as a value slot.
+__device__ __forceinline__ uint64_t ht_key(const HTView& ht, uint32_t e) {
+    return uint64_t(ht.keys[e]) | (ht.keys_hi ? uint64_t(ht.keys_hi[e]) << 32 : 0ull);
+}
+
 __device__ __forceinline__ bool bloom_may_contain(const uint32_t* bloom, uint32_t log2w, uint32_t key) {
     const uint32_t hh = key_hash_hi(key);
     const uint32_t bits = bloom_bits_fast(hh, hh >> 5);

@@ -691,8 +691,10 @@ class Executor {
         for (size_t s = 0; s < np; s++) {
             uint32_t k = order[s];
             const HTView& ht = by_stage[s];
-            if (items.rows == nullptr) {
-                // Scan stage: stream the key pages of the scanned table.
+            if (items.rows == nullptr && col(pp.probes[k].probe_attr).type == kInt32) {
+                // Scan stage: stream the key pages of the scanned table. (An
+                // INT64 key column takes the item stages below, over the
+                // implicit items 0..rows-1.)
                 const BuiltHT& bh = hts_[pp.probes[k].child];
                 const DevColumn& key = col(pp.probes[k].probe_attr);
                 bool bloom = ht.bloom && rate[k] < 0.5;
@@ -870,7 +872,11 @@ class Executor {
         ba.src = src;
         ba.ps = make_probe_set(probes.data(), items.nprobes);
         TupleBuf& tb = ba.tb;
+        // INT64 keys (no reference counterpart) keep their high halves beside
+        // the low ones and build no bloom filter.
+        const bool wide = ba.key.type == kInt64;
         tb.keys = alloc<uint32_t>(n);
+        tb.keys_hi = wide ? alloc<uint32_t>(n) : nullptr;
         tb.mult = alloc<uint64_t>(n);
         tb.pay = alloc<uint64_t>(size_t(n) * std::max<uint32_t>(width, 1));
         tb.pnull = alloc<uint32_t>(n);
@@ -898,7 +904,7 @@ class Executor {
         const uint32_t blog2 = std::max<uint32_t>(bit_width(nrep), 4);
         ba.shift = 64 - blog2;
         pb.nb = uint32_t(1) << blog2;
-        pb.with_bloom = uint64_t(nrep) * 8 <= (uint64_t(32) << kBloomMaxLog2);
+        pb.with_bloom = !wide && uint64_t(nrep) * 8 <= (uint64_t(32) << kBloomMaxLog2);
         pb.wlog2 = pb.with_bloom ? std::min<uint32_t>(kBloomMaxLog2,
                                                       std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1)))
                                  : 0;
@@ -915,6 +921,7 @@ class Executor {
         HTView& ht = pb.ht;
         ht.buckets = pb.buckets;
         ht.keys = alloc<uint32_t>(nrep);
+        ht.keys_hi = wide ? alloc<uint32_t>(nrep) : nullptr;
         ht.mult = alloc<uint64_t>(nrep);
         ht.pay = alloc<uint64_t>(size_t(nrep) * std::max<uint32_t>(width, 1));
         ht.pnull = alloc<uint32_t>(nrep);

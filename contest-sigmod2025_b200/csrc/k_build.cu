@@ -34,8 +34,13 @@
 namespace bj {
 namespace {
 
+__device__ __forceinline__ uint64_t tuple_key(const TupleBuf& t, uint32_t i) {
+    return uint64_t(t.keys[i]) | (t.keys_hi ? uint64_t(t.keys_hi[i]) << 32 : 0ull);
+}
+
 __device__ __forceinline__ uint64_t tuple_hash(const TupleBuf& t, uint32_t i) {
     uint64_t h = mix64(uint64_t(t.keys[i]) ^ (uint64_t(t.pnull[i]) << 32));
+    if (t.keys_hi) h = mix64(h ^ t.keys_hi[i]);
     const uint64_t* p = t.pay + size_t(i) * t.width;
     for (uint32_t j = 0; j < t.width; j++) h = mix64(h ^ (p[j] + 0x9E3779B97F4A7C15ull * (j + 1)));
     return h;
@@ -44,6 +49,7 @@ __device__ __forceinline__ uint64_t tuple_hash(const TupleBuf& t, uint32_t i) {
 // Tuple a (written by another thread, read through L2) equals tuple b.
 __device__ __forceinline__ bool tuple_equal_cg(const TupleBuf& t, uint32_t a, uint32_t b) {
     if (__ldcg(t.keys + a) != t.keys[b] || __ldcg(t.pnull + a) != t.pnull[b]) return false;
+    if (t.keys_hi && __ldcg(t.keys_hi + a) != t.keys_hi[b]) return false;
     const uint64_t* pa = t.pay + size_t(a) * t.width;
     const uint64_t* pb = t.pay + size_t(b) * t.width;
     for (uint32_t j = 0; j < t.width; j++)
@@ -73,6 +79,7 @@ __device__ __forceinline__ void emit_tuple_to(const EmitTarget& a, uint32_t i, u
                                               Slot&& slot) {
     const TupleBuf& t = a.tb;
     t.keys[i] = uint32_t(kv);
+    if (t.keys_hi) t.keys_hi[i] = uint32_t(kv >> 32);
     t.mult[i] = m;
     uint32_t nulls = 0;
     for (int j = 0; j < nslots; j++) {
@@ -90,7 +97,7 @@ __device__ __forceinline__ void emit_tuple_to(const EmitTarget& a, uint32_t i, u
     }
     if (a.distinct) {
         a.is_rep[i] = 1;
-        atomicAdd(&a.counts[uint32_t(key_hash(uint32_t(kv)) >> a.shift)], 1u);
+        atomicAdd(&a.counts[bucket_of(kv, t.keys_hi != nullptr, a.shift)], 1u);
     }
 }
 
@@ -108,7 +115,7 @@ __device__ __forceinline__ void aggregate_tuple(const EmitTarget& a, uint32_t i)
         const uint32_t cur = atomicCAS(&a.table[pos], 0u, i + 1);
         if (cur == 0) {
             a.is_rep[i] = 1;
-            atomicAdd(&a.counts[uint32_t(key_hash(t.keys[i]) >> a.shift)], 1u);
+            atomicAdd(&a.counts[bucket_of(tuple_key(t, i), t.keys_hi != nullptr, a.shift)], 1u);
             return;
         }
         if (tuple_equal_cg(t, cur - 1, i)) {
@@ -154,17 +161,20 @@ __device__ __forceinline__ void scatter_tuple(const TupleBuf& t, const uint32_t*
                                               uint32_t* __restrict__ err, uint32_t i) {
     if (!is_rep[i]) return;
     const uint32_t key = t.keys[i];
-    const uint32_t b = uint32_t(key_hash(key) >> shift);
+    const uint32_t b = bucket_of(tuple_key(t, i), t.keys_hi != nullptr, shift);
     const uint32_t first = buckets[b].x;
     const uint32_t pos = first + atomicAdd(&cursor[b], 1u);
-    const uint32_t hh = key_hash_hi(key);
-    if (bloom) atomicOr(&bloom[bloom_word_hi(hh, log2w)], bloom_bits_fast(hh, hh >> 5));
+    if (bloom) {  // INT32 keys only (INT64 tables are built without a filter)
+        const uint32_t hh = key_hash_hi(key);
+        atomicOr(&bloom[bloom_word_hi(hh, log2w)], bloom_bits_fast(hh, hh >> 5));
+    }
     if (pos >= buckets[b + 1].x || pos >= ht.nentries) {
         record_error(err, kErrCapacity);
         return;
     }
     if (pos == first) buckets[b].y = key;  // the bucket's first entry
     const_cast<uint32_t*>(ht.keys)[pos] = key;
+    if (t.keys_hi) const_cast<uint32_t*>(ht.keys_hi)[pos] = t.keys_hi[i];
     const_cast<uint64_t*>(ht.mult)[pos] = t.mult[i];
     const_cast<uint32_t*>(ht.pnull)[pos] = t.pnull[i];
     uint64_t* dst = const_cast<uint64_t*>(ht.pay) + size_t(pos) * t.width;
@@ -182,15 +192,15 @@ __global__ void k_scatter_bloom(TupleBuf t, const uint32_t* __restrict__ is_rep,
 // Flags of entry e of a built table (see ht_flags).
 __device__ __forceinline__ void flag_entry(const HTView& ht, uint32_t e, uint32_t* __restrict__ flags) {
     if (ht.mult[e] > 1) flags[1] = 1;
-    uint32_t key = ht.keys[e];
-    uint32_t b = uint32_t(key_hash(key) >> ht.shift);
+    const uint64_t key = ht_key(ht, e);
+    uint32_t b = ht_bucket(ht, key);
     uint32_t s = ht.buckets[b].x;
     if (e - s > 256) {
         flags[0] = 1;  // long bucket: assume repeats (only steers capacity choices)
         return;
     }
     for (uint32_t j = s; j < e; j++)
-        if (ht.keys[j] == key) {
+        if (ht_key_eq(ht, j, key)) {
             flags[0] = 1;
             break;
         }
@@ -349,10 +359,9 @@ __global__ void k_sample_probes(SampleSet set, uint32_t nsample, uint32_t* hits)
     const uint32_t row = uint32_t((uint64_t(i) * sp.key.nrows) / nsample);
     uint64_t v;
     if (!col_get(sp.key, row, v)) return;
-    const uint32_t k = uint32_t(v);
-    const uint32_t b = uint32_t(key_hash(k) >> sp.ht.shift);
+    const uint32_t b = ht_bucket(sp.ht, v);
     for (uint32_t j = sp.ht.buckets[b].x; j < sp.ht.buckets[b + 1].x; j++)
-        if (sp.ht.keys[j] == k) {
+        if (ht_key_eq(sp.ht, j, v)) {
             atomicAdd(hits + blockIdx.y, 1u);
             return;
         }

@@ -15,6 +15,8 @@
 // The probe itself follows HashtableProbe::operator() (engine/op/Hashtable.hpp:
 // 228-241): hash the 32-bit key, find its bucket, compare every key in the
 // bucket. Buckets here are contiguous runs of entries (CSR), not chains.
+// INT64 keys (no reference counterpart: the reference reads every join key as
+// 32 bits) hash all 64 bits and compare both halves.
 #include "launch.h"
 
 #include <algorithm>
@@ -24,20 +26,21 @@ namespace {
 
 
 // Entries of `ht` whose key equals `key`: calls fn(entry) for each.
+// `key` is a value slot: an INT32 key zero-extended, or an INT64 key (the
+// table then carries keys_hi and no bloom filter).
 template <typename Fn>
-__device__ __forceinline__ uint32_t for_matches(const HTView& ht, uint32_t key, bool use_bloom, Fn&& fn) {
-    if (use_bloom && ht.bloom && !bloom_may_contain(ht.bloom, ht.bloom_log2, key)) return 0;
-    uint64_t h = key_hash(key);
-    uint32_t b = uint32_t(h >> ht.shift);
+__device__ __forceinline__ uint32_t for_matches(const HTView& ht, uint64_t key, bool use_bloom, Fn&& fn) {
+    if (use_bloom && ht.bloom && !bloom_may_contain(ht.bloom, ht.bloom_log2, uint32_t(key))) return 0;
+    const uint32_t b = ht_bucket(ht, key);
     const uint2 b0 = ht.buckets[b];
     const uint32_t e = ht.buckets[b + 1].x;
     uint32_t n = 0;
-    if (b0.x < e && b0.y == key) {
+    if (b0.x < e && b0.y == uint32_t(key) && (!ht.keys_hi || ht.keys_hi[b0.x] == uint32_t(key >> 32))) {
         fn(b0.x);
         n++;
     }
     for (uint32_t j = b0.x + 1; j < e; j++) {
-        if (ht.keys[j] == key) {
+        if (ht_key_eq(ht, j, key)) {
             fn(j);
             n++;
         }
@@ -90,7 +93,7 @@ __global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HT
         }
         uint64_t v;
         if (!col_get(key, row, v)) continue;
-        mine += for_matches(ht, uint32_t(v), use_bloom != 0, [](uint32_t) {});
+        mine += for_matches(ht, v, use_bloom != 0, [](uint32_t) {});
     }
     __shared__ uint32_t total;
     uint32_t base = block_exclusive_sum<uint32_t>(mine, &total);
@@ -105,7 +108,7 @@ __global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HT
         uint64_t v;
         if (!col_get(key, row, v)) continue;
         uint64_t m = item_mult(in, i);
-        for_matches(ht, uint32_t(v), use_bloom != 0, [&](uint32_t e) {
+        for_matches(ht, v, use_bloom != 0, [&](uint32_t e) {
             out.rows[o] = row;
             for (int p = 0; p < in.nprobes; p++) out.ents[p][o] = in.ents[p][i];
             out.ents[in.nprobes][o] = e;
@@ -149,7 +152,7 @@ __global__ void __launch_bounds__(256) k_probe_chain(Items in, ProbeChain ch, It
                 hit = false;
             } else {
                 bool found = false;
-                for_matches(c.ht, uint32_t(v), c.use_bloom != 0, [&](uint32_t j) {
+                for_matches(c.ht, v, c.use_bloom != 0, [&](uint32_t j) {
                     if (!found) e[t] = j;
                     found = true;
                 });

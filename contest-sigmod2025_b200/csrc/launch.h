@@ -188,7 +188,7 @@ __device__ __forceinline__ bool slot_value(const SlotSource& s, const Items& in,
     if (s.kind == 0) return column_value(s.col, row, v);
     const uint32_t e = in.ents[s.probe][i];
     if (s.kind == 2) {
-        v = ps.ht[s.probe].keys[e];
+        v = ht_key(ps.ht[s.probe], e);
         return true;
     }
     const HTView& ht = ps.ht[s.probe];
@@ -232,6 +232,7 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
 // mult 0), payload from `src`, mult from the item.
 struct TupleBuf {
     uint32_t* keys;
+    uint32_t* keys_hi; // INT64 build keys: high halves; null for INT32
     uint64_t* mult;
     uint64_t* pay;     // count * width
     uint32_t* pnull;

@@ -78,9 +78,12 @@ struct Importer {
         if (n.left_attr >= l.size() || n.right_attr >= r.size()) return fail(BJ_ERR_INVALID, "join attribute out of range");
         uint32_t la = l[n.left_attr], ra = r[n.right_attr];
         // Join keys are 32-bit integers in the reference (engine/op/TableScan.cpp:328,
-        // engine/op/Hashtable.hpp:35-39); it would misread any other type.
-        if (ex.attrs[la].type != BJ_INT32 || ex.attrs[ra].type != BJ_INT32)
-            return fail(BJ_ERR_UNSUPPORTED, "join keys must be INT32");
+        // engine/op/Hashtable.hpp:35-39), which misreads any other type. Here
+        // INT64 keys are joined by their full 64-bit value too (no reference
+        // counterpart); both sides of a join must have the same key type.
+        const int32_t lt = ex.attrs[la].type, rt = ex.attrs[ra].type;
+        if (lt != rt || (lt != BJ_INT32 && lt != BJ_INT64))
+            return fail(BJ_ERR_UNSUPPORTED, "join keys must be INT32 or INT64, the same type on both sides");
         uf.merge(la, ra);
         edges.push_back(Edge{ex.attrs[la].input, ex.attrs[ra].input, la, ra});
         for (uint64_t a = 0; a < n.num_output_attrs; a++) {

@@ -388,8 +388,19 @@ double schema20_count(const QuerySpec& q, const std::vector<uint32_t>& parent,
     return total;
 }
 
+// With wide keys, every other table (odd ids) keys its rows by INT64 values
+// whose low 32 bits are the INT32 key's and whose high half is a small
+// signed number that varies per row (so low halves repeat across keys), and
+// its children's foreign keys are INT64 too (no reference counterpart: the
+// reference reads join keys as 32 bits).
+constexpr int64_t wide_key(int32_t k) {
+    const int64_t hi = int64_t((uint32_t(k) * 2654435761u) >> 29) - 4;  // -4 .. 3
+    return int64_t(uint64_t(hi) << 32 | uint32_t(k));
+}
+
 void make_schema20(plan_io::OwnedPlan& p, uint64_t seed, double scale, uint32_t nqueries,
-                   std::vector<uint32_t>& parent, std::vector<QuerySpec>& queries, std::vector<uint64_t>& rows) {
+                   std::vector<uint32_t>& parent, std::vector<QuerySpec>& queries, std::vector<uint64_t>& rows,
+                   const std::vector<uint8_t>& wide) {
     std::vector<std::vector<uint32_t>> prow;
     Rng g(stream_seed(seed, 200, 0, 0));
     rows.assign(kSchemaTables, 0);
@@ -453,8 +464,17 @@ void make_schema20(plan_io::OwnedPlan& p, uint64_t seed, double scale, uint32_t 
         auto& tab = p.tables[t];
         tab.num_rows = c0.size();
         tab.columns.resize(5);
-        encode_any(tab.columns[0], BJ_INT32, c0.size(), c0.data(), nullptr, nullptr, nullptr);
-        encode_any(tab.columns[1], BJ_INT32, c1.size(), c1.data(), nullptr, nullptr, nullptr);
+        auto encode_key = [&](plan_io::OwnedColumn& col, const std::vector<int32_t>& v, bool w64) {
+            if (!w64) {
+                encode_any(col, BJ_INT32, v.size(), v.data(), nullptr, nullptr, nullptr);
+                return;
+            }
+            std::vector<int64_t> v64(v.size());
+            for (size_t i = 0; i < v.size(); i++) v64[i] = wide_key(v[i]);
+            encode_any(col, BJ_INT64, v64.size(), v64.data(), nullptr, nullptr, nullptr);
+        };
+        encode_key(tab.columns[0], c0, wide[t]);
+        encode_key(tab.columns[1], c1, t && wide[parent[t]]);
         encode_any(tab.columns[2], BJ_INT32, c2.size(), c2.data(), nullptr, nullptr, nullptr);
         encode_any(tab.columns[3], BJ_FP64, c3.size(), c3.data(), nullptr, nullptr, nullptr);
         encode_any(tab.columns[4], BJ_VARCHAR, c0.size(), nullptr, nullptr, off.data(), bytes.data());
@@ -527,10 +547,11 @@ void make_schema20(plan_io::OwnedPlan& p, uint64_t seed, double scale, uint32_t 
 // each join appends a table joined on its edge to an earlier one (child's c1
 // = parent's c0) and keeps every attribute; the root projects the query's
 // outputs.
-void schema20_plan(const QuerySpec& q, const std::vector<uint32_t>& parent, std::vector<bj_node>& nodes,
-                   std::vector<std::vector<bj_attr>>& attrs, uint64_t& root) {
+void schema20_plan(const QuerySpec& q, const std::vector<uint32_t>& parent, const std::vector<uint8_t>& wide,
+                   std::vector<bj_node>& nodes, std::vector<std::vector<bj_attr>>& attrs, uint64_t& root) {
     nodes.clear();
     attrs.clear();
+    auto kt = [&](bool w) { return w ? BJ_INT64 : BJ_INT32; };
     auto type_of = [](uint32_t c) { return c == 3 ? BJ_FP64 : c == 4 ? BJ_VARCHAR : BJ_INT32; };
     std::vector<uint32_t> base;  // attribute index of each table's c0 in the growing join output
     std::vector<bj_attr> acc;    // the growing join output
@@ -538,7 +559,7 @@ void schema20_plan(const QuerySpec& q, const std::vector<uint32_t>& parent, std:
     for (size_t i = 0; i < q.tables.size(); i++) {
         const uint32_t t = q.tables[i];
         nodes.push_back(scan_node(t));
-        attrs.push_back({{0, BJ_INT32, 0}, {1, BJ_INT32, 0}, {q.payload[i], type_of(q.payload[i]), 0}});
+        attrs.push_back({{0, kt(wide[t]), 0}, {1, kt(t && wide[parent[t]]), 0}, {q.payload[i], type_of(q.payload[i]), 0}});
         const uint64_t scan = nodes.size() - 1;
         if (i == 0) {
             left = scan;
@@ -620,20 +641,23 @@ int bjw_workload_create_queries(const char* name, uint64_t seed, double scale, u
             make_join2(w->plan, seed, scale);
         } else if (n == "snowflake") {
             make_snowflake(w->plan, seed, scale);
-        } else if (n == "schema20") {
+        } else if (n == "schema20" || n == "schema20w") {
             std::vector<uint32_t> parent;
             std::vector<QuerySpec> specs;
+            std::vector<uint8_t> wide(kSchemaTables, 0);
+            if (n == "schema20w")
+                for (uint32_t t = 1; t < kSchemaTables; t += 2) wide[t] = 1;
             if (nqueries < 1 || nqueries > (1u << 20)) return BJ_ERR_INVALID;
-            make_schema20(w->plan, seed, scale, uint32_t(nqueries), parent, specs, w->base_rows);
+            make_schema20(w->plan, seed, scale, uint32_t(nqueries), parent, specs, w->base_rows, wide);
             // Query 0 is the workload's own plan; every query is also a plan
             // over the shared tables.
-            schema20_plan(specs[0], parent, w->plan.nodes, w->plan.attrs, w->plan.root);
+            schema20_plan(specs[0], parent, wide, w->plan.nodes, w->plan.attrs, w->plan.root);
             w->view = w->plan.view();
             for (const QuerySpec& q : specs) {
                 auto v = std::make_unique<VariantPlan>();
                 v->tables.assign(w->view.inputs, w->view.inputs + w->view.num_inputs);
                 uint64_t root = 0;
-                schema20_plan(q, parent, v->nodes, v->attrs, root);
+                schema20_plan(q, parent, wide, v->nodes, v->attrs, root);
                 for (size_t i = 0; i < v->nodes.size(); i++) {
                     v->nodes[i].num_output_attrs = v->attrs[i].size();
                     v->nodes[i].output_attrs = v->attrs[i].data();

@@ -25,6 +25,12 @@
  *               INT32 key, INT32 FK, INT32 / FP64 / VARCHAR payloads) and 256
  *               random acyclic queries of 2-12 tables over them
  *               (bjw_workload_query); the workload's plan is query 0.
+ *   "schema20w" the same tables and queries with INT64 join keys on every
+ *               other table (odd ids key their rows, and their children
+ *               reference them, by INT64 values whose low 32 bits are the
+ *               INT32 key's and whose high halves vary from -4 to 3); no
+ *               reference counterpart (the reference reads join keys as 32
+ *               bits), so results are checked against the oracle only.
  *
  * `scale` multiplies every row count (1.0 = the sizes above).
  */

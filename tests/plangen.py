@@ -5,6 +5,12 @@ Random join trees over 1-6 tables: INT32 join keys drawn from small domains
 payloads with NULLs, empty and long (>8185 byte) strings, intermediate
 projections that drop attributes, and root outputs that repeat or reorder
 attributes. Table sizes span empty, one row and multi-page columns.
+
+With int64_keys, every table also has an INT64 key column whose values share
+their low 32 bits across several high halves (negative ones included), and
+joins pair INT64 keys where both sides carry one: keys that only a full
+64-bit comparison tells apart. (The reference reads join keys as 32 bits,
+engine/op/TableScan.cpp:328; these plans are checked against the oracle.)
 """
 import random
 
@@ -25,7 +31,13 @@ def _value(rng, ty, dom, null_p, long_p):
     return "".join(chr(32 + rng.randrange(95)) for _ in range(rng.randrange(0, 24)))
 
 
-def random_case(seed, max_tables=5, max_rows=3000, min_tables=1, max_width=None):
+def _key64(rng, dom, null_p):
+    if rng.random() < null_p:
+        return None
+    return (rng.choice([0, 1, 7, -1, -5]) << 32) | rng.randrange(dom)
+
+
+def random_case(seed, max_tables=5, max_rows=3000, min_tables=1, max_width=None, int64_keys=False):
     """max_width caps the attributes a join node outputs (the reference only
     instantiates pipelines carrying a few attributes, engine/genpipelines.py:15-49)."""
     """Returns (tables, nodes, root) in the form tests/golden/make_golden.py uses."""
@@ -42,7 +54,11 @@ def random_case(seed, max_tables=5, max_rows=3000, min_tables=1, max_width=None)
         null_p = rng.choice([0.0, 0.0, 0.05, 0.3])
         long_p = 0.002 if rng.random() < 0.3 else 0.0
         rows = [[_value(rng, ty, dom, null_p, long_p) for ty in types] for _ in range(nrows)]
-        tables.append({"types": types, "rows": rows})
+        if int64_keys:
+            types.insert(1, INT64)
+            for r in rows:
+                r.insert(1, _key64(rng, dom, null_p))
+        tables.append({"types": types, "rows": rows, "keys64": {1} if int64_keys else set()})
     nodes = []
     subtrees = []  # (node id, [type per output attr])
     for t, tab in enumerate(tables):
@@ -51,14 +67,22 @@ def random_case(seed, max_tables=5, max_rows=3000, min_tables=1, max_width=None)
         keep = cols[:rng.randint(1, len(cols))]
         if not any(tab["types"][c] == INT32 for c in keep):
             keep.append(next(c for c in cols if tab["types"][c] == INT32))
+        if int64_keys and 1 not in keep and rng.random() < 0.8:
+            keep.append(1)
         attrs = [[c, tab["types"][c]] for c in keep]
         nodes.append({"kind": "scan", "table": t, "attrs": attrs})
-        subtrees.append((len(nodes) - 1, [a[1] for a in attrs]))
+        # per output attribute: (type, is a key column)
+        subtrees.append((len(nodes) - 1, [a[1] for a in attrs],
+                         [a[1] == INT32 or a[0] in tab["keys64"] for a in attrs]))
     while len(subtrees) > 1:
         a = subtrees.pop(rng.randrange(len(subtrees)))
         b = subtrees.pop(rng.randrange(len(subtrees)))
-        la = rng.choice([i for i, ty in enumerate(a[1]) if ty == INT32])
-        ra = rng.choice([i for i, ty in enumerate(b[1]) if ty == INT32])
+        key_ty = INT32
+        if int64_keys and rng.random() < 0.6:
+            if any(t == INT64 and k for t, k in zip(a[1], a[2])) and any(t == INT64 and k for t, k in zip(b[1], b[2])):
+                key_ty = INT64
+        la = rng.choice([i for i, ty in enumerate(a[1]) if ty == key_ty and a[2][i]])
+        ra = rng.choice([i for i, ty in enumerate(b[1]) if ty == key_ty and b[2][i]])
         both = a[1] + b[1]
         idx = list(range(len(both)))
         if rng.random() < 0.5 or (max_width and len(idx) > max_width):
@@ -66,11 +90,12 @@ def random_case(seed, max_tables=5, max_rows=3000, min_tables=1, max_width=None)
             idx = idx[:rng.randint(1, min(len(idx), max_width or len(idx)))]
         if not any(both[i] == INT32 for i in idx):
             idx.append(next(i for i in range(len(both)) if both[i] == INT32))
+        keyflags = a[2] + b[2]
         attrs = [[i, both[i]] for i in idx]
         nodes.append({"kind": "join", "build_left": rng.random() < 0.5, "left": a[0], "right": b[0], "left_attr": la,
                       "right_attr": ra, "attrs": attrs})
-        subtrees.append((len(nodes) - 1, [x[1] for x in attrs]))
-    root, rtypes = subtrees[0]
+        subtrees.append((len(nodes) - 1, [x[1] for x in attrs], [keyflags[i] for i in idx]))
+    root, rtypes, _ = subtrees[0]
     if rng.random() < 0.3 and nodes[root]["kind"] == "join":
         # Root output repeating / reordering attributes.
         n = nodes[root]

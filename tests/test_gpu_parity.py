@@ -39,6 +39,23 @@ def test_random_plans(pkg, ctx, oracle, seed):
     check_against_oracle(pkg, ctx, oracle, cp, f"seed {1000 + seed}")
 
 
+@pytest.mark.parametrize("seed", range(24))
+def test_random_plans_int64_keys(pkg, ctx, oracle, seed):
+    """INT64 join keys (no reference counterpart: the reference reads join
+    keys as 32 bits) whose low halves collide across high halves, mixed with
+    INT32 joins in one plan; checked against the oracle's 64-bit comparison."""
+    tables, nodes, root = plangen.random_case(9000 + seed, max_rows=3000, int64_keys=True)
+    cp = pkg.CPlan(plangen.to_plan(pkg, tables, nodes, root))
+    check_against_oracle(pkg, ctx, oracle, cp, f"int64 seed {9000 + seed}")
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_random_plans_int64_keys_wide_tables(pkg, ctx, oracle, seed):
+    tables, nodes, root = plangen.random_case(9500 + seed, max_tables=3, max_rows=40000, int64_keys=True)
+    cp = pkg.CPlan(plangen.to_plan(pkg, tables, nodes, root))
+    check_against_oracle(pkg, ctx, oracle, cp, f"int64 seed {9500 + seed}")
+
+
 @pytest.mark.parametrize("seed", range(10))
 def test_random_plans_wide_tables(pkg, ctx, oracle, seed):
     """Larger inputs: columns of many pages, long chains of duplicates."""
@@ -91,14 +108,14 @@ def test_repeated_calls_reuse_context(pkg, ctx, oracle):
         check_against_oracle(pkg, ctx, oracle, w.plan_ptr(), "repeat")
 
 
-def test_non_int32_join_key_is_rejected(pkg, ctx):
+@pytest.mark.parametrize("lt,rt", [(1, 0), (2, 2)])  # INT64 = INT32, FP64 = FP64
+def test_unsupported_join_key_is_rejected(pkg, ctx, lt, rt):
     plan = pkg.Plan()
-    t = pkg.table_from_rows([[1], [2]], [pkg.INT64])
-    plan.new_input(t)
-    plan.new_input(t)
-    plan.new_scan_node(0, [(0, pkg.INT64)])
-    plan.new_scan_node(1, [(0, pkg.INT64)])
-    plan.new_join_node(True, 0, 1, 0, 0, [(0, pkg.INT64)])
+    plan.new_input(pkg.table_from_rows([[1], [2]], [lt]))
+    plan.new_input(pkg.table_from_rows([[1], [2]], [rt]))
+    plan.new_scan_node(0, [(0, lt)])
+    plan.new_scan_node(1, [(0, rt)])
+    plan.new_join_node(True, 0, 1, 0, 0, [(0, lt)])
     plan.root = 2
     with pytest.raises(pkg.EngineError) as e:
         ctx.execute(plan)

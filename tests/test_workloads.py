@@ -102,3 +102,32 @@ def test_schema20_widest_queries_match_reference_engine(pkg, oracle, seed):
         ref_struct, keep = table_struct(pkg, ref)
         ora = oracle.execute(q)
         oracle_lib.assert_same_rows(oracle, ctypes.byref(ref_struct), ora.view(), f"schema20 seed {seed} query {k}")
+
+
+def test_schema20w_has_int64_keys_and_the_same_results(pkg, oracle, schema20):
+    """schema20w: the same tables with INT64 keys on every other table (low
+    halves kept, high halves varying). Each query joins the same rows, so the
+    oracle's row count matches schema20's; the reference reads join keys as
+    32 bits, so these are checked against the oracle alone."""
+    w = pkg.Workload("schema20w", 3, SCALE)
+    plan = w.plan_ptr().contents
+    types = [plan.inputs[t].columns[0].type for t in range(plan.num_inputs)]
+    assert types.count(pkg.INT64) == 10 and types.count(pkg.INT32) == 10
+    for k in range(0, 256, 16):
+        a = len(_rows(oracle, w.query_ptr(k)))
+        b = len(_rows(oracle, schema20.query_ptr(k)))
+        assert a == b, f"query {k}: {a} != {b}"
+
+
+def test_schema20_more_queries_extends_the_batch(pkg):
+    """Query k depends only on (seed, scale, k): a workload of 300 queries
+    starts with the default 256."""
+    a = pkg.Workload("schema20", 3, SCALE)
+    b = pkg.Workload("schema20", 3, SCALE, queries=300)
+    assert b.num_queries() == 300
+    for k in (0, 17, 255):
+        qa, qb = a.query_ptr(k).contents, b.query_ptr(k).contents
+        assert (qa.num_nodes, qa.root) == (qb.num_nodes, qb.root)
+        assert [qa.nodes[i].base_table_id for i in range(qa.num_nodes)] == \
+               [qb.nodes[i].base_table_id for i in range(qb.num_nodes)]
+    assert a.base_rows(0) >= a.plan_ptr().contents.inputs[0].num_rows
