@@ -109,6 +109,12 @@ ABI = {
     "bj_plan_explain": (_INT, [ctypes.POINTER(BjPlan), ctypes.c_char_p, _U64, ctypes.POINTER(_U64)]),
     "bj_result_wait": (_INT, [_VP]),
     "bj_context_set_ordering": (_INT, [_VP, _INT, _VP]),
+    "bj_server_set_ordering": (_INT, [_VP, _INT, _VP]),
+    "bj_server_set_graphs": (None, [_VP, _INT]),
+    "bj_context_set_graphs": (None, [_VP, _INT]),
+    "bj_plan_scratch_estimate": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), ctypes.POINTER(_U64)]),
+    "bj_server_run_load": (_INT, [_VP, _VP, _U64, _VP, _VP, _U64, ctypes.c_double, ctypes.c_uint32, _U64, _VP,
+                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_U64)]),
     "bj_resident_set_base_rows": (_INT, [_VP, _U64]),
     "bj_subplans": (_INT, [ctypes.POINTER(BjPlan), ctypes.c_uint32, _U64, _VP, ctypes.POINTER(_U64)]),
     "bj_subplan_cards": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), _VP, _U64, _VP]),
@@ -618,6 +624,17 @@ class Context:
         self._check(fn(self.handle, p, arr, m.ctypes.data, len(m), out.ctypes.data), what)
         return out
 
+    def scratch_estimate(self, plan, residents) -> int:
+        """Estimated device scratch of a resident plan (bj_plan_scratch_estimate)."""
+        arr = (ctypes.c_void_p * max(len(residents), 1))(*[x.handle for x in residents])
+        p = plan.ref() if isinstance(plan, CPlan) else plan
+        out = ctypes.c_uint64()
+        self._check(lib().bj_plan_scratch_estimate(self.handle, p, arr, ctypes.byref(out)), "bj_plan_scratch_estimate")
+        return out.value
+
+    def set_graphs(self, on: bool) -> None:
+        lib().bj_context_set_graphs(self.handle, 1 if on else 0)
+
     def subplan_cards(self, plan, residents, masks):
         """Exact cardinality of each sub-plan (device counts)."""
         import numpy as np
@@ -801,11 +818,37 @@ def subplan_corpus(ctx: "Context", workload: "Workload", residents, queries, max
     return out
 
 
+def set_cards_of(ctx: "Context", plan, residents, mode: int, estimator: Optional["Estimator"] = None):
+    """Set cardinalities of every connected input set of a plan, as an array
+    over input masks (2^scans entries): exact device counts (mode None), join
+    samples (ORDER_SAMPLING) or the learned estimator (ORDER_LEARNED; sets of
+    one input keep their row counts, as in the engine)."""
+    import numpy as np
+    masks = subplans(plan, 32)
+    n = max(int(m).bit_length() for m in masks)
+    cards = np.zeros(1 << n, dtype=np.float64)
+    if mode is None:
+        vals = ctx.subplan_cards(plan, residents, masks)
+    else:
+        vals = ctx.subplan_sample_cards(plan, residents, masks)
+        if mode == ORDER_LEARNED:
+            multi = np.array([bin(int(m)).count("1") > 1 for m in masks])
+            if multi.any():
+                f = ctx.subplan_features(plan, residents, masks[multi])
+                vals = vals.copy()
+                vals[multi] = np.maximum(np.exp2(estimator.predict(f).astype(np.float64)) - 1.0, 0.0)
+    cards[masks] = vals
+    return cards
+
+
 class ServerResident:
     """A resident table shared by a server's workers."""
 
     def __init__(self, server: "Server", handle):
         self._server, self.handle = server, handle
+
+    def set_base_rows(self, base_rows: int) -> None:
+        lib().bj_resident_set_base_rows(self.handle, base_rows)
 
     def free(self):
         if self.handle:
@@ -841,6 +884,33 @@ class Server:
             raise EngineError(st, "bj_server_submit failed")
         self._plans[t.value] = arr  # the table array must outlive the query
         return t.value
+
+    def set_ordering(self, mode: int, estimator: Optional["Estimator"] = None) -> None:
+        st = lib().bj_server_set_ordering(self.handle, mode, estimator.handle if estimator else None)
+        if st != 0:
+            raise EngineError(st, "bj_server_set_ordering failed")
+
+    def set_graphs(self, on: bool) -> None:
+        lib().bj_server_set_graphs(self.handle, 1 if on else 0)
+
+    def run_load(self, plan_ptrs, residents: Sequence[ServerResident], seq, rate_qps: float = 0.0,
+                 window: int = 16, seed: int = 0):
+        """The C++ load generator (bj_server_run_load): queries plan_ptrs[seq[i]]
+        as a Poisson stream of rate_qps (closed loop of `window` outstanding
+        queries when rate_qps <= 0). Returns (latencies in ms, elapsed seconds,
+        summed result rows)."""
+        import numpy as np
+        plans = (ctypes.c_void_p * len(plan_ptrs))(*[ctypes.cast(p, ctypes.c_void_p).value for p in plan_ptrs])
+        arr = (ctypes.c_void_p * len(residents))(*[x.handle for x in residents])
+        sq = np.ascontiguousarray(seq, dtype=np.uint32)
+        lat = np.zeros(max(len(sq), 1), dtype=np.float64)
+        el = ctypes.c_double()
+        rows = ctypes.c_uint64()
+        st = lib().bj_server_run_load(self.handle, plans, len(plan_ptrs), arr, sq.ctypes.data, len(sq), rate_qps,
+                                      window, seed, lat.ctypes.data, ctypes.byref(el), ctypes.byref(rows))
+        if st != 0:
+            raise EngineError(st, "bj_server_run_load: a query failed")
+        return lat[:len(sq)], el.value, rows.value
 
     def wait(self, ticket: int):
         """(Result, latency in ms) of a submitted query."""

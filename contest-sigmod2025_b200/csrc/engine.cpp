@@ -1978,6 +1978,15 @@ BJ_API const char* bj_last_error(const bj_context* ctx) { return ctx ? ctx->last
 
 BJ_API void* bj_context_stream(bj_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
 
+BJ_API void bj_context_set_graphs(bj_context* ctx, int on) {
+    if (!ctx) return;
+    if (!on) {
+        // Graphs already captured stay valid but are no longer used.
+        ctx->sync_all();
+    }
+    ctx->graphs = on != 0;
+}
+
 BJ_API void bj_context_profile(bj_context* ctx, int on) {
     if (ctx) ctx->profile = on != 0;
 }

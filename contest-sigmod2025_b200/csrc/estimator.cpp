@@ -677,6 +677,65 @@ BJ_API int bj_join_order(const bj_plan* plan, const double* card, int driver_in,
     return join_order(*plan, card ? &cards : nullptr, driver_in, *driver, *cost, err);
 }
 
+BJ_API int bj_plan_scratch_estimate(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables,
+                                    uint64_t* bytes) {
+    if (!ctx || !plan || !tables || !bytes) return BJ_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    try {
+        // Cardinalities: the context's estimator, or join samples when the
+        // context orders by row counts (which say nothing about sizes).
+        std::vector<double> cards;
+        const int mode = ctx->ordering;
+        if (mode == BJ_ORDER_ROWS) ctx->ordering = BJ_ORDER_SAMPLING;
+        try {
+            estimate_set_cards(ctx, *plan, tables, cards);
+        } catch (...) {
+            ctx->ordering = mode;
+            throw;
+        }
+        ctx->ordering = mode;
+        ExecPlan ex;
+        std::string err;
+        const int st = make_exec_plan(*plan, ex, err, false, cards.empty() ? nullptr : &cards);
+        if (st != BJ_OK) throw Fail{st, err};
+        if (ex.empty) {
+            *bytes = 0;
+            return BJ_OK;
+        }
+        auto card = [&](uint32_t m) {
+            if (!cards.empty()) return cards[m];
+            double c = 0;  // the row-count model: the largest input
+            for (uint32_t i = 0; i < ex.inputs.size(); i++)
+                if (m >> i & 1) c = std::max(c, double(ex.inputs[i].rows));
+            return c;
+        };
+        // Pipelines run children first: each one's input set is its own input
+        // plus its children's.
+        std::vector<uint32_t> sub(ex.pipelines.size(), 0);
+        double total = 0;
+        for (size_t p = 0; p < ex.pipelines.size(); p++) {
+            const PipelinePlan& pp = ex.pipelines[p];
+            sub[p] = 1u << pp.input;
+            for (const auto& pr : pp.probes) sub[p] |= sub[pr.child];
+            const double n = card(sub[p]);
+            const double w = double(pp.slots.size());
+            total += 2.0 * n * (12.0 + 4.0 * double(pp.probes.size()));  // items in and out of the stages
+            if (pp.build_key >= 0) {
+                // tuples and table entries (key, mult, payload, NULL mask,
+                // representative flag), buckets, aggregation slots
+                total += n * (2.0 * (20.0 + 8.0 * w) + 8.0) + 16.0 * std::exp2(double(bit_width(uint64_t(n) + 1)));
+            } else {
+                total += n * 17.0 * double(ex.out_slot.size());  // flat values + result pages
+            }
+        }
+        *bytes = uint64_t(std::min(total, 1.8e19));
+        ctx->arena.reset();
+    } catch (const Fail& f) {
+        return fail_to_status(ctx, f);
+    }
+    return BJ_OK;
+}
+
 BJ_API uint64_t bj_estimator_num_params(void) { return uint64_t(kParams); }
 
 BJ_API int bj_estimator_create(int device, uint64_t seed, bj_estimator** out) {

@@ -106,6 +106,7 @@ typedef struct bj_plan {
 typedef struct bj_context bj_context;
 typedef struct bj_result bj_result;
 typedef struct bj_resident bj_resident;
+typedef struct bj_estimator bj_estimator;
 
 /* Per-call counters, filled by bj_result_stats. */
 typedef struct bj_stats {
@@ -238,6 +239,23 @@ BJ_API int bj_server_submit(bj_server* s, const bj_plan* plan, bj_resident* cons
  * the query's status. */
 BJ_API int bj_server_wait(bj_server* s, uint64_t ticket, bj_result** out, double* latency_ms);
 BJ_API void bj_server_resident_free(bj_server* s, bj_resident* table);
+/* Ordering mode of every worker context (bj_context_set_ordering) and of the
+ * server's planning context (admission estimates). */
+BJ_API int bj_server_set_ordering(bj_server* s, int mode, bj_estimator* estimator);
+/* CUDA-graph replay of repeated queries on (1, the default) or off (0: every
+ * query runs as per-query launches) on every worker. */
+BJ_API void bj_server_set_graphs(bj_server* s, int on);
+/* Load generator (no reference counterpart): submits queries plans[seq[i]]
+ * over `tables` (flags BJ_RESULT_DEVICE) as a Poisson stream of rate_qps
+ * queries per second (seeded exponential gaps), or, with rate_qps <= 0, as a
+ * closed loop keeping `window` queries outstanding; a second thread waits
+ * for each in submission order and frees its result. latency_ms[i] receives
+ * query i's submit-to-completion time, *elapsed_s the run's wall time from
+ * the first submission to the last completion, *rows (optional) the summed
+ * result rows. Returns the first failing query's status. */
+BJ_API int bj_server_run_load(bj_server* s, const bj_plan* const* plans, uint64_t nplans, bj_resident* const* tables,
+                              const uint32_t* seq, uint64_t n, double rate_qps, uint32_t window, uint64_t seed,
+                              double* latency_ms, double* elapsed_s, uint64_t* rows);
 
 /* ---- Join ordering: sub-plan cardinalities and the learned estimator ----
  *
@@ -266,8 +284,6 @@ BJ_API void bj_server_resident_free(bj_server* s, bj_resident* table);
 #define BJ_EST_MAX_TABLES 12
 #define BJ_EST_FEATURES 1792
 #define BJ_EST_HIDDEN 256
-
-typedef struct bj_estimator bj_estimator;
 
 /* Ordering mode of a context (estimator: required for BJ_ORDER_LEARNED, must
  * outlive its use by the context). */
@@ -332,6 +348,18 @@ BJ_API int bj_estimator_gradients(bj_estimator* e, const float* features, const 
                                   float* loss, float* grads);
 BJ_API int bj_estimator_save(bj_estimator* e, const char* path);
 BJ_API int bj_estimator_load(int device, const char* path, bj_estimator** out);
+
+/* Device scratch (intermediate memory) a resident plan is expected to need,
+ * from the set cardinalities of the context's ordering mode (join samples
+ * under BJ_ORDER_ROWS): per pipeline, its items and, for a build, its tuples,
+ * entries and buckets; for the output, its values and pages. Servers admit
+ * plans that have not run yet by this estimate. */
+BJ_API int bj_plan_scratch_estimate(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables,
+                                    uint64_t* bytes);
+
+/* Replay of repeated resident queries as CUDA graphs on (1, the default) or
+ * off (0) for this context (B200JOIN_GRAPHS=0 sets the default to off). */
+BJ_API void bj_context_set_graphs(bj_context* ctx, int on);
 
 /* Turns per-kernel event timing of the scan-side probe stage on (1) or off (0).
  * Adds two event records per timed launch; off by default. */
