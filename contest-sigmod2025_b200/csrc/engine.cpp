@@ -706,8 +706,8 @@ class Executor {
                     out.rows = alloc<uint32_t>(cap);
                     out.ents[0] = alloc<uint32_t>(cap);
                     out.mult = bh.unit_mult ? nullptr : alloc<uint64_t>(cap);
-                    uint32_t* cursor = alloc<uint32_t>(1);
-                    BJ_CK(cudaMemsetAsync(cursor, 0, sizeof(uint32_t), st_));
+                    uint32_t* cursor = alloc<uint32_t>(2);  // item cursor, candidate count (split scan)
+                    BJ_CK(cudaMemsetAsync(cursor, 0, 2 * sizeof(uint32_t), st_));
                     // The next stage reads the count on the device.
                     Items next{};
                     next.rows = out.rows;
@@ -737,8 +737,18 @@ class Executor {
                         }
                         continue;
                     }
-                    launched(scan_probe(key, ht, 2, bloom, nullptr, nullptr, cursor, out.rows, out.ents[0], out.mult,
-                                        cap, ctx_->d_err, ctx_->num_sms, st_));
+                    if (bloom && ctx_->scan_split) {
+                        // Scan + filter, then a probe of the survivors (two
+                        // kernels; the scan carries no probe code). The
+                        // candidate count is the cursor's neighbour, zeroed
+                        // with it.
+                        uint32_t* cand = alloc<uint32_t>(2 * size_t(cap));
+                        launched(scan_probe_split(key, ht, cursor, out.rows, out.ents[0], out.mult, cap, cand,
+                                                  cand + cap, cursor + 1, cap, ctx_->d_err, ctx_->num_sms, st_));
+                    } else {
+                        launched(scan_probe(key, ht, 2, bloom, nullptr, nullptr, cursor, out.rows, out.ents[0],
+                                            out.mult, cap, ctx_->d_err, ctx_->num_sms, st_));
+                    }
                     if (timed) end_timed(page_bytes);
                     trace("scan-side probe enqueued");
                     items = next;
@@ -1941,6 +1951,7 @@ BJ_API int bj_context_create(int device, bj_context** out) {
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (const char* zc = std::getenv("B200JOIN_ZERO_COPY")) ctx->zero_copy = std::atoi(zc) != 0;
     if (const char* gr = std::getenv("B200JOIN_GRAPHS")) ctx->graphs = std::atoi(gr) != 0;
+    if (const char* sp = std::getenv("B200JOIN_SCAN_SPLIT")) ctx->scan_split = std::atoi(sp) != 0;
     if (const char* ss = std::getenv("B200JOIN_STREAM_SCAN")) ctx->stream_scans = std::atoi(ss) != 0;
     if (const char* lb = std::getenv("B200JOIN_LEAF_BATCH")) ctx->leaf_batch = std::atoi(lb) != 0;
     unsigned hw = std::max(1u, std::thread::hardware_concurrency());

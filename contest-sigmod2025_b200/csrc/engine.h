@@ -289,6 +289,7 @@ struct bj_context {
     cudaStream_t copy = nullptr;           // host-to-HBM copies of a streamed scan
     bool stream_scans = true;              // scans of host pages copy them through HBM windows
     bool leaf_batch = true;                // leaf builds batched (one launch per pass)
+    bool scan_split = true;                // scan-side probe with a bloom: filter kernel + candidate probe kernel
     // Join ordering of resident queries (bj_context_set_ordering): the
     // cardinalities the join-order program is given.
     int ordering = 0;                      // BJ_ORDER_ROWS / _SAMPLING / _LEARNED

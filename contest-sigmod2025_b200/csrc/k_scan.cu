@@ -71,6 +71,13 @@ struct ScanArgs {
     uint32_t capacity;         // items the outputs can hold
     uint32_t* err;
     uint32_t row_base;         // row of the first page when rows follow from key.rpp (a window of a column)
+    // Split form (scan_probe_split): the filter kernel appends every bloom
+    // survivor (key, row) here instead of probing it; the probe kernel then
+    // probes them all.
+    uint32_t* cand_key;
+    uint32_t* cand_row;
+    uint32_t* cand_count;      // zero before the filter kernel
+    uint32_t cand_cap;
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
@@ -255,9 +262,33 @@ __device__ __forceinline__ void push_bits(const ScanArgs& a, WarpState& w, uint3
     }
 }
 
+// Split form: appends the candidates flagged in `take` to the global
+// candidate list, one atomic per warp (candidates numbered in lane order).
+template <typename Map>
+__device__ __forceinline__ void append_bits(const ScanArgs& a, uint32_t take, Map&& map) {
+    if (!__any_sync(0xffffffffu, take != 0)) return;
+    uint32_t total;
+    const uint32_t off = warp_excl(__popc(take), total);
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(a.cand_count, total);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    uint32_t o = base + off;
+    for (uint32_t t = take; t; t &= t - 1, o++) {
+        uint32_t key, row;
+        map(__ffs(t) - 1, key, row);
+        if (o < a.cand_cap) {
+            a.cand_key[o] = key;
+            a.cand_row[o] = row;
+        } else {
+            record_error(a.err, kErrCapacity);
+        }
+    }
+}
+
 // Candidates of one step of a page without NULLs: bit c of `take` is value
 // vi0 + 128 (c / 4) + c % 4 of the page of unit p (values at vals, first row
 // row0); the key is read again from the page, which this warp has just loaded.
+template <bool kFilter>
 __device__ __forceinline__ void push_step(const ScanArgs& a, WarpState& w, uint32_t take, int vi0,
                                           const uint32_t* vals, uint32_t row0, uint32_t p, bool dense) {
     auto cand = [&](uint32_t c, uint32_t& key, uint32_t& row) {
@@ -265,7 +296,9 @@ __device__ __forceinline__ void push_step(const ScanArgs& a, WarpState& w, uint3
         key = __ldg(vals + vi);
         row = row0 + vi;
     };
-    if (dense)
+    if (kFilter)
+        append_bits(a, take, cand);
+    else if (dense)
         probe_bits(a, w, take, p, cand);
     else
         push_bits(a, w, take, p, cand);
@@ -313,6 +346,7 @@ __device__ __forceinline__ uint32_t step_valid(int vi0, uint32_t n) {
 // of their 64-row chunk, plus the popcount of the chunk's lower word for an
 // upper half, gives the value index of the first valid row. Without a bloom
 // every valid row is a candidate and no value is read before the probe.
+template <bool kFilter>
 __device__ __forceinline__ void scan_rows_nulls(const ScanArgs& a, WarpState& w, const uint32_t* bloom,
                                                 bool use_bloom, uint32_t unit, uint32_t p, uint32_t n,
                                                 uint32_t row0, uint32_t r_begin, uint32_t r_end) {
@@ -361,17 +395,22 @@ __device__ __forceinline__ void scan_rows_nulls(const ScanArgs& a, WarpState& w,
             key = __ldg(vals + d0 + __popc(wb & ((1u << c) - 1)));
             row = row0 + r + c;
         };
-        if (use_bloom)
+        if (kFilter)
+            append_bits(a, take, cand);
+        else if (use_bloom)
             push_bits(a, w, take, unit, cand);
         else
             probe_bits(a, w, take, unit, cand);
     }
 }
 
+// kFilter: the filter kernel of the split form (no probes; survivors go to
+// the candidate list). Otherwise the fused scan-side probe.
+template <bool kFilter>
 __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
     extern __shared__ uint4 bloom4[];
-    __shared__ uint32_t bkey[kWarpsPerCta][kBatch];
-    __shared__ uint32_t brow[kWarpsPerCta][kBatch];
+    __shared__ uint32_t bkey[kFilter ? 1 : kWarpsPerCta][kFilter ? 1 : kBatch];
+    __shared__ uint32_t brow[kFilter ? 1 : kWarpsPerCta][kFilter ? 1 : kBatch];
     const uint32_t* bloom = reinterpret_cast<const uint32_t*>(bloom4);
     const bool use_bloom = a.use_bloom != 0;
     const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
@@ -411,7 +450,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
     }
     __syncthreads();
 
-    WarpState w{bkey[warp], brow[warp], 0, 0};
+    WarpState w{bkey[kFilter ? 0 : warp], brow[kFilter ? 0 : warp], 0, 0};
     for (uint32_t u = first; u < nunits; u += total_warps) {
         const uint32_t p = u / kUnitsPerPage, part = u % kUnitsPerPage;
         load_unit(u, q, hdr_l, row0_l);
@@ -437,21 +476,64 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
         if (nn == n) {
             const int vi0 = 4 * int(lane) - 1 + int(part * 4 * kWordsPerStep);
             if (vi0 - int(lane) * 4 < int(n))  // some value of the unit is below n
-                push_step(a, w, step_take(a, q, bloom, use_bloom) & step_valid(vi0, n), vi0, vals, row0, u,
-                          !use_bloom);
+                push_step<kFilter>(a, w, step_take(a, q, bloom, use_bloom) & step_valid(vi0, n), vi0, vals, row0,
+                                   u, !use_bloom);
         } else {
             // A page with NULLs: unit k takes rows [1024 k, 1024 (k + 1)), the
             // last unit every row from there on.
             const uint32_t r_begin = part * 1024;
             const uint32_t r_end = part + 1 == kUnitsPerPage ? n : min(n, r_begin + 1024);
-            if (r_begin < r_end) scan_rows_nulls(a, w, bloom, use_bloom, u, p, n, row0, r_begin, r_end);
+            if (r_begin < r_end) scan_rows_nulls<kFilter>(a, w, bloom, use_bloom, u, p, n, row0, r_begin, r_end);
         }
-        if (a.mode != 2) {
+        if (!kFilter && a.mode != 2) {
             flush(a, w, u);
             if (a.mode == 0 && lane == 0) a.page_counts[u] = w.page_cnt;
         }
     }
-    if (a.mode == 2) flush(a, w, 0);
+    if (!kFilter && a.mode == 2) flush(a, w, 0);
+}
+
+// The probe kernel of the split form: every candidate of the list, 128 per
+// warp (four per lane), probed against the table and appended as items
+// (mode 2: unique build keys).
+__global__ void __launch_bounds__(256) k_probe_candidates(ScanArgs a) {
+    const uint32_t n = min(*a.cand_count, a.cand_cap);
+    const uint32_t lane = lane_id();
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    WarpState w{nullptr, nullptr, 0, 0};
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kBatch; base < n;
+         base += warps * kBatch) {
+        uint32_t key[kPerLane], row[kPerLane], has = 0;
+#pragma unroll
+        for (int i = 0; i < kPerLane; i++) {
+            const uint32_t h = base + lane + 32 * i;
+            key[i] = row[i] = 0;
+            if (h < n) {
+                key[i] = a.cand_key[h];
+                row[i] = a.cand_row[h];
+                has |= 1u << i;
+            }
+        }
+        probe_batch(a, w, key, row, has, 0);
+    }
+}
+
+template <bool kFilter>
+void launch_scan(const ScanArgs& a, size_t bloom_bytes, int num_sms, cudaStream_t st) {
+    // Once per process and form (thread-safe static initialisation; server
+    // workers launch from several threads).
+    static const bool configured = [] {
+        cudaFuncSetAttribute(k_scan_probe<kFilter>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBloomSmemMax));
+        return true;
+    }();
+    (void)configured;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan_probe<kFilter>, kCtaThreads, bloom_bytes);
+    per_sm = std::max(1, per_sm);
+    const uint64_t ctas =
+        std::min<uint64_t>((uint64_t(kUnitsPerPage) * a.key.npages + kWarpsPerCta - 1) / kWarpsPerCta,
+                           uint64_t(num_sms) * per_sm);
+    k_scan_probe<kFilter><<<unsigned(ctas), kCtaThreads, bloom_bytes, st>>>(a);
 }
 
 } // namespace
@@ -475,21 +557,26 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
     const uint32_t prefetch = (key.flags & kColHostPages) ? 0u : ahead;
     ScanArgs a{key,      ht,       uint32_t(mode), bloom_bytes ? 1u : 0u, prefetch,
                ht.bloom_log2 ? (1u << ht.bloom_log2) : 0u, 1u << 27,
-               page_counts, page_off, cursor, out_rows, out_ents, out_mult, capacity, err, row_base};
-    // Once per process (thread-safe static initialisation; server workers
-    // launch from several threads).
-    static const bool configured = [] {
-        cudaFuncSetAttribute(k_scan_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBloomSmemMax));
-        return true;
-    }();
-    (void)configured;
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scan_probe, kCtaThreads, bloom_bytes);
-    per_sm = std::max(1, per_sm);
-    const uint64_t ctas = std::min<uint64_t>((uint64_t(scan_probe_units(key.npages)) + kWarpsPerCta - 1) / kWarpsPerCta,
-                                             uint64_t(num_sms) * per_sm);
-    k_scan_probe<<<unsigned(ctas), kCtaThreads, bloom_bytes, st>>>(a);
+               page_counts, page_off, cursor, out_rows, out_ents, out_mult, capacity, err, row_base,
+               nullptr, nullptr, nullptr, 0};
+    launch_scan<false>(a, bloom_bytes, num_sms, st);
     return 1;
+}
+
+int scan_probe_split(const DevColumn& key, const HTView& ht, uint32_t* cursor, uint32_t* out_rows, uint32_t* out_ents,
+                     uint64_t* out_mult, uint32_t capacity, uint32_t* cand_key, uint32_t* cand_row,
+                     uint32_t* cand_count, uint32_t cand_cap, uint32_t* err, int num_sms, cudaStream_t st,
+                     uint32_t row_base) {
+    if (!key.npages) return 0;
+    size_t bloom_bytes = ht.bloom ? (sizeof(uint32_t) << ht.bloom_log2) : 0;
+    if (bloom_bytes > kBloomSmemMax) bloom_bytes = 0;
+    ScanArgs a{key,      ht,       2u, bloom_bytes ? 1u : 0u, 0u,
+               ht.bloom_log2 ? (1u << ht.bloom_log2) : 0u, 1u << 27,
+               nullptr, nullptr, cursor, out_rows, out_ents, out_mult, capacity, err, row_base,
+               cand_key, cand_row, cand_count, cand_cap};
+    launch_scan<true>(a, bloom_bytes, num_sms, st);
+    k_probe_candidates<<<unsigned(num_sms) * 4, 256, 0, st>>>(a);
+    return 2;
 }
 
 } // namespace bj

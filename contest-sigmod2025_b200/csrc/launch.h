@@ -227,6 +227,16 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
                const uint32_t* page_off, uint32_t* cursor, uint32_t* out_rows, uint32_t* out_ents, uint64_t* out_mult,
                uint32_t capacity, uint32_t* err, int num_sms, cudaStream_t st, uint32_t row_base = 0);
 
+// The same stage (mode 2: unique build keys, bloom filter present) as two
+// kernels: the scan streams the key pages and appends every bloom survivor
+// (key, row) to a candidate list (cand_count zero before; room for
+// cand_cap, at most the column's rows), then a probe kernel probes the list
+// and appends items at *cursor. The scan then carries no probe code.
+int scan_probe_split(const DevColumn& key, const HTView& ht, uint32_t* cursor, uint32_t* out_rows, uint32_t* out_ents,
+                     uint64_t* out_mult, uint32_t capacity, uint32_t* cand_key, uint32_t* cand_row,
+                     uint32_t* cand_count, uint32_t cand_cap, uint32_t* err, int num_sms, cudaStream_t st,
+                     uint32_t row_base = 0);
+
 // ---- hash table build (k_build.cu) ----
 // Tuples of a build pipeline, one per item: key from `key` (NULL key ->
 // mult 0), payload from `src`, mult from the item.
