@@ -19,7 +19,6 @@ import numpy as np
 import pytest
 
 import mlp_ref
-import oracle_lib
 
 pytestmark = pytest.mark.gpu
 
@@ -128,7 +127,8 @@ def test_subplan_cards_match_cpu_counts(pkg, schema, oracle):
             checked += 1
         # The whole query: the oracle's row count.
         full = (1 << len(_graph(plan)[0])) - 1
-        want_full = len(oracle.rows(oracle.execute(plan_ptr).view()))
+        result = oracle.execute(plan_ptr)  # held while its rows are read
+        want_full = len(oracle.rows(result.view()))
         assert ctx.subplan_cards(plan_ptr, res, [full])[0] == want_full
     assert checked >= 20
 

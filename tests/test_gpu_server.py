@@ -75,7 +75,11 @@ def test_orderings_and_load_generator_give_the_oracle_rows(pkg, oracle):
 
     w = pkg.Workload("schema20", 3, 0.01, queries=300)
     queries = list(range(0, 64, 2))
-    wants = {k: len(oracle.rows(oracle.execute(w.query_ptr(k)).view())) for k in queries}
+    def oracle_rows(k):
+        result = oracle.execute(w.query_ptr(k))  # held while its rows are read
+        return len(oracle.rows(result.view()))
+
+    wants = {k: oracle_rows(k) for k in queries}
     est = pkg.Estimator(0, seed=1)
     # A quickly trained estimator: its estimates only steer the order.
     with pkg.Context(0) as ctx:
@@ -87,10 +91,10 @@ def test_orderings_and_load_generator_give_the_oracle_rows(pkg, oracle):
             ctx.set_ordering(mode, est if mode == pkg.ORDER_LEARNED else None)
             for k in queries[:12]:
                 q = w.query_ptr(k)
+                want = oracle.execute(q)
                 with ctx.execute_resident(q, res) as r:
                     got, keep = r.table_struct()
-                    oracle_lib.assert_same_rows(oracle, ctypes.byref(got), oracle.execute(q).view(),
-                                                f"query {k} ordering {mode}")
+                    oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), f"query {k} ordering {mode}")
             assert ctx.scratch_estimate(w.query_ptr(queries[0]), res) > 0
         for x in res:
             x.free()

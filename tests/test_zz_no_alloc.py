@@ -84,8 +84,8 @@ def test_join_count_static_matches_oracle(pkg, oracle):
         for seed, (nb, npr, dom, null_p, neg_p) in enumerate(CASES):
             tb, tp = make_tables(pkg, 77 + seed, nb, npr, dom, null_p, neg_p)
             cplan = join_plan(pkg, tb, tp)
-            want = oracle.rows(oracle.execute(cplan.ref()).view())
-            want_n = len(want)
+            result = oracle.execute(cplan.ref())  # held while its rows are read
+            want_n = len(oracle.rows(result.view()))
             with ctx.execute_raw(cplan.ref()) as r:
                 assert r.num_rows == want_n, f"case {seed}: bj_execute {r.num_rows} != oracle {want_n}"
             db, nbp = device_pages(tb)
@@ -113,7 +113,9 @@ def test_join_count_static_flags_bad_input(pkg, oracle):
     import torch
 
     tb, tp = make_tables(pkg, 5, 4000, 9000, 3000, 0.0, 0.0)
-    want_n = len(oracle.rows(oracle.execute(join_plan(pkg, tb, tp).ref()).view()))
+    cplan = join_plan(pkg, tb, tp)  # its page buffers live as long as it does
+    result = oracle.execute(cplan.ref())
+    want_n = len(oracle.rows(result.view()))
     db, nbp = device_pages(tb)
     dp, npp = device_pages(tp)
     out = torch.zeros(1, dtype=torch.int64, device="cuda")
