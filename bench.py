@@ -188,6 +188,79 @@ def profiled_traffic():
         return None
 
 
+def resident_rate(pkg, ctx, plan, residents, steps, warmup, stream, torch):
+    """Queries/s of a resident plan (device-timed, one query issued ahead,
+    every result waited for), then a profiled pass: the scan-side probe
+    stage's launches, their time and page bytes."""
+    for _ in range(warmup):
+        ctx.execute_resident(plan, residents, flags=pkg.RESULT_DEVICE).free()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    pending, rows, lat = None, 0, []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        r = ctx.execute_resident(plan, residents, flags=pkg.RESULT_DEVICE | pkg.RESULT_ASYNC)
+        if pending:
+            pending[0].wait()
+            rows = pending[0].num_rows
+            lat.append((time.perf_counter() - pending[1]) * 1e3)
+            pending[0].free()
+        pending = (r, t0)
+    if pending:
+        pending[0].wait()
+        rows = pending[0].num_rows
+        lat.append((time.perf_counter() - pending[1]) * 1e3)
+        pending[0].free()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    ctx.profile(True)
+    scan_ms = scan_bytes = scan_n = 0
+    for i in range(3 + min(steps, 50)):
+        r = ctx.execute_resident(plan, residents, flags=pkg.RESULT_DEVICE)
+        st = r.stats()
+        r.free()
+        if i >= 3:
+            scan_ms += st.scan_kernel_ms
+            scan_bytes += st.scan_kernel_bytes
+            scan_n += st.scan_kernel_launches
+    ctx.profile(False)
+    return {"value": steps / (ms / 1e3), "ms_per_step": ms / steps, "p50_ms": statistics.median(lat), "rows": rows,
+            "scan_ms": scan_ms, "scan_bytes": scan_bytes, "scan_launches": scan_n}
+
+
+def join2_line(pkg, local, steps, warmup, torch):
+    """The two-table join (R 1M rows, S 8M rows with 10% NULL keys, output
+    R.payload, S.payload, S.fk) over resident tables: queries/s, the
+    algorithmic bytes of a query (input pages scanned + result pages
+    written) per second, and the scan-side probe stage against HBM."""
+    w = pkg.Workload("join2", 1, 1.0)
+    plan = w.plan_ptr()
+    with pkg.Context(local) as ctx:
+        inputs = plan.contents
+        res = [ctx.upload(inputs.inputs[i]) for i in range(inputs.num_inputs)]
+        r = ctx.execute_resident(plan, res)
+        out_pages = sum(r.column_pages(c) for c in range(r.num_columns))
+        r.free()
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+        m = resident_rate(pkg, ctx, plan, res, steps, warmup, stream, torch)
+        for x in res:
+            x.free()
+    peak, kind = measured_peak()
+    b_alg = w.scan_bytes() + out_pages * pkg.PAGE_SIZE
+    scan = (m["scan_bytes"] / m["scan_launches"]) / (m["scan_ms"] / m["scan_launches"] / 1e3) / 1e9 \
+        if m["scan_launches"] and m["scan_ms"] > 0 else None
+    return {"workload": "join2: R 1M rows (INT32 key, INT64 payload), S 8M rows (INT32 fk, 10% NULL; INT32 "
+                        "payload); output R.payload, S.payload, S.fk", "value": m["value"], "unit": "queries/s",
+            "ms_per_step": m["ms_per_step"], "p50_ms": m["p50_ms"], "rows": m["rows"],
+            "alg_bytes_per_query": b_alg, "alg_gbs": b_alg * m["value"] / 1e9,
+            "roofline": {"bound": "hbm", "achieved": scan, "peak": peak, "unit": "GB/s",
+                         "frac": scan / peak if scan else None, "kernel": "scan-side probe stage over S.fk pages",
+                         "peak_kind": f"{kind} HBM copy bandwidth"},
+            "whole_query_frac": b_alg * m["value"] / 1e9 / peak}
+
+
 class Replicas:
     """The ranks of a multi-GPU run: one process per GPU, each running whole
     queries on its own replica of the tables (no data exchange). Timing is the
@@ -517,6 +590,9 @@ def main():
 
     if args.mode == "e2e":
         args.steps = 0
+    # The autotuner picks build and scan parameters for this plan's shape
+    # class before anything is timed (bj_context_autotune).
+    tune_report = ctx.autotune(plan, residents, repeats=3) if args.steps else ""
     # ---- value: tables resident in HBM ----
     # The timed steps run without instrumentation. A second, shorter pass with
     # the engine's CUDA-event profiling on gives the scan kernel's launch time
@@ -652,6 +728,8 @@ def main():
     for x in residents:
         x.free()
     ctx.close()
+    # ---- the two-table join (config 1) as its own sub-line ----
+    join2 = join2_line(pkg, local, max(args.steps, 20), args.warmup, torch) if world == 1 else None
     # ---- serving headline: learned+batched vs plain (one GPU, rank 0) ----
     serving = serve_headline(pkg, args, local) if args.serve_queries > 0 and world == 1 else None
     if dist:
@@ -684,6 +762,8 @@ def main():
         "gpu_launches": launches,
         "phases": phases,
         "serving": serving,
+        "join2": join2,
+        "autotune": [l for l in tune_report.splitlines() if l.startswith("chosen")],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "traffic": traffic,
                      "kernel": "k_scan_probe over the fact's key pages",

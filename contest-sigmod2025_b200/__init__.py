@@ -112,6 +112,8 @@ ABI = {
     "bj_server_set_ordering": (_INT, [_VP, _INT, _VP]),
     "bj_server_set_graphs": (None, [_VP, _INT]),
     "bj_context_set_graphs": (None, [_VP, _INT]),
+    "bj_context_autotune": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), _INT, ctypes.c_char_p, _U64,
+                                   ctypes.POINTER(_U64)]),
     "bj_plan_scratch_estimate": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), ctypes.POINTER(_U64)]),
     "bj_server_run_load": (_INT, [_VP, _VP, _U64, _VP, _VP, _U64, ctypes.c_double, ctypes.c_uint32, _U64, _VP,
                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_U64)]),
@@ -634,6 +636,17 @@ class Context:
 
     def set_graphs(self, on: bool) -> None:
         lib().bj_context_set_graphs(self.handle, 1 if on else 0)
+
+    def autotune(self, plan, residents, repeats: int = 5) -> str:
+        """Tunes build and scan parameters for the plan's shape class
+        (bj_context_autotune); returns the report."""
+        arr = (ctypes.c_void_p * max(len(residents), 1))(*[x.handle for x in residents])
+        p = plan.ref() if isinstance(plan, CPlan) else plan
+        buf = ctypes.create_string_buffer(8192)
+        n = ctypes.c_uint64()
+        self._check(lib().bj_context_autotune(self.handle, p, arr, repeats, buf, 8192, ctypes.byref(n)),
+                    "bj_context_autotune")
+        return buf.value.decode()
 
     def subplan_cards(self, plan, residents, masks):
         """Exact cardinality of each sub-plan (device counts)."""

@@ -406,6 +406,33 @@ int guess_first_probe(const ExecPlan& ex, const bj_plan& plan) {
     return best;
 }
 
+// Shape class of a plan for the autotuner: the rows of its largest and its
+// second largest input (powers of two) and its number of inputs -- what
+// the plan is, not how it was ordered. Plans of one class share tuned build
+// and scan parameters.
+uint64_t shape_class(const ExecPlan& ex) {
+    uint64_t a = 0, b = 0;
+    for (const PlanInput& in : ex.inputs) {
+        if (in.rows > a) {
+            b = a;
+            a = in.rows;
+        } else if (in.rows > b) {
+            b = in.rows;
+        }
+    }
+    return (uint64_t(bit_width(a)) << 16) | (uint64_t(bit_width(b)) << 8) | std::min<uint64_t>(ex.inputs.size(), 255);
+}
+
+// The parameters of a call: the tuner's override, else the class's tuned
+// ones, else the defaults.
+TuneConfig tune_for(const bj_context* ctx, const ExecPlan& ex) {
+    if (ctx->tune_override) return *ctx->tune_override;
+    const uint64_t key = shape_class(ex);
+    for (const auto& [k, c] : ctx->tuned)
+        if (k == key) return c;
+    return TuneConfig{};
+}
+
 class Executor {
     public:
     Executor(bj_context* ctx, const ExecPlan& ex, std::vector<const DevTable*> tables)
@@ -737,7 +764,7 @@ class Executor {
                         }
                         continue;
                     }
-                    if (bloom && ctx_->scan_split) {
+                    if (bloom && ctx_->scan_split && ctx_->tune.scan_split) {
                         // Scan + filter, then a probe of the survivors (two
                         // kernels; the scan carries no probe code). The
                         // candidate count is the cursor's neighbour, zeroed
@@ -911,12 +938,14 @@ class Executor {
         ba.distinct = items.rows == nullptr && items.mult == nullptr && items.nprobes == 0 ? 1u : 0u;
         ba.tlog2 = ba.distinct ? 1u : std::max<uint32_t>(1, bit_width(uint64_t(n) * 2));
         const uint32_t nrep = n;
-        const uint32_t blog2 = std::max<uint32_t>(bit_width(nrep), 4);
+        // Autotuned: bucket count (fill factor) and bloom bits per key.
+        const TuneConfig& tc = ctx_->tune;
+        const uint32_t blog2 = std::min<uint32_t>(31, std::max<uint32_t>(bit_width(nrep), 4) + tc.bucket_extra);
         ba.shift = 64 - blog2;
         pb.nb = uint32_t(1) << blog2;
         pb.with_bloom = !wide && uint64_t(nrep) * 8 <= (uint64_t(32) << kBloomMaxLog2);
         pb.wlog2 = pb.with_bloom ? std::min<uint32_t>(kBloomMaxLog2,
-                                                      std::max<uint32_t>(5, bit_width((uint64_t(nrep) * 16 + 31) / 32 - 1)))
+                                                      std::max<uint32_t>(5, bit_width((uint64_t(nrep) * tc.bloom_bits + 31) / 32 - 1)))
                                  : 0;
         pb.zb_table = sizeof(uint32_t) << ba.tlog2;
         pb.zb_counts = sizeof(uint32_t) * pb.nb;
@@ -1366,6 +1395,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
         }
         int st = make_exec_plan(*plan, ex, err, false, use_cards);
         if (st != BJ_OK) throw Fail{st, err};
+        ctx->tune = tune_for(ctx, ex);
         res->types = ex.out_types;
         uint64_t launches0 = ctx->launches;
         BJ_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(uint32_t), ctx->stream));
@@ -1595,6 +1625,7 @@ bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resid
         std::string err;
         if (make_exec_plan(*plan, ex, err, false, g.cards.empty() ? nullptr : &g.cards) != BJ_OK || ex.empty)
             return false;
+        ctx->tune = tune_for(ctx, ex);
         std::vector<const DevTable*> tables(plan->num_inputs);
         for (uint64_t i = 0; i < plan->num_inputs; i++) tables[i] = &resident[i]->table;
         g.tape.pos = 0;
@@ -1988,6 +2019,86 @@ BJ_API void bj_context_destroy(bj_context* ctx) {
 BJ_API const char* bj_last_error(const bj_context* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
 
 BJ_API void* bj_context_stream(bj_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+BJ_API int bj_context_autotune(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int repeats,
+                               char* report, uint64_t cap, uint64_t* len) {
+    if (!ctx || !plan || !tables || repeats < 1) return BJ_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    ExecPlan ex;
+    std::string err;
+    int st = make_exec_plan(*plan, ex, err);
+    if (st != BJ_OK) {
+        ctx->last_error = err;
+        return st;
+    }
+    const uint64_t key = shape_class(ex);
+    std::string text = "shape class " + std::to_string(key >> 16) + "/" + std::to_string((key >> 8) & 255) + "/" +
+                       std::to_string(key & 255) + " (log2 rows of the largest and second largest input / inputs)\n";
+    const bool graphs = ctx->graphs;
+    ctx->graphs = false;  // every run executes (no replay)
+    TuneConfig best{};
+    double best_ms = -1;
+    int64_t rows = -1;  // every parameter set must return the same row count
+    for (uint8_t split : {uint8_t(1), uint8_t(0)})
+        for (uint8_t bits : {uint8_t(8), uint8_t(16), uint8_t(32)})
+            for (uint8_t extra : {uint8_t(0), uint8_t(1)}) {
+                TuneConfig c{split, bits, extra};
+                ctx->tune_override = &c;
+                std::vector<double> ms;
+                for (int r = 0; r <= repeats && st == BJ_OK; r++) {
+                    bj_result* res = nullptr;
+                    st = bj_execute_resident(ctx, plan, tables, BJ_RESULT_DEVICE, &res);
+                    if (st != BJ_OK) break;
+                    bj_stats s{};
+                    bj_result_stats(res, &s);
+                    const int64_t n = int64_t(bj_result_num_rows(res));
+                    bj_result_free(res);
+                    if (rows >= 0 && n != rows) {
+                        ctx->last_error = "autotune: parameter sets returned different row counts";
+                        st = BJ_ERR_INTERNAL;
+                        break;
+                    }
+                    rows = n;
+                    if (r > 0) ms.push_back(s.device_ms);  // the first run warms up
+                }
+                ctx->tune_override = nullptr;
+                if (st != BJ_OK) break;
+                std::sort(ms.begin(), ms.end());
+                const double med = ms[ms.size() / 2];
+                char line[160];
+                std::snprintf(line, sizeof(line), "scan %s, bloom %2u bits/key, buckets x%u: %.4f ms\n",
+                              split ? "split" : "fused", unsigned(bits), 1u << extra, med);
+                text += line;
+                if (best_ms < 0 || med < best_ms) {
+                    best_ms = med;
+                    best = c;
+                }
+            }
+    ctx->graphs = graphs;
+    if (st != BJ_OK) return st;
+    bool found = false;
+    for (auto& [k, c] : ctx->tuned)
+        if (k == key) {
+            c = best;
+            found = true;
+        }
+    if (!found) ctx->tuned.push_back({key, best});
+    // Graphs captured under other parameters are dropped.
+    ctx->sync_all();
+    for (auto& g : ctx->graph_cache) destroy_graph(*g);
+    ctx->graph_cache.clear();
+    char line[160];
+    std::snprintf(line, sizeof(line), "chosen: scan %s, bloom %u bits/key, buckets x%u (%.4f ms)\n",
+                  best.scan_split ? "split" : "fused", unsigned(best.bloom_bits), 1u << best.bucket_extra, best_ms);
+    text += line;
+    if (len) *len = text.size();
+    if (report && cap) {
+        const size_t n = std::min<size_t>(cap - 1, text.size());
+        std::memcpy(report, text.data(), n);
+        report[n] = 0;
+    }
+    return BJ_OK;
+}
 
 BJ_API void bj_context_set_graphs(bj_context* ctx, int on) {
     if (!ctx) return;

@@ -221,6 +221,17 @@ struct ReadbackTape {
     size_t pos = 0;
 };
 
+// Build and scan parameters the autotuner chooses per plan shape class
+// (bj_context_autotune): the defaults are the engine's fixed choices.
+struct TuneConfig {
+    uint8_t scan_split = 1;    // scan-side probe with a bloom: filter + candidate probe kernels (1) or fused (0)
+    uint8_t bloom_bits = 16;   // bloom filter bits per key (capped at 128 KiB per filter)
+    uint8_t bucket_extra = 0;  // buckets = 2^(bit_width(tuples) + extra): lower fill factors for extra > 0
+    bool operator==(const TuneConfig& o) const {
+        return scan_split == o.scan_split && bloom_bits == o.bloom_bits && bucket_extra == o.bucket_extra;
+    }
+};
+
 // Statistics of one join-key column of a resident table (estimator.cpp).
 struct ColStats {
     bool ready = false;
@@ -290,6 +301,11 @@ struct bj_context {
     bool stream_scans = true;              // scans of host pages copy them through HBM windows
     bool leaf_batch = true;                // leaf builds batched (one launch per pass)
     bool scan_split = true;                // scan-side probe with a bloom: filter kernel + candidate probe kernel
+    // Autotuned parameters per plan shape class (key: shape_class), the
+    // configuration of the running call, and an override while tuning.
+    std::vector<std::pair<uint64_t, bj::TuneConfig>> tuned;
+    bj::TuneConfig tune{};
+    const bj::TuneConfig* tune_override = nullptr;
     // Join ordering of resident queries (bj_context_set_ordering): the
     // cardinalities the join-order program is given.
     int ordering = 0;                      // BJ_ORDER_ROWS / _SAMPLING / _LEARNED

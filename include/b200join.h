@@ -357,6 +357,20 @@ BJ_API int bj_estimator_load(int device, const char* path, bj_estimator** out);
 BJ_API int bj_plan_scratch_estimate(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables,
                                     uint64_t* bytes);
 
+/* Autotuner (no reference counterpart): runs a resident plan `repeats` times
+ * (after one warm-up run) under each combination of the engine's tunable
+ * build and scan parameters -- scan-side probe as one fused kernel or as a
+ * filter kernel plus a candidate probe kernel; bloom filter bits per key
+ * 8/16/32; hash buckets x1/x2 the reference's count (fill factor) -- keeps
+ * the fastest by median device time for the plan's shape class (log2 rows of
+ * its largest and second largest inputs, number of inputs), and
+ * uses it for every later plan of that class on this context. Results are
+ * the same rows under every parameter set. Drops the context's captured
+ * graphs. `report` (optional, cap bytes) receives one line per
+ * combination and the choice; *len its length. */
+BJ_API int bj_context_autotune(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int repeats,
+                               char* report, uint64_t cap, uint64_t* len);
+
 /* Replay of repeated resident queries as CUDA graphs on (1, the default) or
  * off (0) for this context (B200JOIN_GRAPHS=0 sets the default to off). */
 BJ_API void bj_context_set_graphs(bj_context* ctx, int on);
