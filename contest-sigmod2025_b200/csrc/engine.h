@@ -224,7 +224,7 @@ struct ReadbackTape {
 // Build and scan parameters the autotuner chooses per plan shape class
 // (bj_context_autotune): the defaults are the engine's fixed choices.
 struct TuneConfig {
-    uint8_t scan_split = 1;    // scan-side probe with a bloom: filter + candidate probe kernels (1) or fused (0)
+    uint8_t scan_split = 0;    // scan-side probe with a bloom: filter + candidate probe kernels (1) or fused (0)
     uint8_t bloom_bits = 16;   // bloom filter bits per key (capped at 128 KiB per filter)
     uint8_t bucket_extra = 0;  // buckets = 2^(bit_width(tuples) + extra): lower fill factors for extra > 0
     bool operator==(const TuneConfig& o) const {
@@ -300,7 +300,7 @@ struct bj_context {
     cudaStream_t copy = nullptr;           // host-to-HBM copies of a streamed scan
     bool stream_scans = true;              // scans of host pages copy them through HBM windows
     bool leaf_batch = true;                // leaf builds batched (one launch per pass)
-    bool scan_split = true;                // scan-side probe with a bloom: filter kernel + candidate probe kernel
+    bool scan_split = true;                // allow the split scan where the tuned parameters ask for it
     // Autotuned parameters per plan shape class (key: shape_class), the
     // configuration of the running call, and an override while tuning.
     std::vector<std::pair<uint64_t, bj::TuneConfig>> tuned;
