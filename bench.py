@@ -67,6 +67,8 @@ def parse():
                     help="open-loop run length per rate (queries = rate x seconds, 100 to --serve-queries)")
     ap.add_argument("--est-per-query", type=int, default=64, help="training sub-plans per query (768 queries)")
     ap.add_argument("--est-epochs", type=int, default=30)
+    ap.add_argument("--autotune-repeats", type=int, default=3,
+                    help="runs per parameter set of the autotuner before timing (0: engine defaults)")
     ap.add_argument("--mode", default="all", choices=["all", "value", "e2e", "serve", "batch", "estimator"],
                     help="value / e2e run one measurement only (for profiling); all prints the bench line; "
                          "batch runs every query of a batched workload (--workload schema20); serve runs the "
@@ -592,7 +594,8 @@ def main():
         args.steps = 0
     # The autotuner picks build and scan parameters for this plan's shape
     # class before anything is timed (bj_context_autotune).
-    tune_report = ctx.autotune(plan, residents, repeats=3) if args.steps else ""
+    tune_report = ctx.autotune(plan, residents, repeats=args.autotune_repeats) \
+        if args.steps and args.autotune_repeats > 0 else ""
     # ---- value: tables resident in HBM ----
     # The timed steps run without instrumentation. A second, shorter pass with
     # the engine's CUDA-event profiling on gives the scan kernel's launch time

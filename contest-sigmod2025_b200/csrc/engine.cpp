@@ -642,6 +642,24 @@ class Executor {
         readback(ctx_, 1);
         return uint32_t(ctx_->h_small[0]);
     }
+    // The same for counts of items (rows of an intermediate result), which are
+    // 32-bit: the counts are also summed in 64 bits, and a join step whose
+    // result would not fit fails with kItemOverflow instead of wrapping.
+    uint32_t item_total(const uint32_t* in, uint32_t* out, size_t n) {
+        launched(scan_exclusive_u32(in, out, n, A_, st_));
+        auto* wide = reinterpret_cast<unsigned long long*>(alloc<uint64_t>(1));
+        launched(sum_u32_wide(in, n, wide, st_));
+        stash_u32(ctx_, out + n, 0);
+        stash_u64(ctx_, reinterpret_cast<const uint64_t*>(wide), 1);
+        stash_err(ctx_);
+        readback(ctx_, 2);
+        if (ctx_->h_small[1] > 0xfffffffeull) {
+            ctx_->item_overflow = true;
+            throw Fail{BJ_ERR_UNSUPPORTED, "a join step yields " + std::to_string(ctx_->h_small[1]) +
+                                               " intermediate rows, more than 2^32 - 2"};
+        }
+        return uint32_t(ctx_->h_small[0]);
+    }
     uint64_t scan_total_u64(const uint64_t* in, uint64_t* out, size_t n) {
         launched(scan_exclusive_u64(in, out, n, A_, st_));
         stash_u64(ctx_, out + n, 0);
@@ -790,7 +808,7 @@ class Executor {
                     launched(scan_probe(key, ht, 0, bloom, pc, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
                                         ctx_->d_err, ctx_->num_sms, st_));
                     if (timed) end_timed(page_bytes);
-                    total = scan_total_u32(pc, poff, units);
+                    total = item_total(pc, poff, units);
                     if (total) {
                         out.rows = alloc<uint32_t>(total);
                         out.ents[0] = alloc<uint32_t>(total);
@@ -832,13 +850,13 @@ class Executor {
             uint32_t* toff = alloc<uint32_t>(tiles + 1);
             ItemsOut none{};
             launched(probe_stage(items, key, ht, 0, tc, nullptr, none, bloom, ctx_->d_err, st_));
-            uint32_t total = scan_total_u32(tc, toff, tiles);
+            uint32_t total = item_total(tc, toff, tiles);
             if (total == 0) return false;
             ItemsOut out{};
             out.rows = alloc<uint32_t>(total);
             for (size_t j = 0; j <= s; j++) out.ents[j] = alloc<uint32_t>(total);
             out.mult = alloc<uint64_t>(total);
-            launched(probe_stage(items, key, ht, 1, nullptr, toff, out, bloom, ctx_->d_err, st_));
+            launched(probe_stage(items, key, ht, 1, nullptr, toff, out, bloom, ctx_->d_err, st_, total));
             Items next{};
             next.rows = out.rows;
             for (size_t j = 0; j <= s; j++) next.ents[j] = out.ents[j];
@@ -1376,6 +1394,8 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
     std::unique_ptr<bj_result> res(new bj_result);
     res->ctx = ctx;
     SpecCheck spec;
+    bool planned_with_cards = false;
+    ctx->item_overflow = false;
     try {
         ExecPlan ex;
         std::string err;
@@ -1384,7 +1404,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
         // ordering mode (none: the row-count model).
         std::vector<double> cards;
         const std::vector<double>* use_cards = nullptr;
-        if (resident && ctx->ordering != BJ_ORDER_ROWS) {
+        if (resident && ctx->ordering != BJ_ORDER_ROWS && !ctx->rows_plan_only) {
             if (ctx->cards_in) {
                 use_cards = ctx->cards_in->empty() ? nullptr : ctx->cards_in;
             } else {
@@ -1393,6 +1413,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
                 if (ctx->cards_out) *ctx->cards_out = cards;
             }
         }
+        planned_with_cards = use_cards != nullptr;
         int st = make_exec_plan(*plan, ex, err, false, use_cards);
         if (st != BJ_OK) throw Fail{st, err};
         ctx->tune = tune_for(ctx, ex);
@@ -1563,6 +1584,20 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
             ctx->last_error.clear();
             res.reset();
             return execute_common(ctx, plan, resident, flags, out, false);
+        }
+        // An order picked from estimated cardinalities whose intermediate
+        // result outgrew 32-bit item counts: run the row-count model's plan
+        // instead (and record that choice for the query's graph).
+        if (ctx->item_overflow && planned_with_cards) {
+            fail_to_status(ctx, f);
+            ctx->last_error.clear();
+            res.reset();
+            if (ctx->tape && ctx->tape_mode == 1) ctx->tape->slots.clear();
+            if (ctx->cards_out) ctx->cards_out->clear();
+            ctx->rows_plan_only = true;
+            const int rst = execute_common(ctx, plan, resident, flags, out, speculate);
+            ctx->rows_plan_only = false;
+            return rst;
         }
         return fail_to_status(ctx, f);
     } catch (const std::bad_alloc&) {

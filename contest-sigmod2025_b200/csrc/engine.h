@@ -311,6 +311,8 @@ struct bj_context {
     int ordering = 0;                      // BJ_ORDER_ROWS / _SAMPLING / _LEARNED
     bj_estimator* estimator = nullptr;
     const std::vector<double>* cards_in = nullptr;  // a graph's recorded set cardinalities (capture)
+    bool item_overflow = false;                     // the call's plan outgrew 32-bit item counts
+    bool rows_plan_only = false;                    // plan with the row-count model (after an overflow)
     std::vector<double>* cards_out = nullptr;       // where a first run records them
     std::vector<cudaEvent_t> pipe_events;  // one per pipeline, reused across calls
     std::vector<cudaEvent_t> window_events;  // a streamed scan's copy and release marks

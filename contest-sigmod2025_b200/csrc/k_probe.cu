@@ -81,10 +81,10 @@ __device__ __forceinline__ T block_exclusive_sum(T v, T* total) {
 template <int kMode>
 __global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HTView ht, uint32_t* tile_counts,
                                                      const uint32_t* tile_offsets, ItemsOut out, int use_bloom,
-                                                     uint32_t* err) {
+                                                     uint32_t* err, uint32_t capacity) {
     uint32_t t0 = blockIdx.x * kTile;
     uint32_t t1 = min(in.count, t0 + kTile);
-    uint32_t mine = 0;
+    unsigned long long mine = 0;
     for (uint32_t i = t0 + threadIdx.x; i < t1; i += blockDim.x) {
         uint32_t row = item_row(in, i);
         if (row >= key.nrows) {
@@ -95,13 +95,18 @@ __global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HT
         if (!col_get(key, row, v)) continue;
         mine += for_matches(ht, v, use_bloom != 0, [](uint32_t) {});
     }
-    __shared__ uint32_t total;
-    uint32_t base = block_exclusive_sum<uint32_t>(mine, &total);
+    __shared__ unsigned long long total;
+    const unsigned long long base = block_exclusive_sum<unsigned long long>(mine, &total);
     if (kMode == 0) {
-        if (threadIdx.x == 0) tile_counts[blockIdx.x] = total;
+        // A tile's matches beyond 2^32 - 1 cannot be items (their count is
+        // 32-bit): saturate, and the host refuses the stage.
+        if (threadIdx.x == 0) {
+            if (total > 0xffffffffull) record_error(err, kErrCapacity);
+            tile_counts[blockIdx.x] = uint32_t(min(total, 0xffffffffull));
+        }
         return;
     }
-    uint32_t o = tile_offsets[blockIdx.x] + base;
+    unsigned long long o = tile_offsets[blockIdx.x] + base;
     for (uint32_t i = t0 + threadIdx.x; i < t1; i += blockDim.x) {
         uint32_t row = item_row(in, i);
         if (row >= key.nrows) continue;
@@ -109,6 +114,10 @@ __global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HT
         if (!col_get(key, row, v)) continue;
         uint64_t m = item_mult(in, i);
         for_matches(ht, v, use_bloom != 0, [&](uint32_t e) {
+            if (o >= capacity) {
+                record_error(err, kErrCapacity);
+                return;
+            }
             out.rows[o] = row;
             for (int p = 0; p < in.nprobes; p++) out.ents[p][o] = in.ents[p][i];
             out.ents[in.nprobes][o] = e;
@@ -209,13 +218,16 @@ __global__ void __launch_bounds__(256) k_emit_output(Items in, const uint64_t* o
 } // namespace
 
 int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mode, uint32_t* tile_counts,
-                const uint32_t* tile_offsets, ItemsOut out, bool use_bloom, uint32_t* err, cudaStream_t st) {
+                const uint32_t* tile_offsets, ItemsOut out, bool use_bloom, uint32_t* err, cudaStream_t st,
+                uint32_t capacity) {
     uint32_t tiles = (in.count + kTile - 1) / kTile;
     if (!tiles) return 0;
     if (mode == 0)
-        k_probe_stage<0><<<tiles, 256, 0, st>>>(in, key, ht, tile_counts, tile_offsets, out, use_bloom, err);
+        k_probe_stage<0><<<tiles, 256, 0, st>>>(in, key, ht, tile_counts, tile_offsets, out, use_bloom, err,
+                                                 capacity);
     else
-        k_probe_stage<1><<<tiles, 256, 0, st>>>(in, key, ht, tile_counts, tile_offsets, out, use_bloom, err);
+        k_probe_stage<1><<<tiles, 256, 0, st>>>(in, key, ht, tile_counts, tile_offsets, out, use_bloom, err,
+                                                 capacity);
     return 1;
 }
 

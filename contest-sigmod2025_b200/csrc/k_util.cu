@@ -252,11 +252,33 @@ __global__ void k_gather_values(GatherList g, uint64_t* dst) {
     dst[g.slot[i]] = g.wide[i] ? *static_cast<const uint64_t*>(g.src[i]) : *static_cast<const uint32_t*>(g.src[i]);
 }
 
+// Sum of n u32 counts in 64 bits (one CTA): the total a u32 scan of the same
+// counts would wrap.
+__global__ void __launch_bounds__(1024) k_sum_u32_wide(const uint32_t* __restrict__ in, size_t n,
+                                                       unsigned long long* __restrict__ out) {
+    unsigned long long s = 0;
+    for (size_t i = threadIdx.x; i < n; i += blockDim.x) s += in[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __shared__ unsigned long long part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < int(blockDim.x >> 5); w++) t += part[w];
+        *out = t;
+    }
+}
+
 __global__ void k_fill_u32(uint32_t* p, uint32_t v, size_t n) {
     for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) p[i] = v;
 }
 
 } // namespace
+
+int sum_u32_wide(const uint32_t* in, size_t n, unsigned long long* out, cudaStream_t st) {
+    k_sum_u32_wide<<<1, 1024, 0, st>>>(in, n, out);
+    return 1;
+}
 
 int scan_exclusive_u32(const uint32_t* in, uint32_t* out, size_t n, Scratch& s, cudaStream_t st) {
     return scan_impl<uint32_t>(in, out, n, s, st);

@@ -54,6 +54,8 @@ struct ScanBatch64 {
 };
 int scan_exclusive_u64_batch(const ScanBatch64& b, size_t n, Scratch& s, cudaStream_t st);
 int fill_u32(uint32_t* p, uint32_t v, size_t n, cudaStream_t st);
+// *out = the sum of n u32 values in 64 bits (one launch).
+int sum_u32_wide(const uint32_t* in, size_t n, unsigned long long* out, cudaStream_t st);
 // Gathers device values into dst[slot] (u32 zero-extended, or u64): the
 // values a host read-back needs, in one launch.
 constexpr int kMaxGather = 64;
@@ -116,8 +118,11 @@ constexpr uint32_t kTile = 256;  // items per CTA tile in stage kernels (one per
 // Probe stage: for each item, read the key `key` at its row, probe `ht`,
 // and emit one item per matching entry. mode 0 counts matches per tile into
 // tile_counts; mode 1 writes items at tile_offsets (exclusive scan of counts).
+// Mode 0 saturates a tile's count at 2^32 - 1 (recording kErrCapacity);
+// mode 1 writes at most `capacity` items (more record kErrCapacity).
 int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mode, uint32_t* tile_counts,
-                const uint32_t* tile_offsets, ItemsOut out, bool use_bloom, uint32_t* err, cudaStream_t st);
+                const uint32_t* tile_offsets, ItemsOut out, bool use_bloom, uint32_t* err, cudaStream_t st,
+                uint32_t capacity = 0xffffffffu);
 
 // Consecutive probe stages against tables with unique keys (at most one
 // match per item and stage), fused: an item probes the stages in order and

@@ -430,3 +430,25 @@ def test_resident_snapshot_round_trip(pkg, ctx, oracle, tmp_path):
     # The context is still usable.
     w2 = pkg.Workload("join2", 15, 0.01)
     check_against_oracle(pkg, ctx, oracle, w2.plan_ptr(), "after bad snapshots")
+
+
+def test_intermediate_result_beyond_32_bit_items_is_refused(pkg, ctx, oracle):
+    """A join step whose result would exceed 2^32 - 2 rows (here 300K x 100K
+    matches of one key in the second probe stage) is refused with
+    BJ_ERR_UNSUPPORTED instead of wrapping its 32-bit item count; the context
+    stays usable."""
+    plan = pkg.Plan()
+    plan.new_input(pkg.table_from_rows([[1, 1]] * 300_000, [pkg.INT32, pkg.INT32]))  # C: the driver
+    plan.new_input(pkg.table_from_rows([[1]] + [[k] for k in range(2, 100_001)], [pkg.INT32]))  # A: unique keys
+    plan.new_input(pkg.table_from_rows([[1]] * 100_000, [pkg.INT32]))  # B: one key, 100K times
+    plan.new_scan_node(0, [(0, pkg.INT32), (1, pkg.INT32)])
+    plan.new_scan_node(1, [(0, pkg.INT32)])
+    plan.new_scan_node(2, [(0, pkg.INT32)])
+    plan.new_join_node(False, 0, 1, 0, 0, [(0, pkg.INT32), (1, pkg.INT32)])
+    plan.new_join_node(False, 3, 2, 1, 0, [(0, pkg.INT32)])
+    plan.root = 4
+    with pytest.raises(pkg.EngineError) as e:
+        ctx.execute(plan)
+    assert e.value.status == 4 and "intermediate rows" in str(e.value)
+    w = pkg.Workload("join2", 4, 0.01)
+    check_against_oracle(pkg, ctx, oracle, w.plan_ptr(), "after an intermediate overflow")
