@@ -112,6 +112,7 @@ ABI = {
     "bj_server_set_ordering": (_INT, [_VP, _INT, _VP]),
     "bj_server_set_graphs": (None, [_VP, _INT]),
     "bj_context_set_graphs": (None, [_VP, _INT]),
+    "bj_context_set_plan_space": (_INT, [_VP, _INT]),
     "bj_context_autotune": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), _INT, ctypes.c_char_p, _U64,
                                    ctypes.POINTER(_U64)]),
     "bj_plan_scratch_estimate": (_INT, [_VP, ctypes.POINTER(BjPlan), ctypes.POINTER(_VP), ctypes.POINTER(_U64)]),
@@ -137,6 +138,7 @@ ABI = {
 }
 
 ORDER_ROWS, ORDER_SAMPLING, ORDER_LEARNED = 0, 1, 2
+PLAN_AUTO, PLAN_ROOTED, PLAN_REFERENCE = 0, 1, 2
 EST_FEATURES, EST_HIDDEN, EST_MAX_TABLES = 1792, 256, 12
 
 WORKLOAD_ABI = {
@@ -636,6 +638,10 @@ class Context:
 
     def set_graphs(self, on: bool) -> None:
         lib().bj_context_set_graphs(self.handle, 1 if on else 0)
+
+    def set_plan_space(self, space: int) -> None:
+        """PLAN_AUTO (the cheaper), PLAN_ROOTED or PLAN_REFERENCE."""
+        self._check(lib().bj_context_set_plan_space(self.handle, space), "bj_context_set_plan_space")
 
     def autotune(self, plan, residents, repeats: int = 5) -> str:
         """Tunes build and scan parameters for the plan's shape class

@@ -374,7 +374,7 @@ int guess_first_probe(const ExecPlan& ex, const bj_plan& plan) {
     double best_density = 2.0;
     for (size_t k = 0; k < root.probes.size(); k++) {
         const PipelinePlan& child = ex.pipelines[root.probes[k].child];
-        if (child.build_key < 0) continue;
+        if (child.build_key < 0 || root.probes[k].key_probe >= 0 || child.build_key_probe >= 0) continue;
         const PlanAttr& a = ex.attrs[size_t(child.build_key)];
         const uint32_t table = ex.inputs[a.input].table;
         if (table >= plan.num_inputs || a.column >= plan.inputs[table].num_columns) continue;
@@ -552,8 +552,19 @@ class Executor {
         size_t s2 = s;
         while (s2 < order.size() && r.ch.n < kMaxChain && hts_[pp.probes[order[s2]].child].unique) {
             const uint32_t k2 = order[s2];
+            const PipelinePlan::Probe& pr = pp.probes[k2];
+            KeySource src{-1, 0, HTView{}};
+            if (pr.key_probe >= 0) {
+                // Keyed on an earlier stage's payload: that stage's entries
+                // must come from an earlier launch, so a source inside this
+                // chain ends the chain here.
+                const size_t pos = size_t(std::find(order.begin(), order.end(), uint32_t(pr.key_probe)) - order.begin());
+                if (pos >= s) break;
+                src = KeySource{int32_t(pos), pr.key_slot, by_stage[pos]};
+            }
             ChainStage& c = r.ch.st[r.ch.n++];
-            c.key = col(pp.probes[k2].probe_attr);
+            c.key = col(pr.probe_attr);
+            c.src = src;
             c.ht = by_stage[s2];
             c.use_bloom = (c.ht.bloom && rate[k2] < 0.5) ? 1 : 0;
             unit = unit && hts_[pp.probes[k2].child].unit_mult;
@@ -725,6 +736,21 @@ class Executor {
                 child.unit_mult = ctx_->h_small[17 + 2 * k] == 0;
             }
             std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return rate[a] < rate[b]; });
+            // A probe keyed on an earlier probe's payload runs after it (the
+            // first stage is then always keyed on the scanned input).
+            std::vector<uint32_t> placed;
+            std::vector<uint8_t> done(np, 0);
+            while (placed.size() < np) {
+                size_t before = placed.size();
+                for (uint32_t k : order)
+                    if (!done[k] && (pp.probes[k].key_probe < 0 || done[size_t(pp.probes[k].key_probe)])) {
+                        placed.push_back(k);
+                        done[k] = 1;
+                        break;
+                    }
+                if (placed.size() == before) throw Fail{BJ_ERR_INTERNAL, "probe keys depend on each other"};
+            }
+            order = placed;
         }
         if (root) mark_phase();
         std::vector<uint32_t> stage_of(np);
@@ -832,6 +858,11 @@ class Executor {
             const BuiltHT& bh = hts_[pp.probes[k].child];
             bool bloom = ht.bloom && rate[k] < 0.5;
             const DevColumn& key = col(pp.probes[k].probe_attr);
+            KeySource ksrc{-1, 0, HTView{}};
+            if (pp.probes[k].key_probe >= 0) {
+                const uint32_t src_stage = stage_of[size_t(pp.probes[k].key_probe)];
+                ksrc = KeySource{int32_t(src_stage), pp.probes[k].key_slot, by_stage[src_stage]};
+            }
             if (bh.unique) {
                 // This stage and the unique-key stages right after it run as
                 // one fused chain.
@@ -849,14 +880,14 @@ class Executor {
             uint32_t* tc = alloc<uint32_t>(tiles);
             uint32_t* toff = alloc<uint32_t>(tiles + 1);
             ItemsOut none{};
-            launched(probe_stage(items, key, ht, 0, tc, nullptr, none, bloom, ctx_->d_err, st_));
+            launched(probe_stage(items, key, ht, 0, tc, nullptr, none, bloom, ctx_->d_err, st_, 0xffffffffu, ksrc));
             uint32_t total = item_total(tc, toff, tiles);
             if (total == 0) return false;
             ItemsOut out{};
             out.rows = alloc<uint32_t>(total);
             for (size_t j = 0; j <= s; j++) out.ents[j] = alloc<uint32_t>(total);
             out.mult = alloc<uint64_t>(total);
-            launched(probe_stage(items, key, ht, 1, nullptr, toff, out, bloom, ctx_->d_err, st_, total));
+            launched(probe_stage(items, key, ht, 1, nullptr, toff, out, bloom, ctx_->d_err, st_, total, ksrc));
             Items next{};
             next.rows = out.rows;
             for (size_t j = 0; j <= s; j++) next.ents[j] = out.ents[j];
@@ -890,7 +921,9 @@ class Executor {
                 s.slot = int(sp.slot);
             }
         }
-        if (pp.build_key >= 0) return build(pi, items, src, by_stage);
+        if (pp.build_key >= 0)
+            return build(pi, items, src, by_stage,
+                         pp.build_key_probe >= 0 ? int32_t(stage_of[size_t(pp.build_key_probe)]) : -1);
         mark_phase();
         output(items, src, by_stage, *res, flags);
         mark_phase();
@@ -916,7 +949,7 @@ class Executor {
     static size_t round256(size_t x) { return (x + 255) & ~size_t(255); }
 
     PreparedBuild prepare_build(size_t pi, const Items& items, const SlotSources& src,
-                                const std::vector<HTView>& probes) {
+                                const std::vector<HTView>& probes, int32_t key_stage = -1) {
         const PipelinePlan& pp = ex_.pipelines[pi];
         PreparedBuild pb;
         const uint32_t n = items.count;
@@ -924,6 +957,10 @@ class Executor {
         BuildArgs& ba = pb.ba;
         ba.in = items;
         ba.key = col(uint32_t(pp.build_key));
+        // Keyed on an attribute of a probed input (key_stage >= 0: the stage
+        // of that probe in this pipeline), carried as its payload.
+        ba.key_stage = key_stage;
+        ba.key_slot = key_stage >= 0 ? pp.build_key_slot : 0;
         ba.src = src;
         ba.ps = make_probe_set(probes.data(), items.nprobes);
         TupleBuf& tb = ba.tb;
@@ -1011,8 +1048,9 @@ class Executor {
         hts_[pi].dflags = pb.dflags;
     }
 
-    bool build(size_t pi, const Items& items, const SlotSources& src, const std::vector<HTView>& probes) {
-        PreparedBuild pb = prepare_build(pi, items, src, probes);
+    bool build(size_t pi, const Items& items, const SlotSources& src, const std::vector<HTView>& probes,
+               int32_t key_stage) {
+        PreparedBuild pb = prepare_build(pi, items, src, probes, key_stage);
         uint8_t* z = alloc<uint8_t>(pb.zbytes);
         BJ_CK(cudaMemsetAsync(z, 0, pb.zbytes, st_));
         place_zero(pb, z);
@@ -1414,7 +1452,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
             }
         }
         planned_with_cards = use_cards != nullptr;
-        int st = make_exec_plan(*plan, ex, err, false, use_cards);
+        int st = make_exec_plan(*plan, ex, err, false, use_cards, ctx->plan_space);
         if (st != BJ_OK) throw Fail{st, err};
         ctx->tune = tune_for(ctx, ex);
         res->types = ex.out_types;
@@ -1658,7 +1696,8 @@ bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resid
     try {
         ExecPlan ex;
         std::string err;
-        if (make_exec_plan(*plan, ex, err, false, g.cards.empty() ? nullptr : &g.cards) != BJ_OK || ex.empty)
+        if (make_exec_plan(*plan, ex, err, false, g.cards.empty() ? nullptr : &g.cards, ctx->plan_space) != BJ_OK ||
+            ex.empty)
             return false;
         ctx->tune = tune_for(ctx, ex);
         std::vector<const DevTable*> tables(plan->num_inputs);
@@ -1844,6 +1883,7 @@ int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* co
     std::vector<uint64_t> key = graph_key(*plan, tables, flags & ~BJ_RESULT_ASYNC, ctx->profile);
     key.push_back(uint64_t(ctx->ordering));
     key.push_back(reinterpret_cast<uint64_t>(ctx->estimator));
+    key.push_back(uint64_t(ctx->plan_space));
     uint64_t hash = 0x9e3779b97f4a7c15ull;
     for (uint64_t v : key) hash = (hash ^ v) * 0x100000001b3ull + (hash >> 29);
     GraphEntry* g = nullptr;
@@ -1948,16 +1988,32 @@ BJ_API int bj_plan_explain(const bj_plan* plan, char* buf, uint64_t cap, uint64_
                     std::snprintf(line, sizeof line, "%s pipeline %u on attr %u", k ? "," : ", probe", pp.probes[k].child,
                                   pp.probes[k].probe_attr);
                     out += line;
+                    if (pp.probes[k].key_probe >= 0) {
+                        std::snprintf(line, sizeof line, " (payload of pipeline %u)",
+                                      pp.probes[size_t(pp.probes[k].key_probe)].child);
+                        out += line;
+                    }
                 }
                 if (pp.build_key >= 0) {
                     std::snprintf(line, sizeof line, " -> hash table on attr %lld", static_cast<long long>(pp.build_key));
                     out += line;
+                    if (pp.build_key_probe >= 0) {
+                        std::snprintf(line, sizeof line, " (payload of pipeline %u)",
+                                      pp.probes[size_t(pp.build_key_probe)].child);
+                        out += line;
+                    }
                 } else {
                     out += " -> result";
                 }
                 out += "\n";
             }
             if (!ex.ref_plan.empty()) out += "reference plan space, cheapest: " + ex.ref_plan + "\n";
+            if (ex.rooted_cost >= 0) {
+                std::snprintf(line, sizeof line, "rooted plan space, cheapest: driver input %u, cost %.4g\n",
+                              ex.rooted_driver, ex.rooted_cost);
+                out += line;
+            }
+            out += ex.reference_space ? "runs: the reference space's plan\n" : "runs: the rooted plan\n";
             // The drop-in path's guess of the probe scanned first (it starts
             // copying that column's pages before the device sampling decides).
             const int g = guess_first_probe(ex, *plan);
@@ -2132,6 +2188,12 @@ BJ_API int bj_context_autotune(bj_context* ctx, const bj_plan* plan, bj_resident
         std::memcpy(report, text.data(), n);
         report[n] = 0;
     }
+    return BJ_OK;
+}
+
+BJ_API int bj_context_set_plan_space(bj_context* ctx, int space) {
+    if (!ctx || space < 0 || space > 2) return BJ_ERR_INVALID;
+    ctx->plan_space = PlanSpace(space);
     return BJ_OK;
 }
 

@@ -312,6 +312,7 @@ struct bj_context {
     bj_estimator* estimator = nullptr;
     const std::vector<double>* cards_in = nullptr;  // a graph's recorded set cardinalities (capture)
     bool item_overflow = false;                     // the call's plan outgrew 32-bit item counts
+    bj::PlanSpace plan_space = bj::plan_space_default();  // which plan space make_exec_plan runs
     bool rows_plan_only = false;                    // plan with the row-count model (after an overflow)
     std::vector<double>* cards_out = nullptr;       // where a first run records them
     std::vector<cudaEvent_t> pipe_events;  // one per pipeline, reused across calls

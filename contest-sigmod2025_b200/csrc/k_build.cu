@@ -137,8 +137,17 @@ __device__ __forceinline__ EmitTarget emit_target(const BuildArgs& a) {
 __device__ __forceinline__ void emit_tuple(const BuildArgs& a, uint32_t i) {
     const uint32_t row = item_row(a.in, i);
     uint64_t kv = 0;
-    const bool key_ok = row < a.key.nrows && col_get(a.key, row, kv);
-    if (row >= a.key.nrows) record_error(a.err, kErrRowRange);
+    bool key_ok;
+    if (a.key_stage >= 0) {
+        // The key is an attribute of an input probed by this pipeline.
+        const HTView& src = a.ps.ht[a.key_stage];
+        const uint32_t e = a.in.ents[a.key_stage][i];
+        key_ok = !((src.pnull[e] >> a.key_slot) & 1);
+        if (key_ok) kv = src.pay[size_t(e) * src.width + a.key_slot];
+    } else {
+        key_ok = row < a.key.nrows && col_get(a.key, row, kv);
+        if (row >= a.key.nrows) record_error(a.err, kErrRowRange);
+    }
     const uint64_t m = key_ok ? item_mult(a.in, i) : 0ull;
     emit_tuple_to(emit_target(a), i, kv, m, a.src.n,
                   [&](int j, uint64_t& v) { return slot_value(a.src.s[j], a.in, i, row, a.ps, v); });

@@ -78,21 +78,29 @@ __device__ __forceinline__ T block_exclusive_sum(T v, T* total) {
     return r;
 }
 
+// Key of item i (row `row`) for a stage: a column of the scanned input, or an
+// earlier stage's payload.
+__device__ __forceinline__ bool stage_key(const DevColumn& key, const KeySource& src, const Items& in, uint32_t i,
+                                          uint32_t row, uint32_t* err, uint64_t& v) {
+    if (src.stage >= 0) return payload_key(src, in.ents, i, v);
+    if (row >= key.nrows) {
+        record_error(err, kErrRowRange);
+        return false;
+    }
+    return col_get(key, row, v);
+}
+
 template <int kMode>
 __global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HTView ht, uint32_t* tile_counts,
                                                      const uint32_t* tile_offsets, ItemsOut out, int use_bloom,
-                                                     uint32_t* err, uint32_t capacity) {
+                                                     uint32_t* err, uint32_t capacity, KeySource src) {
     uint32_t t0 = blockIdx.x * kTile;
     uint32_t t1 = min(in.count, t0 + kTile);
     unsigned long long mine = 0;
     for (uint32_t i = t0 + threadIdx.x; i < t1; i += blockDim.x) {
         uint32_t row = item_row(in, i);
-        if (row >= key.nrows) {
-            record_error(err, kErrRowRange);
-            continue;
-        }
         uint64_t v;
-        if (!col_get(key, row, v)) continue;
+        if (!stage_key(key, src, in, i, row, err, v)) continue;
         mine += for_matches(ht, v, use_bloom != 0, [](uint32_t) {});
     }
     __shared__ unsigned long long total;
@@ -109,9 +117,8 @@ __global__ void __launch_bounds__(256) k_probe_stage(Items in, DevColumn key, HT
     unsigned long long o = tile_offsets[blockIdx.x] + base;
     for (uint32_t i = t0 + threadIdx.x; i < t1; i += blockDim.x) {
         uint32_t row = item_row(in, i);
-        if (row >= key.nrows) continue;
         uint64_t v;
-        if (!col_get(key, row, v)) continue;
+        if (!stage_key(key, src, in, i, row, nullptr, v)) continue;
         uint64_t m = item_mult(in, i);
         for_matches(ht, v, use_bloom != 0, [&](uint32_t e) {
             if (o >= capacity) {
@@ -154,10 +161,7 @@ __global__ void __launch_bounds__(256) k_probe_chain(Items in, ProbeChain ch, It
             if (t >= ch.n || !hit) continue;
             const ChainStage& c = ch.st[t];
             uint64_t v;
-            if (row >= c.key.nrows) {
-                record_error(err, kErrRowRange);
-                hit = false;
-            } else if (!col_get(c.key, row, v)) {
+            if (!stage_key(c.key, c.src, in, i, row, err, v)) {
                 hit = false;
             } else {
                 bool found = false;
@@ -219,15 +223,15 @@ __global__ void __launch_bounds__(256) k_emit_output(Items in, const uint64_t* o
 
 int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mode, uint32_t* tile_counts,
                 const uint32_t* tile_offsets, ItemsOut out, bool use_bloom, uint32_t* err, cudaStream_t st,
-                uint32_t capacity) {
+                uint32_t capacity, KeySource src) {
     uint32_t tiles = (in.count + kTile - 1) / kTile;
     if (!tiles) return 0;
     if (mode == 0)
         k_probe_stage<0><<<tiles, 256, 0, st>>>(in, key, ht, tile_counts, tile_offsets, out, use_bloom, err,
-                                                 capacity);
+                                                 capacity, src);
     else
         k_probe_stage<1><<<tiles, 256, 0, st>>>(in, key, ht, tile_counts, tile_offsets, out, use_bloom, err,
-                                                 capacity);
+                                                 capacity, src);
     return 1;
 }
 

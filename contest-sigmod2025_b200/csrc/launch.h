@@ -114,6 +114,15 @@ struct ItemsOut {
     uint64_t* mult;
 };
 constexpr uint32_t kTile = 256;  // items per CTA tile in stage kernels (one per thread)
+// Where a stage's probe key comes from: a column of the scanned input at the
+// item's row (stage < 0), or payload slot `slot` of the entry that an earlier
+// stage `stage` matched (table ht), an attribute of an input probed before.
+struct KeySource {
+    int32_t stage;
+    uint32_t slot;
+    HTView ht;
+};
+
 
 // Probe stage: for each item, read the key `key` at its row, probe `ht`,
 // and emit one item per matching entry. mode 0 counts matches per tile into
@@ -122,7 +131,7 @@ constexpr uint32_t kTile = 256;  // items per CTA tile in stage kernels (one per
 // mode 1 writes at most `capacity` items (more record kErrCapacity).
 int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mode, uint32_t* tile_counts,
                 const uint32_t* tile_offsets, ItemsOut out, bool use_bloom, uint32_t* err, cudaStream_t st,
-                uint32_t capacity = 0xffffffffu);
+                uint32_t capacity = 0xffffffffu, KeySource src = KeySource{-1, 0, HTView{}});
 
 // Consecutive probe stages against tables with unique keys (at most one
 // match per item and stage), fused: an item probes the stages in order and
@@ -133,9 +142,10 @@ int probe_stage(const Items& in, const DevColumn& key, const HTView& ht, int mod
 // only multiplicity 1.
 constexpr int kMaxChain = 8;
 struct ChainStage {
-    DevColumn key;   // probe key column of the scanned input
+    DevColumn key;   // probe key column of the scanned input (src.stage < 0)
     HTView ht;
     int use_bloom;   // test ht.bloom (in global memory) first
+    KeySource src;   // src.stage >= 0: the key is an earlier stage's payload (from an earlier launch)
 };
 struct ProbeChain {
     ChainStage st[kMaxChain];
@@ -173,6 +183,14 @@ inline ProbeSet make_probe_set(const HTView* probes, int n) {
 }
 
 #if defined(__CUDACC__)
+// Key of item i from a payload source (src.stage >= 0); false for NULL.
+__device__ __forceinline__ bool payload_key(const KeySource& src, const uint32_t* const* ents, uint32_t i,
+                                            uint64_t& v) {
+    const uint32_t e = ents[src.stage][i];
+    if ((src.ht.pnull[e] >> src.slot) & 1) return false;
+    v = src.ht.pay[size_t(e) * src.ht.width + src.slot];
+    return true;
+}
 __device__ __forceinline__ uint32_t item_row(const Items& in, uint32_t i) { return in.rows ? in.rows[i] : i; }
 __device__ __forceinline__ uint64_t item_mult(const Items& in, uint32_t i) { return in.mult ? in.mult[i] : 1ull; }
 // Value of `row` of column c as a slot carries it. A VARCHAR column without
@@ -259,7 +277,9 @@ struct TupleBuf {
 // and counts (one per bucket) must be zero.
 struct BuildArgs {
     Items in;
-    DevColumn key;
+    DevColumn key;       // key column of the scanned input, or (key_stage >= 0) only its type
+    int32_t key_stage;   // >= 0: the key is payload slot key_slot of the entry stage key_stage matched
+    uint32_t key_slot;
     SlotSources src;
     ProbeSet ps;
     TupleBuf tb;

@@ -2,6 +2,7 @@
 #include "planner.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <functional>
 #include <limits>
 #include <numeric>
@@ -195,13 +196,25 @@ uint32_t choose_driver(const std::vector<double>& card, const std::vector<Edge>&
 // cheapest full plan's cost, or -1 above kMaxDpInputs inputs.
 // `plan_text` (optional) receives the cheapest plan in the notation
 // probe(R, hash(L)): input R's pipeline (or the pipeline of plan R) probes the
-// hash table built from plan L.
+// hash table built from plan L. `tree` (optional) receives it as nodes: a
+// base input (probes == 0) or probe(right, hash(left)); node 0 is the root.
+// `set_card` (optional) gives every connected set's cardinality, as for
+// choose_driver.
+struct RefNode {
+    uint32_t set;
+    int probes;          // probes in this node's top pipeline; 0: a base input
+    int32_t left = -1;   // hashed plan
+    int32_t right = -1;  // plan whose pipeline continues
+};
+
 double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge>& edges,
-                         std::string* plan_text = nullptr) {
+                         std::string* plan_text = nullptr, const std::vector<double>* set_card = nullptr,
+                         std::vector<RefNode>* tree = nullptr) {
     const uint32_t n = uint32_t(card.size());
     if (n == 0 || n > kMaxDpInputs) return -1;
     if (n == 1) {
         if (plan_text) *plan_text = "input 0";
+        if (tree) *tree = {RefNode{1u, 0, -1, -1}};
         return card[0];
     }
     std::vector<uint32_t> nbr(n, 0);
@@ -228,15 +241,17 @@ double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge
         uint32_t left = 0, right = 0;
         int lpipes = 0, rpipes = 0;
     };
-    std::vector<Choice> how(plan_text ? size_t(full + 1) * kPipes : 0);
+    std::vector<Choice> how(plan_text || tree ? size_t(full + 1) * kPipes : 0);
     for (uint32_t S = 1; S <= full; S++) {
         const uint32_t low = __builtin_ctz(S);
         setcard[S] = std::max(setcard[S & (S - 1)], card[low]);
         if (S == (1u << low)) {
-            best[size_t(S) * kPipes] = card[low];  // a base relation costs its cardinality
+            if (set_card) setcard[S] = (*set_card)[S];
+            best[size_t(S) * kPipes] = setcard[S];  // a base relation costs its cardinality
             continue;
         }
         if (reach(low, S) != S) continue;
+        if (set_card) setcard[S] = (*set_card)[S];
         // Each edge of S splits it into two connected sides; either side can
         // be the hash table joined into the other's pipeline.
         for (uint32_t us = S; us; us &= us - 1) {
@@ -260,7 +275,7 @@ double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge
                         double& t = best[size_t(S) * kPipes + rp + 1];
                         if (c < t) {
                             t = c;
-                            if (plan_text) how[size_t(S) * kPipes + rp + 1] = Choice{left, right, lpick, rp};
+                            if (plan_text || tree) how[size_t(S) * kPipes + rp + 1] = Choice{left, right, lpick, rp};
                         }
                     }
                 }
@@ -282,7 +297,170 @@ double reference_dp_cost(const std::vector<double>& card, const std::vector<Edge
         };
         *plan_text = show(full, rp);
     }
+    if (tree && r < inf) {
+        tree->clear();
+        std::function<int32_t(uint32_t, int)> add = [&](uint32_t S, int p) -> int32_t {
+            const int32_t id = int32_t(tree->size());
+            tree->push_back(RefNode{S, p, -1, -1});
+            if (p > 0) {
+                const Choice& c = how[size_t(S) * kPipes + p];
+                const int32_t l = add(c.left, c.lpipes);
+                const int32_t rr = add(c.right, c.rpipes);
+                (*tree)[size_t(id)].left = l;
+                (*tree)[size_t(id)].right = rr;
+            }
+            return id;
+        };
+        add(full, rp);
+    }
     return r;
+}
+
+// Pipelines of a plan of the reference's space (tree from reference_dp_cost).
+// A node's pipeline scans the base input at the bottom of its right spine and
+// probes, bottom up, the tables hashed from the left plans along the spine.
+// A hashed plan's pipeline carries, as payload, every attribute of its
+// inputs that is a result column or the endpoint of a join edge leaving its
+// set; its build key is its endpoint of the edge to the rest of its parent's
+// set. A probe's or build's key is the scanned input's column when its input
+// is scanned, else the payload of the earlier probe whose set holds it.
+bool reference_pipelines(ExecPlan& ex, const std::vector<Edge>& edges, const std::vector<RefNode>& tree,
+                         const std::vector<uint32_t>& out_src, std::string& err) {
+    std::vector<uint8_t> is_out(ex.attrs.size(), 0);
+    for (uint32_t a : out_src) is_out[a] = 1;
+    // The output pipeline carries each distinct result attribute once.
+    std::vector<uint32_t> root_carry = out_src;
+    std::sort(root_carry.begin(), root_carry.end());
+    root_carry.erase(std::unique(root_carry.begin(), root_carry.end()), root_carry.end());
+    // Attributes a set of inputs must hand on.
+    auto needed = [&](uint32_t set) {
+        std::vector<uint32_t> v;
+        for (uint32_t a = 0; a < ex.attrs.size(); a++)
+            if ((set >> ex.attrs[a].input & 1) && is_out[a]) v.push_back(a);
+        for (const Edge& e : edges) {
+            const bool ia = set >> e.a & 1, ib = set >> e.b & 1;
+            if (ia && !ib) v.push_back(e.attr_a);
+            if (ib && !ia) v.push_back(e.attr_b);
+        }
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        return v;
+    };
+    // The edge between two disjoint sets (their union is connected by one edge).
+    auto edge_between = [&](uint32_t x, uint32_t y, uint32_t& ax, uint32_t& ay) {
+        for (const Edge& e : edges) {
+            if ((x >> e.a & 1) && (y >> e.b & 1)) {
+                ax = e.attr_a;
+                ay = e.attr_b;
+                return true;
+            }
+            if ((x >> e.b & 1) && (y >> e.a & 1)) {
+                ax = e.attr_b;
+                ay = e.attr_a;
+                return true;
+            }
+        }
+        return false;
+    };
+    std::vector<uint32_t> pipe_set;  // per pipeline: its input set
+    // Emits node `id`'s pipeline (hashed plans first); build_key: attr of the
+    // set used as its key (-1: the output pipeline). Returns its index.
+    std::function<int64_t(int32_t, int64_t)> emit = [&](int32_t id, int64_t build_key) -> int64_t {
+        std::vector<int32_t> hashed;  // bottom-up
+        int32_t n = id;
+        while (tree[size_t(n)].probes > 0) {
+            hashed.push_back(tree[size_t(n)].left);
+            n = tree[size_t(n)].right;
+        }
+        std::reverse(hashed.begin(), hashed.end());
+        const uint32_t base = __builtin_ctz(tree[size_t(n)].set);
+        PipelinePlan pp;
+        pp.input = base;
+        uint32_t have = 1u << base;
+        std::vector<uint32_t> probe_sets;
+        std::vector<std::vector<uint32_t>> probe_carry;
+        // Where attr a is available: -1 the scanned input, else (probe, slot).
+        auto locate = [&](uint32_t a, int32_t& probe, uint32_t& slot) {
+            if (ex.attrs[a].input == base) {
+                probe = -1;
+                return true;
+            }
+            for (size_t k = 0; k < probe_sets.size(); k++)
+                if (probe_sets[k] >> ex.attrs[a].input & 1) {
+                    const auto& c = probe_carry[k];
+                    const auto it = std::find(c.begin(), c.end(), a);
+                    if (it == c.end()) return false;
+                    probe = int32_t(k);
+                    slot = uint32_t(it - c.begin());
+                    return true;
+                }
+            return false;
+        };
+        for (int32_t h : hashed) {
+            const uint32_t hs = tree[size_t(h)].set;
+            uint32_t ah = 0, ar = 0;
+            if (!edge_between(hs, have, ah, ar)) return -1;
+            const int64_t child = emit(h, int64_t(ah));
+            if (child < 0) return -1;
+            PipelinePlan::Probe pr;
+            pr.child = uint32_t(child);
+            pr.probe_attr = ar;
+            int32_t kp;
+            uint32_t ks = 0;
+            if (!locate(ar, kp, ks)) return -1;
+            pr.key_probe = kp;
+            pr.key_slot = ks;
+            pp.probes.push_back(pr);
+            probe_sets.push_back(hs);
+            std::vector<uint32_t> carry;
+            for (const SlotPlan& sl : ex.pipelines[size_t(child)].slots) carry.push_back(sl.attr);
+            probe_carry.push_back(carry);
+            have |= hs;
+        }
+        pp.build_key = build_key;
+        if (build_key >= 0) {
+            int32_t kp;
+            uint32_t ks = 0;
+            if (!locate(uint32_t(build_key), kp, ks)) return -1;
+            pp.build_key_probe = kp;
+            pp.build_key_slot = ks;
+        }
+        const std::vector<uint32_t> carry = build_key >= 0 ? needed(have) : root_carry;
+        for (uint32_t a : carry) {
+            int32_t kp;
+            uint32_t ks = 0;
+            if (!locate(a, kp, ks)) return -1;
+            if (kp < 0)
+                pp.slots.push_back(SlotPlan{0, a, 0, 0});
+            else
+                pp.slots.push_back(SlotPlan{1, a, uint32_t(kp), ks});
+        }
+        if (pp.probes.size() > 16 || pp.slots.size() > 32) return -1;
+        ex.pipelines.push_back(std::move(pp));
+        pipe_set.push_back(have);
+        return int64_t(ex.pipelines.size() - 1);
+    };
+    ex.pipelines.clear();
+    const int64_t root = emit(0, -1);
+    if (root < 0 || size_t(root) + 1 != ex.pipelines.size()) {
+        err = "internal: a plan of the reference's space has no pipelines for it";
+        return false;
+    }
+    ex.driver = ex.pipelines.back().input;
+    ex.out_slot.clear();
+    const PipelinePlan& rp = ex.pipelines.back();
+    for (uint32_t a : out_src)
+        for (uint32_t j = 0; j < rp.slots.size(); j++)
+            if (rp.slots[j].attr == a) {
+                ex.out_slot.push_back(j);
+                break;
+            }
+    if (ex.out_slot.size() != out_src.size()) {
+        err = "internal: result column without a source";
+        return false;
+    }
+    ex.reference_space = true;
+    return true;
 }
 
 } // namespace
@@ -330,8 +508,18 @@ int join_order(const bj_plan& plan, const std::vector<double>* set_card, int for
     return BJ_OK;
 }
 
+PlanSpace plan_space_default() {
+    static const PlanSpace space = [] {
+        const char* e = std::getenv("B200JOIN_PLAN_SPACE");
+        if (!e) return PlanSpace::Auto;
+        const std::string v(e);
+        return v == "rooted" ? PlanSpace::Rooted : v == "reference" ? PlanSpace::Reference : PlanSpace::Auto;
+    }();
+    return space;
+}
+
 int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err, bool reference_cost,
-                   const std::vector<double>* set_card) {
+                   const std::vector<double>* set_card, PlanSpace space) {
     ex = ExecPlan{};
     if (plan.num_nodes == 0 || !plan.nodes) {
         err = "empty plan";
@@ -363,7 +551,9 @@ int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err, bool ref
     if (set_card && set_card->size() < (size_t(1) << std::min<uint32_t>(ni, 31))) set_card = nullptr;
     const uint32_t driver = choose_driver(card, im.edges, ex.est_cost, set_card);
     ex.driver = driver;
-    if (reference_cost) ex.ref_cost = reference_dp_cost(card, im.edges, &ex.ref_plan);
+    ex.rooted_driver = driver;
+    ex.rooted_cost = ex.est_cost;
+    if (reference_cost) ex.ref_cost = reference_dp_cost(card, im.edges, &ex.ref_plan, set_card);
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> adj(ni);  // (neighbour, edge)
     for (uint32_t e = 0; e < im.edges.size(); e++) {
         adj[im.edges[e].a].push_back({im.edges[e].b, e});
@@ -473,6 +663,25 @@ int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err, bool ref
     if (ex.out_slot.size() != out_src.size()) {
         err = "internal: result column without a source";
         return BJ_ERR_INTERNAL;
+    }
+    // The reference's plan space (probes and builds keyed on an earlier
+    // probe's payload, at most two probes per pipeline) under the same
+    // cardinalities: run its plan when it is cheaper (or when asked to).
+    if (space != PlanSpace::Rooted && ni >= 2 && ni <= kMaxDpInputs) {
+        std::vector<RefNode> tree;
+        const double rc = reference_dp_cost(card, im.edges, nullptr, set_card, &tree);
+        if (rc >= 0 && !tree.empty() &&
+            (space == PlanSpace::Reference || (ex.est_cost >= 0 && rc < ex.est_cost * (1.0 - 1e-9)))) {
+            ExecPlan alt = ex;
+            std::string aerr;
+            if (reference_pipelines(alt, im.edges, tree, root_attrs, aerr)) {
+                alt.est_cost = rc;
+                ex = std::move(alt);
+            } else if (space == PlanSpace::Reference) {
+                err = aerr;
+                return BJ_ERR_INTERNAL;
+            }
+        }
     }
     return BJ_OK;
 }

@@ -50,9 +50,19 @@ struct SlotPlan {
 struct PipelinePlan {
     uint32_t input;
     int64_t build_key = -1;  // attr id of the hash key; -1 for the output pipeline
+    // The build key comes from payload slot build_key_slot of probe
+    // build_key_probe when that is >= 0 (an attribute of an input this
+    // pipeline probed), else from the scanned input's column.
+    int32_t build_key_probe = -1;
+    uint32_t build_key_slot = 0;
     struct Probe {
         uint32_t child;       // pipeline index of the child
-        uint32_t probe_attr;  // attr of `input` probing the child's table
+        uint32_t probe_attr;  // attr whose values probe the child's table
+        // key_probe >= 0: probe_attr is carried as payload slot key_slot of
+        // the table probed by probes[key_probe] (which must run earlier);
+        // otherwise it is a column of `input`.
+        int32_t key_probe = -1;
+        uint32_t key_slot = 0;
     };
     std::vector<Probe> probes;
     std::vector<SlotPlan> slots;  // payload (build) or output sources (root)
@@ -67,9 +77,20 @@ struct ExecPlan {
     bool empty = false;                   // some input has no rows
     uint32_t driver = 0;                  // input scanned by the output pipeline
     double est_cost = -1;                 // cost of the chosen plan (-1: not costed)
+    double rooted_cost = -1;              // the cheapest rooted plan's cost, and its driver
+    uint32_t rooted_driver = 0;
     double ref_cost = -1;                 // the cheapest plan of the reference's plan space, same cost model
     std::string ref_plan;                 // that plan, as probe(R, hash(L)) over input indices
+    // The pipelines run are the reference space's plan (probes and builds
+    // may be keyed on an earlier probe's payload) rather than a rooted tree.
+    bool reference_space = false;
 };
+
+// Which plan space make_exec_plan runs: the cheaper of the two (auto), or
+// one of them (for tests and measurements; B200JOIN_PLAN_SPACE=rooted /
+// reference overrides auto).
+enum class PlanSpace { Auto = 0, Rooted = 1, Reference = 2 };
+PlanSpace plan_space_default();
 
 // Builds the execution plan; returns BJ_OK or a status with `err` set.
 // reference_cost: also cost the reference's plan space (ExecPlan::ref_cost;
@@ -80,7 +101,7 @@ struct ExecPlan {
 // read. Without it, a set's cardinality is its largest input's row count
 // (the reference's model, engine/query/QueryGraph.cpp:53-68).
 int make_exec_plan(const bj_plan& plan, ExecPlan& out, std::string& err, bool reference_cost = false,
-                   const std::vector<double>* set_card = nullptr);
+                   const std::vector<double>* set_card = nullptr, PlanSpace space = plan_space_default());
 
 // The join graph of a plan: its scans (inputs, numbered in the order a
 // depth-first walk from the root reaches them, left child first) and one

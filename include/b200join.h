@@ -371,6 +371,19 @@ BJ_API int bj_plan_scratch_estimate(bj_context* ctx, const bj_plan* plan, bj_res
 BJ_API int bj_context_autotune(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int repeats,
                                char* report, uint64_t cap, uint64_t* len);
 
+/* Plan space of this context's calls. BJ_PLAN_AUTO (the default): the
+ * cheaper, under the reference's cost model, of the executor's rooted plans
+ * (every pipeline probes and builds with its scanned input's columns, any
+ * number of probes) and the reference's own space (engine/query/
+ * QueryGraph.cpp:107-216: probes and builds keyed on an earlier probe's
+ * payload, at most two probes per pipeline); BJ_PLAN_ROOTED or
+ * BJ_PLAN_REFERENCE: that space only. B200JOIN_PLAN_SPACE=rooted|reference
+ * sets the default. Results are the same rows in every space. */
+#define BJ_PLAN_AUTO 0
+#define BJ_PLAN_ROOTED 1
+#define BJ_PLAN_REFERENCE 2
+BJ_API int bj_context_set_plan_space(bj_context* ctx, int space);
+
 /* Replay of repeated resident queries as CUDA graphs on (1, the default) or
  * off (0) for this context (B200JOIN_GRAPHS=0 sets the default to off). */
 BJ_API void bj_context_set_graphs(bj_context* ctx, int on);

@@ -452,3 +452,31 @@ def test_intermediate_result_beyond_32_bit_items_is_refused(pkg, ctx, oracle):
     assert e.value.status == 4 and "intermediate rows" in str(e.value)
     w = pkg.Workload("join2", 4, 0.01)
     check_against_oracle(pkg, ctx, oracle, w.plan_ptr(), "after an intermediate overflow")
+
+
+@pytest.fixture(scope="module")
+def ref_ctx(pkg):
+    """A context that always runs the reference space's plans (probes and
+    builds keyed on an earlier probe's payload, at most two probes per
+    pipeline)."""
+    c = pkg.Context(0)
+    c.set_plan_space(pkg.PLAN_REFERENCE)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_plans_reference_space(pkg, ref_ctx, oracle, seed):
+    tables, nodes, root = plangen.random_case(1000 + seed, max_rows=3000, int64_keys=seed % 2 == 1)
+    cp = pkg.CPlan(plangen.to_plan(pkg, tables, nodes, root))
+    check_against_oracle(pkg, ref_ctx, oracle, cp, f"reference space seed {1000 + seed}")
+
+
+def test_workloads_reference_space(pkg, ref_ctx, oracle):
+    """The snowflake and 64 schema20 queries (2-12 tables) as plans of the
+    reference's space, from host pages, equal to the oracle."""
+    w = pkg.Workload("snowflake", 7, 0.05)
+    assert check_against_oracle(pkg, ref_ctx, oracle, w.plan_ptr(), "snowflake reference space") > 0
+    s = pkg.Workload("schema20", 3, 0.01)
+    for k in range(0, 256, 4):
+        check_against_oracle(pkg, ref_ctx, oracle, s.query_ptr(k), f"schema20 query {k} reference space")
