@@ -208,3 +208,13 @@ def test_reference_space_cheaper_with_payload_keys(pkg):
     assert est == pytest.approx(5410) and ref == pytest.approx(3510)
     text = pkg.explain(plan)
     assert "reference plan space, cheapest: probe(input 0, hash(probe(input 2, hash(input 1))))" in text, text
+    # ... and that plan is the one that runs: E's pipeline probes D's table and
+    # hashes its result on D's key (D's payload); the fact probes it.
+    assert "runs: the reference space's plan" in text, text
+    pipes = [l for l in text.strip().splitlines() if l.startswith("pipeline")]
+    assert len(pipes) == 3, text
+    assert pipes[0].startswith("pipeline 0: scan input 1") and "hash table" in pipes[0], text
+    assert pipes[1].startswith("pipeline 1: scan input 2") and "probe pipeline 0" in pipes[1], text
+    assert "(payload of pipeline 0)" in pipes[1], text
+    assert pipes[2].startswith("pipeline 2: scan input 0") and "probe pipeline 1" in pipes[2], text
+    assert pipes[2].endswith("-> result"), text
