@@ -1442,11 +1442,22 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
         // ordering mode (none: the row-count model).
         std::vector<double> cards;
         const std::vector<double>* use_cards = nullptr;
-        if (resident && ctx->ordering != BJ_ORDER_ROWS && !ctx->rows_plan_only) {
-            if (ctx->cards_in) {
-                use_cards = ctx->cards_in->empty() ? nullptr : ctx->cards_in;
-            } else {
-                estimate_set_cards(ctx, *plan, resident, cards);
+        const int ordering = ctx->retry_ordering >= 0 ? ctx->retry_ordering : ctx->ordering;
+        if (resident && ctx->cards_in) {
+            use_cards = ctx->cards_in->empty() ? nullptr : ctx->cards_in;
+        } else if (resident && ordering == BJ_ORDER_ROWS) {
+            if (ctx->cards_out) ctx->cards_out->clear();
+        } else if (resident) {
+            {
+                const int saved = ctx->ordering;
+                ctx->ordering = ordering;
+                try {
+                    estimate_set_cards(ctx, *plan, resident, cards);
+                } catch (...) {
+                    ctx->ordering = saved;
+                    throw;
+                }
+                ctx->ordering = saved;
                 if (!cards.empty()) use_cards = &cards;
                 if (ctx->cards_out) *ctx->cards_out = cards;
             }
@@ -1623,18 +1634,18 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
             res.reset();
             return execute_common(ctx, plan, resident, flags, out, false);
         }
-        // An order picked from estimated cardinalities whose intermediate
-        // result outgrew 32-bit item counts: run the row-count model's plan
-        // instead (and record that choice for the query's graph).
-        if (ctx->item_overflow && planned_with_cards) {
+        // A join order whose intermediate result outgrew 32-bit item counts:
+        // one rerun with the other cardinality source -- the row-count model
+        // after estimated cardinalities, join samples after the row-count
+        // model (resident tables only) -- recorded for the query's graph.
+        if (ctx->item_overflow && ctx->retry_ordering < 0 && !ctx->cards_in && (planned_with_cards || resident)) {
             fail_to_status(ctx, f);
             ctx->last_error.clear();
             res.reset();
             if (ctx->tape && ctx->tape_mode == 1) ctx->tape->slots.clear();
-            if (ctx->cards_out) ctx->cards_out->clear();
-            ctx->rows_plan_only = true;
+            ctx->retry_ordering = planned_with_cards ? BJ_ORDER_ROWS : BJ_ORDER_SAMPLING;
             const int rst = execute_common(ctx, plan, resident, flags, out, speculate);
-            ctx->rows_plan_only = false;
+            ctx->retry_ordering = -1;
             return rst;
         }
         return fail_to_status(ctx, f);

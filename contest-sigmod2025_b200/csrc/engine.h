@@ -313,7 +313,7 @@ struct bj_context {
     const std::vector<double>* cards_in = nullptr;  // a graph's recorded set cardinalities (capture)
     bool item_overflow = false;                     // the call's plan outgrew 32-bit item counts
     bj::PlanSpace plan_space = bj::plan_space_default();  // which plan space make_exec_plan runs
-    bool rows_plan_only = false;                    // plan with the row-count model (after an overflow)
+    int retry_ordering = -1;                        // after an overflow: the ordering of the rerun (-1: none)
     std::vector<double>* cards_out = nullptr;       // where a first run records them
     std::vector<cudaEvent_t> pipe_events;  // one per pipeline, reused across calls
     std::vector<cudaEvent_t> window_events;  // a streamed scan's copy and release marks
