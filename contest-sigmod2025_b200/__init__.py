@@ -830,7 +830,10 @@ def subplan_corpus(ctx: "Context", workload: "Workload", residents, queries, max
             feats.append(ctx.subplan_features(plan, residents, m))
         qids.append(np.full(len(m), k, dtype=np.int64))
         masks.append(m)
-    out = {"card": np.concatenate(cards), "sample": np.concatenate(samples), "query": np.concatenate(qids),
+    card = np.concatenate(cards)
+    # A count past 2^64 - 1 comes back infinite; as a label it is 2^64.
+    card = np.where(np.isfinite(card), card, 2.0 ** 64)
+    out = {"card": card, "sample": np.concatenate(samples), "query": np.concatenate(qids),
            "mask": np.concatenate(masks)}
     if with_features:
         out["features"] = np.concatenate(feats)

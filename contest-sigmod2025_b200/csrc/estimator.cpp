@@ -807,6 +807,8 @@ BJ_API int bj_estimator_train(bj_estimator* e, const float* features, const floa
                               uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float* epoch_loss) {
     if (!e || !features || !targets || n == 0 || batch == 0 || batch > 8192 || n > (1ull << 24))
         return BJ_ERR_INVALID;
+    for (uint64_t i = 0; i < n; i++)
+        if (!std::isfinite(targets[i])) return BJ_ERR_INVALID;  // a NaN or infinite label would poison the fit
     std::lock_guard<std::mutex> g(e->m);
     cudaSetDevice(e->device);
     try {

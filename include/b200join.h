@@ -334,7 +334,8 @@ BJ_API uint64_t bj_estimator_num_params(void);
 BJ_API int bj_estimator_get_params(bj_estimator* e, float* out);
 BJ_API int bj_estimator_set_params(bj_estimator* e, const float* in);
 /* Trains on n rows (features as bj_subplan_features writes them, rounded to
- * BF16; targets log2(cardinality + 1)) for `epochs` passes in shuffled
+ * BF16; targets log2(cardinality + 1), all finite: a count reported as
+ * infinite is past 2^64 and should be given as 64) for `epochs` passes in shuffled
  * batches of `batch` rows, learning rate `lr` (cosine decay to a tenth).
  * epoch_loss (optional, `epochs` entries) receives each pass's mean squared
  * error. */
