@@ -1433,6 +1433,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
     res->ctx = ctx;
     SpecCheck spec;
     bool planned_with_cards = false;
+    bool planned_reference = false;
     ctx->item_overflow = false;
     try {
         ExecPlan ex;
@@ -1463,7 +1464,11 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
             }
         }
         planned_with_cards = use_cards != nullptr;
-        int st = make_exec_plan(*plan, ex, err, false, use_cards, ctx->plan_space);
+        const PlanSpace space =
+            ctx->space_in ? *ctx->space_in : ctx->retry_rooted ? PlanSpace::Rooted : ctx->plan_space;
+        int st = make_exec_plan(*plan, ex, err, false, use_cards, space);
+        planned_reference = ex.reference_space;
+        if (ctx->space_out) *ctx->space_out = space;
         if (st != BJ_OK) throw Fail{st, err};
         ctx->tune = tune_for(ctx, ex);
         res->types = ex.out_types;
@@ -1634,18 +1639,25 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
             res.reset();
             return execute_common(ctx, plan, resident, flags, out, false);
         }
-        // A join order whose intermediate result outgrew 32-bit item counts:
-        // one rerun with the other cardinality source -- the row-count model
-        // after estimated cardinalities, join samples after the row-count
-        // model (resident tables only) -- recorded for the query's graph.
-        if (ctx->item_overflow && ctx->retry_ordering < 0 && !ctx->cards_in && (planned_with_cards || resident)) {
+        // A join order whose intermediate result outgrew 32-bit item counts
+        // or the device memory: one rerun with another plan -- the rooted
+        // plan of the same cardinalities after a plan of the reference's
+        // space; else the row-count model after estimated cardinalities, join
+        // samples after the row-count model (resident tables only).
+        const bool too_big = ctx->item_overflow || f.status == BJ_ERR_OOM;
+        if (too_big && ctx->retry_ordering < 0 && !ctx->retry_rooted && !ctx->cards_in && !ctx->space_in &&
+            (planned_reference || planned_with_cards || resident)) {
             fail_to_status(ctx, f);
             ctx->last_error.clear();
             res.reset();
             if (ctx->tape && ctx->tape_mode == 1) ctx->tape->slots.clear();
-            ctx->retry_ordering = planned_with_cards ? BJ_ORDER_ROWS : BJ_ORDER_SAMPLING;
+            if (planned_reference)
+                ctx->retry_rooted = true;
+            else
+                ctx->retry_ordering = planned_with_cards ? BJ_ORDER_ROWS : BJ_ORDER_SAMPLING;
             const int rst = execute_common(ctx, plan, resident, flags, out, speculate);
             ctx->retry_ordering = -1;
+            ctx->retry_rooted = false;
             return rst;
         }
         return fail_to_status(ctx, f);
@@ -1707,7 +1719,7 @@ bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resid
     try {
         ExecPlan ex;
         std::string err;
-        if (make_exec_plan(*plan, ex, err, false, g.cards.empty() ? nullptr : &g.cards, ctx->plan_space) != BJ_OK ||
+        if (make_exec_plan(*plan, ex, err, false, g.cards.empty() ? nullptr : &g.cards, g.space) != BJ_OK ||
             ex.empty)
             return false;
         ctx->tune = tune_for(ctx, ex);
@@ -1914,8 +1926,10 @@ int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* co
         ctx->tape = &e->tape;
         ctx->tape_mode = 1;
         ctx->cards_out = &e->cards;
+        ctx->space_out = &e->space;
         int st = execute_common(ctx, plan, tables, flags, out);
         ctx->cards_out = nullptr;
+        ctx->space_out = nullptr;
         ctx->tape_mode = 0;
         ctx->tape = nullptr;
         if (st == BJ_OK) {
@@ -1930,8 +1944,10 @@ int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* co
     if (!g->failed && !g->exec && !capture_graph(ctx, *g, plan, tables, flags)) g->failed = true;
     if (g->failed) {
         ctx->cards_in = &g->cards;  // plan as the first run did
+        ctx->space_in = &g->space;
         int st = execute_common(ctx, plan, tables, flags, out);
         ctx->cards_in = nullptr;
+        ctx->space_in = nullptr;
         return st;
     }
     return replay_graph(ctx, *g, g->out_types, flags, out);

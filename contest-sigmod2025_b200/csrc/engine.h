@@ -258,6 +258,7 @@ struct GraphEntry {
     std::vector<cudaEvent_t> phase;          // phase marks inside the graph
     uint64_t prof_bytes = 0;
     std::vector<double> cards;               // set cardinalities the first run planned with (empty: none)
+    PlanSpace space = PlanSpace::Auto;       // plan space the first run used
 };
 
 // Records a failed call's message on the context, leaves its streams idle and
@@ -314,6 +315,9 @@ struct bj_context {
     bool item_overflow = false;                     // the call's plan outgrew 32-bit item counts
     bj::PlanSpace plan_space = bj::plan_space_default();  // which plan space make_exec_plan runs
     int retry_ordering = -1;                        // after an overflow: the ordering of the rerun (-1: none)
+    bool retry_rooted = false;                      // after an overflow: the rerun plans in the rooted space
+    bj::PlanSpace* space_out = nullptr;             // where a first run records the plan space it ran
+    const bj::PlanSpace* space_in = nullptr;        // a graph's recorded plan space
     std::vector<double>* cards_out = nullptr;       // where a first run records them
     std::vector<cudaEvent_t> pipe_events;  // one per pipeline, reused across calls
     std::vector<cudaEvent_t> window_events;  // a streamed scan's copy and release marks
