@@ -1,5 +1,7 @@
-// Host side of the B200 join engine: context, memory, page upload, pipeline
-// driver and the C ABI of include/b200join.h.
+// Host side of the B200 join engine: page upload and indexing, the pipeline
+// driver (Executor) and the shared execute path. The context's life cycle and
+// the C ABI are in api.cpp, CUDA-graph replay in graphs.cpp, resident tables
+// and snapshots in resident.cpp.
 //
 // Replaces, for the join path:
 //  * Contest::build_context / execute / destroy_context (engine/Execute.cpp:
@@ -37,8 +39,7 @@
 
 using namespace bj;
 
-// Phase marks of a profiled call (bj_stats.phase_ms).
-constexpr size_t kPhaseMarks = 5;
+namespace bj {
 
 // Phase durations from the five phase marks of a call (bj_stats.phase_ms).
 void phase_stats(const std::vector<cudaEvent_t>& marks, bj_stats& st) {
@@ -50,8 +51,6 @@ void phase_stats(const std::vector<cudaEvent_t>& marks, bj_stats& st) {
     }
 }
 
-namespace bj {
-namespace {
 
 // Reads back `n` u64 slots of ctx->d_small after the stream drains; checks the
 // device error word.
@@ -124,14 +123,6 @@ void stash_err(bj_context* ctx) { stash_value(ctx, ctx->d_err, 63, false); }
 // ---------------------------------------------------------------------------
 // Page upload and indexing.
 
-struct ColumnJob {
-    const bj_column* src;  // host pages
-    uint8_t* dpages;       // device-accessible address of the pages
-    uint64_t rows;         // rows the table claims
-    DevColumn* out;
-    bool in_place = false; // pages are read where they are (pinned host memory): no copy
-    const uint8_t* pinned = nullptr;  // pages back to back in pinned host memory: one DMA from here
-};
 
 // A column's pages when they lie back to back in pinned host memory (the
 // first and the last byte pinned, both mapped to one device range when
@@ -432,6 +423,8 @@ TuneConfig tune_for(const bj_context* ctx, const ExecPlan& ex) {
         if (k == key) return c;
     return TuneConfig{};
 }
+
+namespace {
 
 class Executor {
     public:
@@ -1347,6 +1340,14 @@ void set_empty_result(bj_result& r, const ExecPlan& ex) {
 
 } // namespace
 
+bool run_pipelines(bj_context* ctx, const ExecPlan& ex, const std::vector<const DevTable*>& tables, bj_result& res,
+                   int flags, uint64_t& pipelines) {
+    Executor exe(ctx, ex, tables);
+    const bool nonempty = exe.run(res, flags);
+    pipelines = exe.pipelines_run();
+    return nonempty;
+}
+
 int fail_to_status(bj_context* ctx, const Fail& f) {
     ctx->last_error = f.msg;
     ctx->gather.n = 0;
@@ -1420,9 +1421,11 @@ struct SpecCheck {
     }
 };
 
+} // namespace
+
 // Shared tail of bj_execute / bj_execute_resident.
 int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* resident, int flags, bj_result** out,
-                   bool speculate = true) {
+                   bool speculate) {
     auto t0 = std::chrono::steady_clock::now();
     if (!ctx || !plan || !out) return BJ_ERR_INVALID;
     trace_begin(ctx->stream);
@@ -1673,882 +1676,4 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
     return BJ_OK;
 }
 
-// ---------------------------------------------------------------------------
-// CUDA-graph replay of repeated resident queries.
-//
-// A serving process runs the same query shapes over the same resident tables
-// again and again. The first run of a (plan, tables, flags) key executes
-// normally and records every host read-back (probe hit rates, table flags,
-// counts) on a tape. The second run executes the same host logic under
-// stream capture, answering read-backs from the tape instead of
-// synchronising, so every kernel, copy and cross-stream dependency of the
-// query lands in one CUDA graph. Later runs launch that graph -- all kernels
-// run again, on the same resident inputs -- and copy the result pages out.
-// The tables are immutable once resident, so the recorded counts stay exact;
-// freeing a table drops the graphs that read it.
-
-std::vector<uint64_t> graph_key(const bj_plan& plan, bj_resident* const* tables, int flags, bool profile) {
-    std::vector<uint64_t> k{plan.num_nodes, plan.num_inputs, plan.root, uint64_t(flags), uint64_t(profile)};
-    for (uint64_t i = 0; i < plan.num_nodes; i++) {
-        const bj_node& n = plan.nodes[i];
-        k.insert(k.end(), {uint64_t(n.kind), uint64_t(n.build_left), n.base_table_id, n.left, n.right, n.left_attr,
-                           n.right_attr, n.num_output_attrs});
-        for (uint64_t a = 0; a < n.num_output_attrs; a++) {
-            k.push_back(n.output_attrs[a].index);
-            k.push_back(uint64_t(uint32_t(n.output_attrs[a].type)));
-        }
-    }
-    for (uint64_t i = 0; i < plan.num_inputs; i++) k.push_back(reinterpret_cast<uint64_t>(tables[i]));
-    return k;
-}
-
-void destroy_graph(GraphEntry& g) {
-    if (g.exec) cudaGraphExecDestroy(g.exec);
-    g.exec = nullptr;
-    for (cudaEvent_t e : g.prof) cudaEventDestroy(e);
-    g.prof.clear();
-    for (cudaEvent_t e : g.phase) cudaEventDestroy(e);
-    g.phase.clear();
-}
-
-bool capture_graph(bj_context* ctx, GraphEntry& g, const bj_plan* plan, bj_resident* const* resident, int flags) {
-    bool capturing = false;
-    bj_result res;
-    res.ctx = ctx;
-    uint64_t launches0 = ctx->launches;
-    try {
-        ExecPlan ex;
-        std::string err;
-        if (make_exec_plan(*plan, ex, err, false, g.cards.empty() ? nullptr : &g.cards, g.space) != BJ_OK ||
-            ex.empty)
-            return false;
-        ctx->tune = tune_for(ctx, ex);
-        std::vector<const DevTable*> tables(plan->num_inputs);
-        for (uint64_t i = 0; i < plan->num_inputs; i++) tables[i] = &resident[i]->table;
-        g.tape.pos = 0;
-        ctx->tape = &g.tape;
-        ctx->tape_mode = 2;
-        ctx->graph_output = true;
-        BJ_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
-        capturing = true;
-        // The graph clears the device error word first and copies it to the
-        // pinned read-back slot last, so a replay needs no other call.
-        BJ_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(uint32_t), ctx->stream));
-        Executor exe(ctx, ex, tables);
-        bool nonempty = exe.run(res, flags);
-        BJ_CK(cudaMemcpyAsync(&ctx->h_small[63], ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
-        capturing = false;
-        cudaGraph_t graph = nullptr;
-        BJ_CK(cudaStreamEndCapture(ctx->stream, &graph));
-        ctx->tape_mode = 0;
-        ctx->tape = nullptr;
-        ctx->graph_output = false;
-        // The recording ends with the call's final error check, not replayed here.
-        if (!graph || g.tape.pos + 1 != g.tape.slots.size()) {
-            if (graph) cudaGraphDestroy(graph);
-            throw Fail{BJ_ERR_INTERNAL, "graph capture diverged from its recording"};
-        }
-        cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (ie != cudaSuccess) throw Fail{BJ_ERR_CUDA, "cudaGraphInstantiate failed"};
-        g.out_types = ex.out_types;
-        if (nonempty) {
-            g.rows = res.rows;
-            g.npages = res.npages;
-            g.page_base = res.page_base;
-            g.total_pages = res.total_pages;
-            g.pages = res.arena_pages;
-        } else {
-            g.rows = 0;
-            g.npages.assign(ex.out_types.size(), 0);
-            g.page_base.assign(ex.out_types.size(), 0);
-            g.total_pages = 0;
-            g.pages = nullptr;
-        }
-        g.stats = bj_stats{};
-        g.stats.kernel_launches = ctx->launches - launches0;
-        g.stats.pipelines = exe.pipelines_run();
-        g.stats.arena_bytes = ctx->arena.used_total();
-        for (uint64_t i = 0; i < plan->num_inputs; i++) {
-            std::vector<uint8_t> used;
-            collect_columns(ex, uint32_t(i), tables[i]->cols.size(), used);
-            for (size_t c = 0; c < used.size(); c++)
-                if (used[c]) g.stats.input_pages += tables[i]->cols[c].npages;
-        }
-        g.prof = ctx->prof_events;
-        g.phase = ctx->phase_events;
-        g.prof_bytes = ctx->prof_bytes;
-        ctx->prof_events.clear();
-        ctx->phase_events.clear();
-        ctx->prof_bytes = 0;
-        ctx->arena.reset();
-        return true;
-    } catch (const Fail&) {
-        if (capturing) {
-            cudaGraph_t gr = nullptr;
-            cudaStreamEndCapture(ctx->stream, &gr);
-            if (gr) cudaGraphDestroy(gr);
-        }
-        cudaGetLastError();
-        ctx->gather.n = 0;
-        ctx->tape_mode = 0;
-        ctx->tape = nullptr;
-        ctx->graph_output = false;
-        for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
-        ctx->prof_events.clear();
-        for (cudaEvent_t e : ctx->phase_events) cudaEventDestroy(e);
-        ctx->phase_events.clear();
-        ctx->prof_bytes = 0;
-        ctx->sync_all();
-        ctx->arena.reset();
-        return false;
-    }
-}
-
-int replay_graph(bj_context* ctx, GraphEntry& g, const std::vector<int32_t>& types, int flags, bj_result** out) {
-    auto t0 = std::chrono::steady_clock::now();
-    std::unique_ptr<bj_result> res(new bj_result);
-    res->ctx = ctx;
-    try {
-        res->types = types;
-        ctx->h_small[63] = 0;  // the graph's last node writes the low half
-        BJ_CK(cudaEventRecord(ctx->ev0, ctx->stream));
-        BJ_CK(cudaGraphLaunch(g.exec, ctx->stream));
-        res->rows = g.rows;
-        res->npages = g.npages;
-        res->page_base = g.page_base;
-        res->total_pages = g.total_pages;
-        size_t bytes = g.total_pages * kPageSize;
-        if (bytes && (flags & BJ_RESULT_DEVICE)) {
-            BJ_CK(cudaMallocAsync(reinterpret_cast<void**>(&res->dev), bytes, ctx->stream));
-            BJ_CK(cudaMemcpyAsync(res->dev, g.pages, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-        } else if (bytes) {
-            res->host = ctx->take_pinned(bytes);
-            BJ_CK(cudaMemcpyAsync(res->host.p, g.pages, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-            res->stats.d2h_bytes = bytes;
-        }
-        BJ_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-        bool async = (flags & BJ_RESULT_ASYNC) && ctx->async_err && g.prof.empty() && g.phase.empty();
-        if (async) {
-            // The error word of this query goes to its own slot; the result
-            // completes in bj_result_wait (device_ms is not measured).
-            {
-                std::lock_guard<std::mutex> lk(ctx->release_m);
-                async = !ctx->free_slots.empty();
-                if (async) {
-                    res->slot = ctx->free_slots.back();
-                    ctx->free_slots.pop_back();
-                    if (!ctx->free_done.empty()) {
-                        res->done = ctx->free_done.back();
-                        ctx->free_done.pop_back();
-                    }
-                }
-            }
-            if (async && !res->done && cudaEventCreateWithFlags(&res->done, cudaEventDisableTiming) != cudaSuccess) {
-                cudaGetLastError();
-                std::lock_guard<std::mutex> lk(ctx->release_m);
-                ctx->free_slots.push_back(res->slot);
-                throw Fail{BJ_ERR_CUDA, "event creation failed"};
-            }
-        }
-        if (async) {
-            ctx->async_err[res->slot] = 0;
-            res->pending = true;
-            BJ_CK(cudaMemcpyAsync(ctx->async_err + res->slot, ctx->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                  ctx->stream));
-            BJ_CK(cudaEventRecord(res->done, ctx->stream));
-        } else {
-            BJ_CK(cudaStreamSynchronize(ctx->stream));
-            if (uint32_t code = uint32_t(ctx->h_small[63]))
-                throw Fail{BJ_ERR_INVALID, std::string("device check failed: ") + dev_error_text(code)};
-            float ms = 0;
-            BJ_CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-            res->stats.device_ms = ms;
-        }
-        for (size_t i = 0; i + 1 < g.prof.size(); i += 2) {
-            float k = 0;
-            BJ_CK(cudaEventElapsedTime(&k, g.prof[i], g.prof[i + 1]));
-            res->stats.scan_kernel_ms += k;
-            res->stats.scan_kernel_launches++;
-        }
-        phase_stats(g.phase, res->stats);
-        res->stats.scan_kernel_bytes = g.prof_bytes;
-        res->stats.kernel_launches = g.stats.kernel_launches;
-        res->stats.pipelines = g.stats.pipelines;
-        res->stats.arena_bytes = g.stats.arena_bytes;
-        res->stats.input_pages = g.stats.input_pages;
-        res->stats.output_pages = g.total_pages;
-        ctx->launches += g.stats.kernel_launches;
-    } catch (const Fail& f) {
-        int st = fail_to_status(ctx, f);  // waits for the stream
-        if (res->pending) {
-            std::lock_guard<std::mutex> lk(ctx->release_m);
-            ctx->free_slots.push_back(res->slot);
-            ctx->free_done.push_back(res->done);
-            res->pending = false;
-        }
-        if (res->dev) cudaFree(res->dev);
-        res->dev = nullptr;
-        ctx->give_pinned(res->host);
-        res->host = PinnedBlock{};
-        return st;
-    }
-    res->stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    ctx->live_results++;
-    ctx->last_error.clear();
-    *out = res.release();
-    return BJ_OK;
-}
-
-int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int flags,
-                           bj_result** out) {
-    ctx->drain_releases();
-    std::vector<uint64_t> key = graph_key(*plan, tables, flags & ~BJ_RESULT_ASYNC, ctx->profile);
-    key.push_back(uint64_t(ctx->ordering));
-    key.push_back(reinterpret_cast<uint64_t>(ctx->estimator));
-    key.push_back(uint64_t(ctx->plan_space));
-    uint64_t hash = 0x9e3779b97f4a7c15ull;
-    for (uint64_t v : key) hash = (hash ^ v) * 0x100000001b3ull + (hash >> 29);
-    GraphEntry* g = nullptr;
-    auto& gc = ctx->graph_cache;
-    for (size_t i = gc.size(); i-- > 0;)
-        if (gc[i]->hash == hash && gc[i]->key == key) {
-            // Most recently used goes last.
-            std::rotate(gc.begin() + i, gc.begin() + i + 1, gc.end());
-            g = gc.back().get();
-            break;
-        }
-    if (!g) {
-        auto e = std::make_unique<GraphEntry>();
-        e->key = std::move(key);
-        e->hash = hash;
-        e->tables.assign(tables, tables + plan->num_inputs);
-        ctx->tape = &e->tape;
-        ctx->tape_mode = 1;
-        ctx->cards_out = &e->cards;
-        ctx->space_out = &e->space;
-        int st = execute_common(ctx, plan, tables, flags, out);
-        ctx->cards_out = nullptr;
-        ctx->space_out = nullptr;
-        ctx->tape_mode = 0;
-        ctx->tape = nullptr;
-        if (st == BJ_OK) {
-            if (gc.size() >= bj_context::kGraphCache) {
-                destroy_graph(*gc.front());
-                gc.erase(gc.begin());
-            }
-            gc.push_back(std::move(e));
-        }
-        return st;
-    }
-    if (!g->failed && !g->exec && !capture_graph(ctx, *g, plan, tables, flags)) g->failed = true;
-    if (g->failed) {
-        ctx->cards_in = &g->cards;  // plan as the first run did
-        ctx->space_in = &g->space;
-        int st = execute_common(ctx, plan, tables, flags, out);
-        ctx->cards_in = nullptr;
-        ctx->space_in = nullptr;
-        return st;
-    }
-    return replay_graph(ctx, *g, g->out_types, flags, out);
-}
-
-} // namespace
 } // namespace bj
-
-namespace bj {
-// Waits for ctx's work, then drops its graphs that read table t.
-void drop_graphs_using(bj_context* ctx, const bj_resident* t) {
-    ctx->sync_all();
-    auto& gc = ctx->graph_cache;
-    for (size_t i = 0; i < gc.size();) {
-        const auto& tabs = gc[i]->tables;
-        if (std::find(tabs.begin(), tabs.end(), t) != tabs.end()) {
-            destroy_graph(*gc[i]);
-            gc.erase(gc.begin() + i);
-        } else {
-            i++;
-        }
-    }
-}
-} // namespace bj
-
-extern "C" {
-
-BJ_API const char* bj_version(void) { return "b200join 0.1 (sm_100a)"; }
-
-BJ_API int bj_plan_explain(const bj_plan* plan, char* buf, uint64_t cap, uint64_t* len) {
-    if (!plan || !len || (cap && !buf)) return BJ_ERR_INVALID;
-    try {
-        ExecPlan ex;
-        std::string err;
-        int st = make_exec_plan(*plan, ex, err, true);
-        if (st != BJ_OK) return st;
-        std::string out;
-        char line[256];
-        auto input_text = [&](uint32_t i) {
-            char t[96];
-            std::snprintf(t, sizeof t, "input %u (table %u, %llu rows)", i, ex.inputs[i].table,
-                          static_cast<unsigned long long>(ex.inputs[i].rows));
-            return std::string(t);
-        };
-        if (ex.empty) {
-            out = "empty: an input has no rows\n";
-        } else {
-            out = "driver: " + input_text(ex.driver);
-            if (ex.est_cost >= 0) {
-                std::snprintf(line, sizeof line, "; estimated cost %.4g (result card + 10 x hashed card per join)",
-                              ex.est_cost);
-                out += line;
-            }
-            if (ex.ref_cost >= 0) {
-                std::snprintf(line, sizeof line, "; the reference's plan space at best %.4g", ex.ref_cost);
-                out += line;
-            }
-            out += "\n";
-            for (size_t p = 0; p < ex.pipelines.size(); p++) {
-                const PipelinePlan& pp = ex.pipelines[p];
-                std::snprintf(line, sizeof line, "pipeline %zu: scan ", p);
-                out += line;
-                out += input_text(pp.input);
-                for (size_t k = 0; k < pp.probes.size(); k++) {
-                    std::snprintf(line, sizeof line, "%s pipeline %u on attr %u", k ? "," : ", probe", pp.probes[k].child,
-                                  pp.probes[k].probe_attr);
-                    out += line;
-                    if (pp.probes[k].key_probe >= 0) {
-                        std::snprintf(line, sizeof line, " (payload of pipeline %u)",
-                                      pp.probes[size_t(pp.probes[k].key_probe)].child);
-                        out += line;
-                    }
-                }
-                if (pp.build_key >= 0) {
-                    std::snprintf(line, sizeof line, " -> hash table on attr %lld", static_cast<long long>(pp.build_key));
-                    out += line;
-                    if (pp.build_key_probe >= 0) {
-                        std::snprintf(line, sizeof line, " (payload of pipeline %u)",
-                                      pp.probes[size_t(pp.build_key_probe)].child);
-                        out += line;
-                    }
-                } else {
-                    out += " -> result";
-                }
-                out += "\n";
-            }
-            if (!ex.ref_plan.empty()) out += "reference plan space, cheapest: " + ex.ref_plan + "\n";
-            if (ex.rooted_cost >= 0) {
-                std::snprintf(line, sizeof line, "rooted plan space, cheapest: driver input %u, cost %.4g\n",
-                              ex.rooted_driver, ex.rooted_cost);
-                out += line;
-            }
-            out += ex.reference_space ? "runs: the reference space's plan\n" : "runs: the rooted plan\n";
-            // The drop-in path's guess of the probe scanned first (it starts
-            // copying that column's pages before the device sampling decides).
-            const int g = guess_first_probe(ex, *plan);
-            if (g >= 0) {
-                const PipelinePlan& root = ex.pipelines.back();
-                std::snprintf(line, sizeof line, "scan guess: pipeline %u on attr %u\n", root.probes[size_t(g)].child,
-                              root.probes[size_t(g)].probe_attr);
-                out += line;
-            }
-        }
-        *len = out.size();
-        if (cap) {
-            const size_t n = std::min<size_t>(out.size(), cap - 1);
-            std::memcpy(buf, out.data(), n);
-            buf[n] = '\0';
-        }
-        return BJ_OK;
-    } catch (...) {
-        return BJ_ERR_INTERNAL;
-    }
-}
-
-BJ_API int bj_context_create(int device, bj_context** out) {
-    if (!out) return BJ_ERR_INVALID;
-    *out = nullptr;
-    int n = 0;
-    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
-        cudaGetLastError();
-        return BJ_ERR_NO_DEVICE;
-    }
-    if (device < 0 || device >= n) return BJ_ERR_INVALID;
-    if (cudaSetDevice(device) != cudaSuccess) return BJ_ERR_CUDA;
-    auto ctx = std::make_unique<bj_context>();
-    ctx->device = device;
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return BJ_ERR_CUDA;
-    for (auto& s : ctx->side)
-        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return BJ_ERR_CUDA;
-    if (cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking) != cudaSuccess) return BJ_ERR_CUDA;
-    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) return BJ_ERR_CUDA;
-    if (cudaMalloc(&ctx->d_err, 256) != cudaSuccess) return BJ_ERR_OOM;
-    ctx->arena.err = ctx->d_err;
-    if (cudaMalloc(&ctx->d_small, sizeof(uint64_t) * 64) != cudaSuccess) return BJ_ERR_OOM;
-    if (cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_small), sizeof(uint64_t) * 64, cudaHostAllocDefault) != cudaSuccess)
-        return BJ_ERR_OOM;
-    cudaMemset(ctx->d_err, 0, 256);
-    cudaMemset(ctx->d_small, 0, sizeof(uint64_t) * 64);
-    if (cudaHostAlloc(reinterpret_cast<void**>(&ctx->async_err), sizeof(uint32_t) * bj_context::kAsyncSlots,
-                      cudaHostAllocDefault) != cudaSuccess)
-        return BJ_ERR_OOM;
-    for (uint32_t i = bj_context::kAsyncSlots; i > 0; i--) ctx->free_slots.push_back(i - 1);
-    // Keep freed result buffers cached in the stream-ordered pool.
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-        uint64_t threshold = ~0ull;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
-    }
-    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
-    if (const char* zc = std::getenv("B200JOIN_ZERO_COPY")) ctx->zero_copy = std::atoi(zc) != 0;
-    if (const char* gr = std::getenv("B200JOIN_GRAPHS")) ctx->graphs = std::atoi(gr) != 0;
-    if (const char* sp = std::getenv("B200JOIN_SCAN_SPLIT")) ctx->scan_split = std::atoi(sp) != 0;
-    if (const char* ss = std::getenv("B200JOIN_STREAM_SCAN")) ctx->stream_scans = std::atoi(ss) != 0;
-    if (const char* lb = std::getenv("B200JOIN_LEAF_BATCH")) ctx->leaf_batch = std::atoi(lb) != 0;
-    unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    ctx->pool = std::make_unique<ThreadPool>(std::min(hw, 16u) - 1);
-    *out = ctx.release();
-    return BJ_OK;
-}
-
-BJ_API void bj_context_destroy(bj_context* ctx) {
-    if (!ctx) return;
-    cudaSetDevice(ctx->device);
-    ctx->sync_all();
-    for (auto& g : ctx->graph_cache) destroy_graph(*g);
-    ctx->graph_cache.clear();
-    for (cudaEvent_t e : ctx->pipe_events) cudaEventDestroy(e);
-    for (cudaEvent_t e : ctx->window_events) cudaEventDestroy(e);
-    for (cudaEvent_t e : ctx->free_done) cudaEventDestroy(e);
-    if (ctx->async_err) cudaFreeHost(ctx->async_err);
-    for (uint8_t* p : ctx->release_dev) cudaFree(p);
-    for (cudaStream_t s : ctx->side)
-        if (s) cudaStreamDestroy(s);
-    if (ctx->copy) cudaStreamDestroy(ctx->copy);
-    for (auto& b : ctx->pinned_free) cudaFreeHost(b.p);
-    if (ctx->stage.p) cudaFreeHost(ctx->stage.p);
-    if (ctx->h_small) cudaFreeHost(ctx->h_small);
-    if (ctx->d_small) cudaFree(ctx->d_small);
-    if (ctx->d_err) cudaFree(ctx->d_err);
-    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
-    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
-    delete ctx;
-}
-
-BJ_API const char* bj_last_error(const bj_context* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
-
-BJ_API void* bj_context_stream(bj_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
-
-BJ_API int bj_context_autotune(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int repeats,
-                               char* report, uint64_t cap, uint64_t* len) {
-    if (!ctx || !plan || !tables || repeats < 1) return BJ_ERR_INVALID;
-    cudaSetDevice(ctx->device);
-    ExecPlan ex;
-    std::string err;
-    int st = make_exec_plan(*plan, ex, err);
-    if (st != BJ_OK) {
-        ctx->last_error = err;
-        return st;
-    }
-    const uint64_t key = shape_class(ex);
-    std::string text = "shape class " + std::to_string(key >> 16) + "/" + std::to_string((key >> 8) & 255) + "/" +
-                       std::to_string(key & 255) + " (log2 rows of the largest and second largest input / inputs)\n";
-    const bool graphs = ctx->graphs;
-    ctx->graphs = false;  // every run executes (no replay)
-    TuneConfig best{};
-    double best_ms = -1;
-    int64_t rows = -1;  // every parameter set must return the same row count
-    for (uint8_t split : {uint8_t(1), uint8_t(0)})
-        for (uint8_t bits : {uint8_t(8), uint8_t(16), uint8_t(32)})
-            for (uint8_t extra : {uint8_t(0), uint8_t(1)}) {
-                TuneConfig c{split, bits, extra};
-                ctx->tune_override = &c;
-                std::vector<double> ms;
-                for (int r = 0; r <= repeats && st == BJ_OK; r++) {
-                    bj_result* res = nullptr;
-                    st = bj_execute_resident(ctx, plan, tables, BJ_RESULT_DEVICE, &res);
-                    if (st != BJ_OK) break;
-                    bj_stats s{};
-                    bj_result_stats(res, &s);
-                    const int64_t n = int64_t(bj_result_num_rows(res));
-                    bj_result_free(res);
-                    if (rows >= 0 && n != rows) {
-                        ctx->last_error = "autotune: parameter sets returned different row counts";
-                        st = BJ_ERR_INTERNAL;
-                        break;
-                    }
-                    rows = n;
-                    if (r > 0) ms.push_back(s.device_ms);  // the first run warms up
-                }
-                ctx->tune_override = nullptr;
-                if (st != BJ_OK) break;
-                std::sort(ms.begin(), ms.end());
-                const double med = ms[ms.size() / 2];
-                char line[160];
-                std::snprintf(line, sizeof(line), "scan %s, bloom %2u bits/key, buckets x%u: %.4f ms\n",
-                              split ? "split" : "fused", unsigned(bits), 1u << extra, med);
-                text += line;
-                if (best_ms < 0 || med < best_ms) {
-                    best_ms = med;
-                    best = c;
-                }
-            }
-    ctx->graphs = graphs;
-    if (st != BJ_OK) return st;
-    bool found = false;
-    for (auto& [k, c] : ctx->tuned)
-        if (k == key) {
-            c = best;
-            found = true;
-        }
-    if (!found) ctx->tuned.push_back({key, best});
-    // Graphs captured under other parameters are dropped.
-    ctx->sync_all();
-    for (auto& g : ctx->graph_cache) destroy_graph(*g);
-    ctx->graph_cache.clear();
-    char line[160];
-    std::snprintf(line, sizeof(line), "chosen: scan %s, bloom %u bits/key, buckets x%u (%.4f ms)\n",
-                  best.scan_split ? "split" : "fused", unsigned(best.bloom_bits), 1u << best.bucket_extra, best_ms);
-    text += line;
-    if (len) *len = text.size();
-    if (report && cap) {
-        const size_t n = std::min<size_t>(cap - 1, text.size());
-        std::memcpy(report, text.data(), n);
-        report[n] = 0;
-    }
-    return BJ_OK;
-}
-
-BJ_API int bj_context_set_plan_space(bj_context* ctx, int space) {
-    if (!ctx || space < 0 || space > 2) return BJ_ERR_INVALID;
-    ctx->plan_space = PlanSpace(space);
-    return BJ_OK;
-}
-
-BJ_API void bj_context_set_graphs(bj_context* ctx, int on) {
-    if (!ctx) return;
-    if (!on) {
-        // Graphs already captured stay valid but are no longer used.
-        ctx->sync_all();
-    }
-    ctx->graphs = on != 0;
-}
-
-BJ_API void bj_context_profile(bj_context* ctx, int on) {
-    if (ctx) ctx->profile = on != 0;
-}
-
-BJ_API int bj_execute(bj_context* ctx, const bj_plan* plan, bj_result** out) {
-    if (!ctx) return BJ_ERR_INVALID;
-    cudaSetDevice(ctx->device);
-    return execute_common(ctx, plan, nullptr, BJ_RESULT_HOST, out);
-}
-
-BJ_API int bj_execute_resident(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int flags,
-                               bj_result** out) {
-    if (!ctx || !tables) return BJ_ERR_INVALID;
-    cudaSetDevice(ctx->device);
-    if (ctx->graphs && plan) return execute_resident_graph(ctx, plan, tables, flags, out);
-    return execute_common(ctx, plan, tables, flags, out);
-}
-
-BJ_API int bj_resident_upload(bj_context* ctx, const bj_table* table, bj_resident** out) {
-    if (!ctx || !table || !out) return BJ_ERR_INVALID;
-    *out = nullptr;
-    cudaSetDevice(ctx->device);
-    auto r = std::make_unique<bj_resident>();
-    try {
-        DevTable& d = r->table;
-        d.rows = table->num_rows;
-        d.cols.assign(table->num_columns, DevColumn{});
-        d.present.assign(table->num_columns, 0);
-        if (table->num_rows >= (1ull << 32) - 2) throw Fail{BJ_ERR_UNSUPPORTED, "tables are limited to 2^32-2 rows"};
-        std::vector<ColumnJob> jobs;
-        if (table->num_rows) {
-            if (table->num_columns && !table->columns) throw Fail{BJ_ERR_INVALID, "table without column array"};
-            for (uint64_t c = 0; c < table->num_columns; c++) {
-                const bj_column& hc = table->columns[c];
-                if (hc.type < BJ_INT32 || hc.type > BJ_VARCHAR) throw Fail{BJ_ERR_INVALID, "unknown column type"};
-                if (hc.num_pages && !hc.pages) throw Fail{BJ_ERR_INVALID, "column without page array"};
-                d.cols[c].type = hc.type;
-                d.present[c] = 1;
-                uint8_t* dp = static_cast<uint8_t*>(r->mem.alloc(std::max<uint64_t>(hc.num_pages, 1) * kPageSize));
-                uint8_t* mapped = nullptr;
-                const uint8_t* pinned = pinned_base(hc, mapped);
-                jobs.push_back(ColumnJob{&hc, dp, table->num_rows, &d.cols[c], false, pinned});
-            }
-        } else {
-            for (uint64_t c = 0; c < table->num_columns; c++) d.present[c] = 1;
-        }
-        BJ_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(uint32_t), ctx->stream));
-        upload_pages(ctx, jobs);
-        index_columns(ctx, jobs, r->mem);
-        BJ_CK(cudaStreamSynchronize(ctx->stream));
-        ctx->arena.reset();
-    } catch (const Fail& f) {
-        return fail_to_status(ctx, f);
-    } catch (const std::exception& e) {
-        return fail_to_status(ctx, Fail{BJ_ERR_INTERNAL, e.what()});
-    }
-    *out = r.release();
-    return BJ_OK;
-}
-
-
-// Snapshot of a resident table (bj_resident_save / bj_resident_load): the
-// role of the reference's table cache file (engine/infra/DataSource.cpp:50-159),
-// which reloads tables without re-parsing them. Layout (little-endian):
-//   "BJRES001", u64 rows, u64 columns;
-//   per column: i32 type, u32 present, u32 pages, u32 rows, u32 flags, u32 rpp,
-//               u64 chunks, u64 blocks;
-//   then per column: pages (pages * 8192 B), hdr (pages u32), row_start and
-//   chunk_base (pages + 1 u32 each), dense_base (chunks u32), page_of_blk
-//   (blocks u32).
-// Loading copies the arrays straight to HBM: no page index pass.
-namespace {
-constexpr char kSnapMagic[8] = {'B', 'J', 'R', 'E', 'S', '0', '0', '1'};
-struct SnapColumn {
-    int32_t type;
-    uint32_t present, npages, nrows, flags, rpp;
-    uint64_t chunks, blocks;
-};
-constexpr size_t kSnapChunk = size_t(64) << 20;  // bytes per bounce copy
-
-struct FileCloser {
-    void operator()(std::FILE* f) const {
-        if (f) std::fclose(f);
-    }
-};
-using File = std::unique_ptr<std::FILE, FileCloser>;
-
-// Copies device bytes to the file through a pinned bounce buffer.
-void snap_write(std::FILE* f, const void* dev, size_t bytes, uint8_t* bounce) {
-    const uint8_t* src = static_cast<const uint8_t*>(dev);
-    for (size_t off = 0; off < bytes; off += kSnapChunk) {
-        const size_t n = std::min(kSnapChunk, bytes - off);
-        BJ_CK(cudaMemcpy(bounce, src + off, n, cudaMemcpyDeviceToHost));
-        if (std::fwrite(bounce, 1, n, f) != n) throw Fail{BJ_ERR_INVALID, "snapshot write failed"};
-    }
-}
-// Reads file bytes into device memory through a pinned bounce buffer.
-void snap_read(std::FILE* f, void* dev, size_t bytes, uint8_t* bounce) {
-    uint8_t* dst = static_cast<uint8_t*>(dev);
-    for (size_t off = 0; off < bytes; off += kSnapChunk) {
-        const size_t n = std::min(kSnapChunk, bytes - off);
-        if (std::fread(bounce, 1, n, f) != n) throw Fail{BJ_ERR_INVALID, "snapshot file is truncated"};
-        BJ_CK(cudaMemcpy(dst + off, bounce, n, cudaMemcpyHostToDevice));
-    }
-}
-struct Bounce {
-    uint8_t* p = nullptr;
-    Bounce() {
-        if (cudaHostAlloc(reinterpret_cast<void**>(&p), kSnapChunk, cudaHostAllocDefault) != cudaSuccess) {
-            cudaGetLastError();
-            throw Fail{BJ_ERR_OOM, "pinned bounce buffer allocation failed"};
-        }
-    }
-    ~Bounce() {
-        if (p) cudaFreeHost(p);
-    }
-};
-} // namespace
-
-BJ_API int bj_resident_save(bj_context* ctx, const bj_resident* t, const char* path) {
-    if (!ctx || !t || !path) return BJ_ERR_INVALID;
-    cudaSetDevice(ctx->device);
-    try {
-        File f(std::fopen(path, "wb"));
-        if (!f) throw Fail{BJ_ERR_INVALID, std::string("cannot open ") + path};
-        BJ_CK(cudaStreamSynchronize(ctx->stream));
-        const DevTable& d = t->table;
-        std::vector<SnapColumn> cols(d.cols.size());
-        for (size_t c = 0; c < d.cols.size(); c++) {
-            const DevColumn& dc = d.cols[c];
-            SnapColumn& sc = cols[c];
-            sc = SnapColumn{dc.type, d.present[c], dc.npages, dc.nrows, dc.flags & ~kColHostPages, dc.rpp, 0, 0};
-            if (dc.npages) {
-                uint32_t chunks = 0;
-                BJ_CK(cudaMemcpy(&chunks, dc.chunk_base + dc.npages, sizeof(chunks), cudaMemcpyDeviceToHost));
-                sc.chunks = chunks;
-                sc.blocks = (uint64_t(dc.nrows) >> kBlkShift) + 2;
-            }
-        }
-        const uint64_t head[2] = {d.rows, uint64_t(d.cols.size())};
-        bool ok = std::fwrite(kSnapMagic, 1, 8, f.get()) == 8 && std::fwrite(head, sizeof(head), 1, f.get()) == 1 &&
-                  (cols.empty() || std::fwrite(cols.data(), sizeof(SnapColumn), cols.size(), f.get()) == cols.size());
-        if (!ok) throw Fail{BJ_ERR_INVALID, "snapshot write failed"};
-        Bounce b;
-        for (size_t c = 0; c < d.cols.size(); c++) {
-            const DevColumn& dc = d.cols[c];
-            const SnapColumn& sc = cols[c];
-            if (!sc.npages) continue;
-            snap_write(f.get(), dc.pages, size_t(sc.npages) * kPageSize, b.p);
-            snap_write(f.get(), dc.hdr, sizeof(uint32_t) * sc.npages, b.p);
-            snap_write(f.get(), dc.row_start, sizeof(uint32_t) * (sc.npages + 1), b.p);
-            snap_write(f.get(), dc.chunk_base, sizeof(uint32_t) * (sc.npages + 1), b.p);
-            snap_write(f.get(), dc.dense_base, sizeof(uint32_t) * sc.chunks, b.p);
-            snap_write(f.get(), dc.page_of_blk, sizeof(uint32_t) * sc.blocks, b.p);
-        }
-        if (std::fflush(f.get()) != 0) throw Fail{BJ_ERR_INVALID, "snapshot write failed"};
-    } catch (const Fail& fl) {
-        return fail_to_status(ctx, fl);
-    } catch (const std::exception& e) {
-        return fail_to_status(ctx, Fail{BJ_ERR_INTERNAL, e.what()});
-    }
-    ctx->last_error.clear();
-    return BJ_OK;
-}
-
-BJ_API int bj_resident_load(bj_context* ctx, const char* path, bj_resident** out) {
-    if (!ctx || !path || !out) return BJ_ERR_INVALID;
-    *out = nullptr;
-    cudaSetDevice(ctx->device);
-    auto r = std::make_unique<bj_resident>();
-    try {
-        File f(std::fopen(path, "rb"));
-        if (!f) throw Fail{BJ_ERR_INVALID, std::string("cannot open ") + path};
-        char magic[8];
-        uint64_t head[2];
-        if (std::fread(magic, 1, 8, f.get()) != 8 || std::memcmp(magic, kSnapMagic, 8) != 0 ||
-            std::fread(head, sizeof(head), 1, f.get()) != 1)
-            throw Fail{BJ_ERR_INVALID, "not a resident table snapshot"};
-        if (head[0] >= (1ull << 32) - 2 || head[1] > (1u << 20)) throw Fail{BJ_ERR_INVALID, "snapshot header out of range"};
-        std::vector<SnapColumn> cols(head[1]);
-        if (!cols.empty() && std::fread(cols.data(), sizeof(SnapColumn), cols.size(), f.get()) != cols.size())
-            throw Fail{BJ_ERR_INVALID, "snapshot file is truncated"};
-        DevTable& d = r->table;
-        d.rows = head[0];
-        d.cols.assign(cols.size(), DevColumn{});
-        d.present.assign(cols.size(), 0);
-        Bounce b;
-        for (size_t c = 0; c < cols.size(); c++) {
-            const SnapColumn& sc = cols[c];
-            if (sc.type < BJ_INT32 || sc.type > BJ_VARCHAR || sc.present > 1 ||
-                (sc.npages && (sc.nrows != d.rows || sc.chunks > uint64_t(sc.npages) * 1024 ||
-                               sc.blocks != (uint64_t(sc.nrows) >> kBlkShift) + 2)))
-                throw Fail{BJ_ERR_INVALID, "snapshot column descriptor out of range"};
-            DevColumn& dc = d.cols[c];
-            d.present[c] = uint8_t(sc.present);
-            dc.type = sc.type;
-            dc.npages = sc.npages;
-            dc.nrows = sc.nrows;
-            dc.flags = sc.flags;
-            dc.rpp = sc.rpp;
-            if (!sc.npages) continue;
-            auto dev = [&](size_t bytes) { return r->mem.alloc(std::max<size_t>(bytes, 4)); };
-            uint8_t* pages = static_cast<uint8_t*>(dev(size_t(sc.npages) * kPageSize));
-            auto* hdr = static_cast<uint32_t*>(dev(sizeof(uint32_t) * sc.npages));
-            auto* row_start = static_cast<uint32_t*>(dev(sizeof(uint32_t) * (sc.npages + 1)));
-            auto* chunk_base = static_cast<uint32_t*>(dev(sizeof(uint32_t) * (sc.npages + 1)));
-            auto* dense = static_cast<uint32_t*>(dev(sizeof(uint32_t) * sc.chunks));
-            auto* pob = static_cast<uint32_t*>(dev(sizeof(uint32_t) * sc.blocks));
-            snap_read(f.get(), pages, size_t(sc.npages) * kPageSize, b.p);
-            snap_read(f.get(), hdr, sizeof(uint32_t) * sc.npages, b.p);
-            snap_read(f.get(), row_start, sizeof(uint32_t) * (sc.npages + 1), b.p);
-            snap_read(f.get(), chunk_base, sizeof(uint32_t) * (sc.npages + 1), b.p);
-            snap_read(f.get(), dense, sizeof(uint32_t) * sc.chunks, b.p);
-            snap_read(f.get(), pob, sizeof(uint32_t) * sc.blocks, b.p);
-            dc.pages = pages;
-            dc.hdr = hdr;
-            dc.row_start = row_start;
-            dc.chunk_base = chunk_base;
-            dc.dense_base = dense;
-            dc.page_of_blk = pob;
-        }
-    } catch (const Fail& fl) {
-        return fail_to_status(ctx, fl);
-    } catch (const std::exception& e) {
-        return fail_to_status(ctx, Fail{BJ_ERR_INTERNAL, e.what()});
-    }
-    ctx->last_error.clear();
-    *out = r.release();
-    return BJ_OK;
-}
-
-BJ_API void bj_resident_free(bj_context* ctx, bj_resident* t) {
-    if (!t) return;
-    // Graphs that read this table are no longer valid.
-    if (ctx) drop_graphs_using(ctx, t);
-    delete t;
-}
-
-BJ_API uint64_t bj_result_num_rows(const bj_result* r) { return r ? r->rows : 0; }
-BJ_API uint64_t bj_result_num_columns(const bj_result* r) { return r ? r->types.size() : 0; }
-BJ_API int32_t bj_result_column_type(const bj_result* r, uint64_t c) {
-    return r && c < r->types.size() ? r->types[c] : -1;
-}
-BJ_API uint64_t bj_result_column_num_pages(const bj_result* r, uint64_t c) {
-    return r && c < r->npages.size() ? r->npages[c] : 0;
-}
-BJ_API int bj_result_wait(bj_result* r) {
-    if (!r) return BJ_ERR_INVALID;
-    if (!r->pending) return r->status;
-    bj_context* ctx = r->ctx;
-    const cudaError_t e = cudaEventSynchronize(r->done);
-    const uint32_t code = *reinterpret_cast<volatile uint32_t*>(ctx->async_err + r->slot);
-    {
-        std::lock_guard<std::mutex> lk(ctx->release_m);
-        ctx->free_slots.push_back(r->slot);
-        ctx->free_done.push_back(r->done);
-    }
-    r->done = nullptr;
-    r->pending = false;
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        ctx->last_error = std::string("CUDA error: ") + cudaGetErrorString(e);
-        r->status = BJ_ERR_CUDA;
-    } else if (code) {
-        ctx->last_error = std::string("device check failed: ") + dev_error_text(code);
-        r->status = BJ_ERR_INVALID;
-    }
-    return r->status;
-}
-
-// The data accessors complete an asynchronous result first.
-static bool result_ready(const bj_result* r) { return r && bj_result_wait(const_cast<bj_result*>(r)) == BJ_OK; }
-
-BJ_API const void* bj_result_page(const bj_result* r, uint64_t c, uint64_t p) {
-    if (!result_ready(r) || !r->host.p || c >= r->npages.size() || p >= r->npages[c]) return nullptr;
-    return r->host.p + (r->page_base[c] + p) * kPageSize;
-}
-BJ_API const void* bj_result_device_page(const bj_result* r, uint64_t c, uint64_t p) {
-    if (!result_ready(r) || !r->dev || c >= r->npages.size() || p >= r->npages[c]) return nullptr;
-    return r->dev + (r->page_base[c] + p) * kPageSize;
-}
-BJ_API int bj_result_copy_pages(const bj_result* r, uint64_t c, void* const* dst) {
-    if (!r || c >= r->npages.size() || (r->npages[c] && !dst)) return BJ_ERR_INVALID;
-    if (const int st = bj_result_wait(const_cast<bj_result*>(r))) return st;
-    for (uint64_t p = 0; p < r->npages[c]; p++) {
-        if (!dst[p]) return BJ_ERR_INVALID;
-        if (r->host.p) {
-            std::memcpy(dst[p], r->host.p + (r->page_base[c] + p) * kPageSize, kPageSize);
-        } else if (r->dev) {
-            if (cudaMemcpy(dst[p], r->dev + (r->page_base[c] + p) * kPageSize, kPageSize, cudaMemcpyDeviceToHost) !=
-                cudaSuccess)
-                return BJ_ERR_CUDA;
-        } else {
-            return BJ_ERR_INVALID;
-        }
-    }
-    return BJ_OK;
-}
-BJ_API int bj_result_stats(const bj_result* r, bj_stats* out) {
-    if (!r || !out) return BJ_ERR_INVALID;
-    if (const int st = bj_result_wait(const_cast<bj_result*>(r))) return st;
-    *out = r->stats;
-    return BJ_OK;
-}
-BJ_API void bj_result_free(bj_result* r) {
-    if (!r) return;
-    bj_result_wait(r);
-    if (r->ctx) {
-        if (r->dev) {
-            r->ctx->release_device(r->dev);
-            r->dev = nullptr;
-        }
-        if (r->host.p) r->ctx->give_pinned(r->host);
-        r->ctx->live_results--;
-    }
-    delete r;
-}
-
-} // extern "C"

@@ -270,6 +270,55 @@ int fail_to_status(bj_context* ctx, const Fail& f);
 // for BJ_ORDER_ROWS or a plan it does not estimate (estimator.cpp).
 void estimate_set_cards(bj_context* ctx, const bj_plan& plan, bj_resident* const* tables, std::vector<double>& cards);
 
+// ---- Page upload and indexing (engine.cpp) ----
+
+// One column to bring onto the device: its host pages and where they go.
+struct ColumnJob {
+    const bj_column* src;  // host pages
+    uint8_t* dpages;       // device-accessible address of the pages
+    uint64_t rows;         // rows the table claims
+    DevColumn* out;
+    bool in_place = false; // pages are read where they are (pinned host memory): no copy
+    const uint8_t* pinned = nullptr;  // pages back to back in pinned host memory: one DMA from here
+};
+
+// The host address of a column's pages when they lie back to back in pinned
+// host memory (and in `dev` the device address of their mapping, or nullptr);
+// nullptr for pageable or scattered pages.
+const uint8_t* pinned_base(const bj_column& hc, uint8_t*& dev);
+// Copies the jobs' host pages to their device addresses; returns the bytes.
+uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs);
+// Builds the page index of every job's column (pages already on the device).
+void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem);
+// used[c] = 1 for every column of table `table_id` that the plan reads.
+void collect_columns(const ExecPlan& ex, uint32_t table_id, uint64_t ncols, std::vector<uint8_t>& used);
+
+// ---- Execution (engine.cpp) ----
+
+constexpr size_t kPhaseMarks = 5;  // phase marks of a profiled call (bj_stats.phase_ms)
+void phase_stats(const std::vector<cudaEvent_t>& marks, bj_stats& st);
+// Shape class of a plan (log2 rows of its largest and second largest inputs,
+// number of inputs) and the tuned parameters the context holds for it.
+uint64_t shape_class(const ExecPlan& ex);
+TuneConfig tune_for(const bj_context* ctx, const ExecPlan& ex);
+// The drop-in path's guess of the probe the device sampling ranks first.
+int guess_first_probe(const ExecPlan& ex, const bj_plan& plan);
+// Shared tail of bj_execute / bj_execute_resident.
+int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* resident, int flags, bj_result** out,
+                   bool speculate = true);
+// Runs every pipeline of `ex` over device tables into `res` (enqueued on the
+// context's streams; used under stream capture). False: the result is empty.
+bool run_pipelines(bj_context* ctx, const ExecPlan& ex, const std::vector<const DevTable*>& tables, bj_result& res,
+                   int flags, uint64_t& pipelines);
+
+// ---- CUDA-graph replay (graphs.cpp) ----
+
+void destroy_graph(GraphEntry& g);
+int execute_resident_graph(bj_context* ctx, const bj_plan* plan, bj_resident* const* tables, int flags,
+                           bj_result** out);
+// Waits for ctx's work, then drops its graphs that read table t.
+void drop_graphs_using(bj_context* ctx, const bj_resident* t);
+
 } // namespace bj
 
 struct bj_context {
