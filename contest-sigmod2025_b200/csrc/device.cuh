@@ -177,45 +177,33 @@ BJ_HD uint64_t key_hash_any(uint64_t key, int32_t type) {
     return type == kInt32 ? key_hash(uint32_t(key)) : mix64(key) * 0x9E3779B97F4A7C15ull;
 }
 
-// Blocked bloom filter: one 64-bit block (two 32-bit words) per key with six
-// to eight bits set. The block is the top log2w - 1 bits of the high half hh
-// of the key hash (a filter of 2^log2w words, log2w at most 15, so at most
-// 128 KiB: it fits in shared memory). The bits are rotations of fixed two-bit
-// patterns: in the low word P1 rotated by hh mod 32 and P2 by (hh >> 5) mod
-// 32, in the high word P3 by (hh >> 10) mod 32 and P4 by (hh >> 15) mod 32;
-// each mask is made by one funnel shift per pattern, with no mask table. On
-// the snowflake's 1% dimension (50K keys in 128 KiB) this passes 77K of the
-// fact's 49.7M non-matching rows where one 32-bit word with two patterns
-// passed 614K. (The reference uses a 16-bit word per bucket and a 2048-entry
-// mask table, engine/infra/JoinFilter.hpp:9-23; a bloom only removes probes,
-// never results.)
+// Blocked bloom filter: one 32-bit word per key with up to four bits set.
+// The word is the top log2w bits (at most 15, so a filter is at most 128 KiB
+// and fits in shared memory) of the high half hh of the key hash. The bits
+// are two rotations of fixed two-bit patterns, P1 rotated by hh mod 32 and
+// P2 by (hh >> 5) mod 32: 1024 masks of three or four bits, each made by one
+// funnel shift per pattern, with no mask table. (The reference uses a 16-bit
+// word per bucket and a 2048-entry mask table, engine/infra/JoinFilter.hpp:
+// 9-23; a bloom only removes probes, never results.)
 constexpr uint32_t kBloomMaxLog2 = 15;
 constexpr uint32_t kBloomP1 = (1u << 0) | (1u << 11);
 constexpr uint32_t kBloomP2 = (1u << 0) | (1u << 19);
-constexpr uint32_t kBloomP3 = (1u << 0) | (1u << 7);
-constexpr uint32_t kBloomP4 = (1u << 0) | (1u << 23);
 BJ_HD uint32_t rotl32(uint32_t x, uint32_t s) {
     s &= 31;
     return s ? (x << s) | (x >> (32 - s)) : x;
 }
-// Block of a key (log2_words >= 5).
-BJ_HD uint32_t bloom_block_hi(uint32_t hh, uint32_t log2_words) { return hh >> (33 - log2_words); }
-BJ_HD uint64_t bloom_mask_hi(uint32_t hh) {
-    const uint32_t lo = rotl32(kBloomP1, hh) | rotl32(kBloomP2, hh >> 5);
-    const uint32_t hi = rotl32(kBloomP3, hh >> 10) | rotl32(kBloomP4, hh >> 15);
-    return uint64_t(lo) | (uint64_t(hi) << 32);
-}
+BJ_HD uint32_t bloom_bits_hi(uint32_t hh) { return rotl32(kBloomP1, hh) | rotl32(kBloomP2, hh >> 5); }
+BJ_HD uint32_t bloom_word_hi(uint32_t hh, uint32_t log2_words) { return log2_words ? hh >> (32 - log2_words) : 0u; }
 // High 32 bits of key_hash(key) (all the bloom filter uses), in two multiplies.
 #if defined(__CUDACC__)
 __device__ __forceinline__ uint32_t key_hash_hi(uint32_t key) {
     return __umulhi(key, 0x7F4A7C15u) + key * 0x9E3779B9u;
 }
-// The two words of bloom_mask_hi given hh and hh >> 5, hh >> 10, hh >> 15
-// (or any values with the same low five bits): a funnel shift of a pattern
-// with itself is a rotation by the shift amount mod 32.
-__device__ __forceinline__ uint2 bloom_mask_fast(uint32_t hh, uint32_t hh5, uint32_t hh10, uint32_t hh15) {
-    return make_uint2(__funnelshift_l(kBloomP1, kBloomP1, hh) | __funnelshift_l(kBloomP2, kBloomP2, hh5),
-                      __funnelshift_l(kBloomP3, kBloomP3, hh10) | __funnelshift_l(kBloomP4, kBloomP4, hh15));
+// bloom_bits_hi given hh and hh >> 5 (or any value with the same low five
+// bits): a funnel shift of a pattern with itself is a rotation by the shift
+// amount mod 32.
+__device__ __forceinline__ uint32_t bloom_bits_fast(uint32_t hh, uint32_t hh5) {
+    return __funnelshift_l(kBloomP1, kBloomP1, hh) | __funnelshift_l(kBloomP2, kBloomP2, hh5);
 }
 #else
 inline uint32_t key_hash_hi(uint32_t key) { return uint32_t(key_hash(key) >> 32); }
@@ -262,9 +250,8 @@ __device__ __forceinline__ uint64_t ht_key(const HTView& ht, uint32_t e) {
 
 __device__ __forceinline__ bool bloom_may_contain(const uint32_t* bloom, uint32_t log2w, uint32_t key) {
     const uint32_t hh = key_hash_hi(key);
-    const uint2 m = bloom_mask_fast(hh, hh >> 5, hh >> 10, hh >> 15);
-    const uint2 w = reinterpret_cast<const uint2*>(bloom)[bloom_block_hi(hh, log2w)];
-    return ((w.x & m.x) == m.x) && ((w.y & m.y) == m.y);
+    const uint32_t bits = bloom_bits_fast(hh, hh >> 5);
+    return (bloom[bloom_word_hi(hh, log2w)] & bits) == bits;
 }
 
 __device__ __forceinline__ void record_error(uint32_t* err, uint32_t code) {

@@ -1643,24 +1643,30 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
             return execute_common(ctx, plan, resident, flags, out, false);
         }
         // A join order whose intermediate result outgrew 32-bit item counts
-        // or the device memory: one rerun with another plan -- the rooted
-        // plan of the same cardinalities after a plan of the reference's
-        // space; else the row-count model after estimated cardinalities, join
-        // samples after the row-count model (resident tables only).
+        // or the device memory: a rerun with another plan, one change at a
+        // time -- the rooted plan of the same cardinalities after a plan of
+        // the reference's space; then (resident tables) the other
+        // cardinality source: the row-count model after estimates, join
+        // samples after the row-count model.
         const bool too_big = ctx->item_overflow || f.status == BJ_ERR_OOM;
-        if (too_big && ctx->retry_ordering < 0 && !ctx->retry_rooted && !ctx->cards_in && !ctx->space_in &&
-            (planned_reference || planned_with_cards || resident)) {
+        const bool to_rooted = planned_reference && !ctx->retry_rooted;
+        const bool to_cards = !to_rooted && ctx->retry_ordering < 0 && (planned_with_cards || resident);
+        if (too_big && !ctx->cards_in && !ctx->space_in && (to_rooted || to_cards)) {
             fail_to_status(ctx, f);
             ctx->last_error.clear();
             res.reset();
             if (ctx->tape && ctx->tape_mode == 1) ctx->tape->slots.clear();
-            if (planned_reference)
+            const int saved_ordering = ctx->retry_ordering;
+            const bool saved_rooted = ctx->retry_rooted;
+            if (to_rooted) {
                 ctx->retry_rooted = true;
-            else
+            } else {
                 ctx->retry_ordering = planned_with_cards ? BJ_ORDER_ROWS : BJ_ORDER_SAMPLING;
+                ctx->retry_rooted = false;
+            }
             const int rst = execute_common(ctx, plan, resident, flags, out, speculate);
-            ctx->retry_ordering = -1;
-            ctx->retry_rooted = false;
+            ctx->retry_ordering = saved_ordering;
+            ctx->retry_rooted = saved_rooted;
             return rst;
         }
         return fail_to_status(ctx, f);

@@ -175,9 +175,7 @@ __device__ __forceinline__ void scatter_tuple(const TupleBuf& t, const uint32_t*
     const uint32_t pos = first + atomicAdd(&cursor[b], 1u);
     if (bloom) {  // INT32 keys only (INT64 tables are built without a filter)
         const uint32_t hh = key_hash_hi(key);
-        const uint2 m = bloom_mask_fast(hh, hh >> 5, hh >> 10, hh >> 15);
-        atomicOr(reinterpret_cast<unsigned long long*>(bloom) + bloom_block_hi(hh, log2w),
-                 (unsigned long long)m.x | ((unsigned long long)m.y << 32));
+        atomicOr(&bloom[bloom_word_hi(hh, log2w)], bloom_bits_fast(hh, hh >> 5));
     }
     if (pos >= buckets[b + 1].x || pos >= ht.nentries) {
         record_error(err, kErrCapacity);

@@ -311,72 +311,16 @@ __device__ __forceinline__ void write_string_page(const uint64_t* __restrict__ h
     store_page(page, dst);
 }
 
-// Column and page of CTA g. Fixed-width pages come first, in order of their
-// first row (ties: column order), so the pages of every column covering one
-// range of rows run together and the items and gathered values they all read
-// are still in L2 for the second and third column; VARCHAR pages follow,
-// column by column.
-__device__ __forceinline__ void cta_page(const OutColumns& cols, uint32_t g, int& k, uint32_t& p) {
-    uint32_t fixed = 0;
-    for (int c = 0; c < cols.n; c++)
-        if (cols.c[c].type != kVarchar) fixed += cols.c[c].npages;
-    if (g < fixed) {
-        // f(r): fixed pages whose first row is at most r.
-        auto f = [&](uint64_t r) {
-            uint64_t n = 0;
-            for (int c = 0; c < cols.n; c++) {
-                const OutColumn& oc = cols.c[c];
-                if (oc.type == kVarchar || !oc.npages) continue;
-                n += min(uint64_t(oc.npages), r / oc.rpp + 1);
-            }
-            return n;
-        };
-        uint64_t lo = 0, hi = cols.nrows;  // the smallest r with f(r) > g lies in [lo, hi]
-        while (lo < hi) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (f(mid) > g)
-                hi = mid;
-            else
-                lo = mid + 1;
-        }
-        uint64_t tie = g - (lo ? f(lo - 1) : 0);  // index among the pages starting at row lo
-        for (int c = 0; c < cols.n; c++) {
-            const OutColumn& oc = cols.c[c];
-            if (oc.type == kVarchar || !oc.npages || lo % oc.rpp || lo / oc.rpp >= oc.npages) continue;
-            if (tie-- == 0) {
-                k = c;
-                p = uint32_t(lo / oc.rpp);
-                return;
-            }
-        }
-    }
-    uint32_t base = fixed;
-    for (int c = 0; c < cols.n; c++) {
-        const OutColumn& oc = cols.c[c];
-        if (oc.type != kVarchar) continue;
-        if (g < base + oc.npages) {
-            k = c;
-            p = g - base;
-            return;
-        }
-        base += oc.npages;
-    }
-    k = -1;  // not reached for g below the launch's page count
-}
-
-// Every page of the result, all columns, one CTA per page (cta_page's order).
+// Every page of the result, all columns: CTA g writes output page g.
 __global__ void __launch_bounds__(256) k_write_pages(OutColumns cols, uint8_t* __restrict__ out,
                                                      uint32_t* __restrict__ err) {
     __shared__ __align__(16) uint8_t page[kPageSize];
+    const uint32_t g = blockIdx.x;
     int k = 0;
-    uint32_t p = 0;
-    cta_page(cols, blockIdx.x, k, p);
-    if (k < 0) {
-        if (threadIdx.x == 0) record_error(err, kErrCapacity);
-        return;
-    }
+    while (k + 1 < cols.n && g >= cols.c[k].page_base + cols.c[k].npages) k++;
     const OutColumn& oc = cols.c[k];
-    uint8_t* dst = out + size_t(oc.page_base + p) * kPageSize;
+    const uint32_t p = g - oc.page_base;
+    uint8_t* dst = out + size_t(g) * kPageSize;
     if (oc.type != kVarchar) {
         if (oc.direct) {
             // Values straight from the items (every item is one output row).

@@ -12,9 +12,9 @@
 //    issued before any is used (every load stays inside the 8 KiB page;
 //    value v sits in 16-byte word (v+1)/4 because values start at byte 4);
 //  * a unit without NULLs gives each lane 32 values. The bloom test
-//    of a value is six multiplies, one 64-bit shared-memory load of the
-//    filter block, four funnel shifts and logic ops (bloom_mask_fast), spread
-//    over the multiply and integer pipes; the lane's survivors form a 32-bit mask, so
+//    of a value is four multiplies, one shared-memory load of the filter word,
+//    two funnel shifts and a logic op (bloom_bits_fast), spread over the
+//    multiply and integer pipes; the lane's survivors form a 32-bit mask, so
 //    a unit costs one vote and at most one warp prefix sum;
 //  * a page with NULLs is read in blocks of 1024 rows, 32 per lane: the null
 //    bitmap word of a lane's rows gives their validity, and the page index's
@@ -60,10 +60,8 @@ struct ScanArgs {
     // Multipliers for the bloom test, given at run time so that the shifts
     // they stand for (hh >> (32 - log2w), hh >> 5) run on the multiply pipe
     // as __umulhi instead of competing with the shifts on the integer pipe.
-    uint32_t word_mul;         // 1 << (ht.bloom_log2 - 1): the block index (hh >> (33 - log2w))
-    uint32_t field_mul;        // 1 << 27: hh >> 5
-    uint32_t field2_mul;       // 1 << 22: hh >> 10
-    uint32_t field3_mul;       // 1 << 17: hh >> 15
+    uint32_t word_mul;         // 1 << ht.bloom_log2
+    uint32_t field_mul;        // 1 << 27
     uint32_t* page_counts;     // mode 0 output: matches per work unit (scan_probe_units(npages))
     const uint32_t* page_off;  // mode 1 input: exclusive scan of page_counts (units + 1)
     uint32_t* cursor;          // mode 2 global item counter
@@ -308,10 +306,8 @@ __device__ __forceinline__ void push_step(const ScanArgs& a, WarpState& w, uint3
 
 __device__ __forceinline__ bool bloom_pass(const ScanArgs& a, const uint32_t* bloom, uint32_t key) {
     const uint32_t hh = key_hash_hi(key);
-    const uint2 m = bloom_mask_fast(hh, __umulhi(hh, a.field_mul), __umulhi(hh, a.field2_mul),
-                                    __umulhi(hh, a.field3_mul));
-    const uint2 w = reinterpret_cast<const uint2*>(bloom)[__umulhi(hh, a.word_mul)];
-    return ((~w.x & m.x) | (~w.y & m.y)) == 0;
+    const uint32_t m = bloom_bits_fast(hh, __umulhi(hh, a.field_mul));
+    return (~bloom[__umulhi(hh, a.word_mul)] & m) == 0;
 }
 
 // Values of one step of a page without NULLs that pass the bloom (or all of
@@ -560,7 +556,7 @@ int scan_probe(const DevColumn& key, const HTView& ht, int mode, bool bloom_smem
     }();
     const uint32_t prefetch = (key.flags & kColHostPages) ? 0u : ahead;
     ScanArgs a{key,      ht,       uint32_t(mode), bloom_bytes ? 1u : 0u, prefetch,
-               ht.bloom_log2 ? (1u << (ht.bloom_log2 - 1)) : 0u, 1u << 27, 1u << 22, 1u << 17,
+               ht.bloom_log2 ? (1u << ht.bloom_log2) : 0u, 1u << 27,
                page_counts, page_off, cursor, out_rows, out_ents, out_mult, capacity, err, row_base,
                nullptr, nullptr, nullptr, 0};
     launch_scan<false>(a, bloom_bytes, num_sms, st);
@@ -575,7 +571,7 @@ int scan_probe_split(const DevColumn& key, const HTView& ht, uint32_t* cursor, u
     size_t bloom_bytes = ht.bloom ? (sizeof(uint32_t) << ht.bloom_log2) : 0;
     if (bloom_bytes > kBloomSmemMax) bloom_bytes = 0;
     ScanArgs a{key,      ht,       2u, bloom_bytes ? 1u : 0u, 0u,
-               ht.bloom_log2 ? (1u << (ht.bloom_log2 - 1)) : 0u, 1u << 27, 1u << 22, 1u << 17,
+               ht.bloom_log2 ? (1u << ht.bloom_log2) : 0u, 1u << 27,
                nullptr, nullptr, cursor, out_rows, out_ents, out_mult, capacity, err, row_base,
                cand_key, cand_row, cand_count, cand_cap};
     launch_scan<true>(a, bloom_bytes, num_sms, st);
