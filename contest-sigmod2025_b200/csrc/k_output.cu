@@ -17,6 +17,8 @@
 // compare row multisets (tests/read_sql.cpp:1208-1213).
 #include "launch.h"
 
+#include <stdexcept>
+
 namespace bj {
 namespace {
 
@@ -64,9 +66,11 @@ __device__ __forceinline__ void store_page(const uint8_t* page, uint8_t* dst) {
 }
 
 // Page pidx of a fixed-width column, by one CTA of 256 threads; each thread
-// owns 8 consecutive rows. get(o, v) gives output row o's value (false: NULL).
-template <typename Get>
-__device__ __forceinline__ void write_fixed_page(Get&& get, uint64_t n, int32_t type, uint32_t rpp, uint32_t pidx,
+// owns 8 consecutive rows. gather(r0, lo, nr, v8) fills v8[k] with the value
+// of output row r0 + lo + k for the rows below nr and returns the mask of
+// those that are not NULL.
+template <typename Gather>
+__device__ __forceinline__ void write_fixed_page(Gather&& gather, uint64_t n, int32_t type, uint32_t rpp, uint32_t pidx,
                                                  uint8_t* page, uint8_t* __restrict__ dst) {
     __shared__ uint32_t total;
     const uint64_t r0 = uint64_t(pidx) * rpp;
@@ -75,16 +79,10 @@ __device__ __forceinline__ void write_fixed_page(Get&& get, uint64_t n, int32_t 
     const uint32_t t = threadIdx.x;
     const uint32_t lo = t * 8;
     uint64_t v8[8];
-    uint32_t bits = 0, cnt = 0;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        v8[k] = 0;
-        if (lo + k < nr && get(r0 + lo + k, v8[k])) {
-            bits |= 1u << k;
-            cnt++;
-        }
-    }
-    uint32_t dense = block_excl_u32(cnt, &total);
+    for (int k = 0; k < 8; k++) v8[k] = 0;
+    const uint32_t bits = lo < nr ? gather(r0, lo, nr, v8) : 0u;
+    uint32_t dense = block_excl_u32(__popc(bits), &total);
     uint8_t* data = page + (type == kInt32 ? 4 : 8);
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -103,6 +101,47 @@ __device__ __forceinline__ void write_fixed_page(Get&& get, uint64_t n, int32_t 
     }
     __syncthreads();
     store_page(page, dst);
+}
+
+// gather of a direct column (every item one output row) in two rounds of
+// independent loads: the items' rows (or matched entries) of all 8 rows,
+// then their 8 values -- not one row's two dependent loads after another's.
+__device__ __forceinline__ uint32_t gather_direct(const OutColumns& cols, const SlotSource& s, uint64_t r0, uint32_t lo,
+                                                  uint32_t nr, uint64_t (&v8)[8]) {
+    const Items& in = cols.items;
+    uint32_t a8[8];
+    uint32_t live = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        a8[k] = 0;
+        if (lo + k < nr) {
+            const uint32_t i = uint32_t(r0 + lo + k);
+            a8[k] = s.kind == 0 ? item_row(in, i) : in.ents[s.probe][i];
+            live |= 1u << k;
+        }
+    }
+    uint32_t bits = 0;
+    if (s.kind == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (((live >> k) & 1) && column_value(s.col, a8[k], v8[k])) bits |= 1u << k;
+        return bits;
+    }
+    const HTView& ht = cols.ps.ht[s.probe];
+    if (s.kind == 2) {
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if ((live >> k) & 1) v8[k] = ht_key(ht, a8[k]);
+        return live;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        if (!((live >> k) & 1)) continue;
+        const uint32_t e = a8[k];
+        v8[k] = ht.pay[size_t(e) * ht.width + s.slot];
+        if (!((ht.pnull[e] >> s.slot) & 1)) bits |= 1u << k;
+    }
+    return bits;
 }
 
 // Byte range of a short string (page p, value d) in its source page.
@@ -311,31 +350,71 @@ __device__ __forceinline__ void write_string_page(const uint64_t* __restrict__ h
     store_page(page, dst);
 }
 
-// Every page of the result, all columns: CTA g writes output page g.
+// Column and page of CTA g (OutColumns' order); false for a round's CTA whose
+// column has no page starting in that round. The fixed-width pages of every
+// column covering the same rows run together, so the items and gathered
+// values they all read are still in L2 for the second and later columns.
+// A page p of a column with rows per page q >= base starts in exactly one
+// round, r = floor(p q / base), and p = ceil(r base / q) recovers it.
+__device__ __forceinline__ bool cta_page(const OutColumns& cols, uint32_t g, int& k, uint32_t& p) {
+    const uint32_t fixed_ctas = cols.nfixed * cols.rounds;
+    if (g < fixed_ctas) {
+        const uint32_t r = g / cols.nfixed;
+        k = cols.fixed_col[g % cols.nfixed];
+        const OutColumn& oc = cols.c[k];
+        if (oc.rpp == cols.base_rpp) {
+            p = r;
+        } else {
+            const uint64_t first = uint64_t(r) * cols.base_rpp;
+            const uint64_t pp = (first + oc.rpp - 1) / oc.rpp;
+            if (pp * oc.rpp >= first + cols.base_rpp) return false;
+            p = uint32_t(pp);
+        }
+        return p < oc.npages;
+    }
+    uint32_t v = g - fixed_ctas;
+    for (k = 0; k < cols.n; k++) {
+        const OutColumn& oc = cols.c[k];
+        if (oc.type != kVarchar) continue;
+        if (v < oc.npages) {
+            p = v;
+            return true;
+        }
+        v -= oc.npages;
+    }
+    return false;
+}
+
+// Every page of the result, all columns, one CTA per page in cta_page's order.
 __global__ void __launch_bounds__(256) k_write_pages(OutColumns cols, uint8_t* __restrict__ out,
                                                      uint32_t* __restrict__ err) {
     __shared__ __align__(16) uint8_t page[kPageSize];
-    const uint32_t g = blockIdx.x;
     int k = 0;
-    while (k + 1 < cols.n && g >= cols.c[k].page_base + cols.c[k].npages) k++;
+    uint32_t p = 0;
+    if (!cta_page(cols, blockIdx.x, k, p)) return;
     const OutColumn& oc = cols.c[k];
-    const uint32_t p = g - oc.page_base;
-    uint8_t* dst = out + size_t(g) * kPageSize;
+    uint8_t* dst = out + size_t(oc.page_base + p) * kPageSize;
     if (oc.type != kVarchar) {
         if (oc.direct) {
             // Values straight from the items (every item is one output row).
             write_fixed_page(
-                [&](uint64_t o, uint64_t& v) {
-                    const uint32_t i = uint32_t(o);
-                    return slot_value(oc.slot, cols.items, i, item_row(cols.items, i), cols.ps, v);
+                [&](uint64_t r0, uint32_t lo, uint32_t nr, uint64_t(&v8)[8]) {
+                    return gather_direct(cols, oc.slot, r0, lo, nr, v8);
                 },
                 cols.nrows, oc.type, oc.rpp, p, page, dst);
         } else {
             write_fixed_page(
-                [&](uint64_t o, uint64_t& v) {
-                    if (!oc.valid[o]) return false;
-                    v = oc.vals[o];
-                    return true;
+                [&](uint64_t r0, uint32_t lo, uint32_t nr, uint64_t(&v8)[8]) {
+                    uint32_t bits = 0;
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        if (lo + k >= nr) continue;
+                        const uint64_t o = r0 + lo + k;
+                        if (!oc.valid[o]) continue;
+                        v8[k] = oc.vals[o];
+                        bits |= 1u << k;
+                    }
+                    return bits;
                 },
                 cols.nrows, oc.type, oc.rpp, p, page, dst);
         }
@@ -389,9 +468,27 @@ int string_pack(const uint32_t* lens, const uint8_t* valid, uint64_t n, int pass
     return 1;
 }
 
-int write_pages(const OutColumns& cols, uint32_t total_pages, uint8_t* out_pages, uint32_t* err, cudaStream_t st) {
-    if (!total_pages || cols.n <= 0) return 0;
-    k_write_pages<<<total_pages, 256, 0, st>>>(cols, out_pages, err);
+int write_pages(const OutColumns& cols_in, uint32_t total_pages, uint8_t* out_pages, uint32_t* err,
+                cudaStream_t st) {
+    if (!total_pages || cols_in.n <= 0) return 0;
+    OutColumns cols = cols_in;
+    cols.nfixed = 0;
+    cols.base_rpp = 0;
+    uint64_t varchar_pages = 0;
+    for (int c = 0; c < cols.n; c++) {
+        const OutColumn& oc = cols.c[c];
+        if (oc.type == kVarchar) {
+            varchar_pages += oc.npages;
+            continue;
+        }
+        if (!oc.npages || !oc.rpp) continue;
+        cols.fixed_col[cols.nfixed++] = c;
+        if (!cols.base_rpp || oc.rpp < cols.base_rpp) cols.base_rpp = oc.rpp;
+    }
+    cols.rounds = cols.nfixed ? uint32_t((cols.nrows + cols.base_rpp - 1) / cols.base_rpp) : 0u;
+    const uint64_t ctas = uint64_t(cols.nfixed) * cols.rounds + varchar_pages;
+    if (ctas > 0x7fffffffull) throw std::length_error("result pages beyond one launch");
+    k_write_pages<<<unsigned(ctas), 256, 0, st>>>(cols, out_pages, err);
     return 1;
 }
 

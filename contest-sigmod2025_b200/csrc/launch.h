@@ -539,6 +539,15 @@ struct OutColumns {
     uint64_t nrows;
     Items items;  // direct columns: item o is output row o
     ProbeSet ps;
+    // CTA order (set by write_pages): fixed-width pages first, in rounds of
+    // base_rpp rows (the smallest rows per page of those columns); round r
+    // holds one CTA per fixed-width column, which writes that column's page
+    // starting within the round's rows, if any. VARCHAR pages follow, column
+    // by column.
+    uint32_t nfixed;
+    uint32_t base_rpp;
+    uint32_t rounds;
+    int32_t fixed_col[kMaxOut];
 };
 int write_pages(const OutColumns& cols, uint32_t total_pages, uint8_t* out_pages, uint32_t* err, cudaStream_t st);
 
