@@ -280,7 +280,7 @@ void index_columns(bj_context* ctx, std::vector<ColumnJob>& jobs, Scratch& mem) 
             c.npages = pc.npages;
             c.nrows = uint32_t(rows);
             c.flags = uint32_t(flg) | (jobs[i].in_place ? kColHostPages : 0u);
-            c.rpp = (c.flags & kColRaggedPages) ? 0u : uint32_t(rows0);
+            set_rpp(c, (c.flags & kColRaggedPages) ? 0u : uint32_t(rows0));
             c.hdr = pc.hdr;
             c.row_start = pc.row_start;
             c.chunk_base = pc.chunk_base;
@@ -1516,7 +1516,7 @@ int execute_common(bj_context* ctx, const bj_plan* plan, bj_resident* const* res
                             dc.npages = uint32_t(hc.num_pages);
                             dc.nrows = uint32_t(t.num_rows);
                             dc.flags = kColHostPages;
-                            dc.rpp = h0 & 0xffff;
+                            set_rpp(dc, h0 & 0xffff);
                             spec.cols.emplace_back(&hc, h0);
                             continue;
                         }

@@ -366,7 +366,8 @@ __device__ __forceinline__ bool cta_page(const OutColumns& cols, uint32_t g, int
             p = r;
         } else {
             const uint64_t first = uint64_t(r) * cols.base_rpp;
-            const uint64_t pp = (first + oc.rpp - 1) / oc.rpp;
+            const uint64_t up = first + oc.rpp - 1;
+            const uint64_t pp = up >> 32 ? up / oc.rpp : uint64_t(uint32_t(up) / oc.rpp);
             if (pp * oc.rpp >= first + cols.base_rpp) return false;
             p = uint32_t(pp);
         }

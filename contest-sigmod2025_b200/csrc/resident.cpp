@@ -197,7 +197,7 @@ BJ_API int bj_resident_load(bj_context* ctx, const char* path, bj_resident** out
             dc.npages = sc.npages;
             dc.nrows = sc.nrows;
             dc.flags = sc.flags;
-            dc.rpp = sc.rpp;
+            set_rpp(dc, sc.rpp);
             if (!sc.npages) continue;
             auto dev = [&](size_t bytes) { return r->mem.alloc(std::max<size_t>(bytes, 4)); };
             uint8_t* pages = static_cast<uint8_t*>(dev(size_t(sc.npages) * kPageSize));
