@@ -801,11 +801,11 @@ class Executor {
                         }
                         continue;
                     }
-                    if (bloom && ctx_->scan_split && ctx_->tune.scan_split) {
-                        // Scan + filter, then a probe of the survivors (two
-                        // kernels; the scan carries no probe code). The
-                        // candidate count is the cursor's neighbour, zeroed
-                        // with it.
+                    if (ctx_->scan_split && ctx_->tune.scan_split) {
+                        // Scan + filter (the bloom, or NOT NULL alone), then a
+                        // probe of the survivors (two kernels; the scan carries
+                        // no probe code). The candidate count is the cursor's
+                        // neighbour, zeroed with it.
                         uint32_t* cand = alloc<uint32_t>(2 * size_t(cap));
                         launched(scan_probe_split(key, ht, cursor, out.rows, out.ents[0], out.mult, cap, cand,
                                                   cand + cap, cursor + 1, cap, ctx_->d_err, ctx_->num_sms, st_));

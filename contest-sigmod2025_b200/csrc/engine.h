@@ -224,7 +224,7 @@ struct ReadbackTape {
 // Build and scan parameters the autotuner chooses per plan shape class
 // (bj_context_autotune): the defaults are the engine's fixed choices.
 struct TuneConfig {
-    uint8_t scan_split = 0;    // scan-side probe with a bloom: filter + candidate probe kernels (1) or fused (0)
+    uint8_t scan_split = 0;    // scan-side probe: filter + candidate probe kernels (1) or fused (0)
     uint8_t bloom_bits = 16;   // bloom filter bits per key (capped at 128 KiB per filter)
     uint8_t bucket_extra = 0;  // buckets = 2^(bit_width(tuples) + extra): lower fill factors for extra > 0
     bool operator==(const TuneConfig& o) const {

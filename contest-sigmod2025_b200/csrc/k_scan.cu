@@ -575,7 +575,7 @@ int scan_probe_split(const DevColumn& key, const HTView& ht, uint32_t* cursor, u
                nullptr, nullptr, cursor, out_rows, out_ents, out_mult, capacity, err, row_base,
                cand_key, cand_row, cand_count, cand_cap};
     launch_scan<true>(a, bloom_bytes, num_sms, st);
-    k_probe_candidates<<<unsigned(num_sms) * 4, 256, 0, st>>>(a);
+    k_probe_candidates<<<unsigned(num_sms) * 8, 256, 0, st>>>(a);  // 64 warps per SM (32 registers)
     return 2;
 }
 
