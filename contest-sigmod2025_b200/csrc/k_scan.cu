@@ -138,7 +138,8 @@ __device__ __forceinline__ void probe_batch(const ScanArgs& a, WarpState& w, con
 #pragma unroll
     for (int i = 0; i < kPerLane; i++) {
         uint32_t c = k0[i] == key[i] ? 1u : 0u, first = c ? lo[i] : hi[i];
-        for (uint32_t e = lo[i] + 1; e < hi[i]; e++)
+        // Mode 2 (unique build keys): nothing after the first match.
+        for (uint32_t e = lo[i] + 1; e < hi[i] && !(a.mode == 2 && c); e++)
             if (a.ht.keys[e] == key[i]) {
                 first = c ? first : e;
                 c++;
