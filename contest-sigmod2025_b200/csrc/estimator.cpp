@@ -300,9 +300,16 @@ double sample_card(const Graph& G, const std::vector<double>& sel, uint32_t mask
 
 float log_feature(double x) { return float(std::log2(x + 1.0) / 32.0); }
 
-// Feature row of one sub-plan (layout in include/b200join.h).
-void subplan_features(bj_context* ctx, const Graph& G, uint32_t mask, float* f) {
-    std::fill(f, f + kF, 0.f);
+// A feature value as stored: FP32 for the public feature API and training,
+// BF16 bits for inference (the device rounds to BF16 anyway).
+inline void put_feature(float* f, size_t i, float v) { f[i] = v; }
+inline void put_feature(uint16_t* f, size_t i, float v) { f[i] = to_bf16(v); }
+
+// Feature row of one sub-plan (layout in include/b200join.h); T is float or
+// BF16 bits (uint16_t). Every entry not written here is zero.
+template <typename T>
+void subplan_features_t(bj_context* ctx, const Graph& G, uint32_t mask, T* f) {
+    std::fill(f, f + kF, T(0));
     if (__builtin_popcount(mask) > kMaxT) throw Fail{BJ_ERR_UNSUPPORTED, "sub-plan larger than the estimator's"};
     uint32_t root = __builtin_ctz(mask);
     for (uint32_t m = mask; m; m &= m - 1) {
@@ -316,25 +323,29 @@ void subplan_features(bj_context* ctx, const Graph& G, uint32_t mask, float* f) 
     for (size_t k = 0; k < order.size(); k++) slot[order[k]] = int(k);
     for (size_t k = 0; k < order.size(); k++) {
         const uint32_t x = order[k];
-        float* s = f + k * kSlotFeatures;
+        T* s = f + k * kSlotFeatures;
         const bj_resident* r = G.res[x];
         const double rows = double(G.g.inputs[x].rows);
         const double base = r->base_rows ? double(r->base_rows) : rows;
-        s[0] = 1.f;
-        s[1] = log_feature(rows);
-        s[2] = float(base > 0 ? std::min(1.0, rows / base) : 1.0);
+        put_feature(s, 0, 1.f);
+        put_feature(s, 1, log_feature(rows));
+        put_feature(s, 2, float(base > 0 ? std::min(1.0, rows / base) : 1.0));
         if (parent[x] < 0) continue;
         const uint32_t e = uint32_t(pedge[x]), p = uint32_t(parent[x]);
         const ColStats& own = column_stats_of(ctx, G.res[x], G.col(x, e));
         const ColStats& par = column_stats_of(ctx, G.res[p], G.col(p, e));
-        s[3] = log_feature(double(own.distinct));
-        s[4] = log_feature(double(par.distinct));
-        s[5 + slot[p]] = 1.f;
+        put_feature(s, 3, log_feature(double(own.distinct)));
+        put_feature(s, 4, log_feature(double(par.distinct)));
+        put_feature(s, 5 + size_t(slot[p]), 1.f);
         for (int b = 0; b < kHistBins; b++) {
-            s[5 + kMaxT + b] = log_feature(own.hist[b]);
-            s[5 + kMaxT + kHistBins + b] = log_feature(par.hist[b]);
+            put_feature(s, 5 + kMaxT + b, log_feature(own.hist[b]));
+            put_feature(s, 5 + kMaxT + kHistBins + b, log_feature(par.hist[b]));
         }
     }
+}
+
+void subplan_features(bj_context* ctx, const Graph& G, uint32_t mask, float* f) {
+    subplan_features_t(ctx, G, mask, f);
 }
 
 } // namespace
@@ -351,7 +362,12 @@ struct bj_estimator {
     int cap = 0;
     bj::DevBuf X, H1, H2, dH2, dH1, y, t, dy, loss, idx;
 
+    // Pinned BF16 feature rows for inference (kPredictChunk of them).
+    uint16_t* hx = nullptr;
+
     ~bj_estimator() {
+        if (stream) cudaStreamSynchronize(stream);
+        if (hx) cudaFreeHost(hx);
         if (stream) cudaStreamDestroy(stream);
     }
     float* W() { return static_cast<float*>(w.p); }
@@ -509,9 +525,47 @@ struct bj_estimator {
         EST_CK(cudaStreamSynchronize(stream));
     }
 
+    static constexpr int kPredictChunk = 4096;
+
+    // Predictions for n rows whose BF16 features fill(i0, rows, dst) writes
+    // into pinned staging (rows i0 .. i0 + rows - 1, row-major, kF each): one
+    // copy per chunk straight from there, no FP32 rows and no conversion pass.
+    template <typename Fill>
+    void predict_rows(uint64_t n, float* out, Fill&& fill) {
+        using namespace bj;
+        reserve(kPredictChunk);
+        if (!hx) {
+            void* p = nullptr;
+            EST_CK(cudaHostAlloc(&p, sizeof(uint16_t) * size_t(kPredictChunk) * kF, cudaHostAllocDefault));
+            hx = static_cast<uint16_t*>(p);
+        }
+        for (uint64_t i0 = 0; i0 < n; i0 += kPredictChunk) {
+            const int rows = int(std::min<uint64_t>(kPredictChunk, n - i0));
+            const int pad = (rows + 63) & ~63;
+            fill(i0, rows, hx);
+            std::memset(hx + size_t(rows) * kF, 0, sizeof(uint16_t) * size_t(pad - rows) * kF);
+            EST_CK(cudaMemcpyAsync(X.p, hx, sizeof(uint16_t) * size_t(pad) * kF, cudaMemcpyHostToDevice, stream));
+            run_head(pad, rows, out + i0);
+        }
+    }
+
+    // Forward and head over the pad rows in X; the first `rows` predictions to out.
+    void run_head(int pad, int rows, float* out) {
+        using namespace bj;
+        forward(pad);
+        MlpHeadArgs h{};
+        h.H2 = static_cast<uint16_t*>(H2.p);
+        h.w3 = WB() + kOffW3;
+        h.b3 = WB() + kOffB3;
+        h.y = static_cast<float*>(y.p);
+        mlp_head(h, rows, stream);
+        EST_CK(cudaMemcpyAsync(out, y.p, sizeof(float) * rows, cudaMemcpyDeviceToHost, stream));
+        EST_CK(cudaStreamSynchronize(stream));
+    }
+
     void predict(const float* f, uint64_t n, float* out) {
         using namespace bj;
-        constexpr int kChunk = 4096;
+        constexpr int kChunk = kPredictChunk;
         reserve(kChunk);
         for (uint64_t i0 = 0; i0 < n; i0 += kChunk) {
             const int rows = int(std::min<uint64_t>(kChunk, n - i0));
@@ -552,12 +606,13 @@ void estimate_set_cards(bj_context* ctx, const bj_plan& plan, bj_resident* const
         std::vector<uint32_t> multi;
         for (uint32_t m : masks)
             if (__builtin_popcount(m) > 1) multi.push_back(m);
-        std::vector<float> f(multi.size() * kF), y(multi.size());
-        for (size_t i = 0; i < multi.size(); i++) subplan_features(ctx, G, multi[i], f.data() + i * kF);
+        std::vector<float> y(multi.size());
         {
             std::lock_guard<std::mutex> g(ctx->estimator->m);
             cudaSetDevice(ctx->estimator->device);
-            ctx->estimator->predict(f.data(), multi.size(), y.data());
+            ctx->estimator->predict_rows(multi.size(), y.data(), [&](uint64_t i0, int rows, uint16_t* dst) {
+                for (int i = 0; i < rows; i++) subplan_features_t(ctx, G, multi[i0 + i], dst + size_t(i) * kF);
+            });
         }
         for (size_t i = 0; i < multi.size(); i++) {
             const double c = std::exp2(double(y[i])) - 1.0;
