@@ -1,5 +1,5 @@
 // Internal declarations shared by the engine's host sources (engine.cpp,
-// graphs.cpp, resident.cpp, api.cpp, estimator.cpp, server.cpp): error type,
+// graphs.cpp, resident.cpp, api.cpp, estimator.cpp): error type,
 // host thread pool, device arena and persistent allocations, the context,
 // resident tables and results. Not part of the public ABI (include/b200join.h).
 #pragma once
