@@ -148,25 +148,29 @@ struct Graph {
         parent.assign(n(), -1);
         pedge.assign(n(), -1);
         // Depth first, neighbours by descending rows (then index) when asked.
-        std::vector<uint32_t> stack{root};
+        // At most 32 inputs (masks are 32-bit), so fixed arrays hold the
+        // stack and a node's children: no allocation per sub-plan.
+        uint32_t stack[32];
+        std::pair<uint32_t, uint32_t> kids[32];
+        uint32_t top = 0;
+        stack[top++] = root;
         uint32_t seen = 1u << root;
-        while (!stack.empty()) {
-            uint32_t x = stack.back();
-            stack.pop_back();
+        while (top) {
+            const uint32_t x = stack[--top];
             order.push_back(x);
-            std::vector<std::pair<uint32_t, uint32_t>> kids;
+            uint32_t nk = 0;
             for (auto [y, e] : adj[x])
-                if ((mask >> y & 1) && !(seen >> y & 1)) kids.push_back({y, e});
+                if ((mask >> y & 1) && !(seen >> y & 1)) kids[nk++] = {y, e};
             if (larger_first)
-                std::sort(kids.begin(), kids.end(), [&](auto a, auto b) {
+                std::sort(kids, kids + nk, [&](auto a, auto b) {
                     const uint64_t ra = g.inputs[a.first].rows, rb = g.inputs[b.first].rows;
                     return ra != rb ? ra > rb : a.first < b.first;
                 });
-            for (size_t i = kids.size(); i-- > 0;) {
+            for (uint32_t i = nk; i-- > 0;) {
                 seen |= 1u << kids[i].first;
                 parent[kids[i].first] = int(x);
                 pedge[kids[i].first] = int(kids[i].second);
-                stack.push_back(kids[i].first);
+                stack[top++] = kids[i].first;
             }
         }
     }
@@ -316,10 +320,11 @@ void subplan_features_t(bj_context* ctx, const Graph& G, uint32_t mask, T* f) {
         const uint32_t i = __builtin_ctz(m);
         if (G.g.inputs[i].rows > G.g.inputs[root].rows) root = i;
     }
-    std::vector<uint32_t> order;
-    std::vector<int> parent, pedge;
+    // Reused across calls (one thread plans one query at a time).
+    thread_local std::vector<uint32_t> order;
+    thread_local std::vector<int> parent, pedge, slot;
     G.tree(mask, root, order, parent, pedge, true);
-    std::vector<int> slot(G.n(), -1);
+    slot.assign(G.n(), -1);
     for (size_t k = 0; k < order.size(); k++) slot[order[k]] = int(k);
     for (size_t k = 0; k < order.size(); k++) {
         const uint32_t x = order[k];
