@@ -163,21 +163,6 @@ __global__ void __launch_bounds__(256) k_aggregate(BuildArgs a) {
     if (i < a.tb.count) aggregate_tuple(emit_target(a), i);
 }
 
-// Stores of a built table's entries under an L2 evict-last policy: a scan
-// that streams a column larger than L2 past the table (normal priority) then
-// evicts its own lines first and leaves the entries for the probes after it.
-__device__ __forceinline__ uint64_t keep_policy() {
-    uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-__device__ __forceinline__ void st_keep(uint32_t* p, uint32_t v, uint64_t pol) {
-    asm volatile("st.global.L2::cache_hint.u32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol) : "memory");
-}
-__device__ __forceinline__ void st_keep(uint64_t* p, uint64_t v, uint64_t pol) {
-    asm volatile("st.global.L2::cache_hint.u64 [%0], %1, %2;" ::"l"(p), "l"(v), "l"(pol) : "memory");
-}
-
 // Places representative i in its bucket's range and sets its bloom bits.
 __device__ __forceinline__ void scatter_tuple(const TupleBuf& t, const uint32_t* __restrict__ is_rep, uint32_t shift,
                                               uint2* __restrict__ buckets, uint32_t* __restrict__ cursor,
@@ -196,15 +181,14 @@ __device__ __forceinline__ void scatter_tuple(const TupleBuf& t, const uint32_t*
         record_error(err, kErrCapacity);
         return;
     }
-    const uint64_t pol = keep_policy();
-    if (pos == first) st_keep(&buckets[b].y, key, pol);  // the bucket's first entry
-    st_keep(const_cast<uint32_t*>(ht.keys) + pos, key, pol);
-    if (t.keys_hi) st_keep(const_cast<uint32_t*>(ht.keys_hi) + pos, t.keys_hi[i], pol);
-    st_keep(const_cast<uint64_t*>(ht.mult) + pos, t.mult[i], pol);
-    st_keep(const_cast<uint32_t*>(ht.pnull) + pos, t.pnull[i], pol);
+    if (pos == first) buckets[b].y = key;  // the bucket's first entry
+    const_cast<uint32_t*>(ht.keys)[pos] = key;
+    if (t.keys_hi) const_cast<uint32_t*>(ht.keys_hi)[pos] = t.keys_hi[i];
+    const_cast<uint64_t*>(ht.mult)[pos] = t.mult[i];
+    const_cast<uint32_t*>(ht.pnull)[pos] = t.pnull[i];
     uint64_t* dst = const_cast<uint64_t*>(ht.pay) + size_t(pos) * t.width;
     const uint64_t* src = t.pay + size_t(i) * t.width;
-    for (uint32_t j = 0; j < t.width; j++) st_keep(dst + j, src[j], pol);
+    for (uint32_t j = 0; j < t.width; j++) dst[j] = src[j];
 }
 
 __global__ void k_scatter_bloom(TupleBuf t, const uint32_t* __restrict__ is_rep, uint32_t shift,

@@ -82,17 +82,14 @@ struct ScanArgs {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 
-// L2 policy for the scanned pages. Without a bloom filter every row probes
-// the table, and the pages are evicted first so that the stream of a column
-// larger than L2 does not push out the table's buckets (join2: 157 -> 145 us);
-// with one, the survivors' keys are read again from the pages just loaded, so
-// the pages keep the normal priority (evict-first there: 63 -> 67 us).
-__device__ __forceinline__ uint64_t stream_policy(bool probe_every_row) {
+// L2 policy for the scanned pages: normal priority, given explicitly (the
+// loads with a cache-policy operand came out at 61 registers instead of 64,
+// and ran 1-2% faster in same-box A/B runs on the snowflake). Evict-first
+// was measured too: slower with a bloom filter (the survivors' keys are read
+// again from the pages just loaded) and no better without one (join2).
+__device__ __forceinline__ uint64_t stream_policy() {
     uint64_t pol;
-    if (probe_every_row)
-        asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    else
-        asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol));
+    asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol));
     return pol;
 }
 // 16-byte read-only load under an L2 policy.
@@ -447,7 +444,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_scan_probe(ScanArgs a) {
     // warps better than whole pages: 10.6 units per warp against 5.3 pages
     // on the 50M-row fact). A unit's loads are all issued before any is
     // used, and every load stays inside its 8 KiB page.
-    const uint64_t pol = stream_policy(!use_bloom);
+    const uint64_t pol = stream_policy();
     auto load_unit = [&](uint32_t u, uint4 (&q)[kStepWords], uint32_t& hdr, uint32_t& row0) {
         const uint4* pw = reinterpret_cast<const uint4*>(a.key.pages + size_t(u / kUnitsPerPage) * kPageSize);
 #pragma unroll
