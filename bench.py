@@ -371,6 +371,7 @@ def batch_bench(args, local):
            "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))], "gpu_launches": launches, "rows": rows,
            "alone": {"p50_ms": alone[len(alone) // 2], "p99_ms": alone[min(len(alone) - 1, int(0.99 * len(alone)))],
                      "queries": len(alone)}}
+    out["concurrent"] = batch_concurrent(pkg, w, queries, args, local, rows // max(args.steps, 1))
     if args.cpu_steps and os.path.exists(REF_RUNNER):
         p = subprocess.run([REF_RUNNER, "batch", args.workload, str(args.seed), str(args.scale), "1"],
                            capture_output=True, text=True, timeout=1800)
@@ -378,6 +379,33 @@ def batch_bench(args, local):
         out["cpu_baseline"] = json.loads(line[-1]) if p.returncode == 0 and line else {"error": p.stderr[-300:]}
     print(json.dumps(out))
     return 0
+
+
+def batch_concurrent(pkg, w, queries, args, local, rows_per_pass):
+    """The same batch through a bj_server: --serve-workers worker contexts
+    over one resident copy of the tables, graph replay, join orders from join
+    samples, the batch submitted --steps times in a closed loop of 2 x workers
+    outstanding (after one warm-up pass per worker). Queries/s to the last
+    completion, submit-to-completion p50/p99, and the summed result rows,
+    which must equal --steps one-at-a-time passes."""
+    import numpy as np
+
+    workers = args.serve_workers
+    inputs = w.plan_ptr().contents
+    with pkg.Server(local, workers=workers, scratch_cap_bytes=120 << 30) as srv:
+        tabs = [srv.upload(inputs.inputs[t]) for t in range(inputs.num_inputs)]
+        try:
+            srv.set_ordering(pkg.ORDER_SAMPLING)
+            srv.set_graphs(True)
+            ids = np.arange(len(queries), dtype=np.uint32)
+            srv.run_load(queries, tabs, np.tile(ids, workers + 1), 0.0, workers)
+            lat, el, rows = srv.run_load(queries, tabs, np.tile(ids, max(args.steps, 1)), 0.0, 2 * workers)
+        finally:
+            for x in tabs:
+                x.free()
+    return {"workers": workers, "queries": len(lat), "value": len(lat) / el, "unit": "queries/s",
+            "p50_ms": float(np.median(lat)), "p99_ms": float(np.quantile(lat, 0.99)),
+            "rows_identical": int(rows) == rows_per_pass * max(args.steps, 1)}
 
 
 def train_schema_estimator(pkg, w, local, queries, per_query, epochs, seed=1):
