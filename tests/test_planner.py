@@ -218,3 +218,70 @@ def test_reference_space_cheaper_with_payload_keys(pkg):
     assert "(payload of pipeline 0)" in pipes[1], text
     assert pipes[2].startswith("pipeline 2: scan input 0") and "probe pipeline 1" in pipes[2], text
     assert pipes[2].endswith("-> result"), text
+
+
+def _reference_space_exhaustive(card, edges):
+    """Cheapest plan of the reference's space by listing every plan: a plan of
+    a set of inputs is one input (its pipeline probes nothing) or probe(R,
+    hash(L)) for two connected halves L and R of the set split at one edge,
+    R's top pipeline taking one probe more, at most two (QueryGraph.hpp:40);
+    it costs its halves' costs + the set's cardinality + 10 x L's, a set's
+    cardinality being its largest input's rows."""
+    n = len(card)
+    nbr = {i: set() for i in range(n)}
+    for a, b in edges:
+        nbr[a].add(b)
+        nbr[b].add(a)
+
+    def side(S, v, away):
+        seen, stack = {v}, [v]
+        while stack:
+            x = stack.pop()
+            for y in nbr[x]:
+                if y in S and y != away and y not in seen:
+                    seen.add(y)
+                    stack.append(y)
+        return frozenset(seen)
+
+    memo = {}
+
+    def plans(S):  # every (cost, probes of the top pipeline) of plans of S
+        if S in memo:
+            return memo[S]
+        if len(S) == 1:
+            out = [(card[next(iter(S))], 0)]
+        else:
+            out = []
+            cs = max(card[i] for i in S)
+            for a, b in edges:
+                if a not in S or b not in S:
+                    continue
+                A, B = side(S, b, a), side(S, a, b)
+                for L, R in ((A, B), (B, A)):
+                    cl = max(card[i] for i in L)
+                    for lc, _ in plans(L):
+                        for rc, rp in plans(R):
+                            if rp < 2:
+                                out.append((lc + rc + cs + 10 * cl, rp + 1))
+        memo[S] = out
+        return out
+
+    return min(c for c, _ in plans(frozenset(range(n))))
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_reference_space_cost_matches_exhaustive(pkg, seed):
+    """The reference space's dynamic program (reference_dp_cost) against the
+    listing of every plan of that space, on random join trees of 2-5 inputs
+    under the row-count model."""
+    rng = random.Random(700 + seed)
+    n = rng.randint(2, 5)
+    rows = [rng.choice([5, 20, 60, 200]) for _ in range(n)]
+    edges = [(rng.randrange(c), c) for c in range(1, n)]
+    plan = _tree_plan(pkg, rows, edges)
+    order = [edges[0][0]] + [c for _, c in edges]  # scan k is input order[k]
+    pos = {t: k for k, t in enumerate(order)}
+    card = [rows[order[k]] for k in range(n)]
+    sedges = [(pos[a], pos[b]) for a, b in edges]
+    _, ref = _costs(pkg, plan)
+    assert ref == pytest.approx(_reference_space_exhaustive(card, sedges))
