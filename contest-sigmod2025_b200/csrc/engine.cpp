@@ -16,7 +16,9 @@
 #include "engine.h"
 
 #include <cuda_runtime.h>
+#if defined(__x86_64__)
 #include <immintrin.h>
+#endif
 
 #include <algorithm>
 #include <array>
@@ -164,6 +166,9 @@ bool read_in_place(const bj_column& hc, const uint8_t* dev) {
 // that follows reads them from memory instead of snooping them out of cache.
 // `dst` is 16-byte aligned (page-aligned staging); `src` needs no alignment.
 inline void copy_page_streaming(uint8_t* dst, const void* src) {
+#if !defined(__x86_64__)
+    std::memcpy(dst, src, kPageSize);  // other hosts: a plain copy
+#else
     const __m128i* s = static_cast<const __m128i*>(src);
     __m128i* d = reinterpret_cast<__m128i*>(dst);
     for (size_t k = 0; k < kPageSize / 16; k += 4) {
@@ -174,6 +179,17 @@ inline void copy_page_streaming(uint8_t* dst, const void* src) {
         _mm_stream_si128(d + k + 2, c);
         _mm_stream_si128(d + k + 3, e);
     }
+#endif
+}
+
+// Orders this thread's streaming stores before the host hands the staging to
+// the copy engine.
+inline void staging_fence() {
+#if defined(__x86_64__)
+    _mm_sfence();
+#else
+    std::atomic_thread_fence(std::memory_order_release);
+#endif
 }
 
 // Copies host pages into `dst` on the device: pages are gathered into pinned
@@ -235,7 +251,7 @@ uint64_t upload_pages(bj_context* ctx, const std::vector<ColumnJob>& jobs) {
         ctx->pool->parallel_for((c1 - c0 + per - 1) / per, [&](size_t t) {
             for (size_t i = c0 + t * per; i < std::min(c1, c0 + (t + 1) * per); i++)
                 copy_page_streaming(stage + i * kPageSize, all[i].page);
-            _mm_sfence();  // this thread's streaming stores are in memory before the DMA is issued
+            staging_fence();  // this thread's streaming stores are in memory before the DMA is issued
         });
         // Consecutive pages of one column (one device allocation) become one
         // copy; a copy never spans two allocations.
