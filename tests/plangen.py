@@ -37,9 +37,27 @@ def _key64(rng, dom, null_p):
     return (rng.choice([0, 1, 7, -1, -5]) << 32) | rng.randrange(dom)
 
 
-def random_case(seed, max_tables=5, max_rows=3000, min_tables=1, max_width=None, int64_keys=False):
+# INT32 keys at the edges of the type and around zero (signed_keys).
+_EDGE32 = [-1, -2, -(1 << 31), (1 << 31) - 1, (1 << 31) - 2, 0, 1]
+
+
+def _key32_signed(rng, dom, null_p, edge_p):
+    """An INT32 key from a small domain that straddles zero, or (with
+    probability edge_p) one of the type's edge values (-1 is 0xFFFFFFFF, the
+    all-ones pattern)."""
+    if rng.random() < null_p:
+        return None
+    if rng.random() < edge_p:
+        return rng.choice(_EDGE32)
+    return rng.randrange(-(dom // 2), dom - dom // 2)  # dom values around zero
+
+
+def random_case(seed, max_tables=5, max_rows=3000, min_tables=1, max_width=None, int64_keys=False,
+                signed_keys=False):
     """max_width caps the attributes a join node outputs (the reference only
-    instantiates pipelines carrying a few attributes, engine/genpipelines.py:15-49)."""
+    instantiates pipelines carrying a few attributes, engine/genpipelines.py:15-49).
+    signed_keys draws the INT32 join keys from a domain around zero plus the
+    type's edge values."""
     """Returns (tables, nodes, root) in the form tests/golden/make_golden.py uses."""
     rng = random.Random(seed)
     ntables = rng.randint(min_tables, max_tables)
@@ -54,6 +72,13 @@ def random_case(seed, max_tables=5, max_rows=3000, min_tables=1, max_width=None,
         null_p = rng.choice([0.0, 0.0, 0.05, 0.3])
         long_p = 0.002 if rng.random() < 0.3 else 0.0
         rows = [[_value(rng, ty, dom, null_p, long_p) for ty in types] for _ in range(nrows)]
+        if signed_keys:
+            # About 20 edge values per table whatever its size: their
+            # repeats multiply across a join chain.
+            edge_p = min(0.2, 20.0 / max(nrows, 1))
+            for r in rows:
+                for k in range(nkeys):
+                    r[k] = _key32_signed(rng, dom, null_p, edge_p)
         if int64_keys:
             types.insert(1, INT64)
             for r in rows:

@@ -49,6 +49,38 @@ def test_random_plans_int64_keys(pkg, ctx, oracle, seed):
     check_against_oracle(pkg, ctx, oracle, cp, f"int64 seed {9000 + seed}")
 
 
+@pytest.mark.parametrize("seed", range(16))
+def test_random_plans_signed_int32_keys(pkg, ctx, oracle, seed):
+    """INT32 join keys around zero and at the type's edges (-1 = 0xFFFFFFFF,
+    INT32_MIN, INT32_MAX): hashing, bloom bits, bucket first keys and the
+    key statistics take every bit pattern."""
+    tables, nodes, root = plangen.random_case(7000 + seed, max_rows=3000 if seed % 4 else 30000,
+                                              signed_keys=True)
+    cp = pkg.CPlan(plangen.to_plan(pkg, tables, nodes, root))
+    check_against_oracle(pkg, ctx, oracle, cp, f"signed seed {7000 + seed}")
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_signed_int32_keys_resident_with_join_samples(pkg, oracle, seed):
+    """The same keys over resident tables with join orders from join samples:
+    the key statistics' key -> count maps (empty slots marked by the all-ones
+    64-bit pattern) take the keys -1, INT32_MIN and INT32_MAX."""
+    tables, nodes, root = plangen.random_case(7100 + seed, min_tables=2, max_rows=3000, signed_keys=True)
+    cp = pkg.CPlan(plangen.to_plan(pkg, tables, nodes, root))
+    plan = cp.struct
+    with pkg.Context(0) as c:
+        c.set_ordering(pkg.ORDER_SAMPLING)
+        res = [c.upload(plan.inputs[i]) for i in range(plan.num_inputs)]
+        try:
+            with c.execute_resident(cp, res) as r:
+                got, keep = r.table_struct()
+                want = oracle.execute(cp.ref())
+                oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(), f"resident signed {7100 + seed}")
+        finally:
+            for x in res:
+                x.free()
+
+
 @pytest.mark.parametrize("seed", range(4))
 def test_random_plans_int64_keys_wide_tables(pkg, ctx, oracle, seed):
     tables, nodes, root = plangen.random_case(9500 + seed, max_tables=3, max_rows=40000, int64_keys=True)
