@@ -69,6 +69,10 @@ BJ_API int bj_plan_explain(const bj_plan* plan, char* buf, uint64_t cap, uint64_
                                       pp.probes[size_t(pp.build_key_probe)].child);
                         out += line;
                     }
+                    if (pp.restrict_by >= 0) {
+                        std::snprintf(line, sizeof line, ", rows restricted by pipeline %d's filter", pp.restrict_by);
+                        out += line;
+                    }
                 } else {
                     out += " -> result";
                 }
@@ -143,6 +147,7 @@ BJ_API int bj_context_create(int device, bj_context** out) {
     if (const char* sp = std::getenv("B200JOIN_SCAN_SPLIT")) ctx->scan_split = std::atoi(sp) != 0;
     if (const char* ss = std::getenv("B200JOIN_STREAM_SCAN")) ctx->stream_scans = std::atoi(ss) != 0;
     if (const char* lb = std::getenv("B200JOIN_LEAF_BATCH")) ctx->leaf_batch = std::atoi(lb) != 0;
+    if (const char* sw = std::getenv("B200JOIN_SIDEWAYS")) ctx->sideways = std::atoi(sw) != 0;
     unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     ctx->pool = std::make_unique<ThreadPool>(std::min(hw, 16u) - 1);
     *out = ctx.release();

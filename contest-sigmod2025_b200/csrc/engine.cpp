@@ -484,6 +484,9 @@ class Executor {
         int next_side = 0;
         // Leaf builds: batched, each pass one launch over all of them, on the
         // main stream (B200JOIN_LEAF_BATCH=0: one pipeline per side stream).
+        // Leaves restricted by another leaf's filter (PipelinePlan::
+        // restrict_by; B200JOIN_SIDEWAYS=0: none) form a second batch, after
+        // the first has built their providers.
         std::vector<uint8_t> batched(np, 0);
         if (ctx_->leaf_batch) {
             std::vector<size_t> leaves;
@@ -491,7 +494,19 @@ class Executor {
                 if (ex_.pipelines[p].probes.empty() && ex_.pipelines[p].slots.size() <= size_t(kMaxLeafSlots))
                     leaves.push_back(p);
             if (!leaves.empty()) {
-                build_leaf_batch(leaves);
+                std::vector<int32_t> by(np, -1);
+                std::vector<size_t> first, second;
+                if (ctx_->sideways) {
+                    std::vector<uint8_t> leaf(np, 0);
+                    for (size_t p : leaves) leaf[p] = 1;
+                    for (size_t p : leaves) {
+                        const int32_t l = ex_.pipelines[p].restrict_by;
+                        if (l >= 0 && leaf[size_t(l)] && ex_.pipelines[size_t(l)].restrict_by < 0) by[p] = l;
+                    }
+                }
+                for (size_t p : leaves) (by[p] >= 0 ? second : first).push_back(p);
+                build_leaf_batch(first, by);
+                if (!second.empty()) build_leaf_batch(second, by);
                 trace("leaf builds enqueued");
                 for (size_t p : leaves) {
                     cudaEvent_t done = ctx_->pipe_event(p);
@@ -1093,10 +1108,13 @@ class Executor {
         return true;
     }
 
+    static_assert(size_t(kMaxLeafSlots) == kLeafBatchMaxSlots, "the planner marks restrictions on batched leaves");
     // The builds of the pipelines in `leaves` (inputs that probe nothing),
     // kMaxLeafBuilds at a time, each pass one launch over all of them on the
     // current stream, with one memset for all their zero-start buffers.
-    void build_leaf_batch(const std::vector<size_t>& leaves) {
+    // by[p] >= 0: leaf p's rows are restricted by the bloom filter of the
+    // table of pipeline by[p] (built earlier on this stream), when it has one.
+    void build_leaf_batch(const std::vector<size_t>& leaves, const std::vector<int32_t>& by) {
         for (size_t i0 = 0; i0 < leaves.size(); i0 += kMaxLeafBuilds) {
             const size_t i1 = std::min(leaves.size(), i0 + kMaxLeafBuilds);
             std::vector<PreparedBuild> pbs;
@@ -1144,6 +1162,11 @@ class Executor {
                 L.log2w = pb.wlog2;
                 L.dflags = pb.dflags;
                 L.ht = pb.ht;
+                const int32_t r = by[leaves[i0 + k]];
+                if (r >= 0 && hts_[size_t(r)].view.bloom) {
+                    L.rbloom = hts_[size_t(r)].view.bloom;
+                    L.rlog2w = hts_[size_t(r)].view.bloom_log2;
+                }
                 batch.tuple_start[batch.n + 1] = batch.tuple_start[batch.n] + pb.ba.tb.count;
                 batch.block_start[batch.n + 1] = batch.block_start[batch.n] + (pb.ba.tb.count + 255) / 256;
                 batch.tile_start[batch.n + 1] =

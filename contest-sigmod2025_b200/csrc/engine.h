@@ -350,6 +350,7 @@ struct bj_context {
     cudaStream_t copy = nullptr;           // host-to-HBM copies of a streamed scan
     bool stream_scans = true;              // scans of host pages copy them through HBM windows
     bool leaf_batch = true;                // leaf builds batched (one launch per pass)
+    bool sideways = true;                  // batched leaf builds restricted by a smaller one's filter
     bool scan_split = true;                // allow the split scan where the tuned parameters ask for it
     // Autotuned parameters per plan shape class (key: shape_class), the
     // configuration of the running call, and an override while tuning.

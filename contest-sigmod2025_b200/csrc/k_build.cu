@@ -289,8 +289,10 @@ __global__ void __launch_bounds__(256) k_leaf_emit(LeafBatch B) {
     if (!leaf_tuple(B, b, i)) return;
     const LeafBuild& L = B.l[b];
     // A leaf's item i is row i, multiplicity 1; its slots are its own columns.
+    // A row whose key the restricting filter cannot hold joins nothing: it
+    // is written with multiplicity 0, like a NULL key.
     uint64_t kv = 0;
-    const bool key_ok = col_get(L.key, i, kv);
+    const bool key_ok = col_get(L.key, i, kv) && (!L.rbloom || bloom_may_contain(L.rbloom, L.rlog2w, uint32_t(kv)));
     emit_tuple_to(leaf_target(B, L), i, kv, key_ok ? 1ull : 0ull, L.nslots,
                   [&](int j, uint64_t& v) { return column_value(L.cols[j], i, v); });
 }

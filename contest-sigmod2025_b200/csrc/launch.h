@@ -321,6 +321,11 @@ struct LeafBuild {
     uint32_t log2w;
     uint32_t* dflags;   // two zero words: table flags (pass 4)
     HTView ht;          // the table's arrays to fill
+    // Sideways restriction: the bloom filter (1 << rlog2w words) of another
+    // table built on the same key class; a row whose key it cannot hold is
+    // not inserted. Null: none.
+    const uint32_t* rbloom;
+    uint32_t rlog2w;
 };
 struct LeafBatch {
     LeafBuild l[kMaxLeafBuilds];

@@ -683,7 +683,39 @@ int make_exec_plan(const bj_plan& plan, ExecPlan& ex, std::string& err, bool ref
             }
         }
     }
+    sideways_restrictions(ex);
     return BJ_OK;
+}
+
+void sideways_restrictions(ExecPlan& ex) {
+    const size_t np = ex.pipelines.size();
+    // A build of an input that probes nothing, keyed on one of its INT32
+    // columns, batched with the other such builds.
+    auto plain_leaf = [&](const PipelinePlan& pp) {
+        return pp.probes.empty() && pp.build_key >= 0 && pp.build_key_probe < 0 &&
+               pp.slots.size() <= kLeafBatchMaxSlots && ex.attrs[size_t(pp.build_key)].type == BJ_INT32;
+    };
+    for (size_t m = 0; m + 1 < np; m++) {
+        PipelinePlan& pm = ex.pipelines[m];
+        pm.restrict_by = -1;
+        if (!plain_leaf(pm)) continue;
+        const uint64_t rows_m = ex.inputs[pm.input].rows;
+        if (rows_m < kSidewaysMinRows) continue;
+        const uint32_t eq = ex.attrs[size_t(pm.build_key)].eq;
+        // The smallest qualifying provider (never itself restricted: any
+        // input that could restrict it would qualify here and be smaller).
+        uint64_t best_rows = 0;
+        for (size_t l = 0; l + 1 < np; l++) {
+            const PipelinePlan& pl = ex.pipelines[l];
+            if (l == m || !plain_leaf(pl) || ex.attrs[size_t(pl.build_key)].eq != eq) continue;
+            const uint64_t rows_l = ex.inputs[pl.input].rows;
+            if (rows_l > kSidewaysMaxFilterRows || rows_l * 4 > rows_m) continue;
+            if (pm.restrict_by < 0 || rows_l < best_rows || (rows_l == best_rows && int32_t(l) < pm.restrict_by)) {
+                pm.restrict_by = int32_t(l);
+                best_rows = rows_l;
+            }
+        }
+    }
 }
 
 } // namespace bj

@@ -66,6 +66,11 @@ struct PipelinePlan {
     };
     std::vector<Probe> probes;
     std::vector<SlotPlan> slots;  // payload (build) or output sources (root)
+    // A sideways restriction (sideways_restrictions): for a build that
+    // probes nothing, the pipeline of a much smaller such build keyed on the
+    // same equivalence class, whose bloom filter drops this build's rows
+    // with keys it cannot hold; -1: none.
+    int32_t restrict_by = -1;
 };
 
 struct ExecPlan {
@@ -85,6 +90,22 @@ struct ExecPlan {
     // may be keyed on an earlier probe's payload) rather than a rooted tree.
     bool reference_space = false;
 };
+
+// Sideways restrictions between the builds of inputs that probe nothing
+// (the reference installs a finished table's Join restriction on every later
+// scan of another input of its key class, engine/query/QueryPlan.cpp:
+// 620-624, :670-676; buildScan applies it, :113-126). A row of such a build
+// whose key a table of the same class cannot hold joins no result row, so
+// the build of a large input is restricted by the filter of a smaller input
+// built on that class. Marked only where it can pay: the restricted input
+// has at least kSidewaysMinRows rows and at least four times the provider's,
+// and the provider is small enough to carry a bloom filter
+// (kSidewaysMaxFilterRows); both keys INT32 and both builds batched
+// (kLeafBatchMaxSlots payload columns at most).
+constexpr uint64_t kSidewaysMinRows = uint64_t(1) << 18;
+constexpr uint64_t kSidewaysMaxFilterRows = uint64_t(1) << 17;
+constexpr size_t kLeafBatchMaxSlots = 4;
+void sideways_restrictions(ExecPlan& ex);
 
 // Which plan space make_exec_plan runs: the cheaper of the two (auto), or
 // one of them (for tests and measurements; B200JOIN_PLAN_SPACE=rooted /

@@ -285,3 +285,66 @@ def test_reference_space_cost_matches_exhaustive(pkg, seed):
     sedges = [(pos[a], pos[b]) for a, b in edges]
     _, ref = _costs(pkg, plan)
     assert ref == pytest.approx(_reference_space_exhaustive(card, sedges))
+
+
+def _star_plan(pkg, rows, key_type=None):
+    """Input 0 joined with every other input on its column 0 = their column 0
+    (one equivalence class over all of them); each input has one key column
+    (INT32 unless `key_type`) and the root outputs every key."""
+    key_type = pkg.INT32 if key_type is None else key_type
+    plan = pkg.Plan()
+    for r in rows:
+        t = pkg.ColumnarTable(num_rows=r)
+        t.columns.append(pkg.encode_column(key_type, [0] * r))
+        plan.new_input(t)
+    node = plan.new_scan_node(0, [(0, key_type)])
+    for i in range(1, len(rows)):
+        scan = plan.new_scan_node(i, [(0, key_type)])
+        node = plan.new_join_node(True, node, scan, 0, 0, [(k, key_type) for k in range(i + 1)])
+    plan.root = node
+    return plan
+
+
+def _restrictions(text):
+    """{input: restricting pipeline's input} from the explain text."""
+    scans = {}
+    marks = {}
+    for line in text.splitlines():
+        m = re.match(r"pipeline (\d+): scan input (\d+)", line)
+        if not m:
+            continue
+        scans[int(m.group(1))] = int(m.group(2))
+        r = re.search(r"rows restricted by pipeline (\d+)'s filter", line)
+        if r:
+            marks[int(m.group(2))] = int(r.group(1))
+    return {i: scans[p] for i, p in marks.items()}
+
+
+def test_sideways_restriction_of_a_large_build(pkg):
+    """A fact with two inputs joined on the same key: the build of the large
+    one (300K rows) is restricted by the small one's filter (2K rows), the
+    reference's Join restriction on a later scan of another input of the
+    class (QueryPlan.cpp:620-624, :670-676)."""
+    text = pkg.explain(_star_plan(pkg, [1_000_000, 2_000, 300_000]))
+    assert _restrictions(text) == {2: 1}, text
+    # three inputs of one class besides the fact: both large ones restricted
+    # by the smallest
+    text = pkg.explain(_star_plan(pkg, [1_000_000, 300_000, 5_000, 400_000]))
+    assert _restrictions(text) == {1: 2, 3: 2}, text
+
+
+@pytest.mark.parametrize("rows", [
+    [1_000_000, 2_000, 200_000],     # restricted input below 2^18 rows
+    [1_000_000, 140_000, 600_000],   # provider too large for a bloom filter
+    [1_000_000, 80_000, 300_000],    # less than four times the provider's rows
+    [1_000_000, 300_000, 300_000],   # equal inputs
+])
+def test_sideways_restriction_not_marked(pkg, rows):
+    text = pkg.explain(_star_plan(pkg, rows))
+    assert _restrictions(text) == {}, text
+
+
+def test_sideways_restriction_not_on_int64_keys(pkg):
+    """INT64-keyed tables carry no bloom filter to restrict with."""
+    text = pkg.explain(_star_plan(pkg, [1_000_000, 2_000, 300_000], pkg.INT64))
+    assert _restrictions(text) == {}, text
