@@ -475,6 +475,7 @@ class Executor {
     bool run(bj_result& res, int flags) {
         const size_t np = ex_.pipelines.size();
         hts_.resize(np);
+        restricted_by_.assign(np, -1);
         cudaStream_t main = ctx_->stream;
         cudaEvent_t start = ctx_->pipe_event(np);
         if (!start) throw Fail{BJ_ERR_CUDA, "event creation failed"};
@@ -779,7 +780,22 @@ class Executor {
                 child.unique = ctx_->h_small[16 + 2 * k] == 0;
                 child.unit_mult = ctx_->h_small[17 + 2 * k] == 0;
             }
-            std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return rate[a] < rate[b]; });
+            // A table whose build was restricted by another probed here holds
+            // only keys that one's filter passes, so it can only look more
+            // selective; it has no filter of its own (it is large), the other
+            // has one: the other goes first, and the restricted table right
+            // after it at the latest.
+            std::vector<double> sort_rate = rate;
+            std::vector<uint8_t> after(np, 0);
+            for (size_t k = 0; k < np; k++)
+                for (size_t j = 0; j < np; j++)
+                    if (j != k && restricted_by_[pp.probes[k].child] == int32_t(pp.probes[j].child)) {
+                        sort_rate[k] = std::max(sort_rate[k], rate[j]);
+                        after[k] = 1;
+                    }
+            std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+                return sort_rate[a] != sort_rate[b] ? sort_rate[a] < sort_rate[b] : after[a] < after[b];
+            });
             // A probe keyed on an earlier probe's payload runs after it (the
             // first stage is then always keyed on the scanned input).
             std::vector<uint32_t> placed;
@@ -1166,6 +1182,7 @@ class Executor {
                 if (r >= 0 && hts_[size_t(r)].view.bloom) {
                     L.rbloom = hts_[size_t(r)].view.bloom;
                     L.rlog2w = hts_[size_t(r)].view.bloom_log2;
+                    restricted_by_[leaves[i0 + k]] = r;
                 }
                 batch.tuple_start[batch.n + 1] = batch.tuple_start[batch.n] + pb.ba.tb.count;
                 batch.block_start[batch.n + 1] = batch.block_start[batch.n] + (pb.ba.tb.count + 255) / 256;
@@ -1386,6 +1403,7 @@ class Executor {
     cudaStream_t st_;
     Arena& A_;
     std::vector<BuiltHT> hts_;
+    std::vector<int32_t> restricted_by_;  // per pipeline: the pipeline whose filter restricted its build, or -1
     uint64_t pipes_ = 0;
 };
 
