@@ -14,6 +14,8 @@ engine/op/TableScan.cpp:328; these plans are checked against the oracle.)
 """
 import random
 
+import numpy as np
+
 INT32, INT64, FP64, VARCHAR = 0, 1, 2, 3
 
 
@@ -141,3 +143,52 @@ def to_plan(pkg, tables, nodes, root):
             plan.new_join_node(n["build_left"], n["left"], n["right"], n["left_attr"], n["right_attr"], attrs)
     plan.root = root
     return plan
+
+
+
+INT32_EDGES = [-1, -2**31, 2**31 - 1, 0, 1]
+
+
+def _star_keys(rng, n, lo, hi, null_p, edges=False):
+    k = rng.integers(lo, hi, size=n, dtype=np.int64)
+    out = [int(x) for x in k]
+    if edges:
+        for i in rng.choice(n, size=min(n, 16), replace=False):
+            out[int(i)] = INT32_EDGES[int(i) % len(INT32_EDGES)]
+    if null_p:
+        for i in np.nonzero(rng.random(n) < null_p)[0]:
+            out[int(i)] = None
+    return out
+
+
+def star_plan(pkg, seed, fact_rows, small_rows, large_rows, small_dom, edges=False):
+    """A fact (INT32 key, INT64 payload) joined on its key with a small input
+    (key, INT32 payload) and a large input (key, VARCHAR payload): one key
+    class over three inputs, the shape whose large build a sideways
+    restriction filters by the small input's bloom filter. Keys of the fact
+    and the large input lie in [0, 200000), the small input's in
+    [0, small_dom); 5% of the fact's keys and 3% of the large input's are
+    NULL; with `edges`, up to 16 keys per table are INT32 edge values (-1,
+    INT32_MIN, INT32_MAX, 0, 1). The root outputs the fact's payload, the small
+    input's payload, the large input's key and payload."""
+    rng = np.random.default_rng(seed)
+    dom = 200_000
+    fact = pkg.ColumnarTable(num_rows=fact_rows)
+    fact.columns.append(pkg.encode_column(pkg.INT32, _star_keys(rng, fact_rows, 0, dom, 0.05, edges)))
+    fact.columns.append(pkg.encode_column(pkg.INT64, [int(x) for x in rng.integers(-2**40, 2**40, size=fact_rows)]))
+    small = pkg.ColumnarTable(num_rows=small_rows)
+    small.columns.append(pkg.encode_column(pkg.INT32, _star_keys(rng, small_rows, 0, small_dom, 0.0, edges)))
+    small.columns.append(pkg.encode_column(pkg.INT32, [int(x) for x in rng.integers(0, 1000, size=small_rows)]))
+    large = pkg.ColumnarTable(num_rows=large_rows)
+    large.columns.append(pkg.encode_column(pkg.INT32, _star_keys(rng, large_rows, 0, dom, 0.03, edges)))
+    large.columns.append(pkg.encode_column(pkg.VARCHAR, [f"v{int(x)}" for x in rng.integers(0, 10**6, size=large_rows)]))
+    plan = pkg.Plan()
+    for t in (fact, small, large):
+        plan.new_input(t)
+    f = plan.new_scan_node(0, [(0, pkg.INT32), (1, pkg.INT64)])
+    s = plan.new_scan_node(1, [(0, pkg.INT32), (1, pkg.INT32)])
+    j1 = plan.new_join_node(True, f, s, 0, 0, [(0, pkg.INT32), (1, pkg.INT64), (2, pkg.INT32), (3, pkg.INT32)])
+    lg = plan.new_scan_node(2, [(0, pkg.INT32), (1, pkg.VARCHAR)])
+    j2 = plan.new_join_node(True, j1, lg, 0, 0, [(1, pkg.INT64), (3, pkg.INT32), (4, pkg.INT32), (5, pkg.VARCHAR)])
+    plan.root = j2
+    return pkg.CPlan(plan)

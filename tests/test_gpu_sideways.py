@@ -10,55 +10,12 @@ import contextlib
 import ctypes
 import os
 
-import numpy as np
 import pytest
 
 import oracle_lib
+from plangen import star_plan
 
 pytestmark = pytest.mark.gpu
-
-INT32_EDGES = [-1, -2**31, 2**31 - 1, 0, 1]
-
-
-def _keys(rng, n, lo, hi, null_p, edges=False):
-    k = rng.integers(lo, hi, size=n, dtype=np.int64)
-    out = [int(x) for x in k]
-    if edges:
-        for i in rng.choice(n, size=min(n, 16), replace=False):
-            out[int(i)] = INT32_EDGES[int(i) % len(INT32_EDGES)]
-    if null_p:
-        for i in np.nonzero(rng.random(n) < null_p)[0]:
-            out[int(i)] = None
-    return out
-
-
-def _star(pkg, seed, fact_rows, small_rows, large_rows, small_dom, edges=False):
-    """Fact (key, INT64 payload) joined on its key with a small input (key,
-    INT32 payload) and a large input (key, VARCHAR payload); the root outputs
-    the fact's payload, the small input's payload, the large input's key and
-    payload. Keys of the fact and the large input are drawn from [0, 200000),
-    the small input's from [0, small_dom)."""
-    rng = np.random.default_rng(seed)
-    dom = 200_000
-    fact = pkg.ColumnarTable(num_rows=fact_rows)
-    fact.columns.append(pkg.encode_column(pkg.INT32, _keys(rng, fact_rows, 0, dom, 0.05, edges)))
-    fact.columns.append(pkg.encode_column(pkg.INT64, [int(x) for x in rng.integers(-2**40, 2**40, size=fact_rows)]))
-    small = pkg.ColumnarTable(num_rows=small_rows)
-    small.columns.append(pkg.encode_column(pkg.INT32, _keys(rng, small_rows, 0, small_dom, 0.0, edges)))
-    small.columns.append(pkg.encode_column(pkg.INT32, [int(x) for x in rng.integers(0, 1000, size=small_rows)]))
-    large = pkg.ColumnarTable(num_rows=large_rows)
-    large.columns.append(pkg.encode_column(pkg.INT32, _keys(rng, large_rows, 0, dom, 0.03, edges)))
-    large.columns.append(pkg.encode_column(pkg.VARCHAR, [f"v{int(x)}" for x in rng.integers(0, 10**6, size=large_rows)]))
-    plan = pkg.Plan()
-    for t in (fact, small, large):
-        plan.new_input(t)
-    f = plan.new_scan_node(0, [(0, pkg.INT32), (1, pkg.INT64)])
-    s = plan.new_scan_node(1, [(0, pkg.INT32), (1, pkg.INT32)])
-    j1 = plan.new_join_node(True, f, s, 0, 0, [(0, pkg.INT32), (1, pkg.INT64), (2, pkg.INT32), (3, pkg.INT32)])
-    l = plan.new_scan_node(2, [(0, pkg.INT32), (1, pkg.VARCHAR)])
-    j2 = plan.new_join_node(True, j1, l, 0, 0, [(1, pkg.INT64), (3, pkg.INT32), (4, pkg.INT32), (5, pkg.VARCHAR)])
-    plan.root = j2
-    return pkg.CPlan(plan)
 
 
 @contextlib.contextmanager
@@ -90,7 +47,7 @@ CASES = [
 @pytest.mark.parametrize("case", CASES, ids=[f"seed{c[0]}" for c in CASES])
 def test_restricted_build_equals_oracle(pkg, oracle, case):
     seed, fact_rows, small_rows, large_rows, small_dom, edges = case
-    cp = _star(pkg, seed, fact_rows, small_rows, large_rows, small_dom, edges)
+    cp = star_plan(pkg, seed, fact_rows, small_rows, large_rows, small_dom, edges)
     text = pkg.explain(cp)
     assert "rows restricted by pipeline" in text, text
     want = oracle.execute(cp.ref())
@@ -108,7 +65,7 @@ def test_restricted_build_equals_oracle(pkg, oracle, case):
 def test_restricted_build_resident_and_replayed(pkg, oracle):
     """Resident tables: the first run records the query, the second replays
     it as a CUDA graph; both equal the oracle."""
-    cp = _star(pkg, 11, 800_000, 5_000, 350_000, 200_000, True)
+    cp = star_plan(pkg, 11, 800_000, 5_000, 350_000, 200_000, True)
     plan = cp.struct
     want = oracle.execute(cp.ref())
     with _context(pkg, True) as c:

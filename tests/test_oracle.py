@@ -108,3 +108,22 @@ def test_oracle_matches_reference_engine_workloads(pkg, oracle, name, seed, scal
     ora = oracle.execute(w.plan_ptr())
     n = oracle_lib.assert_same_rows(oracle, ctypes.byref(ref_struct), ora.view(), name)
     assert n > 0
+
+
+@needs_ref
+@pytest.mark.parametrize("case", [
+    (21, 60_000, 2_000, 40_000, 200_000),   # the small input holds ~1% of the keys
+    (22, 50_000, 8_000, 30_000, 2_000),     # few keys, many repeated on every side
+])
+def test_oracle_matches_reference_engine_star_on_one_key(pkg, oracle, case):
+    """Three inputs joined on one key class, the shape in which the reference
+    restricts the large input's scan by the small input's finished table
+    (engine/query/QueryPlan.cpp:620-624, :670-676): the oracle gives the
+    reference engine's rows."""
+    cp = plangen.star_plan(pkg, *case)
+    with tempfile.TemporaryDirectory() as tmp:
+        ref = run_reference(pkg, cp, tmp)
+    ref_struct, keep = table_struct(pkg, ref)
+    ora = oracle.execute(cp.ref())
+    n = oracle_lib.assert_same_rows(oracle, ctypes.byref(ref_struct), ora.view(), f"star {case}")
+    assert n > 0
