@@ -476,6 +476,7 @@ class Executor {
         const size_t np = ex_.pipelines.size();
         hts_.resize(np);
         restricted_by_.assign(np, -1);
+        batched_.assign(np, 0);
         cudaStream_t main = ctx_->stream;
         cudaEvent_t start = ctx_->pipe_event(np);
         if (!start) throw Fail{BJ_ERR_CUDA, "event creation failed"};
@@ -514,6 +515,7 @@ class Executor {
                     if (!done) throw Fail{BJ_ERR_CUDA, "event creation failed"};
                     BJ_CK(cudaEventRecord(done, main));
                     batched[p] = 1;
+                    batched_[p] = 1;
                 }
             }
         }
@@ -782,14 +784,15 @@ class Executor {
             }
             // A table whose build was restricted by another probed here holds
             // only keys that one's filter passes, so it can only look more
-            // selective; it has no filter of its own (it is large), the other
-            // has one: the other goes first, and the restricted table right
-            // after it at the latest.
+            // selective; when it has no filter of its own (a large build) and
+            // the other has one, the other goes first, and the restricted
+            // table right after it at the latest.
             std::vector<double> sort_rate = rate;
             std::vector<uint8_t> after(np, 0);
             for (size_t k = 0; k < np; k++)
                 for (size_t j = 0; j < np; j++)
-                    if (j != k && restricted_by_[pp.probes[k].child] == int32_t(pp.probes[j].child)) {
+                    if (j != k && restricted_by_[pp.probes[k].child] == int32_t(pp.probes[j].child) &&
+                        !hts_[pp.probes[k].child].view.bloom) {
                         sort_rate[k] = std::max(sort_rate[k], rate[j]);
                         after[k] = 1;
                     }
@@ -1111,6 +1114,15 @@ class Executor {
     bool build(size_t pi, const Items& items, const SlotSources& src, const std::vector<HTView>& probes,
                int32_t key_stage) {
         PreparedBuild pb = prepare_build(pi, items, src, probes, key_stage);
+        // Sideways restriction by a batched leaf's filter (built on the main
+        // stream before any pipeline that probes).
+        const int32_t r = ex_.pipelines[pi].restrict_by;
+        if (r >= 0 && ctx_->sideways && batched_[size_t(r)] && restricted_by_[size_t(r)] < 0 &&
+            hts_[size_t(r)].view.bloom && pb.ba.key.type == kInt32) {
+            pb.ba.rbloom = hts_[size_t(r)].view.bloom;
+            pb.ba.rlog2w = hts_[size_t(r)].view.bloom_log2;
+            restricted_by_[pi] = r;
+        }
         uint8_t* z = alloc<uint8_t>(pb.zbytes);
         BJ_CK(cudaMemsetAsync(z, 0, pb.zbytes, st_));
         place_zero(pb, z);
@@ -1404,6 +1416,7 @@ class Executor {
     Arena& A_;
     std::vector<BuiltHT> hts_;
     std::vector<int32_t> restricted_by_;  // per pipeline: the pipeline whose filter restricted its build, or -1
+    std::vector<uint8_t> batched_;        // per pipeline: a leaf built in the batches before every other pipeline
     uint64_t pipes_ = 0;
 };
 

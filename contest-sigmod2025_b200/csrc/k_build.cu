@@ -148,6 +148,7 @@ __device__ __forceinline__ void emit_tuple(const BuildArgs& a, uint32_t i) {
         key_ok = row < a.key.nrows && col_get(a.key, row, kv);
         if (row >= a.key.nrows) record_error(a.err, kErrRowRange);
     }
+    if (key_ok && a.rbloom && !bloom_may_contain(a.rbloom, a.rlog2w, uint32_t(kv))) key_ok = false;
     const uint64_t m = key_ok ? item_mult(a.in, i) : 0ull;
     emit_tuple_to(emit_target(a), i, kv, m, a.src.n,
                   [&](int j, uint64_t& v) { return slot_value(a.src.s[j], a.in, i, row, a.ps, v); });

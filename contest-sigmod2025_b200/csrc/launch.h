@@ -290,6 +290,11 @@ struct BuildArgs {
     uint32_t shift;    // bucket = key_hash >> shift
     uint32_t* err;
     uint32_t distinct; // 1: no two tuples can be equal (each is its own representative; no table)
+    // Sideways restriction (INT32 keys): the bloom filter (1 << rlog2w words)
+    // of a table built on the same key class; a tuple whose key it cannot
+    // hold is not inserted. Null: none.
+    const uint32_t* rbloom;
+    uint32_t rlog2w;
 };
 int emit_aggregate(const BuildArgs& a, cudaStream_t st);
 // Scatters the representatives into their buckets' ranges (cursor: one zero

@@ -695,19 +695,31 @@ void sideways_restrictions(ExecPlan& ex) {
         return pp.probes.empty() && pp.build_key >= 0 && pp.build_key_probe < 0 &&
                pp.slots.size() <= kLeafBatchMaxSlots && ex.attrs[size_t(pp.build_key)].type == BJ_INT32;
     };
+    // below[p][q]: pipeline q feeds pipeline p through its probes (children
+    // come before parents, so one pass in order completes every row).
+    std::vector<std::vector<uint8_t>> below(np, std::vector<uint8_t>(np, 0));
+    for (size_t p = 0; p < np; p++)
+        for (const auto& pr : ex.pipelines[p].probes) {
+            below[p][pr.child] = 1;
+            for (size_t q = 0; q < np; q++) below[p][q] |= below[pr.child][q];
+        }
     for (size_t m = 0; m + 1 < np; m++) {
         PipelinePlan& pm = ex.pipelines[m];
         pm.restrict_by = -1;
-        if (!plain_leaf(pm)) continue;
+        const bool leaf = plain_leaf(pm);
+        // A build fed by probes runs after every batched leaf and pays only
+        // a filter test per tuple; a leaf restricted pays a second batch.
+        if (!leaf && (pm.probes.empty() || pm.build_key < 0 || ex.attrs[size_t(pm.build_key)].type != BJ_INT32))
+            continue;
         const uint64_t rows_m = ex.inputs[pm.input].rows;
-        if (rows_m < kSidewaysMinRows) continue;
+        if (leaf && rows_m < kSidewaysMinRows) continue;
         const uint32_t eq = ex.attrs[size_t(pm.build_key)].eq;
         // The smallest qualifying provider (never itself restricted: any
         // input that could restrict it would qualify here and be smaller).
         uint64_t best_rows = 0;
         for (size_t l = 0; l + 1 < np; l++) {
             const PipelinePlan& pl = ex.pipelines[l];
-            if (l == m || !plain_leaf(pl) || ex.attrs[size_t(pl.build_key)].eq != eq) continue;
+            if (l == m || below[m][l] || !plain_leaf(pl) || ex.attrs[size_t(pl.build_key)].eq != eq) continue;
             const uint64_t rows_l = ex.inputs[pl.input].rows;
             if (rows_l > kSidewaysMaxFilterRows || rows_l * 4 > rows_m) continue;
             if (pm.restrict_by < 0 || rows_l < best_rows || (rows_l == best_rows && int32_t(l) < pm.restrict_by)) {

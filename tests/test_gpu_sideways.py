@@ -10,6 +10,7 @@ import contextlib
 import ctypes
 import os
 
+import numpy as np
 import pytest
 
 import oracle_lib
@@ -78,3 +79,47 @@ def test_restricted_build_resident_and_replayed(pkg, oracle):
         finally:
             for x in res:
                 x.free()
+
+
+def _branch_plan(pkg, seed):
+    """F (600K rows) joined with A (2K) and X (100K) on one key k, X also
+    joined with Y (5K) on y: X's build probes Y and is restricted by A's
+    filter (A is not below X)."""
+    rng = np.random.default_rng(seed)
+    dom, ydom = 200_000, 5_000
+
+    def table(rows, kdom, ydom_):
+        t = pkg.ColumnarTable(num_rows=rows)
+        k = [int(v) for v in rng.integers(0, kdom, size=rows)]
+        for i in rng.choice(rows, size=max(1, rows // 50), replace=False):
+            k[int(i)] = None
+        t.columns.append(pkg.encode_column(pkg.INT32, k))
+        t.columns.append(pkg.encode_column(pkg.INT32, [int(v) for v in rng.integers(0, ydom_, size=rows)]))
+        return t
+
+    plan = pkg.Plan()
+    for rows in (600_000, 2_000, 100_000, 5_000):
+        plan.new_input(table(rows, dom, ydom))
+    two = [(0, pkg.INT32), (1, pkg.INT32)]
+    j = plan.new_join_node(True, plan.new_scan_node(0, two), plan.new_scan_node(1, two), 0, 0,
+                           [(i, pkg.INT32) for i in range(4)])
+    j = plan.new_join_node(True, j, plan.new_scan_node(2, two), 0, 0, [(i, pkg.INT32) for i in range(6)])
+    j = plan.new_join_node(True, j, plan.new_scan_node(3, two), 5, 1, [(1, pkg.INT32), (3, pkg.INT32), (5, pkg.INT32), (6, pkg.INT32)])
+    plan.root = j
+    return pkg.CPlan(plan)
+
+
+@pytest.mark.parametrize("seed", [31, 32])
+def test_restricted_build_that_probes_equals_oracle(pkg, oracle, seed):
+    """A build fed by a probe, restricted by a leaf's filter in its key
+    class: the same rows with the restriction on and off."""
+    cp = _branch_plan(pkg, seed)
+    text = pkg.explain(cp)
+    assert "probe pipeline" in text and "rows restricted by pipeline" in text, text
+    want = oracle.execute(cp.ref())
+    for sideways in (True, False):
+        with _context(pkg, sideways) as c:
+            with c.execute_raw(cp) as r:
+                got, keep = r.table_struct()
+                oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(),
+                                            f"branch seed {seed} sideways={sideways}")

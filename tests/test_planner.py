@@ -348,3 +348,43 @@ def test_sideways_restriction_not_on_int64_keys(pkg):
     """INT64-keyed tables carry no bloom filter to restrict with."""
     text = pkg.explain(_star_plan(pkg, [1_000_000, 2_000, 300_000], pkg.INT64))
     assert _restrictions(text) == {}, text
+
+
+def _star_with_branch(pkg, rows, y_on_key=False):
+    """Inputs F, A, X, Y (rows in that order), two INT32 columns each (k, y):
+    F.k = A.k, F.k = X.k, and X.y = Y.y (or, with y_on_key, X.k = Y.k), so
+    X's build probes Y and is keyed on the class of F.k and A.k."""
+    plan = pkg.Plan()
+    for r in rows:
+        t = pkg.ColumnarTable(num_rows=r)
+        t.columns.append(pkg.encode_column(pkg.INT32, [0] * r))
+        t.columns.append(pkg.encode_column(pkg.INT32, [0] * r))
+        plan.new_input(t)
+    two = [(0, pkg.INT32), (1, pkg.INT32)]
+    f = plan.new_scan_node(0, two)
+    a = plan.new_scan_node(1, two)
+    j = plan.new_join_node(True, f, a, 0, 0, [(i, pkg.INT32) for i in range(4)])
+    x = plan.new_scan_node(2, two)
+    j = plan.new_join_node(True, j, x, 0, 0, [(i, pkg.INT32) for i in range(6)])
+    y = plan.new_scan_node(3, two)
+    xa = 4 if y_on_key else 5  # X.k or X.y in the join's output
+    j = plan.new_join_node(True, j, y, xa, 0 if y_on_key else 1, [(i, pkg.INT32) for i in range(8)])
+    plan.root = j
+    return plan
+
+
+def test_sideways_restriction_of_a_build_that_probes(pkg):
+    """X's build is fed by its probe of Y and keyed on the class of F.k and
+    A.k: A's filter restricts it (A is not below X). No second batch is
+    needed: every leaf is built before a pipeline that probes."""
+    text = pkg.explain(_star_with_branch(pkg, [1_000_000, 2_000, 100_000, 5_000]))
+    assert _restrictions(text) == {2: 1}, text
+
+
+def test_sideways_restriction_never_by_a_table_below(pkg):
+    """With X.k = Y.k, Y is both in X's key class and below X (X probes it):
+    X's rows already match Y, so only A may restrict X."""
+    text = pkg.explain(_star_with_branch(pkg, [1_000_000, 20_000, 100_000, 1_000], y_on_key=True))
+    # Y (1,000 rows) is the smallest input of the class, A (20,000 rows)
+    # restricts X's build.
+    assert _restrictions(text) == {2: 1}, text
