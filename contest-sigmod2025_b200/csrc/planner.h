@@ -66,10 +66,10 @@ struct PipelinePlan {
     };
     std::vector<Probe> probes;
     std::vector<SlotPlan> slots;  // payload (build) or output sources (root)
-    // A sideways restriction (sideways_restrictions): for a build that
-    // probes nothing, the pipeline of a much smaller such build keyed on the
-    // same equivalence class, whose bloom filter drops this build's rows
-    // with keys it cannot hold; -1: none.
+    // A sideways restriction (sideways_restrictions): the pipeline of a much
+    // smaller build that probes nothing, keyed on the same equivalence class
+    // as this build and not below it, whose bloom filter drops this build's
+    // tuples with keys it cannot hold; -1: none.
     int32_t restrict_by = -1;
 };
 
@@ -91,17 +91,19 @@ struct ExecPlan {
     bool reference_space = false;
 };
 
-// Sideways restrictions between the builds of inputs that probe nothing
-// (the reference installs a finished table's Join restriction on every later
-// scan of another input of its key class, engine/query/QueryPlan.cpp:
-// 620-624, :670-676; buildScan applies it, :113-126). A row of such a build
-// whose key a table of the same class cannot hold joins no result row, so
-// the build of a large input is restricted by the filter of a smaller input
-// built on that class. Marked only where it can pay: the restricted input
-// has at least kSidewaysMinRows rows and at least four times the provider's,
-// and the provider is small enough to carry a bloom filter
-// (kSidewaysMaxFilterRows); both keys INT32 and both builds batched
-// (kLeafBatchMaxSlots payload columns at most).
+// Sideways restrictions (the reference installs a finished table's Join
+// restriction on every later scan of another input of its key class,
+// engine/query/QueryPlan.cpp:620-624, :670-676; buildScan applies it,
+// :113-126). A tuple of a build whose key a table of the same class cannot
+// hold joins no result row, so a build is restricted by the bloom filter of
+// a smaller input that probes nothing (a leaf, built before every pipeline
+// that probes), built on that class and not below the restricted build.
+// The provider is small enough to carry a filter (kSidewaysMaxFilterRows
+// rows at most) and has at most a quarter of the restricted input's rows;
+// both keys INT32; the leaf is batched (kLeafBatchMaxSlots payload columns
+// at most). A restricted leaf costs a second batch of leaf builds, so leaves
+// are restricted only from kSidewaysMinRows rows on; a build fed by probes
+// runs after every leaf anyway and pays one filter test per tuple.
 constexpr uint64_t kSidewaysMinRows = uint64_t(1) << 18;
 constexpr uint64_t kSidewaysMaxFilterRows = uint64_t(1) << 17;
 constexpr size_t kLeafBatchMaxSlots = 4;
