@@ -160,7 +160,8 @@ BJ_API int bj_execute(bj_context* ctx, const bj_plan* plan, bj_result** out);
 /* The pipelines bj_execute runs for `plan`, as text: the driver (the input the
  * output pipeline scans) with the plan's estimated cost, then one line per
  * pipeline in execution order (its scan, the pipelines it probes and with
- * which attribute, the attribute its hash table is keyed on) and, when the
+ * which attribute, the attribute its hash table is keyed on, and the pipeline
+ * whose bloom filter restricts its rows, if any) and, when the
  * plan's tables allow one, the drop-in path's guess of the probe the output
  * pipeline scans first (a line "scan guess: ..."). The role of
  * the reference's plan printer (printPlanRec, engine/query/QueryPlan.cpp:380-411). Needs no
