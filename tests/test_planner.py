@@ -388,3 +388,51 @@ def test_sideways_restriction_never_by_a_table_below(pkg):
     # Y (1,000 rows) is the smallest input of the class, A (20,000 rows)
     # restricts X's build.
     assert _restrictions(text) == {2: 1}, text
+
+
+def _pipelines(text):
+    """[(input, rows, [probed pipelines], restricting pipeline or None)] from
+    the explain text, in pipeline order."""
+    out = []
+    for line in text.splitlines():
+        m = re.match(r"pipeline (\d+): scan input (\d+) \(table \d+, (\d+) rows\)(.*)", line)
+        if not m:
+            continue
+        rest = m.group(4)
+        probes = [int(x) for x in re.findall(r"pipeline (\d+) on attr", rest)]
+        r = re.search(r"rows restricted by pipeline (\d+)'s filter", rest)
+        out.append((int(m.group(2)), int(m.group(3)), probes, int(r.group(1)) if r else None))
+    return out
+
+
+def test_sideways_restrictions_of_schema20_plans_are_sound(pkg):
+    """Every restriction the planner marks over a batch of schema20 queries:
+    the provider is a build that probes nothing, is small enough for a bloom
+    filter, has at most a quarter of the restricted input's rows, is not
+    itself restricted, and is not below the restricted build (it feeds no
+    probe of it, directly or through other pipelines)."""
+    w = pkg.Workload("schema20", 1, 0.3, queries=256)
+    marked = 0
+    try:
+        for q in range(w.num_queries()):
+            pipes = _pipelines(pkg.explain(w.query_ptr(q)))
+            for p, (inp, rows, probes, by) in enumerate(pipes):
+                if by is None:
+                    continue
+                marked += 1
+                assert by != p and by < len(pipes) - 1, (q, p)
+                _, prows, pprobes, pby = pipes[by]
+                assert not pprobes and pby is None, (q, p, by)
+                assert prows <= 131072 and prows * 4 <= rows, (q, p, by)
+                if not probes:
+                    assert rows >= 2**18, (q, p)  # a restricted leaf costs a second batch
+                below, stack = set(), list(probes)
+                while stack:
+                    c = stack.pop()
+                    if c not in below:
+                        below.add(c)
+                        stack.extend(pipes[c][2])
+                assert by not in below, (q, p, by)
+    finally:
+        w.close()
+    assert marked > 0
