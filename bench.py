@@ -69,10 +69,12 @@ def parse():
     ap.add_argument("--est-epochs", type=int, default=30)
     ap.add_argument("--autotune-repeats", type=int, default=3,
                     help="runs per parameter set of the autotuner before timing (0: engine defaults)")
-    ap.add_argument("--mode", default="all", choices=["all", "value", "e2e", "serve", "batch", "estimator"],
+    ap.add_argument("--mode", default="all",
+                    choices=["all", "value", "e2e", "serve", "batch", "estimator", "sideways"],
                     help="value / e2e run one measurement only (for profiling); all prints the bench line; "
                          "batch runs every query of a batched workload (--workload schema20); serve runs the "
-                         "serving headline alone; estimator measures the learned estimator (schema20 at --scale)")
+                         "serving headline alone; estimator measures the learned estimator (schema20 at --scale); "
+                         "sideways times star joins with sideways-restricted builds on and off")
     return ap.parse_args()
 
 
@@ -602,6 +604,76 @@ def estimator_bench(pkg, args, local):
     return 0
 
 
+def sideways_bench(pkg, args, local):
+    """Sideways-restricted leaf builds (B200JOIN_SIDEWAYS on and off, three
+    alternations per shape on one GPU): a fact joined with a small and a
+    large input on one INT32 key (keys uniform over the domain, payloads
+    INT64 / INT32 / INT64), resident tables, the median device time of the
+    graph-replayed calls after three warm-up calls, and the build phase."""
+    import numpy as np
+
+    def star(fact_rows, small_rows, large_rows, dom, seed=5):
+        rng = np.random.default_rng(seed)
+        tables = []
+        for rows, pay in ((fact_rows, pkg.INT64), (small_rows, pkg.INT32), (large_rows, pkg.INT64)):
+            t = pkg.ColumnarTable(num_rows=rows)
+            t.columns.append(pkg.encode_column(pkg.INT32, rng.integers(0, dom, size=rows).tolist()))
+            t.columns.append(pkg.encode_column(pay, rng.integers(0, 1000, size=rows).tolist()))
+            tables.append(t)
+        plan = pkg.Plan()
+        for t in tables:
+            plan.new_input(t)
+        f = plan.new_scan_node(0, [(0, pkg.INT32), (1, pkg.INT64)])
+        s_ = plan.new_scan_node(1, [(0, pkg.INT32), (1, pkg.INT32)])
+        j1 = plan.new_join_node(True, f, s_, 0, 0, [(0, pkg.INT32), (1, pkg.INT64), (2, pkg.INT32), (3, pkg.INT32)])
+        lg = plan.new_scan_node(2, [(0, pkg.INT32), (1, pkg.INT64)])
+        plan.root = plan.new_join_node(True, j1, lg, 0, 0, [(1, pkg.INT64), (3, pkg.INT32), (5, pkg.INT64)])
+        return pkg.CPlan(plan)
+
+    def run(cp, sideways, calls):
+        os.environ["B200JOIN_SIDEWAYS"] = "1" if sideways else "0"
+        try:
+            ctx = pkg.Context(local)
+        finally:
+            del os.environ["B200JOIN_SIDEWAYS"]
+        ms, build_ms, rows = [], [], None
+        try:
+            ctx.profile(True)
+            plan = cp.struct
+            res = [ctx.upload(plan.inputs[i]) for i in range(plan.num_inputs)]
+            for _ in range(calls):
+                with ctx.execute_resident(cp, res) as r:
+                    st = r.stats()
+                    rows = r.num_rows
+                    ms.append(st.device_ms)
+                    build_ms.append(st.phase_ms[0])
+            for x in res:
+                x.free()
+        finally:
+            ctx.close()
+        return statistics.median(ms[3:]), statistics.median(build_ms[3:]), rows
+
+    calls = 3 + max(3, min(args.steps, 12))
+    out = {"mode": "sideways", "calls_timed": calls - 3, "shapes": []}
+    for shape in ((4_000_000, 2_000, 4_000_000, 2_000_000), (2_000_000, 20_000, 1_000_000, 500_000),
+                  (2_000_000, 100_000, 400_000, 200_000)):
+        cp = star(*shape)
+        rec = {"fact_small_large_rows": list(shape[:3]), "key_domain": shape[3],
+               "restricted": "rows restricted by pipeline" in pkg.explain(cp),
+               "on_ms": [], "off_ms": [], "build_on_ms": [], "build_off_ms": [], "rows": []}
+        for _ in range(3):
+            for sideways in (True, False):
+                m, b, n = run(cp, sideways, calls)
+                key = "on" if sideways else "off"
+                rec[key + "_ms"].append(m)
+                rec["build_" + key + "_ms"].append(b)
+                rec["rows"].append(n)
+        rec["rows_equal"] = len(set(rec["rows"])) == 1
+        out["shapes"].append(rec)
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -621,6 +693,9 @@ def main():
     if args.mode == "estimator":
         import importlib
         return estimator_bench(importlib.import_module("contest-sigmod2025_b200"), args, local) if rank == 0 else 0
+    if args.mode == "sideways":
+        import importlib
+        return sideways_bench(importlib.import_module("contest-sigmod2025_b200"), args, local) if rank == 0 else 0
 
     import importlib
     import torch
