@@ -405,13 +405,14 @@ def _pipelines(text):
     return out
 
 
-def test_sideways_restrictions_of_schema20_plans_are_sound(pkg):
+@pytest.mark.parametrize("seed,scale", [(1, 0.3), (2, 0.05)])
+def test_sideways_restrictions_of_schema20_plans_are_sound(pkg, seed, scale):
     """Every restriction the planner marks over a batch of schema20 queries:
     the provider is a build that probes nothing, is small enough for a bloom
     filter, has at most a quarter of the restricted input's rows, is not
     itself restricted, and is not below the restricted build (it feeds no
     probe of it, directly or through other pipelines)."""
-    w = pkg.Workload("schema20", 1, 0.3, queries=256)
+    w = pkg.Workload("schema20", seed, scale, queries=256)
     marked = 0
     try:
         for q in range(w.num_queries()):
