@@ -123,3 +123,27 @@ def test_restricted_build_that_probes_equals_oracle(pkg, oracle, seed):
                 got, keep = r.table_struct()
                 oracle_lib.assert_same_rows(oracle, ctypes.byref(got), want.view(),
                                             f"branch seed {seed} sideways={sideways}")
+
+
+def test_schema20_batch_with_restricted_payload_keyed_builds(pkg, oracle):
+    """schema20 seed 2 at x0.05: 120 of its 256 queries run builds keyed on a
+    probed table's payload and restricted by a leaf's filter (the reference's
+    plan space). Only the restricted queries, over resident tables: recorded,
+    captured and replayed, each equal to the oracle."""
+    w = pkg.Workload("schema20", 2, 0.05)
+    ks = [k for k in range(256) if "rows restricted by pipeline" in pkg.explain(w.query_ptr(k))]
+    assert len(ks) >= 100
+    plan = w.plan_ptr().contents
+    wants = {k: oracle.execute(w.query_ptr(k)) for k in ks}
+    with _context(pkg, True) as c:
+        res = [c.upload(plan.inputs[i]) for i in range(plan.num_inputs)]
+        try:
+            for run in ("record", "capture", "replay"):
+                for k in ks:
+                    with c.execute_resident(w.query_ptr(k), res) as r:
+                        got, keep = r.table_struct()
+                        oracle_lib.assert_same_rows(oracle, ctypes.byref(got), wants[k].view(),
+                                                    f"schema20 seed 2 query {k} ({run})")
+        finally:
+            for x in res:
+                x.free()
